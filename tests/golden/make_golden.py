@@ -1,0 +1,223 @@
+"""Generate the golden fixtures by running the REFERENCE's own code.
+
+Run in the build container (the reference sources are not on the GPU box):
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+JAX is not installed, so the unmodified reference modules (`network.py`,
+`chem.py`, `solver.py`, `jax_step.py`, `photo.py`, `integrate.py`,
+`steady_state_grad.py`, and the caller-contract functions of `outer_loop.py`)
+are imported with ``_jax_numpy_shim`` standing in for ``jax``. A stub
+``vulcan_cfg`` with no species lists is installed first so the reference
+parser does not append config-named species (reference `network.py:157-194`).
+
+Inputs are the package's seeded synthetic cases at small sizes; every input
+array is stored next to the reference output so the fixtures do not depend
+on the generator reproducing bit-identical floats elsewhere.
+"""
+from __future__ import annotations
+
+import argparse
+import ast
+import importlib
+import os
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, REPO)
+
+ATM_KEYS = ["Kzz", "Dzz", "dzi", "vz", "Hpi", "Ti", "Tco", "g", "ms", "alpha", "M", "vm", "vs",
+            "top_flux", "bot_flux", "bot_vdep", "gas_indx_mask"]
+FLAG_KEYS = ["use_vm_mol", "use_settling", "use_topflux", "use_botflux"]
+TABLE_KEYS = ["reactant_idx", "product_idx", "reactant_stoich", "product_stoich", "is_three_body"]
+
+
+def load_reference(ref):
+    import _jax_numpy_shim as shim
+    shim.install()
+    sys.modules["vulcan_cfg"] = types.ModuleType("vulcan_cfg")
+    sys.path.insert(0, ref)
+    mods = {m: importlib.import_module(m) for m in
+            ["network", "chem", "solver", "jax_step", "photo", "integrate", "steady_state_grad"]}
+    # caller-contract functions of outer_loop.py, compiled from the reference source
+    src = open(os.path.join(ref, "outer_loop.py")).read()
+    tree = ast.parse(src)
+    want = {"_compute_atom_loss", "_step_size", "_make_clip_fn", "_make_aggregate_delta_fn"}
+    body = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in want]
+    ns = {"jnp": shim.jnp, "jax": shim.jax, "np": np}
+    exec(compile(ast.Module(body=body, type_ignores=[]), "outer_loop.py", "exec"), ns)
+    mods["contract"] = types.SimpleNamespace(**{k: ns[k] for k in want})
+    return mods, shim
+
+
+def ref_atm(mods, atm):
+    kw = {k: np.asarray(atm[k]) for k in ATM_KEYS}
+    kw.update({k: bool(atm[k]) for k in FLAG_KEYS})
+    return mods["jax_step"].AtmStatic(**kw)
+
+
+def step_fixture(mods, name, case, fix_mask=None, n_steps=0):
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(case.net.text)
+        path = f.name
+    rn = mods["network"].parse_network(path)
+    os.unlink(path)
+    net = mods["chem"].to_jax(rn)
+    atm = ref_atm(mods, case.atm)
+    sol, delta = mods["jax_step"].jax_ros2_step(case.y, case.k, case.dt, atm, net, fix_mask=fix_mask)
+    rhs = mods["chem"].chem_rhs(case.y, case.atm["M"], case.k, net)
+    jac = mods["chem"].chem_jac_analytical(case.y, case.atm["M"], case.k, net)
+    out = dict(net_text=np.array(case.net.text), y=case.y, k=case.k, dt=np.array(case.dt),
+               sol=np.asarray(sol), delta=np.asarray(delta), rhs=np.asarray(rhs), jac=np.asarray(jac),
+               ni=np.array(rn.ni), nr=np.array(rn.nr), compo=case.net.compo)
+    for k in TABLE_KEYS:
+        out["tab_" + k] = np.asarray(getattr(rn, k))
+    for k in ATM_KEYS + FLAG_KEYS:
+        out["atm_" + k] = np.asarray(case.atm[k])
+    if fix_mask is not None:
+        out["fix_mask"] = fix_mask
+    if n_steps:
+        yN, deltas = mods["integrate"].jax_integrate_fixed_dt(case.y, case.k, case.dt, n_steps, atm, net)
+        out["int_y"] = np.asarray(yN)
+        out["int_deltas"] = np.asarray(deltas)
+        out["int_n"] = np.array(n_steps)
+    np.savez_compressed(os.path.join(HERE, f"step_{name}.npz"), **out)
+    print(f"step_{name}: ni={rn.ni} nr={rn.nr} nz={case.y.shape[0]}")
+
+
+def thomas_fixture(mods):
+    """The seeded systems of reference tests/test_block_thomas.py:22-79 and
+    tests/test_block_thomas_diag.py:40-120, solved by the reference solver."""
+    solver = mods["solver"]
+    out = {}
+    rng = np.random.default_rng(42)
+    nz, ni = 8, 5
+    d = rng.standard_normal((nz, ni, ni)) + 10.0 * np.eye(ni)
+    sp = rng.standard_normal((nz - 1, ni, ni))
+    sb = rng.standard_normal((nz - 1, ni, ni))
+    r = rng.standard_normal((nz, ni))
+    out.update(dense_small_diag=d, dense_small_sup=sp, dense_small_sub=sb, dense_small_rhs=r,
+               dense_small_x=np.asarray(solver.block_thomas(d, sp, sb, r)))
+    rng = np.random.default_rng(7)
+    d = rng.standard_normal((nz, ni, ni)) + 10.0 * np.eye(ni)
+    su = rng.standard_normal((nz - 1, ni))
+    sb = rng.standard_normal((nz - 1, ni))
+    r = rng.standard_normal((nz, ni))
+    out.update(diag_small_diag=d, diag_small_sup=su, diag_small_sub=sb, diag_small_rhs=r,
+               diag_small_x=np.asarray(solver.block_thomas_diag_offdiag(d, su, sb, r)))
+    nz2, ni2 = 120, 93
+    d2 = rng.standard_normal((nz2, ni2, ni2)) + 1e10 * np.eye(ni2)
+    su2 = rng.standard_normal((nz2 - 1, ni2)) * 1e-3
+    sb2 = rng.standard_normal((nz2 - 1, ni2)) * 1e-3
+    r2 = rng.standard_normal((nz2, ni2))
+    out.update(diag_big_x=np.asarray(solver.block_thomas_diag_offdiag(d2, su2, sb2, r2)),
+               diag_big_checksum=np.array([d2.sum(), su2.sum(), sb2.sum(), r2.sum()]))
+    np.savez_compressed(os.path.join(HERE, "thomas.npz"), **out)
+    print("thomas: ok")
+
+
+def contract_fixture(mods):
+    c = mods["contract"]
+    rng = np.random.default_rng(17)
+    nz, ni, na = 10, 12, 4
+    sol = rng.normal(0, 1, (nz, ni)) * 10.0 ** rng.uniform(-30, 5, (nz, ni))
+    delta = np.abs(rng.normal(0, 1, (nz, ni))) * np.abs(sol) * 10.0 ** rng.uniform(-4, 0, (nz, ni))
+    ymix_old = 10.0 ** rng.uniform(-26, 0, (nz, ni))
+    compo = rng.integers(0, 4, (ni, na)).astype(np.float64)
+    atom_ini = np.abs(rng.normal(10, 1, na)) * 1e20
+    gas = rng.random(ni) > 0.2
+    clip_g = c._make_clip_fn(True, gas, 1e-22, 0.0, -1.0)
+    clip_a = c._make_clip_fn(False, gas, 1e-22, 0.0, -1.0)
+    yg, mg, sg, ng = clip_g(sol, ymix_old)
+    ya, ma, sa, na_ = clip_a(sol, ymix_old)
+    cz = rng.random((nz, ni)) < 0.1
+    agg = c._make_aggregate_delta_fn(1e-22, 1e-1, False, np.zeros((nz, ni), bool))
+    agg_b = c._make_aggregate_delta_fn(1e-22, 1e-1, True, cz)
+    dts = 10.0 ** rng.uniform(-12, -2, 32)
+    deltas = np.concatenate([[0.0], 10.0 ** rng.uniform(-6, 2, 31)])
+    h = np.array([c._step_size(dt, dl, 0.2, 0.5, 2.0, 1e-14, 1e-2) for dt, dl in zip(dts, deltas)])
+    al = np.asarray(c._compute_atom_loss(np.abs(sol), compo, atom_ini))
+    np.savez_compressed(os.path.join(HERE, "contract.npz"), sol=sol, delta=delta, ymix_old=ymix_old,
+                        compo=compo, atom_ini=atom_ini, gas=gas, cz=cz,
+                        clip_gas_y=np.asarray(yg), clip_gas_mix=np.asarray(mg),
+                        clip_gas_small=np.asarray(sg), clip_gas_nega=np.asarray(ng),
+                        clip_all_y=np.asarray(ya), clip_all_mix=np.asarray(ma),
+                        clip_all_small=np.asarray(sa), clip_all_nega=np.asarray(na_),
+                        agg=np.asarray(agg(np.asarray(yg), delta, ymix_old)),
+                        agg_bot=np.asarray(agg_b(np.asarray(yg), delta, ymix_old)),
+                        dts=dts, deltas=deltas, dt_next=h, atom_loss=al)
+    print("contract: ok")
+
+
+def photo_fixture(mods, syn):
+    photo = mods["photo"]
+    net = syn.make_network(21, 16, 40, n_photo=6)
+    atm, extra = syn.make_atmosphere(21, net, nz=10)
+    bins, din12 = syn.make_bins(2.0, 42.0, 0.25, 1.0, 22.0)
+    ph = syn.make_photo(21, net, atm["Tco"], bins, din12, dbin1=0.25, dbin2=1.0, n_T_abs=1)
+    pd = photo.PhotoData(absp_idx=ph["absp_idx"], absp_cross=ph["absp_cross"],
+                         absp_T_idx=ph["absp_T_idx"], absp_T_cross=ph["absp_T_cross"],
+                         scat_idx=ph["scat_idx"], scat_cross=ph["scat_cross"])
+    y, dz, ymix = extra["y"], extra["dz"], extra["ymix"]
+    tau = np.asarray(photo.compute_tau_jax(y, dz, pd))
+    rng = np.random.default_rng(5)
+    prev = np.abs(rng.normal(0, 1, tau.shape)) * 1e3
+    res = {}
+    for ag0 in (0.0, 0.3):
+        aflux, sflux, dd, du = photo.compute_flux_jax(tau, ph["sflux_top"], ymix, pd, bins,
+                                                      ph["mu_zenith"], ph["edd"], ag0, ph["hc"], prev,
+                                                      ag0_is_zero=(ag0 == 0.0))
+        tag = "ag0" if ag0 == 0.0 else "ag3"
+        res.update({f"{tag}_aflux": np.asarray(aflux), f"{tag}_sflux": np.asarray(sflux),
+                    f"{tag}_dflux_d": np.asarray(dd), f"{tag}_dflux_u": np.asarray(du)})
+    Jb, JbT = photo.compute_J_jax_flat(res["ag0_aflux"], ph["cross_J"], ph["cross_J_T"],
+                                       ph["din12_indx"], ph["dbin1"], ph["dbin2"])
+    k = syn.make_rates(21, net, 10)
+    act = np.ones(len(ph["branch_re_idx"]), bool)
+    act[0] = False
+    actT = np.ones(len(ph["branch_T_re_idx"]), bool)
+    import _jax_numpy_shim as shim
+    k_new = photo.update_k_with_J(k.view(shim.JArr), Jb, JbT, ph["branch_re_idx"], act, ph["branch_T_re_idx"], actT,
+                                  0.5)
+    save = dict(y=y, dz=dz, ymix=ymix, tau=tau, dflux_u_prev=prev, J_br=np.asarray(Jb),
+                J_br_T=np.asarray(JbT), k=k, k_new=np.asarray(k_new), active=act, active_T=actT)
+    save.update(res)
+    for key, v in ph.items():
+        save["ph_" + key] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, "photo.npz"), **save)
+    print("photo: ok", tau.shape)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE", "/root/reference"))
+    args = ap.parse_args()
+    mods, _ = load_reference(args.reference)
+    syn = importlib.import_module("jax-vulcan_b200.synthetic")
+    mild = dict(mild=True, k_range=(-40.0, 4.0))
+    step_fixture(mods, "plain", syn.make_case(seed=5, ni=12, n_fwd=30, nz=10, **mild), n_steps=3)
+    step_fixture(mods, "moldiff", syn.make_case(seed=6, ni=12, n_fwd=30, nz=10, moldiff=True, **mild))
+    step_fixture(mods, "full", syn.make_case(seed=7, ni=12, n_fwd=30, nz=12, moldiff=True,
+                                             advection=True, fluxes=True, n_three_body=8, **mild))
+    case = syn.make_case(seed=8, ni=12, n_fwd=30, nz=10, moldiff=True, fluxes=True, **mild)
+    fm = np.random.default_rng(8).random(case.y.shape) < 0.1
+    step_fixture(mods, "fixmask", case, fix_mask=fm)
+    step_fixture(mods, "medium", syn.make_case(seed=9, ni=30, n_fwd=185, nz=24, moldiff=True,
+                                               n_three_body=20, **mild))
+    # spec-like stiff draw (k log-uniform over [1e-45, 1e-6], dt = 1e-6): an
+    # ill-conditioned step; only its chemistry RHS/Jacobian are compared elementwise.
+    step_fixture(mods, "stiff", syn.make_case(seed=10, ni=30, n_fwd=185, nz=24, k_range=(-45.0, -6.0),
+                                              n_three_body=20))
+    thomas_fixture(mods)
+    contract_fixture(mods)
+    photo_fixture(mods, syn)
+
+
+if __name__ == "__main__":
+    main()

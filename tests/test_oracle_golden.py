@@ -1,0 +1,137 @@
+"""The CPU oracle against fixtures made by running the reference's own code.
+
+The fixtures (``tests/golden/*.npz``) hold the outputs of the unmodified
+reference `jax_step.jax_ros2_step`, `chem.chem_rhs` / `chem_jac_analytical`,
+`solver.*`, `integrate.jax_integrate_fixed_dt`, `photo.*` and the
+`outer_loop.py` caller-contract functions (see ``tests/golden/make_golden.py``).
+The oracle restates the same arithmetic, so agreement is expected to the last
+bit; the assertions allow 1e-13 relative for platform LAPACK differences.
+"""
+import numpy as np
+import pytest
+
+from conftest import STEP_CASES, golden, golden_step, load_pkg
+from oracle import contract as oc
+from oracle import photo as op
+from oracle import ros2 as orc
+
+TABLES = ["reactant_idx", "product_idx", "reactant_stoich", "product_stoich", "is_three_body"]
+
+
+def close(a, b, rtol=1e-13, floor=1e-300):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape
+    same_nonfinite = (~np.isfinite(a)) & (~np.isfinite(b))
+    err = np.where(same_nonfinite, 0.0, np.abs(a - b) / np.maximum(np.abs(b), floor))
+    assert np.nanmax(err, initial=0.0) <= rtol, np.nanmax(err)
+
+
+@pytest.mark.parametrize("name", STEP_CASES + ["stiff"])
+def test_parser_matches_reference_parser(name):
+    net, _, _, _, _, _, g = golden_step(name)
+    assert net.ni == int(g["ni"]) and net.nr == int(g["nr"])
+    for t in TABLES:
+        np.testing.assert_array_equal(getattr(net, t), g["tab_" + t])
+
+
+@pytest.mark.parametrize("name", STEP_CASES + ["stiff"])
+def test_chem_rhs_and_jacobian(name):
+    net, atm, y, k, dt, fm, g = golden_step(name)
+    close(orc.chem_rhs(y, atm["M"], k, net), g["rhs"], rtol=0.0)
+    close(orc.chem_jac(y, atm["M"], k, net), g["jac"], rtol=0.0)
+
+
+@pytest.mark.parametrize("name", STEP_CASES)
+def test_ros2_step(name):
+    net, atm, y, k, dt, fm, g = golden_step(name)
+    sol, delta = orc.ros2_step(y, k, dt, atm, net, fix_mask=fm)
+    close(sol, g["sol"])
+    close(delta, g["delta"])
+
+
+def test_integrate_fixed_dt():
+    net, atm, y, k, dt, fm, g = golden_step("plain")
+    yN, deltas = orc.integrate_fixed_dt(y, k, dt, int(g["int_n"]), atm, net)
+    close(yN, g["int_y"])
+    close(deltas, g["int_deltas"])
+
+
+def test_block_thomas_known_systems():
+    g = golden("thomas.npz")
+    x = orc.block_thomas_dense(g["dense_small_diag"], g["dense_small_sup"], g["dense_small_sub"],
+                               g["dense_small_rhs"])
+    close(x, g["dense_small_x"])
+    x = orc.block_thomas(g["diag_small_diag"], g["diag_small_sup"], g["diag_small_sub"], g["diag_small_rhs"])
+    close(x, g["diag_small_x"])
+    # regenerate the (nz=120, ni=93) system of the reference test from its seed
+    rng = np.random.default_rng(7)
+    nz, ni = 8, 5
+    rng.standard_normal((nz, ni, ni)); rng.standard_normal((nz - 1, ni))
+    rng.standard_normal((nz - 1, ni)); rng.standard_normal((nz, ni))
+    d2 = rng.standard_normal((120, 93, 93)) + 1e10 * np.eye(93)
+    su2 = rng.standard_normal((119, 93)) * 1e-3
+    sb2 = rng.standard_normal((119, 93)) * 1e-3
+    r2 = rng.standard_normal((120, 93))
+    np.testing.assert_allclose([d2.sum(), su2.sum(), sb2.sum(), r2.sum()], g["diag_big_checksum"], rtol=1e-12)
+    close(orc.block_thomas(d2, su2, sb2, r2), g["diag_big_x"], rtol=1e-12)
+
+
+def test_block_thomas_vs_dense_solve():
+    """Reference tests/test_block_thomas_diag.py:129-192: diag-offdiag Thomas
+    equals the dense block Thomas and a dense direct solve."""
+    g = golden("thomas.npz")
+    d, su, sb, r = g["diag_small_diag"], g["diag_small_sup"], g["diag_small_sub"], g["diag_small_rhs"]
+    nz, ni = r.shape
+    Mx = np.zeros((nz * ni, nz * ni))
+    for j in range(nz):
+        Mx[j * ni:(j + 1) * ni, j * ni:(j + 1) * ni] = d[j]
+    for j in range(nz - 1):
+        Mx[j * ni:(j + 1) * ni, (j + 1) * ni:(j + 2) * ni] = np.diag(su[j])
+        Mx[(j + 1) * ni:(j + 2) * ni, j * ni:(j + 1) * ni] = np.diag(sb[j])
+    x_dense = np.linalg.solve(Mx, r.reshape(-1)).reshape(nz, ni)
+    close(orc.block_thomas(d, su, sb, r), x_dense, rtol=1e-12, floor=1e-12)
+
+
+def test_contract_functions():
+    g = golden("contract.npz")
+    y, mix, sm, ng = oc.clip(g["sol"], g["ymix_old"], 1e-22, 0.0, -1.0, gas_mask=g["gas"])
+    close(y, g["clip_gas_y"], 0.0); close(mix, g["clip_gas_mix"], 0.0)
+    close(sm, g["clip_gas_small"], 0.0); close(ng, g["clip_gas_nega"], 0.0)
+    y2, mix2, sm2, ng2 = oc.clip(g["sol"], g["ymix_old"], 1e-22, 0.0, -1.0)
+    close(y2, g["clip_all_y"], 0.0); close(mix2, g["clip_all_mix"], 0.0)
+    close(oc.aggregate_delta(y, g["delta"], g["ymix_old"], 1e-22, 1e-1), g["agg"], 0.0)
+    close(oc.aggregate_delta(y, g["delta"], g["ymix_old"], 1e-22, 1e-1, True, g["cz"]), g["agg_bot"], 0.0)
+    dtn = [oc.step_size(dt, dl, 0.2, 0.5, 2.0, 1e-14, 1e-2) for dt, dl in zip(g["dts"], g["deltas"])]
+    close(dtn, g["dt_next"], 0.0)
+    close(oc.atom_loss(np.abs(g["sol"]), g["compo"], g["atom_ini"]), g["atom_loss"], 1e-15)
+
+
+def _ph(g):
+    return {k[3:]: (g[k].item() if g[k].ndim == 0 else g[k]) for k in g if k.startswith("ph_")}
+
+
+def test_photo_kernels():
+    g = golden("photo.npz")
+    ph = _ph(g)
+    close(op.compute_tau(g["y"], g["dz"], ph), g["tau"], 1e-14)
+    for tag, ag0 in (("ag0", 0.0), ("ag3", 0.3)):
+        p2 = dict(ph, ag0=ag0)
+        aflux, sflux, dd, du = op.compute_flux(g["tau"], g["ymix"], p2, g["dflux_u_prev"])
+        close(aflux, g[f"{tag}_aflux"], 1e-13); close(sflux, g[f"{tag}_sflux"], 1e-13)
+        close(dd, g[f"{tag}_dflux_d"], 1e-13); close(du, g[f"{tag}_dflux_u"], 1e-13)
+    Jb, JbT = op.compute_J(g["ag0_aflux"], ph)
+    close(Jb, g["J_br"], 1e-13); close(JbT, g["J_br_T"], 1e-13)
+    kn = op.update_k_with_J(g["k"], g["J_br"], g["J_br_T"], ph["branch_re_idx"], g["active"],
+                            ph["branch_T_re_idx"], g["active_T"], 0.5)
+    close(kn, g["k_new"], 0.0)
+
+
+def test_synthetic_network_balances_elements():
+    syn = load_pkg("synthetic")
+    net = syn.make_network(0, 69, 700)
+    t = net.tables
+    assert t.ni == 69 and t.nr == 1400
+    for r in range(1, t.nr + 1):
+        lhs = sum(net.compo[i] * s for i, s in zip(t.reactant_idx[r], t.reactant_stoich[r]) if i < t.ni)
+        rhs = sum(net.compo[i] * s for i, s in zip(t.product_idx[r], t.product_stoich[r]) if i < t.ni)
+        np.testing.assert_array_equal(lhs, rhs)
