@@ -1,0 +1,359 @@
+"""Throughput of the B200 Ros2 step (atmosphere-Ros2-steps per second).
+
+Workload (one "step" = one Ros2 step of every atmosphere of the batch):
+config-0-shaped atmospheres - a seeded element-balanced C/H/O/N network with
+ni=69 species and 700+700 reactions, nz=120 layers, rate constants
+log-uniform in [1e-40, 1e-8], mixing ratios log-uniform in [1e-20, 1],
+dt = 1e-6 s - batched B atmospheres per GPU (seeded per atmosphere and per
+rank), FP64. The same inputs are stepped repeatedly (as the reference's
+benchmarks/bench_step.py does). Per-step inputs (rates 172 MB, solver
+workspace 590 MB at B=128) exceed the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl b200|reference]
+
+Multi-GPU: one process per GPU (torchrun); each rank steps its own batch
+(weak scaling, no collective on the data path; the max over ranks of the
+device time is taken with one all-reduce after the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atmosphere-Ros2-steps/s: batched mixed vs plain FP64, 1 B200, ≤1e-6 rel err"
+UNIT = "atmosphere-steps/s"
+
+
+def pkg(name):
+    return importlib.import_module("jax-vulcan_b200." + name)
+
+
+def make_batch(B, rank, nz=120):
+    syn = pkg("synthetic")
+    net = syn.make_network(0, 69, 700)
+    cases = [syn.make_case(seed=(1000 * rank + b,), net=net, nz=nz) for b in range(B)]
+    Y = np.stack([c.y for c in cases])
+    K = np.stack([c.k for c in cases])
+    DT = np.array([c.dt for c in cases])
+    A = {}
+    for key, v in cases[0].atm.items():
+        A[key] = v if isinstance(v, bool) else np.stack([c.atm[key] for c in cases])
+    return net, cases, Y, K, DT, A
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_port(seconds=12.0, max_steps=40):
+    """The oracle (NumPy/SciPy restatement of the reference step) on one
+    config-0 atmosphere, single-threaded, bounded to ~`seconds`."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import ros2 as orc
+    syn = pkg("synthetic")
+    case = syn.config0()
+    with threadpool_limits(1):
+        orc.ros2_step(case.y, case.k, case.dt, case.atm, case.net.tables)
+        n, t0 = 0, time.perf_counter()
+        while n < max_steps and time.perf_counter() - t0 < seconds:
+            orc.ros2_step(case.y, case.k, case.dt, case.atm, case.net.tables)
+            n += 1
+        el = time.perf_counter() - t0
+    return {"value": n / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} single-atmosphere config-0 steps (ni=69, nr=1400, nz=120) of the NumPy/SciPy "
+                      f"restatement of jax_step.jax_ros2_step, 1 thread, {el:.1f} s"}
+
+
+def _ref_worker(args):
+    seed, n_steps = args
+    from threadpoolctl import threadpool_limits
+
+    from oracle import ros2 as orc
+    syn = importlib.import_module("jax-vulcan_b200.synthetic")
+    net = syn.make_network(0, 69, 700)
+    case = syn.make_case(seed=(seed,), net=net)
+    with threadpool_limits(1):
+        t0 = time.perf_counter()
+        for _ in range(n_steps):
+            orc.ros2_step(case.y, case.k, case.dt, case.atm, case.net.tables)
+        return time.perf_counter() - t0
+
+
+def run_reference(args):
+    """Reference arm: the reference's step restated on NumPy/SciPy (JAX is not
+    installed) on all host cores, one atmosphere per process."""
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = len(os.sched_getaffinity(0))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_ref_worker, [(s, 1) for s in range(cores)])            # import + warm
+        for _ in range(args.warmup):
+            pool.map(_ref_worker, [(s, 1) for s in range(cores)])
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pool.map(_ref_worker, [(s, 1) for s in range(cores)])
+        el = time.perf_counter() - t0
+    value = cores * args.steps / el
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic (seeded config-0-shaped atmospheres)",
+            "config": {"workload": "config-0-shaped atmospheres (ni=69, nr=1400, nz=120, dt=1e-6)",
+                       "batch": cores, "precision": "fp64"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"each step: {cores} atmospheres x 1 Ros2 step, one per process "
+                                       f"(NumPy/SciPy restatement of jax_step.jax_ros2_step; JAX absent)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def fp64_peak_tflops(lib, torch, stream):
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    blocks, threads, iters = 148 * 16, 256, 4096
+    lib.vb_fp64_probe(out.data_ptr(), blocks, threads, 64, stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        lib.vb_fp64_probe(out.data_ptr(), blocks, threads, iters, stream)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = max(best, 2.0 * 8 * iters * blocks * threads / (ms * 1e-3) / 1e12)
+    return best
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    _lib = pkg("_lib")
+    chem = pkg("chem")
+    jstep = pkg("jax_step")
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+    sh = _lib.stream_handle(stream)
+
+    B = args.batch
+    net, cases, Y, K, DT, A = make_batch(B, rank)
+    dn = chem.to_device(net.tables)
+    atm = jstep.atm_from_dict(A)
+    step = jstep.Ros2Step(dn, atm)
+    y = torch.as_tensor(Y, device="cuda")
+    k = torch.as_tensor(K, device="cuda")
+    dt = torch.as_tensor(DT, device="cuda")
+    sol = torch.empty_like(y)
+    delta = torch.empty_like(y)
+
+    def one():
+        step(y, k, dt, out=(sol, delta))
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        one()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * B / (ms * 1e-3)
+
+    # per-kernel device times over a separate profiled pass (events on the launch stream)
+    L.vb_profile(1)
+    for _ in range(args.steps):
+        one()
+    torch.cuda.synchronize()
+    site_ms = (np.zeros(8), np.zeros(8, dtype=np.int64))
+    L.vb_profile_read(site_ms[0].ctypes.data, site_ms[1].ctypes.data, 8)
+    L.vb_profile(0)
+    names = _lib.PROFILE_SITES
+    per_kernel = {n: {"ms_per_launch": float(site_ms[0][i] / max(site_ms[1][i], 1)),
+                      "launches": int(site_ms[1][i])} for i, n in enumerate(names)}
+    tot = sum(v["ms_per_launch"] for v in per_kernel.values())
+    for v in per_kernel.values():
+        v["share"] = v["ms_per_launch"] / tot if tot else 0.0
+
+    # end to end through the public API with pinned host buffers
+    y_h = torch.as_tensor(Y).pin_memory()
+    dt_h = torch.as_tensor(DT).pin_memory()
+    sol_h = torch.empty_like(y_h).pin_memory()
+    delta_h = torch.empty_like(y_h).pin_memory()
+    y_d = torch.empty_like(y)
+    dt_d = torch.empty_like(dt)
+
+    def e2e_step():
+        y_d.copy_(y_h, non_blocking=True)
+        dt_d.copy_(dt_h, non_blocking=True)
+        step(y_d, k, dt_d, out=(sol, delta))
+        sol_h.copy_(sol, non_blocking=True)
+        delta_h.copy_(delta, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = y_h.numel() * 8 + dt_h.numel() * 8
+    d2h = 2 * y_h.numel() * 8
+
+    # plain single-instance FP64 step (one atmosphere)
+    step1 = jstep.Ros2Step(dn, jstep.atm_from_dict(cases[0].atm))
+    y1, k1, dt1 = y[:1].contiguous(), k[:1].contiguous(), dt[:1].contiguous()
+    s1, d1 = torch.empty_like(y1), torch.empty_like(y1)
+    for _ in range(3):
+        step1(y1, k1, dt1, out=(s1, d1))
+    torch.cuda.synchronize()
+    n1 = max(3, args.steps)
+    e0.record()
+    for _ in range(n1):
+        step1(y1, k1, dt1, out=(s1, d1))
+    e1.record()
+    torch.cuda.synchronize()
+    single_ms = e0.elapsed_time(e1) / n1
+
+    peak64 = fp64_peak_tflops(L, torch, sh)
+    ni, nz = net.tables.ni, Y.shape[1]
+    fac_flops = B * nz * 2.0 * ni ** 3          # Gauss-Jordan inverse: n^3 FMA per block
+    fac_ms = per_kernel["factor"]["ms_per_launch"]
+    achieved = fac_flops / (fac_ms * 1e-3) / 1e12 if fac_ms > 0 else 0.0
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded config-0-shaped atmospheres; stiff k log-uniform 1e-40..1e-8)",
+            "config": {"workload": f"batched Ros2 step, {B} config-0-shaped atmospheres per GPU "
+                                   f"(ni={ni}, nr={net.tables.nr}, nz={nz}, dt=1e-6)",
+                       "batch_per_gpu": B, "ni": ni, "nr": int(net.tables.nr), "nz": int(nz),
+                       "precision": "fp64", "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (rates 172 MB + workspace 590 MB per GPU at B=128)"},
+            "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h),
+                    "note": "y and dt copied in from pinned host memory, sol and delta read back, every step; "
+                            "rates and atmosphere stay resident (as in the reference runner's device carry)"},
+            "gpu_launches": 6 * args.steps,
+            "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan block inverses, serial in z)",
+                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                         "frac": achieved / peak64 if peak64 else None, "traffic": None,
+                         "peak_source": "measured live: FP64 FMA probe kernel (vb_fp64_probe)",
+                         "algorithmic": f"2*ni^3 flops per layer block x {nz} layers x {B} atmospheres"},
+            "kernels": per_kernel,
+            "single_instance_fp64": {"value": 1.0 / (single_ms * 1e-3), "unit": UNIT, "ms_per_step": single_ms},
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_port()
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

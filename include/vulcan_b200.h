@@ -1,0 +1,141 @@
+/*
+ * vulcan_b200.h - C-ABI of the B200-native Ros2 step and block-Thomas solve.
+ *
+ * Every entry point takes plain pointers and sizes. Array arguments marked
+ * "device" are caller-owned device memory; all compute entry points are
+ * stream-ordered and asynchronous (no host synchronisation, no allocation).
+ * Only vb_net_create / vb_net_destroy allocate (set-up time).
+ *
+ * Return value of every function: 0 on success, otherwise a VB_ERR_* code
+ * (vb_last_error() gives a message). Per-atmosphere numerical status words
+ * (VB_STATUS_*) are written to a caller-provided device int32 array.
+ *
+ * Layouts (FP64 unless stated; "batch" atmospheres, uniform shapes or ragged
+ * layer counts given by the prefix sums `zoff`):
+ *   y, sol, delta     [B][nz][ni]            (species contiguous)
+ *   k                 [B][nr+1][nz]          (layers contiguous; row 0 unused)
+ *   dt                [B]
+ *   fix_mask          [B][nz][ni] uint8 or NULL
+ *   atm blob          [B][VB_ATM_DOUBLES(nz, ni)]  (see vb_atm_offsets)
+ *   workspace         vb_ros2_workspace_bytes(...)
+ * With ragged batches (zoff != NULL, zoff[B] = total layers) atmosphere b has
+ * nz_b = zoff[b+1]-zoff[b] layers and its arrays start at zoff[b]*ni (y),
+ * zoff[b]*(nr+1) (k), vb_atm_offset(...) (atm) in the packed buffers.
+ */
+#ifndef VULCAN_B200_H
+#define VULCAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VB_OK 0
+#define VB_ERR_ARG 1        /* invalid argument (size, pointer, ni too large) */
+#define VB_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define VB_ERR_ALLOC 3      /* set-up allocation failed */
+
+#define VB_STATUS_OK 0
+#define VB_STATUS_ZERO_PIVOT 1     /* an exactly zero pivot in a diagonal block */
+#define VB_STATUS_NONFINITE 2      /* a non-finite value in the result */
+#define VB_STATUS_REFINE_STALL 4   /* mixed path: refinement stalled, FP64 refactor used */
+#define VB_STATUS_WATCHDOG 8       /* a bounded wait gave up (kernel returned early) */
+
+/* Transport switches (reference jax_step.py:46-49 AtmStatic flags). */
+#define VB_USE_VM_MOL 1
+#define VB_USE_SETTLING 2
+#define VB_USE_TOPFLUX 4
+#define VB_USE_BOTFLUX 8
+
+/* Largest species count the kernels accept. */
+#define VB_MAX_NI 128
+
+/* Atmosphere blob: per-atmosphere packing of the reference AtmStatic
+ * (jax_step.py:26-49). Per-layer arrays take nz slots (interface arrays use
+ * the first nz-1). Field order, in doubles from the atmosphere's base:
+ *   Kzz[nz] dzi[nz] vz[nz] Hpi[nz] Ti[nz] Tco[nz] g[nz] M[nz]
+ *   Dzz[nz][ni] vm[nz][ni] vs[nz][ni]
+ *   ms[ni] alpha[ni] top_flux[ni] bot_flux[ni] bot_vdep[ni] gas_mask[ni] (0/1)  */
+#define VB_ATM_DOUBLES(nz, ni) ((size_t)(nz) * (8 + 3 * (size_t)(ni)) + 6 * (size_t)(ni))
+
+typedef struct VbNet VbNet;  /* opaque, device-resident network tables */
+
+const char* vb_last_error(void);
+int vb_version(void);
+
+/* Network tables (reference chem.py:28-80 NetworkArrays, from network.py:197-491).
+ * Host arrays: reactant_idx/product_idx [nr+1][max_terms] (padding index = ni),
+ * reactant/product_stoich [nr+1][max_terms], is_three_body [nr+1].
+ * Builds the gather tables of the RHS and Jacobian scatters on the host and
+ * uploads them (the only allocating call). */
+int vb_net_create(int ni, int nr, int max_terms,
+                  const int64_t* reactant_idx, const int64_t* product_idx,
+                  const double* reactant_stoich, const double* product_stoich,
+                  const uint8_t* is_three_body, VbNet** out);
+int vb_net_destroy(VbNet* net);
+/* Device bytes held by a network. */
+size_t vb_net_device_bytes(const VbNet* net);
+
+/* Ros2 step (replaces reference jax_step.py:249-315 jax_ros2_step, vmapped over
+ * a batch). Inputs y, k, dt, atm, fix_mask (nullable); outputs sol, delta,
+ * status[B]. zoff: NULL for a uniform batch of `nz` layers, else device int64
+ * [B+1] prefix sums (then nz is the maximum layer count). */
+size_t vb_ros2_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host);
+int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff,
+                 const double* y, const double* k, const double* dt,
+                 const double* atm, int32_t atm_flags, const uint8_t* fix_mask,
+                 double* sol, double* delta, int32_t* status,
+                 void* workspace, size_t workspace_bytes, void* stream);
+
+/* Chemistry (reference chem.py:83-131 chem_rhs and chem.py:144-214
+ * chem_jac_analytical, vmapped over layers and a uniform batch):
+ * y [B][nz][ni], M [B][nz], k [B][nr+1][nz] -> dydt [B][nz][ni], jac [B][nz][ni][ni]. */
+int vb_chem_rhs(const VbNet* net, int batch, int nz, const double* y, const double* M,
+                const double* k, double* dydt, void* stream);
+int vb_chem_jac(const VbNet* net, int batch, int nz, const double* y, const double* M,
+                const double* k, double* jac, void* stream);
+
+/* Diffusion (reference jax_step.py:67-246: compute_diff_grav,
+ * _build_diff_coeffs_jax, _apply_diffusion_jax) for a uniform batch:
+ * y [B][nz][ni], atm blob -> diff [B][nz][ni] (BC fluxes included) and the
+ * block-Thomas diagonal terms diag_d [B][nz][ni] (bot_vdep included),
+ * sup_d [B][nz-1][ni], sub_d [B][nz-1][ni] (NOT negated). */
+int vb_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int32_t atm_flags,
+                 double* diff, double* diag_d, double* sup_d, double* sub_d, void* stream);
+
+/* Block-tridiagonal Thomas with dense diagonal blocks and diagonal
+ * off-diagonal blocks (reference solver.py:33-126), for a uniform batch.
+ *   vb_bt_factor:  diag [B][nz][ni][ni], sup_d, sub_d [B][nz-1][ni] (the
+ *                  off-diagonal blocks as passed to the reference solver) ->
+ *                  factors (opaque, vb_bt_factor_bytes) + status.
+ *   vb_bt_solve:   factors + rhs [B][nz][ni] -> x [B][nz][ni].
+ *   vb_bt_solve_T: solves the transposed system (for the adjoint,
+ *                  reference steady_state_grad.py:214-219): x = A^-T rhs. */
+size_t vb_bt_factor_bytes(int batch, int nz, int ni);
+int vb_bt_factor(int batch, int nz, int ni, const double* diag, const double* sup_d,
+                 const double* sub_d, void* factors, int32_t* status, void* stream);
+int vb_bt_solve(int batch, int nz, int ni, const void* factors, const double* rhs, double* x,
+                void* stream);
+int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* rhs, double* x,
+                  void* stream);
+
+/* Profiling: while enabled, every kernel launch of vb_ros2_step is bracketed
+ * by CUDA events recorded on the launching stream (launch sites:
+ * 0 stage-1 assembly, 1 factor, 2 back sweep 1, 3 stage-2 assembly,
+ * 4 forward sweep 2, 5 back sweep 2). vb_profile_read synchronises, writes
+ * the summed milliseconds and launch counts of the first n sites, and clears. */
+#define VB_PROFILE_SITES 8
+int vb_profile(int enable);
+int vb_profile_read(double* ms, int64_t* counts, int n);
+
+/* FP64 throughput probe: a register-resident dependent-FMA loop (8 chains per
+ * thread) over the whole GPU, writes a checksum to out[0]. Used to measure the
+ * FP64 FMA peak that bounds the block factorisation. */
+int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VULCAN_B200_H */

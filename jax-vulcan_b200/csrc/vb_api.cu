@@ -1,0 +1,325 @@
+// C-ABI entry points (include/vulcan_b200.h): network set-up and the
+// stream-ordered launch sequences of the Ros2 step and the block solver.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vb_common.cuh"
+#include "vb_launch.cuh"
+
+
+struct VbNet {
+  vb::NetDev dev;
+  void* base;
+  size_t bytes;
+};
+
+static thread_local std::string g_err;
+
+// ---- optional per-launch event profiling (see vb_profile in the header)
+namespace {
+struct ProfSite {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+};
+bool g_prof = false;
+ProfSite g_sites[VB_PROFILE_SITES];
+
+struct ProfScope {
+  int site;
+  cudaStream_t st;
+  cudaEvent_t b = nullptr, e = nullptr;
+  ProfScope(int s, cudaStream_t stream) : site(s), st(stream) {
+    if (g_prof) {
+      cudaEventCreate(&b);
+      cudaEventCreate(&e);
+      cudaEventRecord(b, st);
+    }
+  }
+  ~ProfScope() {
+    if (g_prof && b) {
+      cudaEventRecord(e, st);
+      g_sites[site].ev.emplace_back(b, e);
+    }
+  }
+};
+}  // namespace
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+static int cuda_fail(cudaError_t e, const char* where) {
+  return fail(VB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define VB_CHECK(call, where)                      \
+  do {                                             \
+    cudaError_t _e = (call);                       \
+    if (_e != cudaSuccess) return cuda_fail(_e, where); \
+  } while (0)
+
+extern "C" {
+
+const char* vb_last_error(void) { return g_err.c_str(); }
+int vb_version(void) { return 1; }
+
+int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_idx, const double* r_st,
+                  const double* p_st, const uint8_t* three, VbNet** out) {
+  if (!out || !r_idx || !p_idx || !r_st || !p_st || !three) return fail(VB_ERR_ARG, "null argument");
+  if (ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "ni must be in [1, 128]");
+  if (nr < 1 || T < 1 || T > 8) return fail(VB_ERR_ARG, "nr >= 1 and 1 <= max_terms <= 8 required");
+  const int R = nr + 1;
+  for (int64_t e = 0; e < (int64_t)R * T; ++e) {
+    if (r_idx[e] < 0 || r_idx[e] > ni || p_idx[e] < 0 || p_idx[e] > ni)
+      return fail(VB_ERR_ARG, "species index out of [0, ni]");
+  }
+  // gather tables in segment_sum order (increasing flat index)
+  std::vector<std::vector<int32_t>> loss(ni), prod(ni), jac((size_t)ni * ni);
+  for (int rs = 0; rs < R * T; ++rs) {
+    if (r_idx[rs] < ni) loss[r_idx[rs]].push_back(rs);
+    if (p_idx[rs] < ni) prod[p_idx[rs]].push_back(rs);
+  }
+  for (int r = 0; r < R; ++r)
+    for (int o = 0; o < 2 * T; ++o) {
+      int64_t row = o < T ? r_idx[(int64_t)r * T + o] : p_idx[(int64_t)r * T + (o - T)];
+      for (int s = 0; s < T; ++s) {
+        int64_t col = r_idx[(int64_t)r * T + s];
+        if (row < ni && col < ni) jac[row * ni + col].push_back((int32_t)(((int64_t)r * 2 * T + o) * T + s));
+      }
+    }
+  auto csr = [](const std::vector<std::vector<int32_t>>& lists, std::vector<int32_t>& ptr,
+                std::vector<int32_t>& ent) {
+    ptr.assign(lists.size() + 1, 0);
+    for (size_t i = 0; i < lists.size(); ++i) ptr[i + 1] = ptr[i] + (int32_t)lists[i].size();
+    ent.clear();
+    for (auto& l : lists) ent.insert(ent.end(), l.begin(), l.end());
+    if (ent.empty()) ent.push_back(0);
+  };
+  std::vector<int32_t> lp, le, pp, pe, jp, je;
+  csr(loss, lp, le);
+  csr(prod, pp, pe);
+  csr(jac, jp, je);
+  std::vector<int32_t> ri(R * T), pi(R * T);
+  for (int e = 0; e < R * T; ++e) { ri[e] = (int32_t)r_idx[e]; pi[e] = (int32_t)p_idx[e]; }
+
+  // one allocation, 256-byte aligned sub-arrays
+  struct Part { const void* src; size_t bytes; size_t off; };
+  std::vector<Part> parts = {
+      {ri.data(), ri.size() * 4, 0}, {pi.data(), pi.size() * 4, 0},
+      {r_st, (size_t)R * T * 8, 0},  {p_st, (size_t)R * T * 8, 0},
+      {three, (size_t)R, 0},         {lp.data(), lp.size() * 4, 0},
+      {le.data(), le.size() * 4, 0}, {pp.data(), pp.size() * 4, 0},
+      {pe.data(), pe.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
+      {je.data(), je.size() * 4, 0}};
+  size_t total = 0;
+  for (auto& p : parts) { p.off = total; total += (p.bytes + 255) & ~(size_t)255; }
+  void* base = nullptr;
+  cudaError_t e = cudaMalloc(&base, total);
+  if (e != cudaSuccess) return fail(VB_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  for (auto& p : parts) {
+    e = cudaMemcpy((char*)base + p.off, p.src, p.bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(base); return cuda_fail(e, "cudaMemcpy"); }
+  }
+  VbNet* net = new VbNet;
+  char* b = (char*)base;
+  vb::NetDev& d = net->dev;
+  d.ni = ni; d.nr = nr; d.T = T;
+  d.r_idx = (const int32_t*)(b + parts[0].off);
+  d.p_idx = (const int32_t*)(b + parts[1].off);
+  d.r_st = (const double*)(b + parts[2].off);
+  d.p_st = (const double*)(b + parts[3].off);
+  d.three = (const uint8_t*)(b + parts[4].off);
+  d.loss_ptr = (const int32_t*)(b + parts[5].off);
+  d.loss_ent = (const int32_t*)(b + parts[6].off);
+  d.prod_ptr = (const int32_t*)(b + parts[7].off);
+  d.prod_ent = (const int32_t*)(b + parts[8].off);
+  d.jac_ptr = (const int32_t*)(b + parts[9].off);
+  d.jac_ent = (const int32_t*)(b + parts[10].off);
+  net->base = base;
+  net->bytes = total;
+  *out = net;
+  return VB_OK;
+}
+
+int vb_net_destroy(VbNet* net) {
+  if (!net) return VB_OK;
+  cudaError_t e = cudaFree(net->base);
+  delete net;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFree");
+  return VB_OK;
+}
+
+size_t vb_net_device_bytes(const VbNet* net) { return net ? net->bytes : 0; }
+
+size_t vb_ros2_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host) {
+  int64_t layers = zoff_host ? zoff_host[batch] : (int64_t)batch * nz;
+  return (size_t)layers * vb::ws_per_layer(ni, vb::round_even(ni)) * sizeof(double);
+}
+
+static vb::Batch make_batch(const VbNet* net, int batch, int nz, const int64_t* zoff) {
+  vb::Batch B;
+  B.count = batch;
+  B.nz = nz;
+  B.ni = net->dev.ni;
+  B.nr = net->dev.nr;
+  B.ld = vb::round_even(B.ni);
+  B.zoff = zoff;
+  return B;
+}
+
+int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
+                 const double* dt, const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol,
+                 double* delta, int32_t* status, void* workspace, size_t ws_bytes, void* stream) {
+  if (!net || !y || !k || !dt || !atm || !sol || !delta || !status || !workspace)
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  if (!zoff && ws_bytes < vb_ros2_workspace_bytes(batch, nz, net->dev.ni, nullptr))
+    return fail(VB_ERR_ARG, "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = make_batch(net, batch, nz, zoff);
+  double* ws = (double*)workspace;
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  {
+    ProfScope p(0, st);
+    VB_CHECK(vb::launch_stage1(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage1");
+  }
+  {
+    ProfScope p(1, st);
+    VB_CHECK(vb::launch_factor(B, ws, status, 1, st), "factor");
+  }
+  vb::SweepArgs a{};
+  a.mode = 1;
+  a.status = status;
+  {
+    ProfScope p(2, st);
+    VB_CHECK(vb::launch_sweep(B, ws, a, st), "back sweep 1");
+  }
+  {
+    ProfScope p(3, st);
+    VB_CHECK(vb::launch_stage2(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage2");
+  }
+  a.mode = 0;
+  {
+    ProfScope p(4, st);
+    VB_CHECK(vb::launch_sweep(B, ws, a, st), "forward sweep 2");
+  }
+  a.mode = 2;
+  a.y = y;
+  a.sol = sol;
+  a.delta = delta;
+  {
+    ProfScope p(5, st);
+    VB_CHECK(vb::launch_sweep(B, ws, a, st), "back sweep 2");
+  }
+  return VB_OK;
+}
+
+int vb_chem_rhs(const VbNet* net, int batch, int nz, const double* y, const double* M, const double* k,
+                double* dydt, void* stream) {
+  if (!net || !y || !M || !k || !dydt) return fail(VB_ERR_ARG, "null argument");
+  VB_CHECK(vb::launch_chem(net->dev, batch, nz, y, M, k, dydt, nullptr, (cudaStream_t)stream), "chem_rhs");
+  return VB_OK;
+}
+
+int vb_chem_jac(const VbNet* net, int batch, int nz, const double* y, const double* M, const double* k,
+                double* jac, void* stream) {
+  if (!net || !y || !M || !k || !jac) return fail(VB_ERR_ARG, "null argument");
+  VB_CHECK(vb::launch_chem(net->dev, batch, nz, y, M, k, nullptr, jac, (cudaStream_t)stream), "chem_jac");
+  return VB_OK;
+}
+
+int vb_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int32_t flags, double* diff,
+                 double* diag_d, double* sup_d, double* sub_d, void* stream) {
+  if (!y || !atm) return fail(VB_ERR_ARG, "null argument");
+  if (nz < 2 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "bad shape");
+  VB_CHECK(vb::launch_diffusion(batch, nz, ni, y, atm, flags, diff, diag_d, sup_d, sub_d,
+                                (cudaStream_t)stream),
+           "diffusion");
+  return VB_OK;
+}
+
+size_t vb_bt_factor_bytes(int batch, int nz, int ni) {
+  return (size_t)batch * nz * vb::ws_per_layer(ni, vb::round_even(ni)) * sizeof(double);
+}
+
+static vb::Batch bt_batch(int batch, int nz, int ni) {
+  vb::Batch B;
+  B.count = batch; B.nz = nz; B.ni = ni; B.nr = 0; B.ld = vb::round_even(ni); B.zoff = nullptr;
+  return B;
+}
+
+int vb_bt_factor(int batch, int nz, int ni, const double* diag, const double* sup_d, const double* sub_d,
+                 void* factors, int32_t* status, void* stream) {
+  if (!diag || !sup_d || !sub_d || !factors || !status) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "bad shape");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = bt_batch(batch, nz, ni);
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  VB_CHECK(vb::launch_pack_blocks(B, diag, sup_d, sub_d, (double*)factors, st), "pack");
+  VB_CHECK(vb::launch_factor(B, (double*)factors, status, 0, st), "factor");
+  return VB_OK;
+}
+
+static int bt_solve(int batch, int nz, int ni, const void* factors, const double* rhs, double* x, int trans,
+                    void* stream) {
+  if (!factors || !rhs || !x) return fail(VB_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = bt_batch(batch, nz, ni);
+  if (x != rhs)
+    VB_CHECK(cudaMemcpyAsync(x, rhs, sizeof(double) * batch * nz * ni, cudaMemcpyDeviceToDevice, st), "copy");
+  vb::SweepArgs a{};
+  a.transposed = trans;
+  a.user = x;
+  a.mode = 0;
+  VB_CHECK(vb::launch_sweep(B, (double*)factors, a, st), "forward sweep");
+  a.mode = 1;
+  VB_CHECK(vb::launch_sweep(B, (double*)factors, a, st), "back sweep");
+  return VB_OK;
+}
+
+int vb_bt_solve(int batch, int nz, int ni, const void* factors, const double* rhs, double* x, void* stream) {
+  return bt_solve(batch, nz, ni, factors, rhs, x, 0, stream);
+}
+
+int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* rhs, double* x,
+                  void* stream) {
+  return bt_solve(batch, nz, ni, factors, rhs, x, 1, stream);
+}
+
+int vb_profile(int enable) {
+  g_prof = enable != 0;
+  return VB_OK;
+}
+
+int vb_profile_read(double* ms, int64_t* counts, int n) {
+  if (n > VB_PROFILE_SITES) n = VB_PROFILE_SITES;
+  for (int s = 0; s < VB_PROFILE_SITES; ++s) {
+    double tot = 0.0;
+    for (auto& pr : g_sites[s].ev) {
+      cudaEventSynchronize(pr.second);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, pr.first, pr.second);
+      tot += t;
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+    if (s < n) {
+      if (ms) ms[s] = tot;
+      if (counts) counts[s] = (int64_t)g_sites[s].ev.size();
+    }
+    g_sites[s].ev.clear();
+  }
+  return VB_OK;
+}
+
+int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream) {
+  if (!out || blocks < 1 || threads < 32 || iters < 1) return fail(VB_ERR_ARG, "bad probe arguments");
+  VB_CHECK(vb::launch_fp64_probe(out, blocks, threads, iters, (cudaStream_t)stream), "fp64 probe");
+  return VB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,361 @@
+// Layer-parallel assembly kernels of the Ros2 step: chemistry RHS (mass-action
+// rates gathered per species), analytic Jacobian (gathered per destination
+// entry), eddy + molecular diffusion and boundary fluxes, fused into
+//   * the stage-1 kernel: rhs(y) and the LHS blocks c0*I - J - diag(diff)
+//     (reference jax_step.py:263-298, chem.py:83-214), and
+//   * the stage-2 kernel: rhs(yk2) - 2/(r dt) k1 (jax_step.py:303-310).
+// One CTA per (layer, atmosphere). Compiled with --fmad=false: the gathers sum
+// in the segment_sum order of the reference, so the RHS and the Jacobian are
+// bit-identical to the reference's.
+#include <cuda_runtime.h>
+
+#include "vb_common.cuh"
+#include "vb_launch.cuh"
+#include "vb_layer.cuh"
+
+namespace vb {
+
+constexpr int LAYER_THREADS = 256;
+
+struct LayerSmem {
+  double* y3;      // [3][ni+1]: layers j-1, j, j+1 (padding slot = 1.0)
+  double* rate;    // [nr+1]
+  double* drate;   // [(nr+1)*T]
+  double* diff;    // [ni]
+  double* diagd;   // [ni]
+  double* scal;    // [8]: ysum(j-1), ysum(j), ysum(j+1), A_e, B_e, C_e
+};
+
+__host__ __device__ inline size_t layer_smem_bytes(int ni, int nr, int T, bool jac) {
+  size_t d = 3 * (size_t)(ni + 1) + (nr + 1) + (jac ? (size_t)(nr + 1) * T : 0) + 2 * (size_t)ni + 8;
+  return d * sizeof(double);
+}
+
+__device__ inline LayerSmem carve(double* s, int ni, int nr, int T, bool jac) {
+  LayerSmem L;
+  L.y3 = s; s += 3 * (ni + 1);
+  L.rate = s; s += nr + 1;
+  L.drate = s; s += jac ? (nr + 1) * T : 0;
+  L.diff = s; s += ni;
+  L.diagd = s; s += ni;
+  L.scal = s;
+  return L;
+}
+
+// rate[r] = k[r] * prod_s y^st (* M) for every reaction slot of one layer
+// (chem.py:92-99); with jac, also drate[r][s] (chem.py:156-182).
+__device__ inline void layer_rates(const NetDev& net, const double* yrow, const double* kcol,
+                                   int64_t kstride, double M, double* rate, double* drate, bool jac) {
+  const int T = net.T;
+  for (int r = threadIdx.x; r <= net.nr; r += blockDim.x) {
+    double f[8];
+    double yr[8];
+    double st[8];
+    for (int s = 0; s < T; ++s) {
+      int idx = net.r_idx[r * T + s];
+      st[s] = net.r_st[r * T + s];
+      yr[s] = yrow[idx];
+      f[s] = st[s] > 0.0 ? pow_st(yr[s], st[s]) : 1.0;
+    }
+    double prod = f[0];
+    for (int s = 1; s < T; ++s) prod = prod * f[s];
+    double kr = kcol[(int64_t)r * kstride];
+    double rt = kr * prod;
+    bool three = net.three[r] != 0;
+    if (three) rt = rt * M;
+    rate[r] = rt;
+    if (jac) {
+      for (int s = 0; s < T; ++s) {
+        double lo = (s == 0) ? 1.0 : f[0];
+        for (int t = 1; t < T; ++t) lo = lo * ((t == s) ? 1.0 : f[t]);
+        double pm1 = st[s] > 0.0 ? pow_st(yr[s], st[s] - 1.0) : 0.0;
+        double d = st[s] * pm1;
+        d = d * lo;
+        d = d * kr;
+        if (three) d = d * M;
+        drate[r * T + s] = d;
+      }
+    }
+  }
+}
+
+// dy_i/dt = prod_i - loss_i, each a sequential gather in segment_sum order.
+__device__ __forceinline__ double species_rhs(const NetDev& net, const double* rate, int i) {
+  const int T = net.T;
+  double loss = 0.0, prod = 0.0;
+  for (int e = net.loss_ptr[i]; e < net.loss_ptr[i + 1]; ++e) {
+    int rs = net.loss_ent[e];
+    loss = loss + net.r_st[rs] * rate[rs / T];
+  }
+  for (int e = net.prod_ptr[i]; e < net.prod_ptr[i + 1]; ++e) {
+    int rs = net.prod_ent[e];
+    prod = prod + net.p_st[rs] * rate[rs / T];
+  }
+  return prod - loss;
+}
+
+// J[row][col] gathered from the flat contributions (chem.py:183-208).
+__device__ __forceinline__ double jac_entry(const NetDev& net, const double* drate, int d) {
+  const int T = net.T;
+  const int T2 = 2 * T;
+  double J = 0.0;
+  for (int e = net.jac_ptr[d]; e < net.jac_ptr[d + 1]; ++e) {
+    int fe = net.jac_ent[e];
+    int s = fe % T;
+    int ro = fe / T;
+    int o = ro % T2;
+    int r = ro / T2;
+    double coef = (o < T) ? -net.r_st[r * T + o] : net.p_st[r * T + (o - T)];
+    J = J + coef * drate[r * T + s];
+  }
+  return J;
+}
+
+// Loads state rows j-1..j+1 (stage 2: yk2 = y + k1/r) and their gas sums.
+__device__ inline void load_rows(const double* y, const double* k1, const double* gas, int nz, int ni,
+                                 int j, double rinv_r, bool stage2, LayerSmem& L) {
+  for (int t = threadIdx.x; t < 3 * (ni + 1); t += blockDim.x) {
+    int w = t / (ni + 1), i = t % (ni + 1);
+    int jj = j - 1 + w;
+    double v = 1.0;
+    if (i < ni) {
+      if (jj >= 0 && jj < nz) {
+        v = y[(int64_t)jj * ni + i];
+        if (stage2) v = v + k1[(int64_t)jj * ni + i] / rinv_r;
+      } else {
+        v = 0.0;
+      }
+    }
+    L.y3[t] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    int w = threadIdx.x;
+    int jj = j - 1 + w;
+    double s = 0.0;
+    if (jj >= 0 && jj < nz) {
+      double tmp[VB_MAX_NI];
+      for (int i = 0; i < ni; ++i) tmp[i] = gas[i] != 0.0 ? L.y3[w * (ni + 1) + i] : 0.0;
+      s = pairwise_sum(tmp, ni);
+    }
+    L.scal[w] = s;
+  }
+  __syncthreads();
+}
+
+// diff[i] (with BC fluxes) and the diagonal diffusion term diag_d[i] of row j;
+// also the sup/sub coefficients of row j when requested.
+__device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, int flags, LayerSmem& L,
+                                       double* sup_out, double* sub_out, bool want_diag) {
+  double ysm = L.scal[0], ys0 = L.scal[1], ysp = L.scal[2];
+  __shared__ double eddy[3];
+  if (threadIdx.x == 0) {
+    double A, B, C;
+    eddy_row(a, nz, j, ysm, ys0, ysp, A, B, C);
+    eddy[0] = A; eddy[1] = B; eddy[2] = C;
+  }
+  __syncthreads();
+  double use_vm = (flags & VB_USE_VM_MOL) ? 1.0 : 0.0;
+  double use_set = (flags & VB_USE_SETTLING) ? 1.0 : 0.0;
+  const double* y0 = L.y3 + (ni + 1);
+  const double* ym = L.y3;
+  const double* yp = L.y3 + 2 * (ni + 1);
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    double Am, Bm, Cm;
+    mol_row(a, nz, ni, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
+    double At = eddy[0] + Am;
+    double Bt = eddy[1] + Bm;
+    double Ct = eddy[2] + Cm;
+    double d;
+    if (j == 0) {
+      d = At * y0[i] + Bt * yp[i];
+    } else if (j == nz - 1) {
+      d = At * y0[i] + Ct * ym[i];
+    } else {
+      d = At * y0[i] + Bt * yp[i] + Ct * ym[i];
+    }
+    if (j == nz - 1) {
+      d = d + ((flags & VB_USE_TOPFLUX) ? a.top[i] / a.dzi[nz - 2] : 0.0);
+    }
+    if (j == 0) {
+      d = d + ((flags & VB_USE_BOTFLUX) ? (a.bot[i] - y0[i] * a.vdep[i]) / a.dzi[0] : 0.0);
+    }
+    L.diff[i] = d;
+    if (want_diag) {
+      double dd = At;
+      if (j == 0) dd = dd + ((flags & VB_USE_BOTFLUX) ? -a.vdep[i] / a.dzi[0] : 0.0);
+      L.diagd[i] = dd;
+    }
+    if (sup_out && j < nz - 1) sup_out[i] = Bt;
+    if (sub_out && j > 0) sub_out[i] = Ct;
+  }
+}
+
+// Stage-1 assembly: rmod[j] = rhs(y), inv[j] = c0*I - J - diag(diag_d),
+// supn[j] = -sup_d, subn[j-1] = -sub_d, with fix_mask (jax_step.py:263-298).
+__global__ void __launch_bounds__(LAYER_THREADS)
+stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
+              const double* __restrict__ dt, const double* __restrict__ atm, int flags,
+              const uint8_t* __restrict__ fix_mask, double* __restrict__ ws) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.y, j = blockIdx.x;
+  Geo g = geo_of(B, b);
+  if (j >= g.nz) return;
+  const int ni = B.ni, nz = g.nz;
+  LayerSmem L = carve(smem, ni, B.nr, net.T, true);
+  AtmRef a = atm_ref(atm + g.atm, nz, ni);
+  WsView w = ws_view(ws, g, ni, B.ld);
+  const double* yb = y + g.z0 * ni;
+  const uint8_t* fm = fix_mask ? fix_mask + g.z0 * ni + (int64_t)j * ni : nullptr;
+  const double r = ros2_r();
+  const double c0 = 1.0 / (r * dt[b]);
+
+  load_rows(yb, nullptr, a.gas, nz, ni, j, r, false, L);
+  layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
+  __shared__ double supb[VB_MAX_NI], subb[VB_MAX_NI];
+  layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);
+  __syncthreads();
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    double v = species_rhs(net, L.rate, i) + L.diff[i];
+    bool fixed = fm && fm[i];
+    if (fixed) v = 0.0;
+    w.rmod[(int64_t)j * ni + i] = v;
+    if (j < nz - 1) {
+      double s = -supb[i];
+      if (fixed) s = 0.0;
+      w.supn[(int64_t)j * ni + i] = s;
+    }
+    if (j > 0) {
+      double s = -subb[i];
+      if (fixed) s = 0.0;
+      w.subn[(int64_t)(j - 1) * ni + i] = s;
+    }
+  }
+  double* blk = w.inv + (int64_t)j * ni * B.ld;
+  for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) {
+    int row = d / ni, col = d - row * ni;
+    double J = jac_entry(net, L.drate, d);
+    double v = (row == col ? c0 : 0.0) - J;
+    if (row == col) v = v + (-L.diagd[row]);
+    if (fm && fm[row]) v = (row == col) ? c0 : 0.0;
+    blk[(int64_t)row * B.ld + col] = v;
+  }
+}
+
+// Stage-2 right-hand side: rmod[j] = rhs(yk2) - 2/(r dt) k1[j] with
+// yk2 = y + k1/r (jax_step.py:303-310).
+__global__ void __launch_bounds__(LAYER_THREADS)
+stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
+              const double* __restrict__ dt, const double* __restrict__ atm, int flags,
+              const uint8_t* __restrict__ fix_mask, double* __restrict__ ws) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.y, j = blockIdx.x;
+  Geo g = geo_of(B, b);
+  if (j >= g.nz) return;
+  const int ni = B.ni, nz = g.nz;
+  LayerSmem L = carve(smem, ni, B.nr, net.T, false);
+  AtmRef a = atm_ref(atm + g.atm, nz, ni);
+  WsView w = ws_view(ws, g, ni, B.ld);
+  const double* yb = y + g.z0 * ni;
+  const uint8_t* fm = fix_mask ? fix_mask + g.z0 * ni + (int64_t)j * ni : nullptr;
+  const double r = ros2_r();
+  const double dtb = dt[b];
+
+  load_rows(yb, w.k1, a.gas, nz, ni, j, r, true, L);
+  layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
+  layer_diffusion(a, nz, ni, j, flags, L, nullptr, nullptr, false);
+  __syncthreads();
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    double v = species_rhs(net, L.rate, i) + L.diff[i];
+    if (fm && fm[i]) v = 0.0;
+    double k1v = w.k1[(int64_t)j * ni + i];
+    w.rmod[(int64_t)j * ni + i] = v - (2.0 / (r * dtb)) * k1v;
+  }
+}
+
+// Standalone chemistry: dydt (and optionally the Jacobian) of a uniform batch.
+__global__ void __launch_bounds__(LAYER_THREADS)
+chem_kernel(NetDev net, int nz, const double* __restrict__ y, const double* __restrict__ M,
+            const double* __restrict__ k, double* __restrict__ dydt, double* __restrict__ jac) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.y, j = blockIdx.x;
+  const int ni = net.ni;
+  bool want_jac = jac != nullptr;
+  LayerSmem L = carve(smem, ni, net.nr, net.T, want_jac);
+  const double* yrow = y + ((int64_t)b * nz + j) * ni;
+  for (int i = threadIdx.x; i <= ni; i += blockDim.x) L.y3[i] = i < ni ? yrow[i] : 1.0;
+  __syncthreads();
+  layer_rates(net, L.y3, k + (int64_t)b * (net.nr + 1) * nz + j, nz, M[(int64_t)b * nz + j], L.rate,
+              L.drate, want_jac);
+  __syncthreads();
+  if (dydt)
+    for (int i = threadIdx.x; i < ni; i += blockDim.x)
+      dydt[((int64_t)b * nz + j) * ni + i] = species_rhs(net, L.rate, i);
+  if (want_jac) {
+    double* out = jac + ((int64_t)b * nz + j) * ni * ni;
+    for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) out[d] = jac_entry(net, L.drate, d);
+  }
+}
+
+// Standalone diffusion of a uniform batch (jax_step.py:67-246).
+__global__ void __launch_bounds__(LAYER_THREADS)
+diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __restrict__ atm,
+                 int flags, double* __restrict__ diff, double* __restrict__ diag_d,
+                 double* __restrict__ sup_d, double* __restrict__ sub_d) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.y, j = blockIdx.x;
+  LayerSmem L = carve(smem, ni, 0, 1, false);
+  AtmRef a = atm_ref(atm + (int64_t)b * VB_ATM_DOUBLES(nz, ni), nz, ni);
+  const double* yb = y + (int64_t)b * nz * ni;
+  load_rows(yb, nullptr, a.gas, nz, ni, j, 1.0, false, L);
+  __syncthreads();
+  double* supo = sup_d ? sup_d + ((int64_t)b * (nz - 1) + j) * ni : nullptr;
+  double* subo = sub_d ? sub_d + ((int64_t)b * (nz - 1) + (j - 1)) * ni : nullptr;
+  layer_diffusion(a, nz, ni, j, flags, L, supo, subo, true);
+  __syncthreads();
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    if (diff) diff[((int64_t)b * nz + j) * ni + i] = L.diff[i];
+    if (diag_d) diag_d[((int64_t)b * nz + j) * ni + i] = L.diagd[i];
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, const double* k,
+                          const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
+                          cudaStream_t st) {
+  size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, true);
+  cudaFuncSetAttribute(stage1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid(B.nz, B.count);
+  stage1_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage2(const NetDev& net, const Batch& B, const double* y, const double* k,
+                          const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
+                          cudaStream_t st) {
+  size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, false);
+  cudaFuncSetAttribute(stage2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid(B.nz, B.count);
+  stage2_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chem(const NetDev& net, int batch, int nz, const double* y, const double* M,
+                        const double* k, double* dydt, double* jac, cudaStream_t st) {
+  size_t sm = layer_smem_bytes(net.ni, net.nr, net.T, jac != nullptr);
+  cudaFuncSetAttribute(chem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid(nz, batch);
+  chem_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, nz, y, M, k, dydt, jac);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int flags,
+                             double* diff, double* diag_d, double* sup_d, double* sub_d,
+                             cudaStream_t st) {
+  size_t sm = layer_smem_bytes(ni, 0, 1, false);
+  dim3 grid(nz, batch);
+  diffusion_kernel<<<grid, LAYER_THREADS, sm, st>>>(nz, ni, y, atm, flags, diff, diag_d, sup_d, sub_d);
+  return cudaGetLastError();
+}
+
+}  // namespace vb

@@ -1,0 +1,36 @@
+// Host-side launchers shared by the C-ABI translation unit and the kernel units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "vb_common.cuh"
+
+namespace vb {
+
+enum SweepMode { SWEEP_FWD = 0, SWEEP_BACK = 1, SWEEP_BACK_FINAL = 2 };
+
+struct SweepArgs {
+  int mode;              // SweepMode
+  int transposed;        // solve with A^T (adjoint)
+  double* user;          // uniform [B][nz][ni] vector (standalone solves), or nullptr (workspace)
+  const double* y;       // SWEEP_BACK_FINAL: state y
+  double* sol;           // SWEEP_BACK_FINAL outputs
+  double* delta;
+  int32_t* status;
+};
+
+cudaError_t launch_stage1(const NetDev&, const Batch&, const double* y, const double* k, const double* dt,
+                          const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t);
+cudaError_t launch_stage2(const NetDev&, const Batch&, const double* y, const double* k, const double* dt,
+                          const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t);
+cudaError_t launch_chem(const NetDev&, int batch, int nz, const double* y, const double* M, const double* k,
+                        double* dydt, double* jac, cudaStream_t);
+cudaError_t launch_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int flags,
+                             double* diff, double* diag_d, double* sup_d, double* sub_d, cudaStream_t);
+cudaError_t launch_factor(const Batch&, double* ws, int32_t* status, int with_rhs, cudaStream_t);
+cudaError_t launch_sweep(const Batch&, double* ws, const SweepArgs&, cudaStream_t);
+cudaError_t launch_pack_blocks(const Batch&, const double* diag, const double* sup_d, const double* sub_d,
+                               double* ws, cudaStream_t);
+
+cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
+
+}  // namespace vb

@@ -1,0 +1,179 @@
+"""The Ros2 step on the GPU (reference `jax_step.py`).
+
+``jax_ros2_step(y, k_arr, dt, atm, net, fix_mask=None) -> (sol, delta_arr)``
+keeps the reference signature and semantics (`jax_step.py:249-315`): y and
+the outputs are ``[nz, ni]`` (or ``[B, nz, ni]`` for a batch, the reference's
+vmap), ``k_arr`` is ``[nr+1, nz]``, ``dt`` a scalar (or ``[B]``), ``atm`` an
+``AtmStatic``. Everything runs in the CUDA kernels of ``libvulcan_b200.so``;
+``Ros2Step`` keeps the packed atmosphere, workspace and status buffers across
+calls for loops that step the same atmospheres repeatedly.
+"""
+from __future__ import annotations
+
+from typing import NamedTuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .chem import NetworkArrays, as_device
+
+
+class AtmStatic(NamedTuple):
+    """Atmosphere held constant within a step (reference `jax_step.py:26-49`).
+
+    Arrays may be NumPy or torch; with a leading batch axis all atmospheres
+    of a batch share the four flags.
+    """
+    Kzz: object        # (nz-1,)
+    Dzz: object        # (nz-1, ni)
+    dzi: object        # (nz-1,)
+    vz: object         # (nz-1,)
+    Hpi: object        # (nz-1,)
+    Ti: object         # (nz-1,)
+    Tco: object        # (nz,)
+    g: object          # (nz,)
+    ms: object         # (ni,)
+    alpha: object      # (ni,)
+    M: object          # (nz,)
+    vm: object         # (nz, ni)
+    vs: object         # (nz-1, ni)
+    top_flux: object   # (ni,)
+    bot_flux: object   # (ni,)
+    bot_vdep: object   # (ni,)
+    gas_indx_mask: object  # (ni,) bool
+    use_vm_mol: bool
+    use_settling: bool
+    use_topflux: bool
+    use_botflux: bool
+
+
+def atm_from_dict(d) -> AtmStatic:
+    return AtmStatic(**{k: d[k] for k in AtmStatic._fields})
+
+
+def atm_flags(atm: AtmStatic) -> int:
+    return ((_lib.VB_USE_VM_MOL if bool(atm.use_vm_mol) else 0)
+            | (_lib.VB_USE_SETTLING if bool(atm.use_settling) else 0)
+            | (_lib.VB_USE_TOPFLUX if bool(atm.use_topflux) else 0)
+            | (_lib.VB_USE_BOTFLUX if bool(atm.use_botflux) else 0))
+
+
+def pack_atm(atm: AtmStatic) -> torch.Tensor:
+    """Pack an AtmStatic (optionally batched) into the device blob layout of
+    ``VB_ATM_DOUBLES`` (include/vulcan_b200.h). Returns ``[B, doubles]``."""
+    Tco = as_device(atm.Tco)
+    batched = Tco.dim() == 2
+    Tco = Tco if batched else Tco.unsqueeze(0)
+    B, nz = Tco.shape
+
+    def f(x, shape):
+        t = as_device(x)
+        return t.reshape((B,) + shape) if batched else t.reshape((1,) + shape)
+
+    ms = f(atm.ms, (-1,))
+    ni = ms.shape[1]
+
+    def pad_z(t):                                  # [B, nz-1, ...] -> [B, nz, ...]
+        z = torch.zeros((B, 1) + tuple(t.shape[2:]), dtype=t.dtype, device=t.device)
+        return torch.cat([t, z], dim=1)
+
+    parts = [
+        pad_z(f(atm.Kzz, (nz - 1,))), pad_z(f(atm.dzi, (nz - 1,))), pad_z(f(atm.vz, (nz - 1,))),
+        pad_z(f(atm.Hpi, (nz - 1,))), pad_z(f(atm.Ti, (nz - 1,))), Tco, f(atm.g, (nz,)), f(atm.M, (nz,)),
+        pad_z(f(atm.Dzz, (nz - 1, ni))), f(atm.vm, (nz, ni)), pad_z(f(atm.vs, (nz - 1, ni))),
+        ms, f(atm.alpha, (ni,)), f(atm.top_flux, (ni,)), f(atm.bot_flux, (ni,)), f(atm.bot_vdep, (ni,)),
+        f(np.asarray(atm.gas_indx_mask, dtype=np.float64) if not isinstance(atm.gas_indx_mask, torch.Tensor)
+          else atm.gas_indx_mask.to(torch.float64), (ni,)),
+    ]
+    blob = torch.cat([p.reshape(B, -1) for p in parts], dim=1).contiguous()
+    assert blob.shape[1] == nz * (8 + 3 * ni) + 6 * ni
+    return blob
+
+
+class Ros2Step:
+    """Reusable batched Ros2 step for ``batch`` atmospheres of one network.
+
+    Holds the packed atmosphere, the solver workspace and the status words,
+    so repeated calls allocate nothing.
+    """
+
+    def __init__(self, net: NetworkArrays, atm: AtmStatic, batch: int | None = None):
+        self.net = net
+        self.blob = pack_atm(atm)
+        self.flags = atm_flags(atm)
+        self.batch = self.blob.shape[0] if batch is None else int(batch)
+        if self.blob.shape[0] != self.batch:
+            if self.blob.shape[0] != 1:
+                raise ValueError("atm batch does not match")
+            self.blob = self.blob.expand(self.batch, -1).contiguous()
+        ni = net.ni
+        self.nz = (self.blob.shape[1] - 6 * ni) // (8 + 3 * ni)
+        L = _lib.lib()
+        self.ws_bytes = int(L.vb_ros2_workspace_bytes(self.batch, self.nz, ni, None))
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
+        self.status = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
+
+    def __call__(self, y, k, dt, fix_mask=None, out=None, stream=None):
+        """Returns (sol, delta, status) as device tensors of the batch shape."""
+        B, nz, ni = self.batch, self.nz, self.net.ni
+        y = as_device(y).reshape(B, nz, ni)
+        k = as_device(k).reshape(B, self.net.nr + 1, nz)
+        dt = as_device(dt).reshape(-1)
+        if dt.numel() == 1 and B > 1:
+            dt = dt.expand(B).contiguous()
+        fm = None if fix_mask is None else as_device(fix_mask, torch.uint8).reshape(B, nz, ni)
+        if out is None:
+            sol = torch.empty_like(y)
+            delta = torch.empty_like(y)
+        else:
+            sol, delta = out
+        _lib.check(_lib.lib().vb_ros2_step(
+            self.net.handle, B, nz, None, _lib.ptr(y), _lib.ptr(k), _lib.ptr(dt), _lib.ptr(self.blob),
+            self.flags, _lib.ptr(fm), _lib.ptr(sol), _lib.ptr(delta), _lib.ptr(self.status),
+            _lib.ptr(self.ws), self.ws_bytes, _lib.stream_handle(stream)), "vb_ros2_step")
+        return sol, delta, self.status
+
+
+def jax_ros2_step(y, k_arr, dt, atm: AtmStatic, net: NetworkArrays, fix_mask=None):
+    """One 2nd-order Rosenbrock step -> (sol, delta_arr) (reference `jax_step.py:249-315`).
+
+    Accepts a single atmosphere (``y [nz, ni]``) or a batch (``y [B, nz, ni]``,
+    ``k_arr [B, nr+1, nz]``, ``dt`` scalar or ``[B]``, batched ``atm``).
+    """
+    yt = as_device(y)
+    single = yt.dim() == 2
+    B = 1 if single else yt.shape[0]
+    step = Ros2Step(net, atm, batch=B)
+    sol, delta, _ = step(yt, k_arr, dt, fix_mask=fix_mask)
+    if single:
+        return sol[0], delta[0]
+    return sol, delta
+
+
+def diffusion(y, atm: AtmStatic, stream=None):
+    """Eddy + molecular diffusion of a state (reference `jax_step.py:67-246`).
+
+    Returns (diff [.., nz, ni] with boundary fluxes, diag_d [.., nz, ni] with the
+    deposition term, sup_d [.., nz-1, ni], sub_d [.., nz-1, ni]) where
+    ``diag_d``/``sup_d``/``sub_d`` are ``A_eddy+A_mol`` (+ bot_vdep term),
+    ``B[:-1]`` and ``C[1:]`` of `jax_step.py:275-283`.
+    """
+    yt = as_device(y)
+    single = yt.dim() == 2
+    if single:
+        yt = yt.unsqueeze(0)
+    B, nz, ni = yt.shape
+    blob = pack_atm(atm)
+    if blob.shape[0] != B:
+        blob = blob.expand(B, -1).contiguous()
+    diff = torch.empty_like(yt)
+    diag_d = torch.empty_like(yt)
+    sup = torch.empty((B, nz - 1, ni), dtype=torch.float64, device=yt.device)
+    sub = torch.empty_like(sup)
+    _lib.check(_lib.lib().vb_diffusion(B, nz, ni, _lib.ptr(yt), _lib.ptr(blob), atm_flags(atm),
+                                       _lib.ptr(diff), _lib.ptr(diag_d), _lib.ptr(sup), _lib.ptr(sub),
+                                       _lib.stream_handle(stream)), "vb_diffusion")
+    if single:
+        return diff[0], diag_d[0], sup[0], sub[0]
+    return diff, diag_d, sup, sub
