@@ -17,42 +17,62 @@
 
 namespace vb {
 
-template <int NP, int NW>
-struct GJ {
+template <int NP, int NW, int PW>
+struct LUK {
   static constexpr int RPW = NP / NW;     // rows per warp
   static constexpr int CPL = NP / 32;     // columns per lane
-  static constexpr int THREADS = NW * 32;
-  static constexpr int SLD = NP + 1;      // smem row stride (doubles)
+  static constexpr int PRL = NP / 32;     // panel rows per lane of the panel warp
+  static constexpr int SLD = NP + 1;      // smem row stride of S (doubles)
+  static constexpr int PLD = PW + 1;      // smem row stride of a panel buffer
+  static constexpr int PBUF = (NP * PLD > RPW * NP) ? NP * PLD : RPW * NP;
   static size_t smem_bytes() {
-    return sizeof(double) * ((size_t)NP * SLD + 2 * NP + 2 * NW) + sizeof(int) * 2 * NP;
+    size_t d = (size_t)NP * SLD          // S: previous inverse, LU factors, new inverse
+               + 2 * (size_t)PBUF        // panel buffers / triangular-solve row buffers
+               + (size_t)PW * NP         // V: pivot rows of the current panel
+               + 2 * (size_t)NP          // vec, rdiag
+               + PW;                     // pivot row broadcast of the panel warp
+    return d * sizeof(double) + sizeof(int) * 2 * NP;
   }
 };
 
-struct Cand {
-  double v;
-  int row;
-};
-
-__device__ __forceinline__ bool cand_better(double v, int row, double bv, int brow) {
-  return v > bv || (v == bv && row < brow);
+// Pivot key of a candidate: |v| as an order-preserving 64-bit pattern (NaN -> 0).
+__device__ __forceinline__ unsigned long long pivot_key(double v) {
+  double a = fabs(v);
+  return (a >= 0.0) ? (unsigned long long)__double_as_longlong(a) : 0ull;
 }
 
 // Factor all layers of one atmosphere. On entry inv[j] holds D_j (row stride
 // ld); on exit inv[j] holds A'_j^{-1}. With rhs != nullptr the first sweep of
 // the right-hand side rhs[nz][ni] is done in place (solver.py:73-88).
-template <int NP, int NW>
+//
+// Each diagonal block is inverted as the reference does (solver.py:46-48):
+// LU with partial pivoting (lu_factor), then the inverse by forward and back
+// substitution on the identity (lu_solve(LU, I)).
+//  * LU: blocked right-looking elimination with implicit row pivoting on a
+//    register-resident tile (warp w owns rows w*RPW.., lane l columns l+32c).
+//    Warp 0 factors each PW-column panel (argmax over unpivoted rows by three
+//    redux.sync reductions, pivot row broadcast through shared memory);
+//    every warp then forms U[K, C] = L_KK^{-1} A[P, C] for its columns and
+//    applies the rank-PW update A[R, C] -= L[R, K] U[K, C] to unpivoted rows.
+//  * The factors are stored in pivot order in shared memory; the tile is
+//    re-used for Y = L^{-1} P and X = U^{-1} Y, one warp's RPW rows per
+//    panel (solved thread-locally, then broadcast and applied by the other
+//    warps), so X = A'^{-1} ends up in natural row order.
+template <int NP, int NW, int PW>
 __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ inv,
                                   const double* __restrict__ supn, const double* __restrict__ subn,
                                   double* __restrict__ rhs, int32_t* status, char* smem_raw) {
-  using G = GJ<NP, NW>;
-  constexpr int RPW = G::RPW, CPL = G::CPL, SLD = G::SLD;
-  double* S = reinterpret_cast<double*>(smem_raw);          // [NP][SLD] previous inverse
-  double* prow = S + NP * SLD;                              // [NP] pivot row
-  double* vec = prow + NP;                                  // [NP] current rhs layer
-  double* cval = vec + NP;                                  // [NW] candidates
-  int* crow = reinterpret_cast<int*>(cval + NW);            // [NW]
-  int* pivs = crow + NW;                                    // [NP] pivot row of step k
-  int* qinv = pivs + NP;                                    // [NP] step of row i
+  using G = LUK<NP, NW, PW>;
+  constexpr int RPW = G::RPW, CPL = G::CPL, PRL = G::PRL, SLD = G::SLD, PLD = G::PLD;
+  double* S = reinterpret_cast<double*>(smem_raw);          // [NP][SLD]
+  double* Pn0 = S + NP * SLD;                               // [PBUF]
+  double* Pn1 = Pn0 + G::PBUF;                              // [PBUF]
+  double* V = Pn1 + G::PBUF;                                // [PW][NP]
+  double* vec = V + PW * NP;                                // [NP]
+  double* rdiag = vec + NP;                                 // [NP]
+  double* prow_s = rdiag + NP;                              // [PW]
+  int* pivs = reinterpret_cast<int*>(prow_s + PW);          // [NP] pivot row of step k
+  int* qinv = pivs + NP;                                    // [NP] step of row i (-1: not yet)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned FULL = 0xffffffffu;
   int st_local = 0;
@@ -60,11 +80,13 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   if (rhs) {
     for (int i = threadIdx.x; i < NP; i += blockDim.x) vec[i] = i < n ? rhs[i] : 0.0;
   }
+  const int npan = (n + PW - 1) / PW;
 
   double a[RPW][CPL];
   for (int j = 0; j < nz; ++j) {
     const double* D = inv + (int64_t)j * n * ld;
-    // ---- load D_j and apply the Hadamard Schur update from Inv_{j-1}
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) qinv[i] = -1;
+    // ---- load D_j and apply the Hadamard Schur update from Inv_{j-1} (solver.py:47)
 #pragma unroll
     for (int r = 0; r < RPW; ++r) {
       int i = warp * RPW + r;
@@ -82,85 +104,254 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         a[r][c] = v;
       }
     }
-    unsigned used = 0;
-    // ---- Gauss-Jordan with partial pivoting
-    for (int k = 0; k < n; ++k) {
-      const int kl = k & 31, kc = k >> 5;
-      double colk[RPW];
+    unsigned usedw = 0;     // warp 0: rows lane + 32*r already pivoted
+    // ================================================================ LU
+    for (int pb = 0; pb < npan; ++pb) {
+      const int k0 = pb * PW;
+      const int kw = min(PW, n - k0);
+      double* Pn = (pb & 1) ? Pn1 : Pn0;
+      // (a) owners of the panel columns stage them
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) {
-        double x = 0.0;
+      for (int c = 0; c < CPL; ++c) {
+        int col = lane + 32 * c;
+        if (col >= k0 && col < k0 + PW) {
 #pragma unroll
-        for (int c = 0; c < CPL; ++c)
-          if (c == kc) x = a[r][c];
-        colk[r] = __shfl_sync(FULL, x, kl);
-      }
-      // local candidate of this warp
-      double bv = -1.0;
-      int br = 0x7fffffff;
-#pragma unroll
-      for (int r = 0; r < RPW; ++r) {
-        int i = warp * RPW + r;
-        if (i < n && !((used >> r) & 1u)) {
-          double v = fabs(colk[r]);
-          if (!(v >= 0.0)) v = -0.5;  // NaN ranks below any number
-          if (cand_better(v, i, bv, br)) { bv = v; br = i; }
+          for (int r = 0; r < RPW; ++r) Pn[(warp * RPW + r) * PLD + (col - k0)] = a[r][c];
         }
       }
-      if (lane == 0) { cval[warp] = bv; crow[warp] = br; }
       __syncthreads();
-      double gv = lane < NW ? cval[lane] : -1.0;
-      int gr = lane < NW ? crow[lane] : 0x7fffffff;
+      // (b) warp 0: unblocked LU of the panel over the unpivoted rows
+      if (warp == 0) {
+        double pv[PRL][PW];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        double ov = __shfl_xor_sync(FULL, gv, off);
-        int orow = __shfl_xor_sync(FULL, gr, off);
-        if (cand_better(ov, orow, gv, gr)) { gv = ov; gr = orow; }
-      }
-      const int p = gr;
-      const int pw = p / RPW, pr = p - pw * RPW;
-      if (warp == pw) {
+        for (int r = 0; r < PRL; ++r)
 #pragma unroll
-        for (int r = 0; r < RPW; ++r)
-          if (r == pr) {
+          for (int t = 0; t < PW; ++t) pv[r][t] = Pn[(lane + 32 * r) * PLD + t];
 #pragma unroll
-            for (int c = 0; c < CPL; ++c) prow[lane + 32 * c] = a[r][c];
+        for (int t = 0; t < PW; ++t) {
+          if (t < kw) {
+            unsigned long long bk = 0ull;
+            unsigned brow = 0xffffffffu;
+#pragma unroll
+            for (int r = 0; r < PRL; ++r) {
+              int i = lane + 32 * r;
+              if (i < n && !((usedw >> r) & 1u)) {
+                unsigned long long kk = pivot_key(pv[r][t]);
+                if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
+              }
+            }
+            unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+            unsigned m1 = __reduce_max_sync(FULL, hi);
+            unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
+            const int p = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
+            const int pl = p & 31, prr = p >> 5;
+            if (lane == pl) {
+#pragma unroll
+              for (int r = 0; r < PRL; ++r)
+                if (r == prr) {
+#pragma unroll
+                  for (int u = 0; u < PW; ++u) prow_s[u] = pv[r][u];
+                  usedw |= 1u << r;
+                }
+            }
+            __syncwarp();
+            double prow[PW];
+#pragma unroll
+            for (int u = 0; u < PW; ++u) prow[u] = prow_s[u];
+            const double piv = prow[t];
+            if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
+            const double rcp = 1.0 / piv;
+#pragma unroll
+            for (int r = 0; r < PRL; ++r) {
+              int i = lane + 32 * r;
+              if (i < n && !((usedw >> r) & 1u)) {
+                const double l = pv[r][t] * rcp;
+                pv[r][t] = l;
+#pragma unroll
+                for (int u = t + 1; u < PW; ++u) pv[r][u] = fma(-l, prow[u], pv[r][u]);
+              }
+            }
+            if (lane == 0) { pivs[k0 + t] = p; qinv[p] = k0 + t; }
+            __syncwarp();
           }
-        used |= 1u << pr;
-      }
-      if (threadIdx.x == 0) { pivs[k] = p; qinv[p] = k; }
-      __syncthreads();
-      const double piv = prow[k];
-      if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
-      const double ip = 1.0 / piv;
-      double pr_s[CPL];
+        }
 #pragma unroll
-      for (int c = 0; c < CPL; ++c) pr_s[c] = prow[lane + 32 * c] * ip;
+        for (int r = 0; r < PRL; ++r)
+#pragma unroll
+          for (int t = 0; t < PW; ++t) Pn[(lane + 32 * r) * PLD + t] = pv[r][t];
+      }
+      __syncthreads();
+      // (c) owners of the new pivot rows stage them: V[t] = A[p_t, :]
 #pragma unroll
       for (int r = 0; r < RPW; ++r) {
         int i = warp * RPW + r;
-        if (i == p) {
+        int q = qinv[i];
+        if (q >= k0 && q < k0 + kw) {
 #pragma unroll
-          for (int c = 0; c < CPL; ++c) a[r][c] = (lane + 32 * c == k) ? ip : pr_s[c];
-        } else {
-          const double f = colk[r];
+          for (int c = 0; c < CPL; ++c) V[(q - k0) * NP + lane + 32 * c] = a[r][c];
+        }
+      }
+      __syncthreads();
+      // (d) U[K, c] = L_KK^{-1} V[:, c]; pivot rows take U, unpivoted rows get
+      //     the rank-kw update, rows pivoted in earlier panels are final.
 #pragma unroll
-          for (int c = 0; c < CPL; ++c)
-            a[r][c] = (lane + 32 * c == k) ? -f * ip : a[r][c] - f * pr_s[c];
+      for (int c = 0; c < CPL; ++c) {
+        const int col = lane + 32 * c;
+        const bool right = col >= k0 + PW;
+        double u[PW];
+#pragma unroll
+        for (int t = 0; t < PW; ++t) {
+          double x = 0.0;
+          if (right && t < kw) {
+            x = V[t * NP + col];
+            const double* lrow = Pn + pivs[k0 + t] * PLD;
+#pragma unroll
+            for (int s2 = 0; s2 < t; ++s2) x = fma(-lrow[s2], u[s2], x);
+          }
+          u[t] = x;
+        }
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+          const int i = warp * RPW + r;
+          const int q = qinv[i];
+          if (col >= k0 && col < k0 + PW) {
+            a[r][c] = Pn[i * PLD + (col - k0)];
+          } else if (right) {
+            if (q >= k0 && q < k0 + kw) {
+              double x = 0.0;
+#pragma unroll
+              for (int t = 0; t < PW; ++t)
+                if (t == q - k0) x = u[t];
+              a[r][c] = x;
+            } else if (q < 0) {
+              double acc = a[r][c];
+#pragma unroll
+              for (int t = 0; t < PW; ++t)
+                if (t < kw) acc = fma(-Pn[i * PLD + t], u[t], acc);
+              a[r][c] = acc;
+            }
+          }
         }
       }
     }
-    // ---- store the un-permuted inverse: Inv[q_i][p_col] = W[i][col]
-    __syncthreads();  // all reads of S (Schur update) are done
+    // ---- factors to shared memory in pivot order (LAPACK layout), 1/U_kk
+    __syncthreads();
 #pragma unroll
     for (int r = 0; r < RPW; ++r) {
       int i = warp * RPW + r;
       if (i < n) {
         int qi = qinv[i];
 #pragma unroll
+        for (int c = 0; c < CPL; ++c) S[qi * SLD + lane + 32 * c] = a[r][c];
+      }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) rdiag[k] = 1.0 / S[k * SLD + k];
+    // ================================================================ Y = L^{-1} P
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+      const int k = warp * RPW + r;
+      const int pk = k < n ? pivs[k] : -1;
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) a[r][c] = (lane + 32 * c == pk) ? 1.0 : 0.0;
+    }
+    for (int w = 0; w < NW; ++w) {
+      const int k0 = w * RPW;
+      if (k0 >= n) break;
+      double* Yb = (w & 1) ? Pn1 : Pn0;
+      if (warp == w) {
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+          const int k = k0 + r;
+#pragma unroll
+          for (int s2 = 0; s2 < r; ++s2) {
+            const double l = k < n ? S[k * SLD + k0 + s2] : 0.0;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) a[r][c] = fma(-l, a[s2][c], a[r][c]);
+          }
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) Yb[r * NP + lane + 32 * c] = a[r][c];
+        }
+      }
+      __syncthreads();
+      if (warp > w) {
+        const int kw = min(RPW, n - k0);
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+          const int k = warp * RPW + r;
+          if (k < n) {
+#pragma unroll
+            for (int s2 = 0; s2 < RPW; ++s2) {
+              if (s2 < kw) {
+                const double l = S[k * SLD + k0 + s2];
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) a[r][c] = fma(-l, Yb[s2 * NP + lane + 32 * c], a[r][c]);
+              }
+            }
+          }
+        }
+      }
+    }
+    // ================================================================ X = U^{-1} Y
+    for (int w = NW - 1; w >= 0; --w) {
+      const int k0 = w * RPW;
+      if (k0 >= n) continue;
+      const int kw = min(RPW, n - k0);
+      double* Yb = (w & 1) ? Pn1 : Pn0;
+      __syncthreads();   // previous readers of this buffer are done
+      if (warp == w) {
+#pragma unroll
+        for (int r = RPW - 1; r >= 0; --r) {
+          const int k = k0 + r;
+          if (r < kw) {
+#pragma unroll
+            for (int s2 = r + 1; s2 < RPW; ++s2) {
+              if (s2 < kw) {
+                const double uu = S[k * SLD + k0 + s2];
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) a[r][c] = fma(-uu, a[s2][c], a[r][c]);
+              }
+            }
+            const double rd = rdiag[k];
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+              a[r][c] = a[r][c] * rd;
+              Yb[r * NP + lane + 32 * c] = a[r][c];
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (warp < w) {
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+          const int k = warp * RPW + r;
+          if (k < n) {
+#pragma unroll
+            for (int s2 = 0; s2 < RPW; ++s2) {
+              if (s2 < kw) {
+                const double uu = S[k * SLD + k0 + s2];
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) a[r][c] = fma(-uu, Yb[s2 * NP + lane + 32 * c], a[r][c]);
+              }
+            }
+          }
+        }
+      }
+    }
+    // ---- the inverse (natural order) to shared and global memory
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+      int i = warp * RPW + r;
+      if (i < n) {
+#pragma unroll
         for (int c = 0; c < CPL; ++c) {
           int col = lane + 32 * c;
-          if (col < n) S[qi * SLD + pivs[col]] = a[r][c];
+          if (col < n) {
+            if (!isfinite(a[r][c])) st_local |= VB_STATUS_NONFINITE;
+            S[i * SLD + col] = a[r][c];
+          }
         }
       }
     }
@@ -168,22 +359,21 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
     double* O = inv + (int64_t)j * n * ld;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
       int i = e / n, col = e - i * n;
-      double v = S[i * SLD + col];
-      if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
-      O[(int64_t)i * ld + col] = v;
+      O[(int64_t)i * ld + col] = S[i * SLD + col];
     }
     // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
     if (rhs && j + 1 < nz) {
+      double* u = Pn0;
       for (int i = warp; i < n; i += NW) {
         double s = 0.0;
         for (int m = lane; m < n; m += 32) s += S[i * SLD + m] * vec[m];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
-        if (lane == 0) prow[i] = s;
+        if (lane == 0) u[i] = s;
       }
       __syncthreads();
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double v = rhs[(int64_t)(j + 1) * n + i] - subn[(int64_t)j * n + i] * prow[i];
+        double v = rhs[(int64_t)(j + 1) * n + i] - subn[(int64_t)j * n + i] * u[i];
         rhs[(int64_t)(j + 1) * n + i] = v;
         vec[i] = v;
       }
@@ -193,15 +383,15 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   if (st_local) atomicOr(status, st_local);
 }
 
-template <int NP, int NW>
+template <int NP, int NW, int PW>
 __global__ void __launch_bounds__(NW * 32, 1)
 factor_kernel(Batch B, double* __restrict__ ws, int32_t* __restrict__ status, int with_rhs) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
-  factor_atmosphere<NP, NW>(g.nz, B.ni, B.ld, w.inv, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
-                            status + b, smem_raw);
+  factor_atmosphere<NP, NW, PW>(g.nz, B.ni, B.ld, w.inv, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
+                                status + b, smem_raw);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -331,22 +521,22 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, c
   return cudaGetLastError();
 }
 
-template <int NP, int NW>
+template <int NP, int NW, int PW>
 static cudaError_t launch_factor_t(const Batch& B, double* ws, int32_t* status, int with_rhs,
                                    cudaStream_t st) {
-  size_t sm = GJ<NP, NW>::smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm);
+  size_t sm = LUK<NP, NW, PW>::smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW, PW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  factor_kernel<NP, NW><<<B.count, NW * 32, sm, st>>>(B, ws, status, with_rhs);
+  factor_kernel<NP, NW, PW><<<B.count, NW * 32, sm, st>>>(B, ws, status, with_rhs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st) {
-  if (B.ni <= 32) return launch_factor_t<32, 8>(B, ws, status, with_rhs, st);
-  if (B.ni <= 64) return launch_factor_t<64, 16>(B, ws, status, with_rhs, st);
-  if (B.ni <= 96) return launch_factor_t<96, 16>(B, ws, status, with_rhs, st);
-  return launch_factor_t<128, 16>(B, ws, status, with_rhs, st);
+  if (B.ni <= 32) return launch_factor_t<32, 8, 8>(B, ws, status, with_rhs, st);
+  if (B.ni <= 64) return launch_factor_t<64, 16, 8>(B, ws, status, with_rhs, st);
+  if (B.ni <= 96) return launch_factor_t<96, 16, 8>(B, ws, status, with_rhs, st);
+  return launch_factor_t<128, 16, 4>(B, ws, status, with_rhs, st);
 }
 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {

@@ -306,7 +306,8 @@ def make_rates(seed, net: SyntheticNetwork, nz, lo=-40.0, hi=-8.0, n_ref=None):
     """Log-uniform rate constants ``k[nr+1, nz]`` with row 0 (unused) zero.
 
     With ``n_ref`` set, each reaction's draw is divided by
-    ``n_ref**(order-1)`` (order = summed reactant stoichiometry), so the
+    ``n_ref**(order-1)`` (order = summed reactant stoichiometry, plus one for a
+    three-body reaction whose rate is multiplied by M), so the
     pseudo-first-order rate ``k * n**(order-1)`` is log-uniform in
     ``[10**lo, 10**hi]`` whatever the molecularity: the "mild" chemistry used
     for well-conditioned parity cases.
@@ -315,7 +316,7 @@ def make_rates(seed, net: SyntheticNetwork, nz, lo=-40.0, hi=-8.0, n_ref=None):
     nr = net.tables.nr
     k = 10.0 ** rng.uniform(lo, hi, (nr + 1, nz))
     if n_ref is not None:
-        order = net.tables.reactant_stoich.sum(axis=1)
+        order = net.tables.reactant_stoich.sum(axis=1) + net.tables.is_three_body
         k = k / float(n_ref) ** np.maximum(order - 1.0, 0.0)[:, None]
     k[0] = 0.0
     k[net.tables.is_photo] = 0.0

@@ -401,3 +401,50 @@ def integrate_fixed_dt(y0, k, dt, n_steps, atm, net):
         deltas.append(np.max(d / np.maximum(np.abs(sol), 1e-30)))
         y = sol
     return y, np.array(deltas)
+
+
+def chem_rhs_abs(y, M, k, net):
+    """Sum of |terms| of each species' RHS gather (the scale of its rounding
+    error bound): sum over slots of |st * rate| for losses and productions."""
+    return np.abs(chem_rhs_terms(y, M, k, net))
+
+
+def chem_rhs_terms(y, M, k, net):
+    nz, ni = y.shape
+    T = net.reactant_idx.shape[1]
+    rate = np.abs(rates(y, M, k, net))
+    rate_rep = np.repeat(rate, T, axis=1)
+    acc = np.zeros((ni + 1, nz))
+    np.add.at(acc, net.reactant_idx.reshape(-1), (np.abs(net.reactant_stoich.reshape(-1))[None, :] * rate_rep).T)
+    np.add.at(acc, net.product_idx.reshape(-1), (np.abs(net.product_stoich.reshape(-1))[None, :] * rate_rep).T)
+    return acc[:ni].T
+
+
+def chem_jac_abs(y, M, k, net):
+    """Sum of |contributions| of each Jacobian entry (its rounding-error scale)."""
+    nz, ni = y.shape
+    T = net.reactant_idx.shape[1]
+    y_r, f = _factors(np.abs(y), net)
+    slots = np.arange(T)
+    cols = []
+    for j in range(T):
+        fe = np.where((slots == j)[None, None, :], 1.0, f)
+        p = fe[:, :, 0].copy()
+        for s in range(1, T):
+            p = p * fe[:, :, s]
+        cols.append(p)
+    leave_out = np.stack(cols, axis=2)
+    st = net.reactant_stoich[None]
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        pm1 = np.where(st > 0, y_r ** (st - 1.0), 0.0)
+    drate = np.abs(st * pm1 * leave_out * np.abs(k).T[:, :, None])
+    drate = np.where(net.is_three_body[None, :, None], drate * np.abs(M)[:, None, None], drate)
+    out_idx = np.concatenate([net.reactant_idx, net.product_idx], axis=1)
+    out_st = np.abs(np.concatenate([net.reactant_stoich, net.product_stoich], axis=1))
+    contrib = out_st[None, :, :, None] * drate[:, :, None, :]
+    row = np.broadcast_to(out_idx[:, :, None], contrib.shape[1:])
+    col = np.broadcast_to(net.reactant_idx[:, None, :], contrib.shape[1:])
+    keys = (row * (ni + 1) + col).reshape(-1)
+    J = np.zeros(((ni + 1) * (ni + 1), nz))
+    np.add.at(J, keys, contrib.reshape(nz, -1).T)
+    return J.T.reshape(nz, ni + 1, ni + 1)[:, :ni, :ni]
