@@ -103,6 +103,30 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   csr(loss, lp, le);
   csr(prod, pp, pe);
   csr(jac, jp, je);
+  std::vector<int32_t> lr(le.size()), pr(pe.size()), jidx(je.size());
+  std::vector<double> jcoef(je.size());
+  for (size_t e = 0; e < le.size(); ++e) lr[e] = le[e] / T;
+  for (size_t e = 0; e < pe.size(); ++e) pr[e] = pe[e] / T;
+  for (size_t e = 0; e < je.size(); ++e) {
+    int fe = je[e], s = fe % T, ro = fe / T, o = ro % (2 * T), r = ro / (2 * T);
+    jidx[e] = r * T + s;
+    jcoef[e] = o < T ? -r_st[(int64_t)r * T + o] : p_st[(int64_t)r * T + (o - T)];
+  }
+  // destination ranges per thread, balanced by entries (+1 per destination)
+  const int NT = vb::LAYER_THREADS;
+  std::vector<int32_t> split(NT + 1, ni * ni);
+  {
+    int64_t nd = (int64_t)ni * ni;
+    int64_t total = jp[nd] + nd;
+    int64_t target = (total + NT - 1) / NT, acc = 0;
+    int t = 0;
+    split[0] = 0;
+    for (int64_t d = 0; d < nd; ++d) {
+      acc += (jp[d + 1] - jp[d]) + 1;
+      if (acc >= target * (t + 1) && t + 1 < NT) split[++t] = (int32_t)(d + 1);
+    }
+    for (int k = t + 1; k <= NT; ++k) split[k] = (int32_t)nd;
+  }
   std::vector<int32_t> ri(R * T), pi(R * T);
   for (int e = 0; e < R * T; ++e) { ri[e] = (int32_t)r_idx[e]; pi[e] = (int32_t)p_idx[e]; }
 
@@ -112,9 +136,11 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
       {ri.data(), ri.size() * 4, 0}, {pi.data(), pi.size() * 4, 0},
       {r_st, (size_t)R * T * 8, 0},  {p_st, (size_t)R * T * 8, 0},
       {three, (size_t)R, 0},         {lp.data(), lp.size() * 4, 0},
-      {le.data(), le.size() * 4, 0}, {pp.data(), pp.size() * 4, 0},
-      {pe.data(), pe.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
-      {je.data(), je.size() * 4, 0}};
+      {le.data(), le.size() * 4, 0}, {lr.data(), lr.size() * 4, 0},
+      {pp.data(), pp.size() * 4, 0}, {pe.data(), pe.size() * 4, 0},
+      {pr.data(), pr.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
+      {jidx.data(), jidx.size() * 4, 0}, {jcoef.data(), jcoef.size() * 8, 0},
+      {split.data(), split.size() * 4, 0}};
   size_t total = 0;
   for (auto& p : parts) { p.off = total; total += (p.bytes + 255) & ~(size_t)255; }
   void* base = nullptr;
@@ -135,10 +161,14 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   d.three = (const uint8_t*)(b + parts[4].off);
   d.loss_ptr = (const int32_t*)(b + parts[5].off);
   d.loss_ent = (const int32_t*)(b + parts[6].off);
-  d.prod_ptr = (const int32_t*)(b + parts[7].off);
-  d.prod_ent = (const int32_t*)(b + parts[8].off);
-  d.jac_ptr = (const int32_t*)(b + parts[9].off);
-  d.jac_ent = (const int32_t*)(b + parts[10].off);
+  d.loss_r = (const int32_t*)(b + parts[7].off);
+  d.prod_ptr = (const int32_t*)(b + parts[8].off);
+  d.prod_ent = (const int32_t*)(b + parts[9].off);
+  d.prod_r = (const int32_t*)(b + parts[10].off);
+  d.jac_ptr = (const int32_t*)(b + parts[11].off);
+  d.jac_idx = (const int32_t*)(b + parts[12].off);
+  d.jac_coef = (const double*)(b + parts[13].off);
+  d.jac_split = (const int32_t*)(b + parts[14].off);
   net->base = base;
   net->bytes = total;
   *out = net;

@@ -15,19 +15,20 @@
 
 namespace vb {
 
-constexpr int LAYER_THREADS = 256;
-
 struct LayerSmem {
   double* y3;      // [3][ni+1]: layers j-1, j, j+1 (padding slot = 1.0)
   double* rate;    // [nr+1]
   double* drate;   // [(nr+1)*T]
+  double* jac;     // [ni*ni] gathered Jacobian
   double* diff;    // [ni]
   double* diagd;   // [ni]
-  double* scal;    // [8]: ysum(j-1), ysum(j), ysum(j+1), A_e, B_e, C_e
+  double* part;    // [2*ni] loss / production partial sums
+  double* scal;    // [8]: ysum(j-1), ysum(j), ysum(j+1)
 };
 
 __host__ __device__ inline size_t layer_smem_bytes(int ni, int nr, int T, bool jac) {
-  size_t d = 3 * (size_t)(ni + 1) + (nr + 1) + (jac ? (size_t)(nr + 1) * T : 0) + 2 * (size_t)ni + 8;
+  size_t d = 3 * (size_t)(ni + 1) + (nr + 1) + (jac ? (size_t)(nr + 1) * T + (size_t)ni * ni : 0) +
+             4 * (size_t)ni + 8;
   return d * sizeof(double);
 }
 
@@ -36,8 +37,10 @@ __device__ inline LayerSmem carve(double* s, int ni, int nr, int T, bool jac) {
   L.y3 = s; s += 3 * (ni + 1);
   L.rate = s; s += nr + 1;
   L.drate = s; s += jac ? (nr + 1) * T : 0;
+  L.jac = s; s += jac ? ni * ni : 0;
   L.diff = s; s += ni;
   L.diagd = s; s += ni;
+  L.part = s; s += 2 * ni;
   L.scal = s;
   return L;
 }
@@ -79,36 +82,37 @@ __device__ inline void layer_rates(const NetDev& net, const double* yrow, const 
   }
 }
 
-// dy_i/dt = prod_i - loss_i, each a sequential gather in segment_sum order.
-__device__ __forceinline__ double species_rhs(const NetDev& net, const double* rate, int i) {
-  const int T = net.T;
-  double loss = 0.0, prod = 0.0;
-  for (int e = net.loss_ptr[i]; e < net.loss_ptr[i + 1]; ++e) {
-    int rs = net.loss_ent[e];
-    loss = loss + net.r_st[rs] * rate[rs / T];
+// Loss and production sums of every species, each a sequential gather in
+// segment_sum order (one thread per sum): part[2i] = loss_i, part[2i+1] = prod_i.
+// The caller synchronises before reading dy_i/dt = part[2i+1] - part[2i].
+__device__ inline void species_sums(const NetDev& net, const double* rate, double* part) {
+  for (int t = threadIdx.x; t < 2 * net.ni; t += blockDim.x) {
+    const int i = t >> 1;
+    double acc = 0.0;
+    if (t & 1) {
+      for (int e = net.prod_ptr[i]; e < net.prod_ptr[i + 1]; ++e)
+        acc = acc + net.p_st[net.prod_ent[e]] * rate[net.prod_r[e]];
+    } else {
+      for (int e = net.loss_ptr[i]; e < net.loss_ptr[i + 1]; ++e)
+        acc = acc + net.r_st[net.loss_ent[e]] * rate[net.loss_r[e]];
+    }
+    part[t] = acc;
   }
-  for (int e = net.prod_ptr[i]; e < net.prod_ptr[i + 1]; ++e) {
-    int rs = net.prod_ent[e];
-    prod = prod + net.p_st[rs] * rate[rs / T];
-  }
-  return prod - loss;
 }
 
-// J[row][col] gathered from the flat contributions (chem.py:183-208).
-__device__ __forceinline__ double jac_entry(const NetDev& net, const double* drate, int d) {
-  const int T = net.T;
-  const int T2 = 2 * T;
-  double J = 0.0;
-  for (int e = net.jac_ptr[d]; e < net.jac_ptr[d + 1]; ++e) {
-    int fe = net.jac_ent[e];
-    int s = fe % T;
-    int ro = fe / T;
-    int o = ro % T2;
-    int r = ro / T2;
-    double coef = (o < T) ? -net.r_st[r * T + o] : net.p_st[r * T + (o - T)];
-    J = J + coef * drate[r * T + s];
+// Dense Jacobian of one layer into jac[ni*ni] (chem.py:183-208): each thread
+// owns a contiguous run of destinations holding about the same number of
+// contributions (jac_split), each summed in the reference's scatter order.
+// Requires blockDim.x == LAYER_THREADS.
+__device__ inline void layer_jacobian(const NetDev& net, const double* drate, double* jac) {
+  const int d0 = net.jac_split[threadIdx.x], d1 = net.jac_split[threadIdx.x + 1];
+  int e = net.jac_ptr[d0];
+  for (int d = d0; d < d1; ++d) {
+    const int e1 = net.jac_ptr[d + 1];
+    double J = 0.0;
+    for (; e < e1; ++e) J = J + net.jac_coef[e] * drate[net.jac_idx[e]];
+    jac[d] = J;
   }
-  return J;
 }
 
 // Loads state rows j-1..j+1 (stage 2: yk2 = y + k1/r) and their gas sums.
@@ -213,10 +217,13 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   load_rows(yb, nullptr, a.gas, nz, ni, j, r, false, L);
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
   __shared__ double supb[VB_MAX_NI], subb[VB_MAX_NI];
+  __syncthreads();
+  species_sums(net, L.rate, L.part);
+  layer_jacobian(net, L.drate, L.jac);
   layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);
   __syncthreads();
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
-    double v = species_rhs(net, L.rate, i) + L.diff[i];
+    double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
     bool fixed = fm && fm[i];
     if (fixed) v = 0.0;
     w.rmod[(int64_t)j * ni + i] = v;
@@ -234,7 +241,7 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   double* blk = w.inv + (int64_t)j * ni * B.ld;
   for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) {
     int row = d / ni, col = d - row * ni;
-    double J = jac_entry(net, L.drate, d);
+    double J = L.jac[d];
     double v = (row == col ? c0 : 0.0) - J;
     if (row == col) v = v + (-L.diagd[row]);
     if (fm && fm[row]) v = (row == col) ? c0 : 0.0;
@@ -263,10 +270,12 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
 
   load_rows(yb, w.k1, a.gas, nz, ni, j, r, true, L);
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
+  __syncthreads();
+  species_sums(net, L.rate, L.part);
   layer_diffusion(a, nz, ni, j, flags, L, nullptr, nullptr, false);
   __syncthreads();
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
-    double v = species_rhs(net, L.rate, i) + L.diff[i];
+    double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
     if (fm && fm[i]) v = 0.0;
     double k1v = w.k1[(int64_t)j * ni + i];
     w.rmod[(int64_t)j * ni + i] = v - (2.0 / (r * dtb)) * k1v;
@@ -288,12 +297,15 @@ chem_kernel(NetDev net, int nz, const double* __restrict__ y, const double* __re
   layer_rates(net, L.y3, k + (int64_t)b * (net.nr + 1) * nz + j, nz, M[(int64_t)b * nz + j], L.rate,
               L.drate, want_jac);
   __syncthreads();
+  species_sums(net, L.rate, L.part);
+  if (want_jac) layer_jacobian(net, L.drate, L.jac);
+  __syncthreads();
   if (dydt)
     for (int i = threadIdx.x; i < ni; i += blockDim.x)
-      dydt[((int64_t)b * nz + j) * ni + i] = species_rhs(net, L.rate, i);
+      dydt[((int64_t)b * nz + j) * ni + i] = L.part[2 * i + 1] - L.part[2 * i];
   if (want_jac) {
     double* out = jac + ((int64_t)b * nz + j) * ni * ni;
-    for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) out[d] = jac_entry(net, L.drate, d);
+    for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) out[d] = L.jac[d];
   }
 }
 

@@ -18,14 +18,22 @@ struct NetDev {
   // RHS gather tables: for species i, the (r*T+s) slots whose reactant (loss)
   // or product (prod) index is i, in increasing flat order (segment_sum order).
   const int32_t* loss_ptr;       // [ni+1]
-  const int32_t* loss_ent;
+  const int32_t* loss_ent;       // slot r*T+s (its stoichiometry is r_st[r*T+s])
+  const int32_t* loss_r;         // reaction r of the slot
   const int32_t* prod_ptr;       // [ni+1]
   const int32_t* prod_ent;
-  // Jacobian gather table: for destination d = row*ni+col, the flat contribution
-  // indices e = (r*2T + o)*T + s in increasing order (chem.py:193-207 scatter order).
+  const int32_t* prod_r;
+  // Jacobian gather table: for destination d = row*ni+col, the contributions
+  // (r, o, s) in increasing flat order (r*2T + o)*T + s (chem.py:193-207 scatter
+  // order), each stored as its drate slot r*T+s and signed stoichiometry.
   const int32_t* jac_ptr;        // [ni*ni+1]
-  const int32_t* jac_ent;
+  const int32_t* jac_idx;        // drate slot r*T+s
+  const double* jac_coef;        // -r_st[r][o] (o < T) or p_st[r][o-T]
+  // Destination ranges of the LAYER_THREADS threads, balanced by entry count.
+  const int32_t* jac_split;      // [LAYER_THREADS+1]
 };
+
+constexpr int LAYER_THREADS = 256;
 
 // Offsets (in doubles) of the fields of one atmosphere in the atm blob.
 struct AtmOff {
@@ -60,9 +68,11 @@ struct Geo {
   int64_t ws;        // workspace offset (doubles)
 };
 
-// Workspace doubles per layer: inverse block + rmod + k1 + sup_neg + sub_neg + spare.
+// Workspace doubles per layer: inverse block + rmod + k1 + sup_neg + sub_neg +
+// spare, rounded up to 16 doubles so every atmosphere's blocks start on a
+// 128-byte boundary (bulk copies need 16-byte aligned addresses and sizes).
 __host__ __device__ inline int64_t ws_per_layer(int ni, int ld) {
-  return (int64_t)ni * ld + 5 * (int64_t)ni;
+  return (((int64_t)ni * ld + 5 * (int64_t)ni) + 15) & ~(int64_t)15;
 }
 
 __device__ __forceinline__ Geo geo_of(const Batch& B, int b) {
@@ -103,6 +113,44 @@ __device__ __forceinline__ WsView ws_view(double* ws, const Geo& g, int ni, int 
 }
 
 __host__ __device__ inline int round_even(int n) { return (n + 1) & ~1; }
+
+// ---------------------------------------------------------------- bulk copies
+// Global -> shared bulk copies (cp.async.bulk, no multicast) completed on an
+// mbarrier. Every wait is bounded: a wait that gives up reports false and the
+// caller sets VB_STATUS_WATCHDOG.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+constexpr long long WAIT_LIMIT = 1ll << 22;
 
 // Ros2 constants (reference jax_step.py:257-258).
 __device__ __forceinline__ double ros2_r() { return 1.0 + 1.0 / sqrt(2.0); }

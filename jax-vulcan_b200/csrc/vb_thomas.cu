@@ -28,9 +28,10 @@ struct LUK {
   static size_t smem_bytes() {
     size_t d = (size_t)NP * SLD          // S: previous inverse, LU factors, new inverse
                + 2 * (size_t)PBUF        // panel buffers / triangular-solve row buffers
+               + (size_t)NP * PLD        // M: update multipliers of the current panel
                + (size_t)PW * NP         // V: pivot rows of the current panel
                + 2 * (size_t)NP          // vec, rdiag
-               + PW;                     // pivot row broadcast of the panel warp
+               + PW + PW * PW;           // pivot row broadcast, L_KK^{-1}
     return d * sizeof(double) + sizeof(int) * 2 * NP;
   }
 };
@@ -67,11 +68,13 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   double* S = reinterpret_cast<double*>(smem_raw);          // [NP][SLD]
   double* Pn0 = S + NP * SLD;                               // [PBUF]
   double* Pn1 = Pn0 + G::PBUF;                              // [PBUF]
-  double* V = Pn1 + G::PBUF;                                // [PW][NP]
+  double* Mb = Pn1 + G::PBUF;                               // [NP][PLD]
+  double* V = Mb + NP * PLD;                                // [PW][NP]
   double* vec = V + PW * NP;                                // [NP]
   double* rdiag = vec + NP;                                 // [NP]
   double* prow_s = rdiag + NP;                              // [PW]
-  int* pivs = reinterpret_cast<int*>(prow_s + PW);          // [NP] pivot row of step k
+  double* Linv = prow_s + PW;                               // [PW][PW]
+  int* pivs = reinterpret_cast<int*>(Linv + PW * PW);       // [NP] pivot row of step k
   int* qinv = pivs + NP;                                    // [NP] step of row i (-1: not yet)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned FULL = 0xffffffffu;
@@ -120,13 +123,9 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         }
       }
       __syncthreads();
-      // (b) warp 0: unblocked LU of the panel over the unpivoted rows
+      // (b) warp 0: unblocked LU of the panel (in shared memory) over the
+      //     unpivoted rows, then L_KK^{-1} of its unit lower triangle
       if (warp == 0) {
-        double pv[PRL][PW];
-#pragma unroll
-        for (int r = 0; r < PRL; ++r)
-#pragma unroll
-          for (int t = 0; t < PW; ++t) pv[r][t] = Pn[(lane + 32 * r) * PLD + t];
 #pragma unroll
         for (int t = 0; t < PW; ++t) {
           if (t < kw) {
@@ -134,53 +133,78 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
             unsigned brow = 0xffffffffu;
 #pragma unroll
             for (int r = 0; r < PRL; ++r) {
-              int i = lane + 32 * r;
+              const int i = lane + 32 * r;
               if (i < n && !((usedw >> r) & 1u)) {
-                unsigned long long kk = pivot_key(pv[r][t]);
+                unsigned long long kk = pivot_key(Pn[i * PLD + t]);
                 if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
               }
             }
-            unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-            unsigned m1 = __reduce_max_sync(FULL, hi);
-            unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
+            const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+            const unsigned m1 = __reduce_max_sync(FULL, hi);
+            const unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
             const int p = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
-            const int pl = p & 31, prr = p >> 5;
-            if (lane == pl) {
-#pragma unroll
-              for (int r = 0; r < PRL; ++r)
-                if (r == prr) {
-#pragma unroll
-                  for (int u = 0; u < PW; ++u) prow_s[u] = pv[r][u];
-                  usedw |= 1u << r;
-                }
-            }
-            __syncwarp();
-            double prow[PW];
-#pragma unroll
-            for (int u = 0; u < PW; ++u) prow[u] = prow_s[u];
+            if ((p & 31) == lane) usedw |= 1u << (p >> 5);
+            const double* prow = Pn + p * PLD;
             const double piv = prow[t];
             if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
             const double rcp = 1.0 / piv;
+            double pr[PW];
+#pragma unroll
+            for (int u = t + 1; u < PW; ++u) pr[u] = prow[u];
 #pragma unroll
             for (int r = 0; r < PRL; ++r) {
-              int i = lane + 32 * r;
+              const int i = lane + 32 * r;
               if (i < n && !((usedw >> r) & 1u)) {
-                const double l = pv[r][t] * rcp;
-                pv[r][t] = l;
+                double* row = Pn + i * PLD;
+                const double l = row[t] * rcp;
+                row[t] = l;
 #pragma unroll
-                for (int u = t + 1; u < PW; ++u) pv[r][u] = fma(-l, prow[u], pv[r][u]);
+                for (int u = t + 1; u < PW; ++u) row[u] = fma(-l, pr[u], row[u]);
               }
             }
             if (lane == 0) { pivs[k0 + t] = p; qinv[p] = k0 + t; }
             __syncwarp();
           }
         }
+        // L_KK^{-1} (unit lower): lane s builds column s from the pivot rows' multipliers
+        if (lane < PW) {
+          const int sc = lane;
+          double li[PW];
 #pragma unroll
-        for (int r = 0; r < PRL; ++r)
+          for (int t = 0; t < PW; ++t) {
+            double x = (t == sc) ? 1.0 : 0.0;
+            if (t > sc && t < kw) {
+              const double* lrow = Pn + pivs[k0 + t] * PLD;
 #pragma unroll
-          for (int t = 0; t < PW; ++t) Pn[(lane + 32 * r) * PLD + t] = pv[r][t];
+              for (int m = 0; m < t; ++m)
+                if (m >= sc) x = fma(-lrow[m], li[m], x);
+            }
+            li[t] = x;
+          }
+#pragma unroll
+          for (int t = 0; t < PW; ++t) Linv[t * PW + sc] = li[t];
+        }
       }
       __syncthreads();
+      // (b') every warp: update multipliers of its own rows. Unpivoted rows
+      //     M = -L[i,K] L_KK^{-1}; pivot row p_t: M = L_KK^{-1}[t,:] - e_t (so
+      //     W + M V = U[t,:]); rows pivoted earlier: 0.
+      for (int e = lane; e < RPW * PW; e += 32) {
+        const int r = e / PW, u = e - r * PW;
+        const int i = warp * RPW + r;
+        const int q = i < n ? qinv[i] : -2;
+        double x = 0.0;
+        if (i < n && q < 0) {
+          const double* row = Pn + i * PLD;
+#pragma unroll
+          for (int s2 = 0; s2 < PW; ++s2)
+            if (s2 >= u && s2 < kw) x = fma(-row[s2], Linv[s2 * PW + u], x);
+        } else if (q >= k0 && q < k0 + kw) {
+          const int t = q - k0;
+          x = (u <= t) ? Linv[t * PW + u] - (u == t ? 1.0 : 0.0) : 0.0;
+        }
+        Mb[i * PLD + u] = x;
+      }
       // (c) owners of the new pivot rows stage them: V[t] = A[p_t, :]
 #pragma unroll
       for (int r = 0; r < RPW; ++r) {
@@ -192,44 +216,28 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         }
       }
       __syncthreads();
-      // (d) U[K, c] = L_KK^{-1} V[:, c]; pivot rows take U, unpivoted rows get
-      //     the rank-kw update, rows pivoted in earlier panels are final.
+      // (d) rank-kw update A[i, C] += M[i, K] V[K, C] (C = columns right of the
+      //     panel): unpivoted rows get the Schur update, pivot rows become
+      //     U[K, C] = L_KK^{-1} V; rows pivoted in earlier panels are final.
 #pragma unroll
-      for (int c = 0; c < CPL; ++c) {
-        const int col = lane + 32 * c;
-        const bool right = col >= k0 + PW;
-        double u[PW];
+      for (int r = 0; r < RPW; ++r) {
+        const int i = warp * RPW + r;
+        const int q = qinv[i];
+        if (q >= 0 && q < k0) continue;
+        double mi[PW];
 #pragma unroll
-        for (int t = 0; t < PW; ++t) {
-          double x = 0.0;
-          if (right && t < kw) {
-            x = V[t * NP + col];
-            const double* lrow = Pn + pivs[k0 + t] * PLD;
+        for (int t = 0; t < PW; ++t) mi[t] = Mb[i * PLD + t];
 #pragma unroll
-            for (int s2 = 0; s2 < t; ++s2) x = fma(-lrow[s2], u[s2], x);
-          }
-          u[t] = x;
-        }
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-          const int i = warp * RPW + r;
-          const int q = qinv[i];
+        for (int c = 0; c < CPL; ++c) {
+          const int col = lane + 32 * c;
           if (col >= k0 && col < k0 + PW) {
             a[r][c] = Pn[i * PLD + (col - k0)];
-          } else if (right) {
-            if (q >= k0 && q < k0 + kw) {
-              double x = 0.0;
+          } else if (col >= k0 + PW) {
+            double acc = a[r][c];
 #pragma unroll
-              for (int t = 0; t < PW; ++t)
-                if (t == q - k0) x = u[t];
-              a[r][c] = x;
-            } else if (q < 0) {
-              double acc = a[r][c];
-#pragma unroll
-              for (int t = 0; t < PW; ++t)
-                if (t < kw) acc = fma(-Pn[i * PLD + t], u[t], acc);
-              a[r][c] = acc;
-            }
+            for (int t = 0; t < PW; ++t)
+              if (t < kw) acc = fma(mi[t], V[t * NP + col], acc);
+            a[r][c] = acc;
           }
         }
       }
@@ -396,15 +404,20 @@ factor_kernel(Batch B, double* __restrict__ ws, int32_t* __restrict__ status, in
 
 // ---------------------------------------------------------------- sweeps
 constexpr int SWEEP_THREADS = 256;
+constexpr int SWEEP_MAX_STAGES = 3;
 
-// out = Inv v (or Inv^T v) for one n x n block in global memory.
-__device__ inline void block_matvec(const double* __restrict__ Inv, int n, int ld, bool trans,
-                                    const double* v, double* out) {
+__host__ __device__ inline size_t sweep_smem_bytes(int ni, int stages) {
+  return (size_t)stages * ni * round_even(ni) * sizeof(double) + 64 + 2 * VB_MAX_NI * sizeof(double);
+}
+
+// out = Inv v (or Inv^T v) for one n x n block held in shared memory.
+__device__ inline void block_matvec_s(const double* __restrict__ Inv, int n, int ld, bool trans,
+                                      const double* v, double* out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (!trans) {
     for (int i = warp; i < n; i += nw) {
       double s = 0.0;
-      for (int m = lane; m < n; m += 32) s += Inv[(int64_t)i * ld + m] * v[m];
+      for (int m = lane; m < n; m += 32) s = fma(Inv[i * ld + m], v[m], s);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
       if (lane == 0) out[i] = s;
@@ -412,65 +425,105 @@ __device__ inline void block_matvec(const double* __restrict__ Inv, int n, int l
   } else {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       double s = 0.0;
-      for (int m = 0; m < n; ++m) s += Inv[(int64_t)m * ld + i] * v[m];
+      for (int m = 0; m < n; ++m) s = fma(Inv[m * ld + i], v[m], s);
       out[i] = s;
     }
   }
 }
 
+// One sweep of one atmosphere over its stored inverses: forward elimination
+// (solver.py:73-88) or back substitution (solver.py:91-111), optionally fused
+// with the Ros2 combination (jax_step.py:313-314). The inverse blocks stream
+// through a ring of `stages` shared-memory buffers filled by bulk copies.
 __global__ void __launch_bounds__(SWEEP_THREADS)
-sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A) {
-  __shared__ double v[VB_MAX_NI];
-  __shared__ double u[VB_MAX_NI];
+sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages) {
+  extern __shared__ __align__(128) char smem_raw[];
   const int b = blockIdx.x;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
   const int n = B.ni, nz = g.nz, ld = B.ld;
+  const int blk = n * ld;
+  const uint32_t blk_bytes = (uint32_t)(blk * sizeof(double));
+  double* ring = reinterpret_cast<double*>(smem_raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + (size_t)stages * blk);
+  double* v = reinterpret_cast<double*>(bars + 8);
+  double* u = v + VB_MAX_NI;
   const bool tr = A.transposed != 0;
   // transposed system: sub/super exchange roles (steady_state_grad.py:218-219)
   const double* up = tr ? w.subn : w.supn;   // couples x[j+1] into row j
   const double* lo = tr ? w.supn : w.subn;   // couples x[j-1] into row j
   double* vecs = A.user ? A.user + g.z0 * n : w.rmod;
-  if (A.mode == SWEEP_FWD) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] = vecs[i];
-    __syncthreads();
-    for (int j = 1; j < nz; ++j) {
-      block_matvec(w.inv + (int64_t)(j - 1) * n * ld, n, ld, tr, v, u);
-      __syncthreads();
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double x = vecs[(int64_t)j * n + i] - lo[(int64_t)(j - 1) * n + i] * u[i];
-        vecs[(int64_t)j * n + i] = x;
-        v[i] = x;
-      }
-      __syncthreads();
+  const bool fwd = A.mode == SWEEP_FWD;
+  const int count = fwd ? nz - 1 : nz;                 // blocks used, in order
+  auto block_of = [&](int s2) { return fwd ? s2 : nz - 1 - s2; };
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < stages; ++st) mbar_init(&bars[st], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < stages && st < count; ++st) {
+      mbar_expect_tx(&bars[st], blk_bytes);
+      bulk_g2s(ring + (size_t)st * blk, w.inv + (int64_t)block_of(st) * blk, blk_bytes, &bars[st]);
     }
-    return;
   }
   double* out = A.user ? A.user + g.z0 * n : w.k1;
   const double r = ros2_r();
-  for (int j = nz - 1; j >= 0; --j) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      double x = vecs[(int64_t)j * n + i];
-      if (j < nz - 1) x = x - up[(int64_t)j * n + i] * u[i];
-      v[i] = x;
+  if (fwd) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] = vecs[i];
+  }
+  int issued = min(stages, count);
+  for (int s2 = 0; s2 < count; ++s2) {
+    const int st = s2 % stages;
+    const uint32_t parity = (uint32_t)((s2 / stages) & 1);
+    const int j = block_of(s2);
+    if (!fwd) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double x = vecs[(int64_t)j * n + i];
+        if (j < nz - 1) x = x - up[(int64_t)j * n + i] * u[i];
+        v[i] = x;
+      }
     }
+    const bool ok = mbar_wait(&bars[st], parity, WAIT_LIMIT);
+    if (__syncthreads_or(!ok)) {
+      // give up: wait (bounded) for the copies still in flight, report, return
+      if (threadIdx.x == 0) {
+        for (int s3 = s2; s3 < issued; ++s3)
+          mbar_wait(&bars[s3 % stages], (uint32_t)((s3 / stages) & 1), WAIT_LIMIT);
+        if (A.status) atomicOr(A.status + b, VB_STATUS_WATCHDOG);
+      }
+      return;
+    }
+    block_matvec_s(ring + (size_t)st * blk, n, ld, tr, v, u);
     __syncthreads();
-    block_matvec(w.inv + (int64_t)j * n * ld, n, ld, tr, v, u);
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      double kj = u[i];
-      if (A.mode == SWEEP_BACK) {
-        out[(int64_t)j * n + i] = kj;
-      } else {
-        // sol = y + 3/(2r) k1 + 1/(2r) k2 ; delta = |sol - yk2| (jax_step.py:313-314)
-        int64_t e = g.z0 * n + (int64_t)j * n + i;
-        double yv = A.y[e];
-        double k1v = w.k1[(int64_t)j * n + i];
-        double s = yv + (3.0 / (2.0 * r)) * k1v + (1.0 / (2.0 * r)) * kj;
-        double yk2 = yv + k1v / r;
-        A.sol[e] = s;
-        A.delta[e] = fabs(s - yk2);
-        if (!isfinite(s)) atomicOr(A.status + b, VB_STATUS_NONFINITE);
+    if (threadIdx.x == 0 && s2 + stages < count) {
+      fence_proxy_async();
+      mbar_expect_tx(&bars[st], blk_bytes);
+      bulk_g2s(ring + (size_t)st * blk, w.inv + (int64_t)block_of(s2 + stages) * blk, blk_bytes, &bars[st]);
+      ++issued;
+    }
+    if (fwd) {
+      // rhs'[j+1] = rhs[j+1] - sub_d[j] o (Inv_j rhs'[j])
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double x = vecs[(int64_t)(j + 1) * n + i] - lo[(int64_t)j * n + i] * u[i];
+        vecs[(int64_t)(j + 1) * n + i] = x;
+        v[i] = x;
+      }
+    } else {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double kj = u[i];
+        if (A.mode == SWEEP_BACK) {
+          out[(int64_t)j * n + i] = kj;
+        } else {
+          // sol = y + 3/(2r) k1 + 1/(2r) k2 ; delta = |sol - yk2| (jax_step.py:313-314)
+          int64_t e = g.z0 * n + (int64_t)j * n + i;
+          double yv = A.y[e];
+          double k1v = w.k1[(int64_t)j * n + i];
+          double s = yv + (3.0 / (2.0 * r)) * k1v + (1.0 / (2.0 * r)) * kj;
+          double yk2 = yv + k1v / r;
+          A.sol[e] = s;
+          A.delta[e] = fabs(s - yk2);
+          if (!isfinite(s)) atomicOr(A.status + b, VB_STATUS_NONFINITE);
+        }
       }
     }
     __syncthreads();
@@ -536,11 +589,16 @@ cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_
   if (B.ni <= 32) return launch_factor_t<32, 8, 8>(B, ws, status, with_rhs, st);
   if (B.ni <= 64) return launch_factor_t<64, 16, 8>(B, ws, status, with_rhs, st);
   if (B.ni <= 96) return launch_factor_t<96, 16, 8>(B, ws, status, with_rhs, st);
-  return launch_factor_t<128, 16, 4>(B, ws, status, with_rhs, st);
+  return launch_factor_t<128, 16, 8>(B, ws, status, with_rhs, st);
 }
 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {
-  sweep_kernel<<<B.count, SWEEP_THREADS, 0, st>>>(B, ws, A);
+  int stages = SWEEP_MAX_STAGES;
+  while (stages > 1 && sweep_smem_bytes(B.ni, stages) > 220 * 1024) --stages;
+  size_t sm = sweep_smem_bytes(B.ni, stages);
+  cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  sweep_kernel<<<B.count, SWEEP_THREADS, sm, st>>>(B, ws, A, stages);
   return cudaGetLastError();
 }
 
