@@ -121,6 +121,65 @@ int vb_bt_solve(int batch, int nz, int ni, const void* factors, const double* rh
 int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* rhs, double* x,
                   void* stream);
 
+/* Steady-state residual f(y) = chem_rhs + diffusion (reference
+ * steady_state_grad.py:116-130) of a (possibly ragged) batch -> f [B][nz][ni]. */
+int vb_residual(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
+                const double* atm, int32_t atm_flags, double* f, void* stream);
+
+/* Implicit steady-state adjoint (reference steady_state_grad.py:153-233,
+ * 284-330): assembles J_y = df/dy at y_star, solves J_y^T lambda = v with the
+ * block-Thomas factors (transposed sweeps), and writes the cotangents
+ * -lambda . df/dtheta (each output nullable): g_k [B][nr+1][nz] (the k_arr
+ * leaf), g_M [B][nz], g_Kzz [B][nz] (interfaces 0..nz-2; packed by layers
+ * like y for ragged batches),
+ * g_top, g_bot, g_vdep [B][ni]; lambda [B][nz][ni] if non-NULL.
+ * Uses the Ros2 workspace (vb_ros2_workspace_bytes). */
+int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y_star, const double* k,
+               const double* atm, int32_t atm_flags, const double* v, double* lambda, double* g_k, double* g_M,
+               double* g_Kzz, double* g_top, double* g_bot, double* g_vdep, int32_t* status, void* workspace,
+               size_t workspace_bytes, void* stream);
+
+/* Photochemistry (reference photo.py). Cross sections and branch tables are
+ * device arrays shared by the batch, except the temperature-dependent tables
+ * absp_T_cross [n_abs_T][nz][nbin] and cross_J_T [n_br_T][nz][nbin], which
+ * advance by T_stride / T_stride_J doubles per atmosphere (0: shared). */
+typedef struct VbPhoto {
+  int32_t nbin, n_abs, n_abs_T, n_scat, n_br, n_br_T, din12, reserved;
+  int64_t T_stride, T_stride_J;
+  const int32_t* absp_idx;      /* [n_abs]   species of the T-independent absorbers */
+  const int32_t* absp_T_idx;    /* [n_abs_T] species of the T-dependent absorbers */
+  const int32_t* scat_idx;      /* [n_scat]  scattering species */
+  const double* absp_cross;     /* [n_abs][nbin] */
+  const double* absp_T_cross;   /* [n_abs_T][nz][nbin] */
+  const double* scat_cross;     /* [n_scat][nbin] */
+  const double* cross_J;        /* [n_br][nbin]   branch cross sections */
+  const double* cross_J_T;      /* [n_br_T][nz][nbin] */
+  const double* bins;           /* [nbin] wavelengths (nm) */
+  const double* sflux_top;      /* [nbin] stellar flux at the top */
+  const int32_t* br_re_idx;     /* [n_br]  k row of each branch */
+  const int32_t* br_T_re_idx;   /* [n_br_T] */
+  const uint8_t* br_active;     /* [n_br]  write the k row (reference remove_list) */
+  const uint8_t* br_T_active;   /* [n_br_T] */
+  double dbin1, dbin2, mu_zenith, edd, ag0, hc, f_diurnal;
+} VbPhoto;
+
+/* Optical depth (reference photo.py:84-123): y [B][nz][ni], dz [B][nz] ->
+ * tau [B][nz+1][nbin] (tau[nz] = 0). */
+int vb_photo_tau(int batch, int nz, int ni, const VbPhoto* photo, const double* y, const double* dz,
+                 double* tau, void* stream);
+/* Two-stream flux (reference photo.py:126-245): tau, ymix [B][nz][ni],
+ * dflux_u_prev [B][nz+1][nbin] -> aflux [B][nz][nbin], sflux, dflux_d,
+ * dflux_u [B][nz+1][nbin]. */
+int vb_photo_flux(int batch, int nz, int ni, const VbPhoto* photo, const double* tau, const double* ymix,
+                  const double* dflux_u_prev, double* aflux, double* sflux, double* dflux_d,
+                  double* dflux_u, void* stream);
+/* J-rates (reference photo.py:309-351) -> J_br [B][n_br][nz], J_br_T
+ * [B][n_br_T][nz] (either nullable), and with k != NULL the photolysis rows
+ * k[B][nr+1][nz] of active branches are set to J * f_diurnal
+ * (photo.py:455-478). */
+int vb_photo_j(int batch, int nz, int nr, const VbPhoto* photo, const double* aflux, double* J_br,
+               double* J_br_T, double* k, void* stream);
+
 /* Profiling: while enabled, every kernel launch of vb_ros2_step is bracketed
  * by CUDA events recorded on the launching stream (launch sites:
  * 0 stage-1 assembly, 1 factor, 2 back sweep 1, 3 stage-2 assembly,

@@ -41,6 +41,11 @@ SIGNATURES = {
     "vb_bt_factor": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_bt_solve": (_i, [_i, _i, _i, _p, _p, _p, _p]),
     "vb_bt_solve_T": (_i, [_i, _i, _i, _p, _p, _p, _p]),
+    "vb_residual": (_i, [_p, _i, _i, _p, _p, _p, _p, _i32, _p, _p]),
+    "vb_adjoint": (_i, [_p, _i, _i, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p]),
+    "vb_photo_tau": (_i, [_i, _i, _i, _p, _p, _p, _p, _p]),
+    "vb_photo_flux": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "vb_photo_j": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_profile": (_i, [_i]),
     "vb_profile_read": (_i, [_p, _p, _i]),
     "vb_fp64_probe": (_i, [_p, _i, _i, _i, _p]),

@@ -24,6 +24,8 @@ UNITS = {
     "vb_api.cu": [],
     "vb_thomas.cu": [],
     "vb_chem.cu": ["--fmad=false"],
+    "vb_photo.cu": ["--fmad=false"],
+    "vb_adjoint.cu": [],
 }
 
 

@@ -320,6 +320,72 @@ int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* 
   return bt_solve(batch, nz, ni, factors, rhs, x, 1, stream);
 }
 
+int vb_residual(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
+                const double* atm, int32_t flags, double* f, void* stream) {
+  if (!net || !y || !k || !atm || !f) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  vb::Batch B = make_batch(net, batch, nz, zoff);
+  VB_CHECK(vb::launch_stage2(net->dev, B, y, k, nullptr, atm, flags, nullptr, nullptr, (cudaStream_t)stream, f),
+           "residual");
+  return VB_OK;
+}
+
+int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
+               const double* atm, int32_t flags, const double* v, double* lambda, double* g_k, double* g_M,
+               double* g_Kzz, double* g_top, double* g_bot, double* g_vdep, int32_t* status, void* workspace,
+               size_t ws_bytes, void* stream) {
+  if (!net || !y || !k || !atm || !v || !status || !workspace) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  if (!zoff && ws_bytes < vb_ros2_workspace_bytes(batch, nz, net->dev.ni, nullptr))
+    return fail(VB_ERR_ARG, "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = make_batch(net, batch, nz, zoff);
+  double* ws = (double*)workspace;
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  VB_CHECK(vb::launch_stage1(net->dev, B, y, k, nullptr, atm, flags, nullptr, ws, st, v), "adjoint blocks");
+  VB_CHECK(vb::launch_factor(B, ws, status, 0, st), "factor");
+  vb::SweepArgs a{};
+  a.transposed = 1;
+  a.status = status;
+  a.mode = 0;
+  VB_CHECK(vb::launch_sweep(B, ws, a, st), "transposed forward sweep");
+  a.mode = 1;
+  VB_CHECK(vb::launch_sweep(B, ws, a, st), "transposed back sweep");
+  // lambda is in the workspace's k1 rows
+  VB_CHECK(vb::launch_gather_k1(B, ws, lambda, st), "lambda");
+  VB_CHECK(vb::launch_vjp(net->dev, B, y, k, atm, flags, ws, g_k, g_M, g_Kzz, g_top, g_bot, g_vdep, st), "vjp");
+  return VB_OK;
+}
+
+int vb_photo_tau(int batch, int nz, int ni, const VbPhoto* photo, const double* y, const double* dz,
+                 double* tau, void* stream) {
+  if (!photo || !y || !dz || !tau) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
+  VB_CHECK(vb::launch_photo_tau(batch, nz, ni, *photo, y, dz, tau, (cudaStream_t)stream), "photo tau");
+  return VB_OK;
+}
+
+int vb_photo_flux(int batch, int nz, int ni, const VbPhoto* photo, const double* tau, const double* ymix,
+                  const double* dflux_u_prev, double* aflux, double* sflux, double* dflux_d, double* dflux_u,
+                  void* stream) {
+  if (!photo || !tau || !ymix || !dflux_u_prev || !aflux || !sflux || !dflux_d || !dflux_u)
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
+  VB_CHECK(vb::launch_photo_flux(batch, nz, ni, *photo, tau, ymix, dflux_u_prev, aflux, sflux, dflux_d, dflux_u,
+                                 (cudaStream_t)stream),
+           "photo flux");
+  return VB_OK;
+}
+
+int vb_photo_j(int batch, int nz, int nr, const VbPhoto* photo, const double* aflux, double* J_br,
+               double* J_br_T, double* k, void* stream) {
+  if (!photo || !aflux) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
+    return fail(VB_ERR_ARG, "bad shape");
+  VB_CHECK(vb::launch_photo_j(batch, nz, nr, *photo, aflux, J_br, J_br_T, k, (cudaStream_t)stream), "photo J");
+  return VB_OK;
+}
+
 int vb_profile(int enable) {
   g_prof = enable != 0;
   return VB_OK;

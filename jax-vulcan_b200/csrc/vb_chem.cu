@@ -185,11 +185,7 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
       d = d + ((flags & VB_USE_BOTFLUX) ? (a.bot[i] - y0[i] * a.vdep[i]) / a.dzi[0] : 0.0);
     }
     L.diff[i] = d;
-    if (want_diag) {
-      double dd = At;
-      if (j == 0) dd = dd + ((flags & VB_USE_BOTFLUX) ? -a.vdep[i] / a.dzi[0] : 0.0);
-      L.diagd[i] = dd;
-    }
+    if (want_diag) L.diagd[i] = At;
     if (sup_out && j < nz - 1) sup_out[i] = Bt;
     if (sub_out && j > 0) sub_out[i] = Ct;
   }
@@ -200,7 +196,7 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
 __global__ void __launch_bounds__(LAYER_THREADS)
 stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
               const double* __restrict__ dt, const double* __restrict__ atm, int flags,
-              const uint8_t* __restrict__ fix_mask, double* __restrict__ ws) {
+              const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, const double* __restrict__ adj_v) {
   extern __shared__ double smem[];
   const int b = blockIdx.y, j = blockIdx.x;
   Geo g = geo_of(B, b);
@@ -211,8 +207,9 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   WsView w = ws_view(ws, g, ni, B.ld);
   const double* yb = y + g.z0 * ni;
   const uint8_t* fm = fix_mask ? fix_mask + g.z0 * ni + (int64_t)j * ni : nullptr;
+  const bool adj = adj_v != nullptr;   // J_y blocks of the steady-state adjoint
   const double r = ros2_r();
-  const double c0 = 1.0 / (r * dt[b]);
+  const double c0 = adj ? 0.0 : 1.0 / (r * dt[b]);
 
   load_rows(yb, nullptr, a.gas, nz, ni, j, r, false, L);
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
@@ -222,6 +219,26 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   layer_jacobian(net, L.drate, L.jac);
   layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);
   __syncthreads();
+  if (adj) {
+    // steady_state_grad.py:153-175: diag = J + diag(A_eddy + A_mol) (+ deposition
+    // at the bottom), sup_d = B[:-1], sub_d = C[1:] (no c0, not negated)
+    for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+      w.rmod[(int64_t)j * ni + i] = adj_v[g.z0 * ni + (int64_t)j * ni + i];
+      if (j < nz - 1) w.supn[(int64_t)j * ni + i] = supb[i];
+      if (j > 0) w.subn[(int64_t)(j - 1) * ni + i] = subb[i];
+    }
+    double* blk = w.inv + (int64_t)j * ni * B.ld;
+    for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) {
+      int row = d / ni, col = d - row * ni;
+      double v = L.jac[d];
+      if (row == col) {
+        v = v + L.diagd[row];
+        if (j == 0) v = v + ((flags & VB_USE_BOTFLUX) ? -a.vdep[row] / a.dzi[0] : 0.0);
+      }
+      blk[(int64_t)row * B.ld + col] = v;
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
     bool fixed = fm && fm[i];
@@ -243,7 +260,12 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
     int row = d / ni, col = d - row * ni;
     double J = L.jac[d];
     double v = (row == col ? c0 : 0.0) - J;
-    if (row == col) v = v + (-L.diagd[row]);
+    if (row == col) {
+      // jax_step.py:283,288: the deposition term joins diag_d before -diag_d is added
+      double dd = L.diagd[row];
+      if (j == 0) dd = dd + ((flags & VB_USE_BOTFLUX) ? -a.vdep[row] / a.dzi[0] : 0.0);
+      v = v + (-dd);
+    }
     if (fm && fm[row]) v = (row == col) ? c0 : 0.0;
     blk[(int64_t)row * B.ld + col] = v;
   }
@@ -254,7 +276,7 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
 __global__ void __launch_bounds__(LAYER_THREADS)
 stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
               const double* __restrict__ dt, const double* __restrict__ atm, int flags,
-              const uint8_t* __restrict__ fix_mask, double* __restrict__ ws) {
+              const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, double* __restrict__ resid) {
   extern __shared__ double smem[];
   const int b = blockIdx.y, j = blockIdx.x;
   Geo g = geo_of(B, b);
@@ -266,9 +288,10 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   const double* yb = y + g.z0 * ni;
   const uint8_t* fm = fix_mask ? fix_mask + g.z0 * ni + (int64_t)j * ni : nullptr;
   const double r = ros2_r();
-  const double dtb = dt[b];
+  const bool res = resid != nullptr;   // steady-state residual f(y) (steady_state_grad.py:116-130)
+  const double dtb = res ? 1.0 : dt[b];
 
-  load_rows(yb, w.k1, a.gas, nz, ni, j, r, true, L);
+  load_rows(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
   __syncthreads();
   species_sums(net, L.rate, L.part);
@@ -276,6 +299,10 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   __syncthreads();
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
+    if (res) {
+      resid[g.z0 * ni + (int64_t)j * ni + i] = v;
+      continue;
+    }
     if (fm && fm[i]) v = 0.0;
     double k1v = w.k1[(int64_t)j * ni + i];
     w.rmod[(int64_t)j * ni + i] = v - (2.0 / (r * dtb)) * k1v;
@@ -327,28 +354,32 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
   __syncthreads();
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     if (diff) diff[((int64_t)b * nz + j) * ni + i] = L.diff[i];
-    if (diag_d) diag_d[((int64_t)b * nz + j) * ni + i] = L.diagd[i];
+    if (diag_d) {
+      double dd = L.diagd[i];
+      if (j == 0) dd = dd + ((flags & VB_USE_BOTFLUX) ? -a.vdep[i] / a.dzi[0] : 0.0);
+      diag_d[((int64_t)b * nz + j) * ni + i] = dd;
+    }
   }
 }
 
 // ---------------------------------------------------------------- launchers
 cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, const double* k,
                           const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
-                          cudaStream_t st) {
+                          cudaStream_t st, const double* adj_v) {
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, true);
   cudaFuncSetAttribute(stage1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(B.nz, B.count);
-  stage1_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
+  stage1_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws, adj_v);
   return cudaGetLastError();
 }
 
 cudaError_t launch_stage2(const NetDev& net, const Batch& B, const double* y, const double* k,
                           const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
-                          cudaStream_t st) {
+                          cudaStream_t st, double* resid) {
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, false);
   cudaFuncSetAttribute(stage2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(B.nz, B.count);
-  stage2_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
+  stage2_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws, resid);
   return cudaGetLastError();
 }
 

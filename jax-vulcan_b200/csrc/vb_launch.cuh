@@ -18,10 +18,21 @@ struct SweepArgs {
   int32_t* status;
 };
 
+// adj_v != nullptr: assemble the steady-state Jacobian blocks J_y and copy the
+// cotangent adj_v [B][nz][ni] into the right-hand side instead of the Ros2 LHS.
 cudaError_t launch_stage1(const NetDev&, const Batch&, const double* y, const double* k, const double* dt,
-                          const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t);
+                          const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t,
+                          const double* adj_v = nullptr);
+// resid != nullptr: write the residual f(y) = chem + diffusion to resid [B][nz][ni]
+// instead of the stage-2 right-hand side.
 cudaError_t launch_stage2(const NetDev&, const Batch&, const double* y, const double* k, const double* dt,
-                          const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t);
+                          const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t,
+                          double* resid = nullptr);
+// Cotangents from lambda held in the workspace's k1 rows (see vb_adjoint).
+cudaError_t launch_vjp(const NetDev&, const Batch&, const double* y, const double* k, const double* atm, int flags,
+                       double* ws, double* g_k, double* g_M, double* g_Kzz, double* g_top, double* g_bot,
+                       double* g_vdep, cudaStream_t);
+cudaError_t launch_gather_k1(const Batch&, double* ws, double* out, cudaStream_t);
 cudaError_t launch_chem(const NetDev&, int batch, int nz, const double* y, const double* M, const double* k,
                         double* dydt, double* jac, cudaStream_t);
 cudaError_t launch_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int flags,
@@ -31,6 +42,13 @@ cudaError_t launch_sweep(const Batch&, double* ws, const SweepArgs&, cudaStream_
 cudaError_t launch_pack_blocks(const Batch&, const double* diag, const double* sup_d, const double* sub_d,
                                double* ws, cudaStream_t);
 
+cudaError_t launch_photo_tau(int batch, int nz, int ni, const VbPhoto& P, const double* y, const double* dz,
+                             double* tau, cudaStream_t);
+cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const double* tau, const double* ymix,
+                              const double* du_prev, double* aflux, double* sflux, double* dd, double* du,
+                              cudaStream_t);
+cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
+                           double* J_br_T, double* k, cudaStream_t);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
 
 }  // namespace vb

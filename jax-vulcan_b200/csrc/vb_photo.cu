@@ -1,0 +1,244 @@
+// Photochemistry kernels (reference photo.py):
+//   tau_kernel   optical depth, a top-down running sum per wavelength bin
+//                (photo.py:84-123);
+//   flux_kernel  two-stream Eddington flux: the down and the up recursions in
+//                z run in one thread per bin, all bins in parallel
+//                (photo.py:126-245);
+//   j_kernel     J-rates, a block reduction over bins per (layer, branch) with
+//                the two-resolution trapezoid correction, fused with the write
+//                of the photolysis rows of k (photo.py:309-351, 455-478).
+// Compiled with --fmad=false: products and sums round as the reference's
+// element-wise expressions do.
+#include <cuda_runtime.h>
+
+#include "vb_common.cuh"
+#include "vb_launch.cuh"
+
+namespace vb {
+
+constexpr int PHOTO_THREADS = 128;
+
+__global__ void __launch_bounds__(PHOTO_THREADS)
+tau_kernel(int nz, int ni, VbPhoto P, const double* __restrict__ y, const double* __restrict__ dz,
+           double* __restrict__ tau) {
+  const int b = blockIdx.y;
+  const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bin >= P.nbin) return;
+  const int nbin = P.nbin;
+  const double* yb = y + (int64_t)b * nz * ni;
+  const double* dzb = dz + (int64_t)b * nz;
+  const double* xT = P.absp_T_cross + (int64_t)b * P.T_stride;
+  double* tb = tau + (int64_t)b * (nz + 1) * nbin;
+  tb[(int64_t)nz * nbin + bin] = 0.0;
+  double acc = 0.0;
+  for (int j = nz - 1; j >= 0; --j) {
+    const double* yj = yb + (int64_t)j * ni;
+    double a = 0.0;
+    if (P.n_abs > 0) {
+      double s = 0.0;
+      for (int k = 0; k < P.n_abs; ++k) s = s + yj[P.absp_idx[k]] * P.absp_cross[(int64_t)k * nbin + bin];
+      a = s * dzb[j];
+    }
+    if (P.n_abs_T > 0) {
+      double s = 0.0;
+      for (int k = 0; k < P.n_abs_T; ++k)
+        s = s + yj[P.absp_T_idx[k]] * xT[((int64_t)k * nz + j) * nbin + bin];
+      a = a + s * dzb[j];
+    }
+    if (P.n_scat > 0) {
+      double s = 0.0;
+      for (int k = 0; k < P.n_scat; ++k) s = s + yj[P.scat_idx[k]] * P.scat_cross[(int64_t)k * nbin + bin];
+      a = a + s * dzb[j];
+    }
+    acc = (j == nz - 1) ? a : acc + a;
+    tb[(int64_t)j * nbin + bin] = acc;
+  }
+}
+
+struct TwoStream {
+  double chi, xi, phi, gp, gm;
+};
+
+// Two-stream coefficients of one layer (photo.py:150-203).
+__device__ inline TwoStream two_stream(const VbPhoto& P, const double* __restrict__ xT, int nz, int ni,
+                                       const double* ymix_j, int j, int bin, double dtau) {
+  const int nbin = P.nbin;
+  double tot_abs = 0.0, tot_scat = 0.0;
+  if (P.n_abs > 0) {
+    double s = 0.0;
+    for (int k = 0; k < P.n_abs; ++k) s = s + ymix_j[P.absp_idx[k]] * P.absp_cross[(int64_t)k * nbin + bin];
+    tot_abs = s;
+  }
+  if (P.n_abs_T > 0) {
+    double s = 0.0;
+    for (int k = 0; k < P.n_abs_T; ++k)
+      s = s + ymix_j[P.absp_T_idx[k]] * xT[((int64_t)k * nz + j) * nbin + bin];
+    tot_abs = tot_abs + s;
+  }
+  if (P.n_scat > 0) {
+    double s = 0.0;
+    for (int k = 0; k < P.n_scat; ++k) s = s + ymix_j[P.scat_idx[k]] * P.scat_cross[(int64_t)k * nbin + bin];
+    tot_scat = s;
+  }
+  double w0 = tot_scat / fmax(tot_abs + tot_scat, 1e-300);
+  if (isnan(w0)) w0 = 0.0;
+  w0 = fmin(w0, 1.0 - 1e-8);
+  const double mu_ang = -1.0 * P.mu_zenith;
+  const double edd = P.edd, ag0 = P.ag0;
+  double tran, zp, zm, ll, gp, gm;
+  if (ag0 == 0.0) {
+    const double sq = sqrt(1.0 - w0);
+    tran = exp(-1.0 / edd * sq * dtau);
+    zp = 0.5 * (1.0 + sq);
+    zm = 0.5 * (1.0 - sq);
+    ll = -1.0 * w0 / (1.0 / (mu_ang * mu_ang) - 1.0 / (edd * edd) * (1.0 - w0));
+    gp = 0.5 * (ll * (1.0 / edd + 1.0 / mu_ang));
+    gm = 0.5 * (ll * (1.0 / edd - 1.0 / mu_ang));
+  } else {
+    const double wa = 1.0 - w0 * ag0;
+    tran = exp(-1.0 / edd * sqrt(wa * (1.0 - w0)) * dtau);
+    const double rt = sqrt((1.0 - w0) / wa);
+    zp = 0.5 * (1.0 + rt);
+    zm = 0.5 * (1.0 - rt);
+    ll = ((1.0 - w0) * wa - 1.0) / (1.0 / (mu_ang * mu_ang) - 1.0 / (edd * edd) * (1.0 - w0) * wa);
+    gp = 0.5 * (ll * (1.0 / edd + 1.0 / (mu_ang * wa)) + w0 * ag0 * mu_ang / wa);
+    gm = 0.5 * (ll * (1.0 / edd - 1.0 / (mu_ang * wa)) - w0 * ag0 * mu_ang / wa);
+  }
+  TwoStream c;
+  c.chi = zm * zm * (tran * tran) - zp * zp;
+  c.xi = zp * zm * (1.0 - tran * tran);
+  c.phi = (zm * zm - zp * zp) * tran;
+  c.gp = gp;
+  c.gm = gm;
+  return c;
+}
+
+__global__ void __launch_bounds__(PHOTO_THREADS)
+flux_kernel(int nz, int ni, VbPhoto P, const double* __restrict__ tau, const double* __restrict__ ymix,
+            const double* __restrict__ du_prev, double* __restrict__ aflux, double* __restrict__ sflux,
+            double* __restrict__ dd, double* __restrict__ du) {
+  const int b = blockIdx.y;
+  const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bin >= P.nbin) return;
+  const int nbin = P.nbin;
+  const int64_t zb = (int64_t)b * (nz + 1) * nbin;
+  const double* tb = tau + zb;
+  const double* ym = ymix + (int64_t)b * nz * ni;
+  const double* xT = P.absp_T_cross + (int64_t)b * P.T_stride;
+  const double* up = du_prev + zb;
+  double* sb = sflux + zb;
+  double* ddb = dd + zb;
+  double* dub = du + zb;
+  double* ab = aflux + (int64_t)b * nz * nbin;
+  const double mu_ang = -1.0 * P.mu_zenith;
+  const double top = P.sflux_top[bin];
+  // direct beam (photo.py:173-174)
+  for (int j = 0; j <= nz; ++j) sb[(int64_t)j * nbin + bin] = top * exp(tb[(int64_t)j * nbin + bin] / mu_ang);
+  // down recursion (photo.py:208-223), dflux_u of the previous call
+  double d_next = 0.0;
+  ddb[(int64_t)nz * nbin + bin] = 0.0;
+  for (int j = nz - 1; j >= 0; --j) {
+    const double t0 = tb[(int64_t)j * nbin + bin], t1 = tb[(int64_t)(j + 1) * nbin + bin];
+    TwoStream c = two_stream(P, xT, nz, ni, ym + (int64_t)j * ni, j, bin, t0 - t1);
+    const double dir0 = sb[(int64_t)j * nbin + bin] * (-mu_ang);
+    const double dir1 = sb[(int64_t)(j + 1) * nbin + bin] * (-mu_ang);
+    const double i_d = c.phi * c.gm * dir1 - (c.chi * c.gm + c.xi * c.gp) * dir0;
+    const double v = (1.0 / c.chi) * (c.phi * d_next - c.xi * up[(int64_t)j * nbin + bin] + i_d / mu_ang);
+    ddb[(int64_t)j * nbin + bin] = v;
+    d_next = v;
+  }
+  // up recursion (photo.py:225-236) and the actinic flux (photo.py:238-244)
+  double u_prev = 0.0;
+  dub[bin] = 0.0;
+  const double conv = P.hc / P.bins[bin];
+  for (int j = 1; j <= nz; ++j) {
+    const double t0 = tb[(int64_t)(j - 1) * nbin + bin], t1 = tb[(int64_t)j * nbin + bin];
+    TwoStream c = two_stream(P, xT, nz, ni, ym + (int64_t)(j - 1) * ni, j - 1, bin, t0 - t1);
+    const double dir0 = sb[(int64_t)(j - 1) * nbin + bin] * (-mu_ang);
+    const double dir1 = sb[(int64_t)j * nbin + bin] * (-mu_ang);
+    const double i_u = c.phi * c.gp * dir0 - (c.xi * c.gm + c.chi * c.gp) * dir1;
+    const double v = (1.0 / c.chi) * (c.phi * u_prev - c.xi * ddb[(int64_t)j * nbin + bin] + i_u / mu_ang);
+    dub[(int64_t)j * nbin + bin] = v;
+    const double ave = 0.5 * (sb[(int64_t)(j - 1) * nbin + bin] + sb[(int64_t)j * nbin + bin]);
+    const double tot = ave + 0.5 * (u_prev + v + ddb[(int64_t)j * nbin + bin] + ddb[(int64_t)(j - 1) * nbin + bin]) / P.edd;
+    ab[(int64_t)(j - 1) * nbin + bin] = tot / conv;
+    u_prev = v;
+  }
+}
+
+// J of one (layer, branch): trapezoid over the two bin resolutions
+// (photo.py:316-349), then the k row (photo.py:465-478).
+__global__ void __launch_bounds__(PHOTO_THREADS)
+j_kernel(int nz, int nr, VbPhoto P, const double* __restrict__ aflux, double* __restrict__ J_br,
+         double* __restrict__ J_br_T, double* __restrict__ k) {
+  const int j = blockIdx.x, br = blockIdx.y, b = blockIdx.z;
+  const int nbin = P.nbin, d12 = P.din12;
+  const bool is_T = br >= P.n_br;
+  const int brl = is_T ? br - P.n_br : br;
+  const double* f = aflux + ((int64_t)b * nz + j) * nbin;
+  const double* c = is_T ? P.cross_J_T + (int64_t)b * P.T_stride_J + ((int64_t)brl * nz + j) * nbin
+                         : P.cross_J + (int64_t)brl * nbin;
+  double s1 = 0.0, s2 = 0.0;
+  for (int q = threadIdx.x; q < nbin; q += blockDim.x) {
+    double v = f[q] * c[q];
+    if (q < d12) s1 = s1 + v; else s2 = s2 + v;
+  }
+  __shared__ double red[2][PHOTO_THREADS / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    s1 = s1 + __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 = s2 + __shfl_xor_sync(0xffffffffu, s2, off);
+  }
+  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = s1; red[1][threadIdx.x >> 5] = s2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a1 = 0.0, a2 = 0.0;
+    for (int w = 0; w < PHOTO_THREADS / 32; ++w) { a1 = a1 + red[0][w]; a2 = a2 + red[1][w]; }
+    double J = 0.0;
+    if (d12 > 0) {
+      double J1 = a1 * P.dbin1;
+      J1 = J1 - 0.5 * (f[0] * c[0] + f[d12 - 1] * c[d12 - 1]) * P.dbin1;
+      J = J1;
+    }
+    if (d12 < nbin) {
+      double J2 = a2 * P.dbin2;
+      J2 = J2 - 0.5 * (f[d12] * c[d12] + f[nbin - 1] * c[nbin - 1]) * P.dbin2;
+      J = (d12 > 0) ? J + J2 : J2;
+    }
+    if (is_T) {
+      if (J_br_T) J_br_T[((int64_t)b * P.n_br_T + brl) * nz + j] = J;
+    } else {
+      if (J_br) J_br[((int64_t)b * P.n_br + brl) * nz + j] = J;
+    }
+    if (k) {
+      const int32_t* ridx = is_T ? P.br_T_re_idx : P.br_re_idx;
+      const uint8_t* act = is_T ? P.br_T_active : P.br_active;
+      if (ridx && act && act[brl]) k[((int64_t)b * (nr + 1) + ridx[brl]) * nz + j] = J * P.f_diurnal;
+    }
+  }
+}
+
+cudaError_t launch_photo_tau(int batch, int nz, int ni, const VbPhoto& P, const double* y, const double* dz,
+                             double* tau, cudaStream_t st) {
+  dim3 grid((P.nbin + PHOTO_THREADS - 1) / PHOTO_THREADS, batch);
+  tau_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, ni, P, y, dz, tau);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const double* tau, const double* ymix,
+                              const double* du_prev, double* aflux, double* sflux, double* dd, double* du,
+                              cudaStream_t st) {
+  dim3 grid((P.nbin + PHOTO_THREADS - 1) / PHOTO_THREADS, batch);
+  flux_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, ni, P, tau, ymix, du_prev, aflux, sflux, dd, du);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
+                           double* J_br_T, double* k, cudaStream_t st) {
+  if (P.n_br + P.n_br_T == 0) return cudaSuccess;
+  dim3 grid(nz, P.n_br + P.n_br_T, batch);
+  j_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, nr, P, aflux, J_br, J_br_T, k);
+  return cudaGetLastError();
+}
+
+}  // namespace vb

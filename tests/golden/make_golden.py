@@ -194,6 +194,75 @@ def photo_fixture(mods, syn):
     print("photo: ok", tau.shape)
 
 
+def chain_problem(mods):
+    """The open chain 0 -> A -> B -> 0 of reference tests/test_steady_state_grad.py:44-132."""
+    chem, jax_step = mods["chem"], mods["jax_step"]
+    ni, nr, PAD, T = 2, 6, 2, 1
+    r_idx = np.full((nr + 1, T), PAD, dtype=np.int64)
+    p_idx = np.full((nr + 1, T), PAD, dtype=np.int64)
+    r_st = np.zeros((nr + 1, T))
+    p_st = np.zeros((nr + 1, T))
+    p_idx[1, 0], p_st[1, 0] = 0, 1.0
+    r_idx[3, 0], r_st[3, 0], p_idx[3, 0], p_st[3, 0] = 0, 1.0, 1, 1.0
+    r_idx[5, 0], r_st[5, 0] = 1, 1.0
+    three = np.zeros(nr + 1, dtype=bool)
+    net = chem.NetworkArrays(ni=ni, nr=nr, reactant_idx=r_idx, product_idx=p_idx, reactant_stoich=r_st,
+                             product_stoich=p_st, is_three_body=three)
+    nz = 4
+    atm = dict(Kzz=np.full(nz - 1, 1e-2), Dzz=np.full((nz - 1, ni), 1e-3), dzi=np.full(nz - 1, 1.0),
+               vz=np.zeros(nz - 1), Hpi=np.full(nz - 1, 1.0), Ti=np.full(nz - 1, 1500.0), Tco=np.full(nz, 1500.0),
+               g=np.full(nz, 1.0), ms=np.full(ni, 1.0), alpha=np.zeros(ni), M=np.full(nz, 1.0),
+               vm=np.zeros((nz, ni)), vs=np.zeros((nz - 1, ni)), top_flux=np.zeros(ni), bot_flux=np.zeros(ni),
+               bot_vdep=np.zeros(ni), gas_indx_mask=np.ones(ni, dtype=bool), use_vm_mol=False,
+               use_settling=False, use_topflux=False, use_botflux=False)
+    k = np.zeros((nr + 1, nz))
+    k[1], k[3], k[5] = 1.0, 0.5, 0.3
+    y0 = np.zeros((nz, ni))
+    y0[:, 0], y0[:, 1] = 2.0, 3.3
+    tables = dict(r_idx=r_idx, p_idx=p_idx, r_st=r_st, p_st=p_st, three=three)
+    return net, atm, k, y0, tables
+
+
+def adjoint_fixture(mods, syn):
+    """Reference _ss_bwd (steady_state_grad.py:306-327) through the stand-in
+    (its jax.vjp of chem_rhs in k is exact: chem_rhs is linear in k)."""
+    import _jax_numpy_shim as shim
+    ssg, solver = mods["steady_state_grad"], mods["solver"]
+    out = {}
+    net, atm_d, k, y0, tab = chain_problem(mods)
+    atm = ref_atm(mods, atm_d)
+    y = y0.copy()
+    for it in range(100):
+        r = np.asarray(ssg.steady_state_residual(y.view(shim.JArr), k.view(shim.JArr), atm, net))
+        if np.max(np.abs(r)) < 1e-9:
+            break
+        diag, sup, sub = ssg._build_jacobian_blocks(y.view(shim.JArr), k.view(shim.JArr), atm, net)
+        y = y + np.asarray(solver.block_thomas_diag_offdiag(diag, sup, sub, -r))
+    v = np.zeros_like(y)
+    v[:, 1] = 2.0 * y[:, 1]                       # d/dy of sum(y[:,1]**2)
+    gk, _ = ssg._ss_bwd(atm, net, (k.view(shim.JArr), y.view(shim.JArr)), v.view(shim.JArr))
+    out.update(chain_y=y, chain_v=v, chain_gk=np.asarray(gk), chain_newton_iters=np.array(it))
+    for key, val in tab.items():
+        out["chain_" + key] = val
+    case = syn.make_case(seed=12, ni=12, n_fwd=30, nz=10, mild=True, k_range=(-40.0, 4.0), moldiff=True,
+                         fluxes=True, n_three_body=6)
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(case.net.text)
+        path = f.name
+    rn = mods["network"].parse_network(path)
+    os.unlink(path)
+    netc = mods["chem"].to_jax(rn)
+    atmc = ref_atm(mods, case.atm)
+    v2 = np.random.default_rng(12).normal(0.0, 1.0, case.y.shape) / np.abs(case.y)
+    gk2, _ = ssg._ss_bwd(atmc, netc, (case.k.view(shim.JArr), case.y.view(shim.JArr)), v2.view(shim.JArr))
+    out.update(case_net_text=np.array(case.net.text), case_y=case.y, case_k=case.k, case_v=v2,
+               case_gk=np.asarray(gk2))
+    for kk in ATM_KEYS + FLAG_KEYS:
+        out["case_atm_" + kk] = np.asarray(case.atm[kk])
+    np.savez_compressed(os.path.join(HERE, "adjoint.npz"), **out)
+    print("adjoint: ok, chain Newton iterations", it)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE", "/root/reference"))
@@ -217,6 +286,7 @@ def main():
     thomas_fixture(mods)
     contract_fixture(mods)
     photo_fixture(mods, syn)
+    adjoint_fixture(mods, syn)
 
 
 if __name__ == "__main__":

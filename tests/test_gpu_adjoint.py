@@ -1,0 +1,92 @@
+"""Implicit steady-state adjoint on the GPU against the reference-generated
+fixture (its own _ss_bwd) and the oracle.
+
+Tolerances: the k-gradient is a sum of signed terms that can cancel, so each
+entry must lie within 1e-10 of its rounding scale P'[r,z] sum|st*lambda|; the
+other cotangents within 1e-9 relative to the largest entry; lambda 1e-10
+relative per layer.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import ATM_KEYS, FLAG_KEYS, golden, load_pkg
+from oracle import adjoint as oa
+from test_oracle_golden import _chain, k_gradient_scale
+
+pytestmark = pytest.mark.gpu
+chem = load_pkg("chem")
+jstep = load_pkg("jax_step")
+ssg = load_pkg("steady_state_grad")
+syn = load_pkg("synthetic")
+
+
+def normwise(a, b):
+    return float(np.max(np.abs(np.asarray(a) - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_chain_gradient_matches_reference():
+    g = golden("adjoint.npz")
+    net, atm, k = _chain(g)
+    dn = chem.to_device(net)
+    cot = ssg.implicit_cotangents(g["chain_y"], k, jstep.atm_from_dict(atm), dn, g["chain_v"])
+    assert normwise(cot["k_arr"].cpu().numpy(), g["chain_gk"]) <= 1e-10
+    assert int(cot["status"].cpu()[0]) == 0
+
+
+def test_k_gradient_matches_reference_case():
+    g = golden("adjoint.npz")
+    net = load_pkg("network").parse_network_text(str(g["case_net_text"]))
+    atm = {kk: g["case_atm_" + kk] for kk in ATM_KEYS}
+    atm.update({kk: bool(g["case_atm_" + kk]) for kk in FLAG_KEYS})
+    dn = chem.to_device(net)
+    cot = ssg.implicit_cotangents(g["case_y"], g["case_k"], jstep.atm_from_dict(atm), dn, g["case_v"])
+    lam_ref, _ = oa.ss_bwd(g["case_y"], g["case_k"], atm, net, g["case_v"])
+    scale = k_gradient_scale(g["case_y"], atm["M"], lam_ref, net)
+    assert np.all(np.abs(cot["k_arr"].cpu().numpy() - g["case_gk"]) <= 1e-10 * scale)
+
+
+def test_all_supported_leaves_batched_against_oracle():
+    net = syn.make_network(44, 30, 185, n_three_body=20)
+    dn = chem.to_device(net.tables)
+    cases = [syn.make_case(seed=50 + b, net=net, nz=24, mild=True, k_range=(-40.0, 4.0), moldiff=True, fluxes=True)
+             for b in range(3)]
+    Y = np.stack([c.y for c in cases])
+    K = np.stack([c.k for c in cases])
+    A = {kk: (np.stack([c.atm[kk] for c in cases]) if not isinstance(cases[0].atm[kk], bool)
+              else cases[0].atm[kk]) for kk in cases[0].atm}
+    V = np.random.default_rng(5).normal(0.0, 1.0, Y.shape) / np.abs(Y)
+    cot = ssg.implicit_cotangents(Y, K, jstep.atm_from_dict(A), dn, V)
+    for b, c in enumerate(cases):
+        lam, _ = oa.ss_bwd(c.y, c.k, c.atm, net.tables, V[b])
+        lam_g = cot["lambda"][b].cpu().numpy()
+        assert normwise(lam_g, lam) <= 1e-10
+        # the VJP kernels given the GPU's lambda
+        ref = oa.vjp_from_lambda(c.y, c.k, c.atm, net.tables, lam_g)
+        scale = k_gradient_scale(c.y, c.atm["M"], lam_g, net.tables)
+        assert np.all(np.abs(cot["k_arr"][b].cpu().numpy() - ref["k_arr"]) <= 1e-12 * scale)
+        for leaf in ("M", "Kzz", "top_flux", "bot_flux", "bot_vdep"):
+            assert normwise(cot[leaf][b].cpu().numpy(), ref[leaf]) <= 1e-10, leaf
+
+
+def test_autograd_function_chain():
+    """torch.autograd through DifferentiableSteadyState gives the reference
+    custom_vjp gradient of sum(y[:,1]**2) (tests/test_steady_state_grad.py)."""
+    g = golden("adjoint.npz")
+    net, atm, k = _chain(g)
+    dn = chem.to_device(net)
+    kt = torch.as_tensor(k, device="cuda").requires_grad_(True)
+    y = torch.as_tensor(g["chain_y"], device="cuda")
+    ys = ssg.differentiable_steady_state(kt, y, jstep.atm_from_dict(atm), dn)
+    (ys[:, 1] ** 2).sum().backward()
+    assert normwise(kt.grad.cpu().numpy(), g["chain_gk"]) <= 1e-10
+
+
+def test_residual_gate():
+    g = golden("adjoint.npz")
+    net, atm, k = _chain(g)
+    dn = chem.to_device(net)
+    r = ssg.validate_steady_state_solution(g["chain_y"], k, jstep.atm_from_dict(atm), dn)
+    assert r < 1e-9
+    with pytest.raises(ValueError):
+        ssg.validate_steady_state_solution(g["chain_y"] * 1.5, k, jstep.atm_from_dict(atm), dn)

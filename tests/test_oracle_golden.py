@@ -135,3 +135,69 @@ def test_synthetic_network_balances_elements():
         lhs = sum(net.compo[i] * s for i, s in zip(t.reactant_idx[r], t.reactant_stoich[r]) if i < t.ni)
         rhs = sum(net.compo[i] * s for i, s in zip(t.product_idx[r], t.product_stoich[r]) if i < t.ni)
         np.testing.assert_array_equal(lhs, rhs)
+
+
+def _chain(g):
+    NT = load_pkg("network").NetworkTables
+    net = NT(species=("A", "B"), ni=2, nr=6, reactant_idx=g["chain_r_idx"], product_idx=g["chain_p_idx"],
+             reactant_stoich=g["chain_r_st"], product_stoich=g["chain_p_st"], is_three_body=g["chain_three"],
+             is_photo=np.zeros(7, bool))
+    nz, ni = 4, 2
+    atm = dict(Kzz=np.full(nz - 1, 1e-2), Dzz=np.full((nz - 1, ni), 1e-3), dzi=np.full(nz - 1, 1.0),
+               vz=np.zeros(nz - 1), Hpi=np.full(nz - 1, 1.0), Ti=np.full(nz - 1, 1500.0), Tco=np.full(nz, 1500.0),
+               g=np.full(nz, 1.0), ms=np.full(ni, 1.0), alpha=np.zeros(ni), M=np.full(nz, 1.0),
+               vm=np.zeros((nz, ni)), vs=np.zeros((nz - 1, ni)), top_flux=np.zeros(ni), bot_flux=np.zeros(ni),
+               bot_vdep=np.zeros(ni), gas_indx_mask=np.ones(ni, dtype=bool), use_vm_mol=False,
+               use_settling=False, use_topflux=False, use_botflux=False)
+    k = np.zeros((7, nz))
+    k[1], k[3], k[5] = 1.0, 0.5, 0.3
+    return net, atm, k
+
+
+def test_adjoint_known_answer_chain():
+    """Reference tests/test_steady_state_grad.py: Newton steady state of the
+    open chain (well mixed: [A]=k1/k3=2, [B]=k1/k5=3.33), the implicit gradient
+    equals the reference's _ss_bwd and central finite differences."""
+    from oracle import adjoint as oa
+    g = golden("adjoint.npz")
+    net, atm, k = _chain(g)
+    y0 = np.zeros((4, 2))
+    y0[:, 0], y0[:, 1] = 2.0, 3.3
+    y, _ = oa.newton_steady_state(y0, k, atm, net)
+    close(y, g["chain_y"], 1e-10)
+    np.testing.assert_allclose(y[:, 0], 2.0, rtol=1e-2)
+    np.testing.assert_allclose(y[:, 1], 1.0 / 0.3, rtol=1e-2)
+    lam, cot = oa.ss_bwd(y, k, atm, net, g["chain_v"])
+    close(cot["k_arr"], g["chain_gk"], 1e-10, floor=1e-12)
+    eps = 1e-6
+    fd = np.zeros_like(k)
+    for i, z in [(i, z) for i in range(7) for z in range(4) if k[i, z] > 0]:
+        kp, km = k.copy(), k.copy()
+        kp[i, z] += eps
+        km[i, z] -= eps
+        yp, _ = oa.newton_steady_state(y0, kp, atm, net)
+        ym, _ = oa.newton_steady_state(y0, km, atm, net)
+        fd[i, z] = (np.sum(yp[:, 1] ** 2) - np.sum(ym[:, 1] ** 2)) / (2 * eps)
+    assert np.max(np.abs(cot["k_arr"] - fd)) / np.max(np.abs(fd)) < 5e-4
+
+
+def test_adjoint_k_gradient_matches_reference():
+    from oracle import adjoint as oa
+    g = golden("adjoint.npz")
+    net = load_pkg("network").parse_network_text(str(g["case_net_text"]))
+    from conftest import ATM_KEYS, FLAG_KEYS
+    atm = {kk: g["case_atm_" + kk] for kk in ATM_KEYS}
+    atm.update({kk: bool(g["case_atm_" + kk]) for kk in FLAG_KEYS})
+    lam, cot = oa.ss_bwd(g["case_y"], g["case_k"], atm, net, g["case_v"])
+    scale = k_gradient_scale(g["case_y"], atm["M"], lam, net)
+    assert np.all(np.abs(cot["k_arr"] - g["case_gk"]) <= 1e-12 * scale)
+
+
+def k_gradient_scale(y, M, lam, net):
+    """Rounding scale of d(lam . f)/dk[r, z]: P'[z, r] * sum_s |st * lam| (the
+    gradient is a sum of signed terms that can cancel)."""
+    Pp = orc.rates(y, M, np.ones((net.nr + 1, y.shape[0])), net)          # [nz, nr+1]
+    lp = np.concatenate([np.abs(lam), np.zeros((y.shape[0], 1))], axis=1)
+    s = (np.abs(net.product_stoich)[None] * lp[:, net.product_idx]).sum(2) + \
+        (np.abs(net.reactant_stoich)[None] * lp[:, net.reactant_idx]).sum(2)
+    return (np.abs(Pp) * s).T
