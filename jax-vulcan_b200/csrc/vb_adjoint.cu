@@ -76,11 +76,7 @@ vjp_transport_kernel(Batch B, const double* __restrict__ y, const double* __rest
   AtmRef a = atm_ref(atm + g.atm, nz, ni);
   const double* yb = y + g.z0 * ni;
   const double* lb = ws_view(ws, g, ni, B.ld).k1;
-  for (int j = threadIdx.x; j < nz; j += blockDim.x) {
-    double tmp[VB_MAX_NI];
-    for (int i = 0; i < ni; ++i) tmp[i] = a.gas[i] != 0.0 ? yb[(int64_t)j * ni + i] : 0.0;
-    ysum[j] = pairwise_sum(tmp, ni);
-  }
+  for (int j = threadIdx.x; j < nz; j += blockDim.x) ysum[j] = pairwise_sum_masked(yb + (int64_t)j * ni, a.gas, ni);
   __syncthreads();
   // stencil-row spacing h_j: dz_ave inside, dzi at the two boundary rows
   auto h_of = [&](int j) {

@@ -26,18 +26,19 @@ struct LayerSmem {
   double* scal;    // [8]: ysum(j-1), ysum(j), ysum(j+1)
 };
 
-__host__ __device__ inline size_t layer_smem_bytes(int ni, int nr, int T, bool jac) {
-  size_t d = 3 * (size_t)(ni + 1) + (nr + 1) + (jac ? (size_t)(nr + 1) * T + (size_t)ni * ni : 0) +
+// jac: drate buffer for the Jacobian; jsm: also a shared-memory Jacobian block.
+__host__ __device__ inline size_t layer_smem_bytes(int ni, int nr, int T, bool jac, bool jsm = false) {
+  size_t d = 3 * (size_t)(ni + 1) + (nr + 1) + (jac ? (size_t)(nr + 1) * T : 0) + (jsm ? (size_t)ni * ni : 0) +
              4 * (size_t)ni + 8;
   return d * sizeof(double);
 }
 
-__device__ inline LayerSmem carve(double* s, int ni, int nr, int T, bool jac) {
+__device__ inline LayerSmem carve(double* s, int ni, int nr, int T, bool jac, bool jsm = false) {
   LayerSmem L;
   L.y3 = s; s += 3 * (ni + 1);
   L.rate = s; s += nr + 1;
   L.drate = s; s += jac ? (nr + 1) * T : 0;
-  L.jac = s; s += jac ? ni * ni : 0;
+  L.jac = s; s += jsm ? ni * ni : 0;
   L.diff = s; s += ni;
   L.diagd = s; s += ni;
   L.part = s; s += 2 * ni;
@@ -104,15 +105,23 @@ __device__ inline void species_sums(const NetDev& net, const double* rate, doubl
 // owns a contiguous run of destinations holding about the same number of
 // contributions (jac_split), each summed in the reference's scatter order.
 // Requires blockDim.x == LAYER_THREADS.
-__device__ inline void layer_jacobian(const NetDev& net, const double* drate, double* jac) {
+template <typename Store>
+__device__ inline void layer_jacobian_each(const NetDev& net, const double* drate, Store store) {
   const int d0 = net.jac_split[threadIdx.x], d1 = net.jac_split[threadIdx.x + 1];
   int e = net.jac_ptr[d0];
+  int row = d0 / net.ni, col = d0 - row * net.ni;
   for (int d = d0; d < d1; ++d) {
     const int e1 = net.jac_ptr[d + 1];
     double J = 0.0;
     for (; e < e1; ++e) J = J + net.jac_coef[e] * drate[net.jac_idx[e]];
-    jac[d] = J;
+    store(row, col, J);
+    if (++col == net.ni) { col = 0; ++row; }
   }
+}
+
+__device__ inline void layer_jacobian(const NetDev& net, const double* drate, double* jac) {
+  const int ni = net.ni;
+  layer_jacobian_each(net, drate, [&](int row, int col, double J) { jac[row * ni + col] = J; });
 }
 
 // Loads state rows j-1..j+1 (stage 2: yk2 = y + k1/r) and their gas sums.
@@ -137,11 +146,7 @@ __device__ inline void load_rows(const double* y, const double* k1, const double
     int w = threadIdx.x;
     int jj = j - 1 + w;
     double s = 0.0;
-    if (jj >= 0 && jj < nz) {
-      double tmp[VB_MAX_NI];
-      for (int i = 0; i < ni; ++i) tmp[i] = gas[i] != 0.0 ? L.y3[w * (ni + 1) + i] : 0.0;
-      s = pairwise_sum(tmp, ni);
-    }
+    if (jj >= 0 && jj < nz) s = pairwise_sum_masked(L.y3 + w * (ni + 1), gas, ni);
     L.scal[w] = s;
   }
   __syncthreads();
@@ -193,7 +198,7 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
 
 // Stage-1 assembly: rmod[j] = rhs(y), inv[j] = c0*I - J - diag(diag_d),
 // supn[j] = -sup_d, subn[j-1] = -sub_d, with fix_mask (jax_step.py:263-298).
-__global__ void __launch_bounds__(LAYER_THREADS)
+__global__ void __launch_bounds__(LAYER_THREADS, 3)
 stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
               const double* __restrict__ dt, const double* __restrict__ atm, int flags,
               const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, const double* __restrict__ adj_v) {
@@ -216,64 +221,62 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   __shared__ double supb[VB_MAX_NI], subb[VB_MAX_NI];
   __syncthreads();
   species_sums(net, L.rate, L.part);
-  layer_jacobian(net, L.drate, L.jac);
   layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);
   __syncthreads();
+  // the Jacobian gather writes each block entry in its final form
+  double* blk = w.inv + (int64_t)j * ni * B.ld;
+  const int ld = B.ld;
+  const double bot = (j == 0 && (flags & VB_USE_BOTFLUX)) ? 1.0 : 0.0;
   if (adj) {
     // steady_state_grad.py:153-175: diag = J + diag(A_eddy + A_mol) (+ deposition
     // at the bottom), sup_d = B[:-1], sub_d = C[1:] (no c0, not negated)
+    layer_jacobian_each(net, L.drate, [&](int row, int col, double J) {
+      double v = J;
+      if (row == col) {
+        v = v + L.diagd[row];
+        if (j == 0) v = v + (bot != 0.0 ? -a.vdep[row] / a.dzi[0] : 0.0);
+      }
+      blk[(int64_t)row * ld + col] = v;
+    });
     for (int i = threadIdx.x; i < ni; i += blockDim.x) {
       w.rmod[(int64_t)j * ni + i] = adj_v[g.z0 * ni + (int64_t)j * ni + i];
       if (j < nz - 1) w.supn[(int64_t)j * ni + i] = supb[i];
       if (j > 0) w.subn[(int64_t)(j - 1) * ni + i] = subb[i];
     }
-    double* blk = w.inv + (int64_t)j * ni * B.ld;
-    for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) {
-      int row = d / ni, col = d - row * ni;
-      double v = L.jac[d];
-      if (row == col) {
-        v = v + L.diagd[row];
-        if (j == 0) v = v + ((flags & VB_USE_BOTFLUX) ? -a.vdep[row] / a.dzi[0] : 0.0);
-      }
-      blk[(int64_t)row * B.ld + col] = v;
-    }
     return;
   }
+  layer_jacobian_each(net, L.drate, [&](int row, int col, double J) {
+    double v = (row == col ? c0 : 0.0) - J;
+    if (row == col) {
+      // jax_step.py:283,288: the deposition term joins diag_d before -diag_d is added
+      double dd = L.diagd[row];
+      if (j == 0) dd = dd + (bot != 0.0 ? -a.vdep[row] / a.dzi[0] : 0.0);
+      v = v + (-dd);
+    }
+    if (fm && fm[row]) v = (row == col) ? c0 : 0.0;
+    blk[(int64_t)row * ld + col] = v;
+  });
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
     bool fixed = fm && fm[i];
     if (fixed) v = 0.0;
     w.rmod[(int64_t)j * ni + i] = v;
     if (j < nz - 1) {
-      double s = -supb[i];
-      if (fixed) s = 0.0;
-      w.supn[(int64_t)j * ni + i] = s;
+      double s2 = -supb[i];
+      if (fixed) s2 = 0.0;
+      w.supn[(int64_t)j * ni + i] = s2;
     }
     if (j > 0) {
-      double s = -subb[i];
-      if (fixed) s = 0.0;
-      w.subn[(int64_t)(j - 1) * ni + i] = s;
+      double s2 = -subb[i];
+      if (fixed) s2 = 0.0;
+      w.subn[(int64_t)(j - 1) * ni + i] = s2;
     }
-  }
-  double* blk = w.inv + (int64_t)j * ni * B.ld;
-  for (int d = threadIdx.x; d < ni * ni; d += blockDim.x) {
-    int row = d / ni, col = d - row * ni;
-    double J = L.jac[d];
-    double v = (row == col ? c0 : 0.0) - J;
-    if (row == col) {
-      // jax_step.py:283,288: the deposition term joins diag_d before -diag_d is added
-      double dd = L.diagd[row];
-      if (j == 0) dd = dd + ((flags & VB_USE_BOTFLUX) ? -a.vdep[row] / a.dzi[0] : 0.0);
-      v = v + (-dd);
-    }
-    if (fm && fm[row]) v = (row == col) ? c0 : 0.0;
-    blk[(int64_t)row * B.ld + col] = v;
   }
 }
 
 // Stage-2 right-hand side: rmod[j] = rhs(yk2) - 2/(r dt) k1[j] with
 // yk2 = y + k1/r (jax_step.py:303-310).
-__global__ void __launch_bounds__(LAYER_THREADS)
+__global__ void __launch_bounds__(LAYER_THREADS, 3)
 stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
               const double* __restrict__ dt, const double* __restrict__ atm, int flags,
               const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, double* __restrict__ resid) {
@@ -317,7 +320,7 @@ chem_kernel(NetDev net, int nz, const double* __restrict__ y, const double* __re
   const int b = blockIdx.y, j = blockIdx.x;
   const int ni = net.ni;
   bool want_jac = jac != nullptr;
-  LayerSmem L = carve(smem, ni, net.nr, net.T, want_jac);
+  LayerSmem L = carve(smem, ni, net.nr, net.T, want_jac, want_jac);
   const double* yrow = y + ((int64_t)b * nz + j) * ni;
   for (int i = threadIdx.x; i <= ni; i += blockDim.x) L.y3[i] = i < ni ? yrow[i] : 1.0;
   __syncthreads();
@@ -385,7 +388,7 @@ cudaError_t launch_stage2(const NetDev& net, const Batch& B, const double* y, co
 
 cudaError_t launch_chem(const NetDev& net, int batch, int nz, const double* y, const double* M,
                         const double* k, double* dydt, double* jac, cudaStream_t st) {
-  size_t sm = layer_smem_bytes(net.ni, net.nr, net.T, jac != nullptr);
+  size_t sm = layer_smem_bytes(net.ni, net.nr, net.T, jac != nullptr, jac != nullptr);
   cudaFuncSetAttribute(chem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(nz, batch);
   chem_kernel<<<grid, LAYER_THREADS, sm, st>>>(net, nz, y, M, k, dydt, jac);

@@ -32,6 +32,27 @@ __device__ inline double pairwise_sum(const double* a, int n) {
   return res;
 }
 
+// pairwise_sum of where(mask != 0, a, 0) without a staging copy.
+__device__ inline double pairwise_sum_masked(const double* a, const double* mask, int n) {
+  auto at = [&](int i) { return mask[i] != 0.0 ? a[i] : 0.0; };
+  if (n < 8) {
+    double r = 0.0;
+    for (int i = 0; i < n; ++i) r = r + at(i);
+    return r;
+  }
+  double r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = at(k);
+  int i = 8;
+  for (; i < n - (n % 8); i += 8) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r[k] = r[k] + at(i + k);
+  }
+  double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+  for (; i < n; ++i) res = res + at(i);
+  return res;
+}
+
 // y**st as NumPy evaluates it for the integer stoichiometries of a network
 // (st = 1, 2 exactly; other values through pow).
 __device__ __forceinline__ double pow_st(double y, double st) {
