@@ -301,12 +301,12 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       }
     }
     // ================================================================ X = U^{-1} Y
+    __syncthreads();   // readers of the forward phase's last buffer are done
     for (int w = NW - 1; w >= 0; --w) {
       const int k0 = w * RPW;
       if (k0 >= n) continue;
       const int kw = min(RPW, n - k0);
-      double* Yb = (w & 1) ? Pn1 : Pn0;
-      __syncthreads();   // previous readers of this buffer are done
+      double* Yb = (w & 1) ? Pn1 : Pn0;   // last read two panels ago, before the previous barrier
       if (warp == w) {
 #pragma unroll
         for (int r = RPW - 1; r >= 0; --r) {
