@@ -194,6 +194,26 @@ int vb_profile_read(double* ms, int64_t* counts, int n);
  * FP64 FMA peak that bounds the block factorisation. */
 int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream);
 
+/* Ros2 step with no caller workspace and no allocation. No counterpart in the
+ * reference: it serves callers that cannot cudaMalloc (a host runtime that
+ * owns all device memory and hands a foreign call no scratch). Same launch
+ * sequence and results as vb_ros2_step for a uniform batch (zoff = NULL),
+ * with the workspace in a module-scope device array of
+ * VB_STATIC_SCRATCH_BYTES that every device loading the library holds until
+ * the process exits. Batches whose vb_ros2_workspace_bytes(batch, nz, ni,
+ * NULL) exceeds that maximum are rejected with VB_ERR_ARG. The first call on
+ * each device looks the array's device address up (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture.
+ * All calls on a device share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU (streams without an ordering
+ * between them) race. Nothing in the array needs to start at zero (every
+ * value is written before it is read); status[B] is cleared by each call. */
+#define VB_STATIC_SCRATCH_BYTES ((size_t)64 << 20)
+int vb_ros2_step_static(const VbNet* net, int batch, int nz,
+                        const double* y, const double* k, const double* dt,
+                        const double* atm, int32_t atm_flags, const uint8_t* fix_mask,
+                        double* sol, double* delta, int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

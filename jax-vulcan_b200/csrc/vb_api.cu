@@ -4,6 +4,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -61,6 +62,33 @@ static int cuda_fail(cudaError_t e, const char* where) {
     cudaError_t _e = (call);                       \
     if (_e != cudaSuccess) return cuda_fail(_e, where); \
   } while (0)
+
+// ---- scratch of vb_ros2_step_static
+// One copy of this array lives on every device that loads the library, for
+// the life of the process. Host code may not use `g_step_scratch` as an
+// address: the device address is looked up once per device with that device
+// current (cudaGetSymbolAddress) and cached.
+static __device__ __align__(256) double g_step_scratch[VB_STATIC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+constexpr int kScratchDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[kScratchDevices] = {};
+}  // namespace
+
+static int static_scratch(double** out) {
+  int dev = 0;
+  VB_CHECK(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kScratchDevices) return fail(VB_ERR_ARG, "device ordinal beyond the static scratch table");
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    VB_CHECK(cudaGetSymbolAddress(&p, g_step_scratch), "cudaGetSymbolAddress(static scratch)");
+    g_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_ptr[dev];
+  return VB_OK;
+}
 
 extern "C" {
 
@@ -415,6 +443,41 @@ int vb_profile_read(double* ms, int64_t* counts, int n) {
 int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream) {
   if (!out || blocks < 1 || threads < 32 || iters < 1) return fail(VB_ERR_ARG, "bad probe arguments");
   VB_CHECK(vb::launch_fp64_probe(out, blocks, threads, iters, (cudaStream_t)stream), "fp64 probe");
+  return VB_OK;
+}
+
+int vb_ros2_step_static(const VbNet* net, int batch, int nz, const double* y, const double* k, const double* dt,
+                        const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol, double* delta,
+                        int32_t* status, void* stream) {
+  if (!net || !y || !k || !dt || !atm || !sol || !delta || !status) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  const size_t need = vb_ros2_workspace_bytes(batch, nz, net->dev.ni, nullptr);
+  if (need > VB_STATIC_SCRATCH_BYTES)
+    return fail(VB_ERR_ARG, "vb_ros2_step_static: batch needs " + std::to_string(need) +
+                                " scratch bytes, above the static maximum of " +
+                                std::to_string((size_t)VB_STATIC_SCRATCH_BYTES) +
+                                " (use vb_ros2_step with a caller workspace)");
+  double* ws = nullptr;
+  if (int rc = static_scratch(&ws)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = make_batch(net, batch, nz, nullptr);
+  // Every scratch value is written before it is read within the call, so
+  // only the status words start at zero.
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  VB_CHECK(vb::launch_stage1(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage1");
+  VB_CHECK(vb::launch_factor(B, ws, status, 1, st), "factor");
+  vb::SweepArgs a{};
+  a.mode = 1;
+  a.status = status;
+  VB_CHECK(vb::launch_sweep(B, ws, a, st), "back sweep 1");
+  VB_CHECK(vb::launch_stage2(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage2");
+  a.mode = 0;
+  VB_CHECK(vb::launch_sweep(B, ws, a, st), "forward sweep 2");
+  a.mode = 2;
+  a.y = y;
+  a.sol = sol;
+  a.delta = delta;
+  VB_CHECK(vb::launch_sweep(B, ws, a, st), "back sweep 2");
   return VB_OK;
 }
 
