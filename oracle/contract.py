@@ -9,9 +9,10 @@ Restates, from reference `outer_loop.py`:
 * ``step_size``      -> `_step_size` (`:181-193`)
 * ``clip``           -> `_make_clip_fn` (`:196-224`)
 * ``aggregate_delta`` -> `_make_aggregate_delta_fn` (`:227-250`)
-* ``controller_step`` -> the accept / force-accept / time / dt logic of
-  `body_fn` (`:733-768`, `:1031-1038`) for a run without photo, condensation,
-  atmosphere refresh or adaptive rtol.
+* ``body_update`` / ``attempt`` -> the state update of one attempt of
+  `body_fn` (`:715-1100`): accept / reject / force-accept, hydrostatic
+  rebalance, counters, adaptive rtol and dt, for a run without photo,
+  condensation, atmosphere refresh, ion balance or bottom pins.
 """
 from __future__ import annotations
 
@@ -56,29 +57,95 @@ def aggregate_delta(sol, delta_arr, ymix_old, mtol, atol, zero_bot_row=False, co
     return np.max(ratio)
 
 
-def controller_step(state, k, atm, net, compo, atom_ini, p):
-    """One attempt of the adaptive loop. ``state``: dict(y, ymix, dt, t,
-    atom_loss_prev, retry). ``p``: rtol, atol, mtol, pos_cut, nega_cut,
-    loss_eps, dt_var_min, dt_var_max, dt_min, dt_max, max_retries.
-    Returns the new state dict plus ``accept``, ``force``, ``delta``."""
-    y, dt = state["y"], state["dt"]
-    sol, delta_arr = ros2.ros2_step(y, k, dt, atm, net)
-    sol_c, ymix_new, _, _ = clip(sol, state["ymix"], p["mtol"], p["pos_cut"], p["nega_cut"])
-    al = atom_loss(sol_c, compo, atom_ini)
-    delta = aggregate_delta(sol_c, delta_arr, state["ymix"], p["mtol"], p["atol"])
-    accept = bool(np.all(sol_c >= 0) and np.max(np.abs(al - state["atom_loss_prev"])) < p["loss_eps"]
-                  and delta <= p["rtol"])
-    next_reject = dt * p["dt_var_min"]
-    force = (not accept) and (next_reject < p["dt_min"] or state["retry"] >= p["max_retries"])
+BODY_FIELDS = ["y", "y_prev", "ymix", "dt", "t", "delta", "accept_count", "retry_count", "atom_loss",
+               "atom_loss_prev", "nega_count", "loss_count", "delta_count", "small_y", "nega_y", "rtol",
+               "loss_criteria"]
+
+
+def mix_from_y(y, gas=None):
+    """`_mix_from_y` (`outer_loop.py:593-600`): y / ysum over gas species (all without a mask)."""
+    if gas is None:
+        return y / np.sum(y, axis=1, keepdims=True)
+    return y / np.sum(np.where(np.asarray(gas, bool)[None, :], y, 0.0), axis=1, keepdims=True)
+
+
+def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partial=False,
+                zero_bot_row=False, fix_mask=None, fix_y=None):
+    """State after one attempt of the reference loop body given the step's
+    (sol, delta_arr): fixed species (`outer_loop.py:733-739`), clip, atom loss,
+    error norm (`:741-743`), accept / force-accept (`:745-756`), reject
+    counters (`:758-764`), time (`:766-768`), hydrostatic rebalance
+    (`:844-853`), next y / ymix / atom loss (`:899-914`), counters
+    (`:916-917`, `:1062-1066`), adaptive rtol (`:990-1020`) and dt
+    (`:1022-1031`). Photo, condensation, atmosphere refresh, ion balance,
+    bottom pins, the convergence ring and save_evolution are not restated.
+
+    ``s``: dict with ``BODY_FIELDS``; ``p``: loss_eps, pos_cut, nega_cut, mtol,
+    atol, dt_var_min, dt_var_max, dt_min, dt_max, batch_max_retries,
+    use_adapt_rtol, rtol_min, rtol_max, adapt_rtol_dec_period,
+    adapt_rtol_inc_period, adapt_rtol_dec, adapt_rtol_inc, adapt_rtol_loss_mul,
+    adapt_rtol_inc_loss_thresh. ``gas``: gas-species mask when non-gas species
+    are present (the ysum of clip and mix), else None.
+    """
+    if fix_mask is not None:
+        sol = np.where(fix_mask, fix_y, sol)
+        delta_arr = np.where(fix_mask, 0.0, delta_arr)
+    sol_clip, ymix_new, small_inc, nega_inc = clip(sol, s["ymix"], p["mtol"], p["pos_cut"], p["nega_cut"], gas)
+    al_new = atom_loss(sol_clip, compo, atom_ini)
+    delta = aggregate_delta(sol_clip, delta_arr, s["ymix"], p["mtol"], p["atol"], zero_bot_row)
+    rtol = s["rtol"]
+    loss_diff = np.max(np.abs(al_new - s["atom_loss_prev"]))
+    accept = bool(np.all(sol_clip >= 0) & (loss_diff < p["loss_eps"]) & (delta <= rtol))
+    next_reject = s["dt"] * p["dt_var_min"]
+    force = bool((next_reject < p["dt_min"]) | (s["retry_count"] >= p["batch_max_retries"])) and not accept
     do_acc = accept or force
-    t_next = state["t"] + (p["dt_min"] if force else dt) if do_acc else state["t"]
-    dt_norm = step_size(dt, delta, p["rtol"], p["dt_var_min"], p["dt_var_max"], p["dt_min"], p["dt_max"])
-    dt_force = step_size(p["dt_min"], delta, p["rtol"], p["dt_var_min"], p["dt_var_max"], p["dt_min"], p["dt_max"])
-    dt_next = dt_force if force else (dt_norm if accept else next_reject)
-    out = dict(state)
-    if do_acc:
-        out.update(y=sol_c, ymix=ymix_new, atom_loss_prev=al, retry=0)
+    reject = not do_acc
+    too_big = bool(delta > rtol)
+    any_neg = bool(np.any(sol_clip < 0))
+    t_next = s["t"] + (p["dt_min"] if force else s["dt"]) if do_acc else s["t"]
+
+    bal_full = M[:, None] * ymix_new
+    if hydro_partial:
+        bal = np.where(np.asarray(gas, bool)[None, :], bal_full, sol_clip)
     else:
-        out.update(retry=state["retry"] + 1)
-    out.update(t=t_next, dt=float(dt_next), accept=accept, force=force, delta=float(delta))
+        bal = bal_full
+    ymix_bal = mix_from_y(bal, gas)
+    al_bal = atom_loss(bal, compo, atom_ini)
+    if force:
+        y_next, ymix_next, al_next = np.where(s["y_prev"] < 0, 0.0, s["y_prev"]), s["ymix"], s["atom_loss_prev"]
+    elif accept:
+        y_next, ymix_next, al_next = bal, ymix_bal, al_bal
+    else:
+        y_next, ymix_next, al_next = s["y_prev"], s["ymix"], s["atom_loss"]
+
+    out = dict(s)
+    out.update(y=y_next, ymix=ymix_next, atom_loss=al_next, t=t_next, delta=delta)
+    if do_acc:
+        out.update(y_prev=y_next, atom_loss_prev=al_next, accept_count=s["accept_count"] + 1, retry_count=0,
+                   small_y=s["small_y"] + small_inc, nega_y=s["nega_y"] + nega_inc)
+    else:
+        out.update(retry_count=s["retry_count"] + 1)
+    out.update(delta_count=s["delta_count"] + int(reject and too_big),
+               nega_count=s["nega_count"] + int(reject and not too_big and any_neg),
+               loss_count=s["loss_count"] + int(reject and not too_big and not any_neg))
+
+    lc = s["loss_criteria"]
+    if p["use_adapt_rtol"] and do_acc:
+        max_loss = np.max(np.abs(al_new))
+        acc = s["accept_count"]
+        if acc % p["adapt_rtol_dec_period"] == 0 and max_loss >= lc:
+            rtol = max(rtol * p["adapt_rtol_dec"], p["rtol_min"])
+            lc = lc * p["adapt_rtol_loss_mul"]
+        if acc % p["adapt_rtol_inc_period"] == 0 and acc > 0 and max_loss < p["adapt_rtol_inc_loss_thresh"]:
+            rtol = min(rtol * p["adapt_rtol_inc"], p["rtol_max"])
+    dt_norm = step_size(s["dt"], delta, rtol, p["dt_var_min"], p["dt_var_max"], p["dt_min"], p["dt_max"])
+    dt_force = step_size(p["dt_min"], delta, rtol, p["dt_var_min"], p["dt_var_max"], p["dt_min"], p["dt_max"])
+    out.update(dt=float(dt_force if force else (dt_norm if accept else next_reject)), rtol=rtol, loss_criteria=lc)
+    out["_accept"], out["_force"] = accept, force
     return out
+
+
+def attempt(s, k, atm, net, compo, atom_ini, p, **kw):
+    """One attempt: the Ros2 step from ``s["y"]`` then ``body_update``."""
+    sol, delta_arr = ros2.ros2_step(s["y"], k, s["dt"], atm, net, fix_mask=kw.get("fix_mask"))
+    return body_update(s, sol, delta_arr, atm["M"], compo, atom_ini, p, **kw)

@@ -17,6 +17,7 @@ on the generator reproducing bit-identical floats elsewhere.
 """
 from __future__ import annotations
 
+import __future__
 import argparse
 import ast
 import importlib
@@ -24,6 +25,7 @@ import os
 import sys
 import tempfile
 import types
+from typing import NamedTuple, Optional
 
 import numpy as np
 
@@ -155,6 +157,179 @@ def contract_fixture(mods):
     print("contract: ok")
 
 
+BODY_FIELDS = ["y", "y_prev", "ymix", "dt", "t", "delta", "accept_count", "retry_count", "atom_loss",
+               "atom_loss_prev", "nega_count", "loss_count", "delta_count", "small_y", "nega_y", "rtol",
+               "loss_criteria"]
+
+
+def load_runner(ref, mods, shim):
+    """`_make_runner` of outer_loop.py with its state/statics types, compiled
+    from the reference source. `jax.jit` is the identity and
+    `jax.lax.while_loop` runs the body exactly once, so one runner call is one
+    accept / reject / force-accept attempt of the reference loop
+    (`outer_loop.py:715-1100`)."""
+    src = open(os.path.join(ref, "outer_loop.py")).read()
+    tree = ast.parse(src)
+    want = {"JaxIntegState", "_Statics", "_compute_atom_loss", "_step_size", "_make_clip_fn",
+            "_make_aggregate_delta_fn", "_make_runner"}
+    body = [n for n in tree.body if isinstance(n, (ast.FunctionDef, ast.ClassDef)) and n.name in want]
+    lax_once = types.SimpleNamespace(while_loop=lambda cond, fn, init: fn(init))
+    ns = {"jnp": shim.jnp, "jax": types.SimpleNamespace(jit=lambda f: f, lax=lax_once), "np": np,
+          "NamedTuple": NamedTuple, "Optional": Optional,
+          "jax_ros2_step": mods["jax_step"].jax_ros2_step, "AtmStatic": mods["jax_step"].AtmStatic}
+    code = compile(ast.Module(body=body, type_ignores=[]), "outer_loop.py", "exec",
+                   flags=__future__.annotations.compiler_flag, dont_inherit=True)
+    exec(code, ns)
+    return ns
+
+
+BODY_PARAMS = dict(loss_eps=0.1, pos_cut=0.0, nega_cut=-1.0, mtol=1e-22, atol=0.1, dt_var_min=0.5,
+                   dt_var_max=2.0, dt_min=1e-14, dt_max=1e4, batch_max_retries=8, use_adapt_rtol=False,
+                   rtol_min=0.02, rtol_max=1.0, adapt_rtol_dec_period=5, adapt_rtol_inc_period=10,
+                   adapt_rtol_dec=0.5, adapt_rtol_inc=1.5, adapt_rtol_loss_mul=10.0,
+                   adapt_rtol_inc_loss_thresh=1e-3, use_fix_species=False, post_conden_rtol=0.2)
+
+
+def body_fixture(mods, syn, ref, shim):
+    """One attempt of the reference adaptive loop per case, from a state we
+    choose, covering accept, the three reject kinds, both force-accept
+    triggers, the gas-only hydrostatic rebalance, fixed species, the
+    bottom-row mask, adaptive rtol, plus a chain of attempts."""
+    ns = load_runner(ref, mods, shim)
+    JS, ST = ns["JaxIntegState"], ns["_Statics"]
+    J = lambda a: np.asarray(a).view(shim.JArr)  # noqa: E731
+    case = syn.make_case(seed=6, ni=12, n_fwd=30, nz=10, moldiff=True, fluxes=True, mild=True,
+                         k_range=(-40.0, 4.0))
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(case.net.text)
+        path = f.name
+    rn = mods["network"].parse_network(path)
+    os.unlink(path)
+    net = mods["chem"].to_jax(rn)
+    atm = ref_atm(mods, case.atm)
+    nz, ni = case.y.shape
+    compo = case.net.compo
+    y0 = case.y.copy()
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * 1.0000001
+    conv_step = 4
+
+    def statics(p):
+        f = {k: None for k in ST._fields}
+        f.update(compo_arr=J(compo), atom_ini_arr=J(atom_ini), initial_rtol=0.2, conv_step=conv_step,
+                 count_min=1, count_max=10 ** 6, conv_stall_window=10 ** 6, runtime=1e30, trun_min=0.0,
+                 st_factor=0.5, yconv_cri=0.01, yconv_min=0.1, slope_cri=1e-4, flux_cri=0.1,
+                 mtol_conv=1e-20, conver_ignore_mask=J(np.zeros(ni, bool)),
+                 condense_zero_conv_mask=J(np.zeros((nz, ni), bool)), n_0=J(case.atm["M"]),
+                 Kzz=J(case.atm["Kzz"]), use_photo=False, use_atm_refresh=False, use_conden=False,
+                 ini_update_photo_frq=1, final_update_photo_frq=1, update_frq=1,
+                 initial_loss_criteria=1e-3, photo_switch_longdy_thresh=0.0,
+                 photo_switch_longdydt_thresh=0.0, hycean_pin_time=1e30, use_ion=False, e_idx=0,
+                 charge_arr=J(np.zeros(ni)), use_fix_all_bot=False, bottom_n=J(np.zeros(ni)),
+                 use_fix_sp_bot=False, fix_sp_bot_idx=J(np.zeros(0, np.int32)),
+                 fix_sp_bot_mix=J(np.zeros(0)), use_fix_H2He=False, h2_idx=-1, he_idx=-1,
+                 fix_species_from_coldtrap_lev=False, fix_species_idx=J(np.zeros(0, np.int32)),
+                 fix_species_sat_mix=J(np.zeros((0, nz))), fix_species_wholecol=J(np.zeros(0, bool)),
+                 save_evolution=False, save_evo_frq=1, save_evo_n_max=1)
+        f.update(p)
+        return ST(**f)
+
+    def mix(y, gas=None):
+        g = np.ones(ni, bool) if gas is None else gas
+        return y / np.sum(np.where(g[None, :], y, 0.0), axis=1, keepdims=True)
+
+    def state(y, ymix, dt, rtol, **over):
+        al = (np.einsum("zi,ia->a", y, compo) - atom_ini) / atom_ini
+        f = {k: None for k in JS._fields}
+        z2 = J(np.zeros((1, 1)))
+        f.update(y=J(y), y_prev=J(y), ymix=J(ymix), dt=np.float64(dt), t=np.float64(1e3),
+                 delta=np.float64(0.0), accept_count=np.int32(7), retry_count=np.int32(0), atom_loss=J(al),
+                 atom_loss_prev=J(al), nega_count=np.int32(1), loss_count=np.int32(2),
+                 delta_count=np.int32(3), small_y=np.float64(1.5), nega_y=np.float64(2.5), k_arr=J(case.k),
+                 tau=z2, aflux=z2, sflux=z2, dflux_d=z2, dflux_u=z2, prev_aflux=z2,
+                 aflux_change=np.float64(0.0), J_br=z2, J_br_T=z2, Jion_br=z2, g=J(case.atm["g"]),
+                 mu=J(np.ones(nz)), Hp=J(np.ones(nz)), dz=J(np.ones(nz)), zco=J(np.zeros(nz + 1)),
+                 dzi=J(case.atm["dzi"]), Hpi=J(case.atm["Hpi"]), top_flux=J(case.atm["top_flux"]),
+                 vs=J(case.atm["vs"]), y_time_ring=J(np.zeros((conv_step, nz, ni))),
+                 t_time_ring=J(np.zeros(conv_step)), longdy=np.float64(1.0), longdydt=np.float64(1.0),
+                 where_varies_most=J(np.zeros((nz, ni))), longdy_seen_min=np.float64(np.inf),
+                 count_since_new_min=np.int32(0), rtol=np.float64(rtol), loss_criteria=np.float64(1e-3),
+                 update_photo_frq=np.int32(1), is_final_photo_frq=np.bool_(False),
+                 fix_species_started=np.bool_(False), fix_y=J(np.zeros((nz, ni))),
+                 fix_mask=J(np.zeros((nz, ni), bool)), fix_pfix_idx=J(np.zeros(0, np.int32)),
+                 h2he_pinned=np.bool_(False), h2he_mix=J(np.zeros(2)), y_evo=J(np.zeros((1, nz, ni))),
+                 t_evo=J(np.zeros(1)), evo_idx=np.int32(0), chunk_target=np.int32(10 ** 6))
+        f.update(over)
+        return JS(**f)
+
+    gas_all = np.ones(ni, bool)
+    gas_part = gas_all.copy()
+    gas_part[[2, 7]] = False
+    y_neg = y0.copy()
+    y_neg[4, 3] = -1e5
+    y_small = y0.copy()
+    y_small[[1, 5, 8], [6, 0, 11]] = -0.3
+    rng = np.random.default_rng(61)
+    fm = rng.random((nz, ni)) < 0.1
+    cases = {
+        # name: (y, rtol, dt, params, runner options, state overrides)
+        "accept": (y0, 0.2, 1e-6, {}, {}, {}),
+        "reject_delta": (y0, 1e-12, 1e-6, {}, {}, {}),
+        "reject_loss": (y0, 0.2, 1e-6, dict(loss_eps=1e-300), {}, {}),
+        "reject_nega": (y_neg, 0.2, 1e-6, {}, {}, {}),
+        "force_retry": (y0, 1e-30, 1e-6, {}, {}, dict(retry_count=np.int32(8))),
+        "force_underflow": (y0, 1e-30, 1.5e-14, {}, {}, {}),
+        "gas_hydro": (y0, 0.2, 1e-6, dict(pos_cut=1e3), dict(non_gas=True, gas=gas_part, hydro_partial=True),
+                      {}),
+        "clip_small": (y_small, 0.2, 1e-6, dict(pos_cut=50.0), {}, {}),
+        "fix": (y0, 0.2, 1e-6, dict(use_fix_species=True), {},
+                dict(fix_mask=J(fm), fix_y=J(y0 * 1.01), fix_species_started=np.bool_(True))),
+        "botrow_adapt": (y0, 0.2, 1e-6, dict(use_adapt_rtol=True), dict(zero_bot_row=True),
+                         dict(accept_count=np.int32(10), loss_criteria=np.float64(1e-12))),
+    }
+    out = dict(net_text=np.array(case.net.text), k=case.k, compo=compo, atom_ini=atom_ini,
+               case_names=np.array(list(cases) + ["chain"]))
+    for kk in ATM_KEYS + FLAG_KEYS:
+        out["atm_" + kk] = np.asarray(case.atm[kk])
+    for k2, v in BODY_PARAMS.items():
+        out["param_" + k2] = np.array(v)
+
+    def run(name, y, rtol, dt, pover, ropt, sover, n_attempts=1):
+        p = dict(BODY_PARAMS)
+        p.update(pover)
+        gas = ropt.get("gas", gas_all)
+        runner = ns["_make_runner"](net, statics(p), ropt.get("non_gas", False), J(gas),
+                                    ropt.get("zero_bot_row", False), J(np.zeros((nz, ni), bool)),
+                                    ropt.get("hydro_partial", False), 1e30, 1e30)
+        s = state(y, mix(np.abs(y), gas), dt, rtol, **sover)
+        pre = {f: np.asarray(getattr(s, f)) for f in BODY_FIELDS}
+        for kk, vv in pre.items():
+            out[f"{name}_in_{kk}"] = vv
+        for kk in ("fix_mask", "fix_y"):
+            out[f"{name}_in_{kk}"] = np.asarray(getattr(s, kk))
+        out[f"{name}_opt"] = np.array([float(pover.get("use_fix_species", False)),
+                                       float(ropt.get("non_gas", False)), float(ropt.get("hydro_partial", False)),
+                                       float(ropt.get("zero_bot_row", False)),
+                                       float(pover.get("use_adapt_rtol", False)),
+                                       float(p["loss_eps"]), float(p["pos_cut"])])
+        out[f"{name}_gas"] = gas
+        hist = []
+        for _ in range(n_attempts):
+            prev_acc, prev_retry = int(s.accept_count), int(s.retry_count)
+            s = runner(s, atm)
+            hist.append((int(s.accept_count) - prev_acc, int(s.retry_count), int(s.delta_count),
+                         int(s.nega_count), int(s.loss_count)))
+        for f_ in BODY_FIELDS:
+            out[f"{name}_out_{f_}"] = np.asarray(getattr(s, f_))
+        out[f"{name}_hist"] = np.array(hist, np.int64)
+        print(f"body {name}: attempts {hist} dt {float(s.dt):.3e} delta {float(s.delta):.3e}")
+
+    for name, (y, rtol, dt, pover, ropt, sover) in cases.items():
+        run(name, y, rtol, dt, pover, ropt, sover)
+    run("chain", y0, 1e-3, 3e-5, {}, {}, {}, n_attempts=8)
+    np.savez_compressed(os.path.join(HERE, "body.npz"), **out)
+    print("body: ok")
+
+
 def photo_fixture(mods, syn):
     photo = mods["photo"]
     net = syn.make_network(21, 16, 40, n_photo=6)
@@ -266,9 +441,18 @@ def adjoint_fixture(mods, syn):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE", "/root/reference"))
+    ap.add_argument("--only", default="", help="comma-separated fixture names (default: all)")
     args = ap.parse_args()
-    mods, _ = load_reference(args.reference)
+    mods, shim = load_reference(args.reference)
     syn = importlib.import_module("jax-vulcan_b200.synthetic")
+    only = set(filter(None, args.only.split(",")))
+    if only:
+        for name in sorted(only):
+            if name == "body":
+                body_fixture(mods, syn, args.reference, shim)
+            else:
+                raise SystemExit(f"--only supports: body (got {name})")
+        return
     mild = dict(mild=True, k_range=(-40.0, 4.0))
     step_fixture(mods, "plain", syn.make_case(seed=5, ni=12, n_fwd=30, nz=10, **mild), n_steps=3)
     step_fixture(mods, "moldiff", syn.make_case(seed=6, ni=12, n_fwd=30, nz=10, moldiff=True, **mild))
@@ -287,6 +471,7 @@ def main():
     contract_fixture(mods)
     photo_fixture(mods, syn)
     adjoint_fixture(mods, syn)
+    body_fixture(mods, syn, args.reference, shim)
 
 
 if __name__ == "__main__":

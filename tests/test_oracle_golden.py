@@ -10,7 +10,7 @@ bit; the assertions allow 1e-13 relative for platform LAPACK differences.
 import numpy as np
 import pytest
 
-from conftest import STEP_CASES, golden, golden_step, load_pkg
+from conftest import BODY_FIELDS, STEP_CASES, body_kwargs, golden, golden_body, golden_step, load_pkg
 from oracle import contract as oc
 from oracle import photo as op
 from oracle import ros2 as orc
@@ -104,6 +104,30 @@ def test_contract_functions():
     dtn = [oc.step_size(dt, dl, 0.2, 0.5, 2.0, 1e-14, 1e-2) for dt, dl in zip(g["dts"], g["deltas"])]
     close(dtn, g["dt_next"], 0.0)
     close(oc.atom_loss(np.abs(g["sol"]), g["compo"], g["atom_ini"]), g["atom_loss"], 1e-15)
+
+
+def check_body_state(got, ref, rtol):
+    """Counters and decisions exact; floating state within ``rtol``."""
+    for f in ("accept_count", "retry_count", "nega_count", "loss_count", "delta_count"):
+        assert int(got[f]) == int(ref[f]), (f, got[f], ref[f])
+    for f in BODY_FIELDS:
+        if f.endswith("_count"):
+            continue
+        close(got[f], ref[f], rtol, floor=1e-30)
+
+
+def test_loop_body_attempts():
+    """The restated loop body against one attempt of the reference runner
+    (`outer_loop.py:715-1100`) per case, and a chain of eight attempts."""
+    net, atm, compo, atom_ini, k, params, cases = golden_body()
+    for name, c in cases.items():
+        p, kw = body_kwargs(c, params)
+        s = dict(c["inp"])
+        for i in range(len(c["hist"])):
+            prev = (s["accept_count"], s["retry_count"])
+            s = oc.attempt(s, k, atm, net, compo, atom_ini, p, **kw)
+            assert s["accept_count"] - prev[0] == c["hist"][i][0], (name, i)
+        check_body_state(s, c["out"], 1e-13)
 
 
 def _ph(g):
