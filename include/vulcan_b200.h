@@ -139,6 +139,50 @@ int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const d
                double* g_Kzz, double* g_top, double* g_bot, double* g_vdep, int32_t* status, void* workspace,
                size_t workspace_bytes, void* stream);
 
+/* Loop body of the adaptive runner (reference outer_loop.py:715-1100, the
+ * decision part of body_fn): given a Ros2 step's sol / delta_arr, applies the
+ * fixed-species override, clip (:196-224), atom loss (:171-178), error norm
+ * (:227-250), accept / force-accept / reject (:745-768), hydrostatic
+ * rebalance (:844-853), next state (:899-917), counters (:1062-1066),
+ * adaptive rtol (:990-1020) and the next dt (:181-193, :1022-1031), per
+ * atmosphere, on the device. Photo, condensation, atmosphere refresh, ion
+ * balance, bottom pins and the convergence ring are not part of it. */
+#define VB_LOOP_MAX_ATOMS 16
+#define VB_LOOP_HYDRO_PARTIAL 1  /* rebalance gas species only (use_condense) */
+#define VB_LOOP_ZERO_BOT_ROW 2   /* drop the bottom layer from the error norm */
+#define VB_LOOP_ADAPT_RTOL 4     /* adaptive rtol */
+typedef struct VbLoopParams {
+  int32_t n_atoms;               /* 1..VB_LOOP_MAX_ATOMS */
+  int32_t batch_max_retries;
+  int32_t flags;                 /* VB_LOOP_* */
+  int32_t adapt_rtol_dec_period, adapt_rtol_inc_period;
+  int32_t reserved;
+  double loss_eps, pos_cut, nega_cut, mtol, atol;
+  double dt_var_min, dt_var_max, dt_min, dt_max;
+  double rtol_min, rtol_max, adapt_rtol_dec, adapt_rtol_inc, adapt_rtol_loss_mul, adapt_rtol_inc_loss_thresh;
+} VbLoopParams;
+/* Per-atmosphere scalars of the loop carry (JaxIntegState fields of the same
+ * names), device memory, updated in place; dt is a separate [B] array so the
+ * same buffer feeds vb_ros2_step. last_decision: 0 reject, 1 accept,
+ * 2 force-accept. */
+typedef struct VbLoopScalars {
+  double t, delta, small_y, nega_y, rtol, loss_criteria;
+  int32_t accept_count, retry_count, nega_count, loss_count, delta_count, last_decision;
+} VbLoopScalars;
+/* Device arrays: gas_mask [ni] uint8 or NULL (non-gas species present: the
+ * ysums of clip and mix run over gas species), compo [ni][n_atoms],
+ * atom_ini [B][n_atoms], fix_mask [B][nz][ni] uint8 and fix_y [B][nz][ni]
+ * (both NULL without fixed species), sol / delta_arr [B][nz][ni] (inputs;
+ * must not alias the state), state: y, y_prev, ymix [B][nz][ni] (y may equal
+ * y_prev), atom_loss, atom_loss_prev [B][n_atoms], dt [B], scalars [B]. The layer
+ * densities n_0 are the atmosphere blob's M. zoff as in vb_ros2_step (nz is
+ * then the maximum layer count). */
+int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopParams* params,
+                 const double* atm, const uint8_t* gas_mask, const double* compo, const double* atom_ini,
+                 const uint8_t* fix_mask, const double* fix_y, const double* sol, const double* delta_arr,
+                 double* y, double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
+                 double* dt, VbLoopScalars* scalars, void* stream);
+
 /* Photochemistry (reference photo.py). Cross sections and branch tables are
  * device arrays shared by the batch, except the temperature-dependent tables
  * absp_T_cross [n_abs_T][nz][nbin] and cross_J_T [n_br_T][nz][nbin], which

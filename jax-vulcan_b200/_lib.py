@@ -50,6 +50,7 @@ SIGNATURES = {
     "vb_profile_read": (_i, [_p, _p, _i]),
     "vb_fp64_probe": (_i, [_p, _i, _i, _i, _p]),
     "vb_ros2_step_static": (_i, [_p, _i, _i, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _p]),
+    "vb_loop_body": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
 }
 
 PROFILE_SITES = ["stage1_assembly", "factor", "back_sweep_1", "stage2_assembly", "forward_sweep_2",

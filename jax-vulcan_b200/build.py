@@ -26,6 +26,7 @@ UNITS = {
     "vb_chem.cu": ["--fmad=false"],
     "vb_photo.cu": ["--fmad=false"],
     "vb_adjoint.cu": [],
+    "vb_control.cu": ["--fmad=false"],
 }
 
 

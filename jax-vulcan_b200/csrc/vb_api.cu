@@ -446,6 +446,33 @@ int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream)
   return VB_OK;
 }
 
+int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopParams* params, const double* atm,
+                 const uint8_t* gas_mask, const double* compo, const double* atom_ini, const uint8_t* fix_mask,
+                 const double* fix_y, const double* sol, const double* delta_arr, double* y, double* y_prev,
+                 double* ymix, double* atom_loss, double* atom_loss_prev, double* dt, VbLoopScalars* scalars,
+                 void* stream) {
+  if (!params || !atm || !compo || !atom_ini || !sol || !delta_arr || !y || !y_prev || !ymix || !atom_loss ||
+      !atom_loss_prev || !dt || !scalars)
+    return fail(VB_ERR_ARG, "null argument");
+  if ((fix_mask == nullptr) != (fix_y == nullptr)) return fail(VB_ERR_ARG, "fix_mask and fix_y go together");
+  if (batch < 1 || nz < 2 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "batch >= 1, nz >= 2, 1 <= ni <= 128");
+  const VbLoopParams& p = *params;
+  if (p.n_atoms < 1 || p.n_atoms > VB_LOOP_MAX_ATOMS) return fail(VB_ERR_ARG, "n_atoms must be in [1, 16]");
+  if ((p.flags & VB_LOOP_ADAPT_RTOL) && (p.adapt_rtol_dec_period < 1 || p.adapt_rtol_inc_period < 1))
+    return fail(VB_ERR_ARG, "adaptive rtol periods must be >= 1");
+  if (2 * (size_t)nz * sizeof(double) > 200 * 1024) return fail(VB_ERR_ARG, "nz too large for the loop body");
+  vb::Batch B{};
+  B.count = batch;
+  B.nz = nz;
+  B.ni = ni;
+  B.ld = vb::round_even(ni);
+  B.zoff = zoff;
+  VB_CHECK(vb::launch_loop_body(B, p, gas_mask, compo, atom_ini, atm, fix_mask, fix_y, sol, delta_arr, y, y_prev,
+                                ymix, atom_loss, atom_loss_prev, dt, scalars, (cudaStream_t)stream),
+           "loop body");
+  return VB_OK;
+}
+
 int vb_ros2_step_static(const VbNet* net, int batch, int nz, const double* y, const double* k, const double* dt,
                         const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol, double* delta,
                         int32_t* status, void* stream) {

@@ -50,5 +50,10 @@ cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const
 cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
                            double* J_br_T, double* k, cudaStream_t);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
+cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_t* gas, const double* compo,
+                             const double* atom_ini, const double* atm, const uint8_t* fix_mask,
+                             const double* fix_y, const double* sol, const double* delta, double* y,
+                             double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
+                             double* dt, VbLoopScalars* st, cudaStream_t stream);
 
 }  // namespace vb

@@ -1,0 +1,166 @@
+"""The loop body on the GPU (``vb_loop_body`` after ``vb_ros2_step``) against
+one attempt of the reference runner per fixture case (``tests/golden/body.npz``,
+made by running the reference `outer_loop.py` body) and against the oracle on
+batches where atmospheres take different decisions in the same launch.
+
+Tolerances: every decision (accept / reject kind / force-accept) and counter
+must be equal. The state inherits the step's error bound
+``|sol - ref| <= 1e-10 |sol_ref|``: y, y_prev and ymix within 1e-10 relative;
+the error norm ``delta = max(delta_arr / sol)`` within 1e-10 absolute (the
+step bound divided by sol); dt, which scales as ``delta^-1/2`` unless clipped,
+within ``0.5e-10 / delta`` relative; atom losses (already relative to the
+initial atom totals) within 1e-10 absolute; small_y / nega_y within 1e-10
+relative; t and rtol within 1e-15 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import BODY_FIELDS, body_kwargs, golden_body, load_pkg
+from oracle import contract as oc
+
+pytestmark = pytest.mark.gpu
+
+chem = load_pkg("chem")
+jstep = load_pkg("jax_step")
+loop = load_pkg("outer_loop")
+syn = load_pkg("synthetic")
+
+COUNTERS = ("accept_count", "retry_count", "nega_count", "loss_count", "delta_count")
+
+
+def statics_of(p, kw):
+    return loop.LoopStatics(**{k: p[k] for k in (
+        "loss_eps", "pos_cut", "nega_cut", "mtol", "atol", "dt_var_min", "dt_var_max", "dt_min", "dt_max",
+        "batch_max_retries", "use_adapt_rtol", "rtol_min", "rtol_max", "adapt_rtol_dec_period",
+        "adapt_rtol_inc_period", "adapt_rtol_dec", "adapt_rtol_inc", "adapt_rtol_loss_mul",
+        "adapt_rtol_inc_loss_thresh")}, zero_bot_row=kw["zero_bot_row"], hydro_partial=kw["hydro_partial"])
+
+
+def state_of(inp):
+    """LoopState of a batch of fixture/oracle states (list of dicts)."""
+    st = lambda f: np.stack([np.asarray(s[f]) for s in inp])  # noqa: E731
+    return loop.LoopState(st("y"), st("ymix"), st("dt"), st("atom_loss"), st("atom_loss_prev"),
+                          y_prev=st("y_prev"), t=st("t"), rtol=st("rtol"), loss_criteria=st("loss_criteria"),
+                          counters={c: st(c) for c in COUNTERS}, small_y=st("small_y"), nega_y=st("nega_y"))
+
+
+def check_state(got, b, ref, what):
+    for c in COUNTERS:
+        assert int(got[c][b]) == int(ref[c]), (what, c, got[c][b], ref[c])
+
+    def rel(a, r, floor=1e-300):
+        return float(np.max(np.abs(np.asarray(a) - r) / np.maximum(np.abs(r), floor), initial=0.0))
+
+    for f in ("y", "y_prev", "ymix"):
+        assert rel(got[f][b], ref[f], 1e-30) <= 1e-10, (what, f, rel(got[f][b], ref[f], 1e-30))
+    assert abs(float(got["delta"][b]) - ref["delta"]) <= 1e-10, (what, "delta", got["delta"][b], ref["delta"])
+    dt_tol = 0.5e-10 / max(ref["delta"], 1e-300) + 1e-15
+    assert rel(got["dt"][b], ref["dt"]) <= dt_tol, (what, "dt", got["dt"][b], ref["dt"])
+    for f in ("atom_loss", "atom_loss_prev"):
+        assert np.max(np.abs(got[f][b] - ref[f])) <= 1e-10, (what, f)
+    for f in ("small_y", "nega_y"):
+        assert rel(got[f][b], ref[f]) <= 1e-10, (what, f)
+    for f in ("t", "rtol", "loss_criteria"):
+        assert rel(got[f][b], ref[f]) <= 1e-15, (what, f, got[f][b], ref[f])
+
+
+def test_loop_body_matches_reference_runner():
+    net, atm, compo, atom_ini, k, params, cases = golden_body()
+    dn = chem.to_device(net)
+    A = jstep.atm_from_dict(atm)
+    for name, c in cases.items():
+        p, kw = body_kwargs(c, params)
+        runner = loop.AdaptiveRunner(dn, A, statics_of(p, kw), compo, atom_ini, gas_mask=kw["gas"])
+        state = state_of([c["inp"]])
+        fm = fy = None
+        if "fix_mask" in kw:
+            fm, fy = kw["fix_mask"][None], kw["fix_y"][None]
+        decisions = []
+        for _ in range(len(c["hist"])):
+            runner.attempt(state, k[None], fix_mask=fm, fix_y=fy)
+            decisions.append(int(state.scalars_host()["last_decision"][0]))
+        got = state.snapshot()
+        assert [d > 0 for d in decisions] == [bool(h[0]) for h in c["hist"]], (name, decisions)
+        check_state(got, 0, c["out"], name)
+
+
+def test_batched_atmospheres_decide_independently():
+    """vmap semantics: three atmospheres in one launch, with rtol / dt /
+    retry budgets that send them down different branches on the same
+    attempt, each against the oracle run on its own."""
+    net, atm, compo, atom_ini, k, params, cases = golden_body()
+    dn = chem.to_device(net)
+    A = jstep.atm_from_dict(atm)
+    base = dict(cases["accept"]["inp"])
+    inp = [dict(base, rtol=0.2, dt=1e-6), dict(base, rtol=1e-3, dt=3e-5),
+           dict(base, rtol=1e-30, dt=1e-6, retry_count=6)]
+    p, kw = body_kwargs(cases["accept"], params)
+    runner = loop.AdaptiveRunner(dn, A, statics_of(p, kw), compo, atom_ini, batch=3)
+    state = state_of(inp)
+    K = np.broadcast_to(k, (3,) + k.shape).copy()
+    refs = [dict(s) for s in inp]
+    seen = set()
+    for it in range(6):
+        runner.attempt(state, K)
+        dec = state.scalars_host()["last_decision"]
+        for b in range(3):
+            refs[b] = oc.attempt(refs[b], k, atm, net, compo, atom_ini, p, **kw)
+            want = 2 if refs[b]["_force"] else (1 if refs[b]["_accept"] else 0)
+            assert int(dec[b]) == want, (it, b, dec, want)
+            seen.add(want)
+    got = state.snapshot()
+    for b in range(3):
+        check_state(got, b, refs[b], f"atmosphere {b}")
+    assert seen == {0, 1, 2}
+
+
+def test_loop_at_benchmark_shape():
+    """ni=69, nz=120 (the benchmark network shape), 2 atmospheres, 3 attempts
+    with rtol tight enough to reject, against the oracle."""
+    case = syn.make_case(seed=31, mild=True, k_range=(-40.0, 4.0), moldiff=True)
+    net, atm = case.net.tables, case.atm
+    dn = chem.to_device(net)
+    compo = case.net.compo
+    y0 = case.y
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * (1 + 1e-7)
+    al0 = (np.einsum("zi,ia->a", y0, compo) - atom_ini) / atom_ini
+    ymix0 = y0 / y0.sum(axis=1, keepdims=True)
+    s0 = dict(y=y0, y_prev=y0, ymix=ymix0, dt=1e-6, t=0.0, delta=0.0, atom_loss=al0, atom_loss_prev=al0,
+              small_y=0.0, nega_y=0.0, rtol=0.05, loss_criteria=1e-3, accept_count=0, retry_count=0,
+              nega_count=0, loss_count=0, delta_count=0)
+    inp = [s0, dict(s0, rtol=1e-6, dt=3e-6)]
+    p = dict(oc_params())
+    A = {kk: (np.stack([atm[kk]] * 2) if not isinstance(atm[kk], bool) else atm[kk]) for kk in atm}
+    runner = loop.AdaptiveRunner(dn, jstep.atm_from_dict(A), loop.LoopStatics(**p), compo, atom_ini, batch=2)
+    state = state_of(inp)
+    K = np.stack([case.k] * 2)
+    refs = [dict(s) for s in inp]
+    for it in range(3):
+        runner.attempt(state, K)
+        for b in range(2):
+            refs[b] = oc.attempt(refs[b], case.k, atm, net, compo, atom_ini, dict(p, use_adapt_rtol=False))
+    got = state.snapshot()
+    for b in range(2):
+        check_state(got, b, refs[b], f"atmosphere {b}")
+
+
+def oc_params():
+    return dict(loss_eps=0.1, pos_cut=0.0, nega_cut=-1.0, mtol=1e-22, atol=0.1, dt_var_min=0.5, dt_var_max=2.0,
+                dt_min=1e-14, dt_max=1e4, batch_max_retries=8, rtol_min=0.02, rtol_max=1.0,
+                adapt_rtol_dec_period=5, adapt_rtol_inc_period=10, adapt_rtol_dec=0.5, adapt_rtol_inc=1.5,
+                adapt_rtol_loss_mul=10.0, adapt_rtol_inc_loss_thresh=1e-3)
+
+
+def test_loop_body_rejects_bad_arguments():
+    L = load_pkg("_lib").lib()
+    p = loop.LoopStatics().params(1)
+    p.n_atoms = 0
+    import ctypes as C
+    dummy = C.c_void_p(16)  # never dereferenced: argument checks come first
+    rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, None, None, dummy, dummy,
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None)
+    assert rc == 1 and b"n_atoms" in L.vb_last_error()
+    rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, dummy, None, dummy, dummy,
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None)
+    assert rc == 1 and b"fix_mask" in L.vb_last_error()
