@@ -4,10 +4,10 @@ Workload (one "step" = one Ros2 step of every atmosphere of the batch):
 config-0-shaped atmospheres - a seeded element-balanced C/H/O/N network with
 ni=69 species and 700+700 reactions, nz=120 layers, rate constants
 log-uniform in [1e-40, 1e-8], mixing ratios log-uniform in [1e-20, 1],
-dt = 1e-6 s - batched B atmospheres per GPU (seeded per atmosphere and per
-rank), FP64. The same inputs are stepped repeatedly (as the reference's
-benchmarks/bench_step.py does). Per-step inputs (rates 172 MB, solver
-workspace 590 MB at B=128) exceed the 126 MB L2.
+dt = 1e-6 s - batched B atmospheres per GPU (default 148, one per SM; seeded
+per atmosphere and per rank), FP64. The same inputs are stepped repeatedly
+(as the reference's benchmarks/bench_step.py does). Per-step inputs (rates
+199 MB, solver workspace 737 MB at B=148) exceed the 126 MB L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl b200|reference]
 
@@ -69,7 +69,7 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -189,9 +189,9 @@ def fp64_peak_tflops(lib, torch, stream):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--batch", type=int, default=148)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -318,9 +318,24 @@ def main():
 
     peak64 = fp64_peak_tflops(L, torch, sh)
     ni, nz = net.tables.ni, Y.shape[1]
-    fac_flops = B * nz * 2.0 * ni ** 3          # Gauss-Jordan inverse: n^3 FMA per block
+    # LU with partial pivoting + inverse of every layer block: 2*ni^3 flops counted
+    fac_flops = B * nz * 2.0 * ni ** 3
     fac_ms = per_kernel["factor"]["ms_per_launch"]
     achieved = fac_flops / (fac_ms * 1e-3) / 1e12 if fac_ms > 0 else 0.0
+    # algorithmic bytes of the factor: read each D_j, write each inverse (ni^2 doubles each)
+    fac_bytes = B * nz * 2.0 * ni * ni * 8
+    # DRAM read + write bytes of one factor launch measured by ncu on 32 atmospheres
+    # (dram__bytes_read.sum + dram__bytes_write.sum = 154.9 MB + 92.5 MB), scaled by atmospheres
+    fac_traffic = (154.92e6 + 92.51e6) / 32 * B
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
+    hbm_achieved = fac_bytes / (fac_ms * 1e-3) / 1e9 if fac_ms > 0 else 0.0
 
     if rank == 0:
         line = {
@@ -332,17 +347,26 @@ def main():
                                    f"(ni={ni}, nr={net.tables.nr}, nz={nz}, dt=1e-6)",
                        "batch_per_gpu": B, "ni": ni, "nr": int(net.tables.nr), "nz": int(nz),
                        "precision": "fp64", "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (rates 172 MB + workspace 590 MB per GPU at B=128)"},
+                       "l2": f"inputs larger than L2 (rates {K.nbytes / 1e6:.0f} MB + solver workspace "
+                             f"{step.ws_bytes / 1e6:.0f} MB per GPU), no flush"},
             "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
                     "note": "y and dt copied in from pinned host memory, sol and delta read back, every step; "
                             "rates and atmosphere stay resident (as in the reference runner's device carry)"},
             "gpu_launches": 6 * args.steps,
-            "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan block inverses, serial in z)",
+            "roofline": {"bound": "fp64", "kernel": "factor (LU with partial pivoting + inverse of each "
+                                                    "layer block, serial in z, one CTA per atmosphere)",
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                         "frac": achieved / peak64 if peak64 else None, "traffic": None,
-                         "peak_source": "measured live: FP64 FMA probe kernel (vb_fp64_probe)",
-                         "algorithmic": f"2*ni^3 flops per layer block x {nz} layers x {B} atmospheres"},
+                         "frac": achieved / peak64 if peak64 else None, "traffic": fac_traffic,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one factor "
+                                           "launch on 32 atmospheres, scaled to the batch",
+                         "peak_source": "measured live: FP64 FMA probe kernel (vb_fp64_probe); "
+                                        "MEASURED_PEAKS.json has no FP64 figure",
+                         "algorithmic": f"2*ni^3 flops per layer block x {nz} layers x {B} atmospheres",
+                         "hbm_view": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                                      "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src,
+                                      "algorithmic": f"read D_j + write inverse, 2*ni^2*8 B per layer x "
+                                                     f"{nz} x {B}"}},
             "kernels": per_kernel,
             "single_instance_fp64": {"value": 1.0 / (single_ms * 1e-3), "unit": UNIT, "ms_per_step": single_ms},
             "clocks": clk,
