@@ -4,10 +4,10 @@ Workload (one "step" = one Ros2 step of every atmosphere of the batch):
 config-0-shaped atmospheres - a seeded element-balanced C/H/O/N network with
 ni=69 species and 700+700 reactions, nz=120 layers, rate constants
 log-uniform in [1e-40, 1e-8], mixing ratios log-uniform in [1e-20, 1],
-dt = 1e-6 s - batched B atmospheres per GPU (default 148, one per SM; seeded
-per atmosphere and per rank), FP64. The same inputs are stepped repeatedly
-(as the reference's benchmarks/bench_step.py does). Per-step inputs (rates
-199 MB, solver workspace 737 MB at B=148) exceed the 126 MB L2.
+dt = 1e-6 s - batched B atmospheres per GPU (default two per SM, 296 on a
+B200; seeded per atmosphere and per rank), FP64. The same inputs are stepped
+repeatedly (as the reference's benchmarks/bench_step.py does). Per-step
+inputs (rates 398 MB, solver workspace 1.47 GB at B=296) exceed the 126 MB L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl b200|reference]
 
@@ -191,7 +191,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=148)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="atmospheres per GPU (default: two per SM, 296 on a B200)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -218,7 +219,7 @@ def main():
     stream = torch.cuda.current_stream()
     sh = _lib.stream_handle(stream)
 
-    B = args.batch
+    B = args.batch or 2 * torch.cuda.get_device_properties(local).multi_processor_count
     net, cases, Y, K, DT, A = make_batch(B, rank)
     dn = chem.to_device(net.tables)
     atm = jstep.atm_from_dict(A)

@@ -4,12 +4,12 @@
 // factor: for each layer j (serial in z)
 //     A'_j  = D_j - (sub_d[j-1] sup_d[j-1]^T) o A'_{j-1}^{-1}     (solver.py:47)
 //     Inv_j = A'_j^{-1}                                            (solver.py:46,48)
-// The inverse is formed by Gauss-Jordan elimination with partial pivoting on
-// a register-resident tile (each warp owns RPW rows, each lane NP/32 columns),
-// with implicit row pivoting (no row exchanges; the permutation is undone when
-// the tile is stored). The forward sweep of the first right-hand side rides
-// along (solver.py:73-88). The stored inverses turn every later solve into
-// matrix-vector products (solver.py:91-111).
+// Each A'_j is factored by LU with partial pivoting on a register-resident
+// tile (implicit row pivoting: no row exchanges, the factors are stored in
+// pivot order), then inverted column block by column block, one block per
+// warp, by substitution with the factors. The forward sweep of the first
+// right-hand side rides along (solver.py:73-88). The stored inverses turn
+// every later solve into matrix-vector products (solver.py:91-111).
 #include <cuda_runtime.h>
 
 #include "vb_common.cuh"
@@ -25,8 +25,10 @@ struct LUK {
   static constexpr int SLD = NP + 1;      // smem row stride of S (doubles)
   static constexpr int PLD = PW + 1;      // smem row stride of a panel buffer
   static constexpr int PBUF = (NP * PLD > RPW * NP) ? NP * PLD : RPW * NP;
+  static_assert(NW * NP <= 2 * PBUF, "partial products of the rhs sweep must fit the panel buffers");
+  static_assert(RPW * CPL * 32 <= NP * PLD + PW * NP, "warp 0's tile must fit Mb..V while it factors a panel");
   static size_t smem_bytes() {
-    size_t d = (size_t)NP * SLD          // S: previous inverse, LU factors, new inverse
+    size_t d = (size_t)NP * SLD          // S: LU factors in pivot order
                + 2 * (size_t)PBUF        // panel buffers / triangular-solve row buffers
                + (size_t)NP * PLD        // M: update multipliers of the current panel
                + (size_t)PW * NP         // V: pivot rows of the current panel
@@ -42,6 +44,82 @@ __device__ __forceinline__ unsigned long long pivot_key(double v) {
   return (a >= 0.0) ? (unsigned long long)__double_as_longlong(a) : 0ull;
 }
 
+// Unblocked LU of one PW-column panel by one warp (lane l holds rows
+// l + 32 r in registers): for each column the argmax over unpivoted rows
+// (three redux.sync reductions of the 64-bit |v| key, ties to the lowest
+// row), the pivot row broadcast by shuffles, and the rank-1 update of the
+// panel's remaining columns. Kept out of line so its registers do not compete
+// with the caller's tile.
+template <int PRL, int PW, int PLD>
+__device__ __noinline__ void panel_lu(double* Pn, int n, int k0, int kw, unsigned& usedw_io, int& st_io,
+                                      int* pivs, int* qinv, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  unsigned usedw = usedw_io;
+  int st_local = 0;
+  // the panel in registers: lane l holds rows l + 32 r, all PW columns
+  double pv[PRL][PW];
+#pragma unroll
+  for (int r = 0; r < PRL; ++r) {
+    const int i = lane + 32 * r;
+#pragma unroll
+    for (int u = 0; u < PW; ++u) pv[r][u] = i < n ? Pn[i * PLD + u] : 0.0;
+  }
+#pragma unroll
+  for (int t = 0; t < PW; ++t) {
+    if (t < kw) {
+      unsigned long long bk = 0ull;
+      unsigned brow = 0xffffffffu;
+#pragma unroll
+      for (int r = 0; r < PRL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < n && !((usedw >> r) & 1u)) {
+          unsigned long long kk = pivot_key(pv[r][t]);
+          if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
+        }
+      }
+      const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+      const unsigned m1 = __reduce_max_sync(FULL, hi);
+      const unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
+      const int p = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
+      if ((p & 31) == lane) usedw |= 1u << (p >> 5);
+      // broadcast the pivot row (columns t..PW-1) from its owner lane
+      const int po = p & 31, pslot = p >> 5;
+      double pr[PW];
+#pragma unroll
+      for (int u = t; u < PW; ++u) {
+        double v = pv[0][u];
+#pragma unroll
+        for (int r = 1; r < PRL; ++r) v = (pslot == r) ? pv[r][u] : v;
+        pr[u] = __shfl_sync(FULL, v, po);
+      }
+      const double piv = pr[t];
+      if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
+      const double rcp = 1.0 / piv;
+#pragma unroll
+      for (int r = 0; r < PRL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < n && !((usedw >> r) & 1u)) {
+          const double l = pv[r][t] * rcp;
+          pv[r][t] = l;
+#pragma unroll
+          for (int u = t + 1; u < PW; ++u) pv[r][u] = fma(-l, pr[u], pv[r][u]);
+        }
+      }
+      if (lane == 0) { pivs[k0 + t] = p; qinv[p] = k0 + t; }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < PRL; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n) {
+#pragma unroll
+      for (int u = 0; u < PW; ++u) Pn[i * PLD + u] = pv[r][u];
+    }
+  }
+  usedw_io = usedw;
+  st_io |= st_local;
+}
+
 // Factor all layers of one atmosphere. On entry inv[j] holds D_j (row stride
 // ld); on exit inv[j] holds A'_j^{-1}. With rhs != nullptr the first sweep of
 // the right-hand side rhs[nz][ni] is done in place (solver.py:73-88).
@@ -55,16 +133,18 @@ __device__ __forceinline__ unsigned long long pivot_key(double v) {
 //    redux.sync reductions, pivot row broadcast through shared memory);
 //    every warp then forms U[K, C] = L_KK^{-1} A[P, C] for its columns and
 //    applies the rank-PW update A[R, C] -= L[R, K] U[K, C] to unpivoted rows.
-//  * The factors are stored in pivot order in shared memory; the tile is
-//    re-used for Y = L^{-1} P and X = U^{-1} Y, one warp's RPW rows per
-//    panel (solved thread-locally, then broadcast and applied by the other
-//    warps), so X = A'^{-1} ends up in natural row order.
+//  * The factors are stored in pivot order in shared memory; warp w then
+//    solves for the RPW columns w*RPW.. of X = A'^{-1} with warp-synchronous
+//    column-oriented substitution (no block barrier), so X lands in natural
+//    row order.
 template <int NP, int NW, int PW>
 __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ inv,
                                   const double* __restrict__ supn, const double* __restrict__ subn,
                                   double* __restrict__ rhs, int32_t* status, char* smem_raw) {
   using G = LUK<NP, NW, PW>;
   constexpr int RPW = G::RPW, CPL = G::CPL, PRL = G::PRL, SLD = G::SLD, PLD = G::PLD;
+  constexpr int CB = RPW > 8 ? (RPW + 1) / 2 : RPW;   // inverse columns per pass
+  constexpr int NCH = (RPW + CB - 1) / CB;
   double* S = reinterpret_cast<double*>(smem_raw);          // [NP][SLD]
   double* Pn0 = S + NP * SLD;                               // [PBUF]
   double* Pn1 = Pn0 + G::PBUF;                              // [PBUF]
@@ -88,6 +168,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   double a[RPW][CPL];
   for (int j = 0; j < nz; ++j) {
     const double* D = inv + (int64_t)j * n * ld;
+    const double* Dp = inv + (int64_t)(j > 0 ? j - 1 : 0) * n * ld;   // Inv_{j-1}
     for (int i = threadIdx.x; i < NP; i += blockDim.x) qinv[i] = -1;
     // ---- load D_j and apply the Hadamard Schur update from Inv_{j-1} (solver.py:47)
 #pragma unroll
@@ -101,7 +182,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
           v = D[(int64_t)i * ld + col];
           if (j > 0) {
             double cb = subn[(int64_t)(j - 1) * n + i] * supn[(int64_t)(j - 1) * n + col];
-            v = v - cb * S[i * SLD + col];
+            v = v - cb * Dp[(int64_t)i * ld + col];
           }
         }
         a[r][c] = v;
@@ -126,46 +207,18 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       // (b) warp 0: unblocked LU of the panel (in shared memory) over the
       //     unpivoted rows, then L_KK^{-1} of its unit lower triangle
       if (warp == 0) {
+        // warp 0's own tile waits in Mb..V (free until the multipliers and
+        // pivot rows are staged) so the panel has the registers
 #pragma unroll
-        for (int t = 0; t < PW; ++t) {
-          if (t < kw) {
-            unsigned long long bk = 0ull;
-            unsigned brow = 0xffffffffu;
+        for (int r = 0; r < RPW; ++r)
 #pragma unroll
-            for (int r = 0; r < PRL; ++r) {
-              const int i = lane + 32 * r;
-              if (i < n && !((usedw >> r) & 1u)) {
-                unsigned long long kk = pivot_key(Pn[i * PLD + t]);
-                if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
-              }
-            }
-            const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-            const unsigned m1 = __reduce_max_sync(FULL, hi);
-            const unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
-            const int p = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
-            if ((p & 31) == lane) usedw |= 1u << (p >> 5);
-            const double* prow = Pn + p * PLD;
-            const double piv = prow[t];
-            if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
-            const double rcp = 1.0 / piv;
-            double pr[PW];
+          for (int c = 0; c < CPL; ++c) Mb[(r * CPL + c) * 32 + lane] = a[r][c];
+        panel_lu<PRL, PW, PLD>(Pn, n, k0, kw, usedw, st_local, pivs, qinv, lane);
 #pragma unroll
-            for (int u = t + 1; u < PW; ++u) pr[u] = prow[u];
+        for (int r = 0; r < RPW; ++r)
 #pragma unroll
-            for (int r = 0; r < PRL; ++r) {
-              const int i = lane + 32 * r;
-              if (i < n && !((usedw >> r) & 1u)) {
-                double* row = Pn + i * PLD;
-                const double l = row[t] * rcp;
-                row[t] = l;
-#pragma unroll
-                for (int u = t + 1; u < PW; ++u) row[u] = fma(-l, pr[u], row[u]);
-              }
-            }
-            if (lane == 0) { pivs[k0 + t] = p; qinv[p] = k0 + t; }
-            __syncwarp();
-          }
-        }
+          for (int c = 0; c < CPL; ++c) a[r][c] = Mb[(r * CPL + c) * 32 + lane];
+        __syncwarp();
         // L_KK^{-1} (unit lower): lane s builds column s from the pivot rows' multipliers
         if (lane < PW) {
           const int sc = lane;
@@ -255,133 +308,109 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
     }
     __syncthreads();
     for (int k = threadIdx.x; k < n; k += blockDim.x) rdiag[k] = 1.0 / S[k * SLD + k];
-    // ================================================================ Y = L^{-1} P
-#pragma unroll
-    for (int r = 0; r < RPW; ++r) {
-      const int k = warp * RPW + r;
-      const int pk = k < n ? pivs[k] : -1;
-#pragma unroll
-      for (int c = 0; c < CPL; ++c) a[r][c] = (lane + 32 * c == pk) ? 1.0 : 0.0;
-    }
-    for (int w = 0; w < NW; ++w) {
-      const int k0 = w * RPW;
-      if (k0 >= n) break;
-      double* Yb = (w & 1) ? Pn1 : Pn0;
-      if (warp == w) {
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-          const int k = k0 + r;
-#pragma unroll
-          for (int s2 = 0; s2 < r; ++s2) {
-            const double l = k < n ? S[k * SLD + k0 + s2] : 0.0;
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) a[r][c] = fma(-l, a[s2][c], a[r][c]);
-          }
-#pragma unroll
-          for (int c = 0; c < CPL; ++c) Yb[r * NP + lane + 32 * c] = a[r][c];
-        }
-      }
-      __syncthreads();
-      if (warp > w) {
-        const int kw = min(RPW, n - k0);
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-          const int k = warp * RPW + r;
-          if (k < n) {
-#pragma unroll
-            for (int s2 = 0; s2 < RPW; ++s2) {
-              if (s2 < kw) {
-                const double l = S[k * SLD + k0 + s2];
-#pragma unroll
-                for (int c = 0; c < CPL; ++c) a[r][c] = fma(-l, Yb[s2 * NP + lane + 32 * c], a[r][c]);
-              }
-            }
-          }
-        }
-      }
-    }
-    // ================================================================ X = U^{-1} Y
-    __syncthreads();   // readers of the forward phase's last buffer are done
-    for (int w = NW - 1; w >= 0; --w) {
-      const int k0 = w * RPW;
-      if (k0 >= n) continue;
-      const int kw = min(RPW, n - k0);
-      double* Yb = (w & 1) ? Pn1 : Pn0;   // last read two panels ago, before the previous barrier
-      if (warp == w) {
-#pragma unroll
-        for (int r = RPW - 1; r >= 0; --r) {
-          const int k = k0 + r;
-          if (r < kw) {
-#pragma unroll
-            for (int s2 = r + 1; s2 < RPW; ++s2) {
-              if (s2 < kw) {
-                const double uu = S[k * SLD + k0 + s2];
-#pragma unroll
-                for (int c = 0; c < CPL; ++c) a[r][c] = fma(-uu, a[s2][c], a[r][c]);
-              }
-            }
-            const double rd = rdiag[k];
-#pragma unroll
-            for (int c = 0; c < CPL; ++c) {
-              a[r][c] = a[r][c] * rd;
-              Yb[r * NP + lane + 32 * c] = a[r][c];
-            }
-          }
-        }
-      }
-      __syncthreads();
-      if (warp < w) {
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-          const int k = warp * RPW + r;
-          if (k < n) {
-#pragma unroll
-            for (int s2 = 0; s2 < RPW; ++s2) {
-              if (s2 < kw) {
-                const double uu = S[k * SLD + k0 + s2];
-#pragma unroll
-                for (int c = 0; c < CPL; ++c) a[r][c] = fma(-uu, Yb[s2 * NP + lane + 32 * c], a[r][c]);
-              }
-            }
-          }
-        }
-      }
-    }
-    // ---- the inverse (natural order) to shared and global memory
     __syncthreads();
-#pragma unroll
-    for (int r = 0; r < RPW; ++r) {
-      int i = warp * RPW + r;
-      if (i < n) {
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          int col = lane + 32 * c;
-          if (col < n) {
-            if (!isfinite(a[r][c])) st_local |= VB_STATUS_NONFINITE;
-            S[i * SLD + col] = a[r][c];
-          }
-        }
-      }
-    }
-    __syncthreads();
+    // ================================================================ inverse by column blocks
+    // X = U^{-1} L^{-1} P (lu_solve(LU, I)), columns split over warps: warp w
+    // solves L U x = P e_col for col = w*RPW + cc, CB columns at a time,
+    // column-oriented as LAPACK's getrs / dtrsm: forward with the unit lower
+    // factor from the pivot step of col downwards, then backward with U.
+    // Lane l holds rows l + 32 t; no block barrier (the factors in S are read
+    // only). Each finished chunk goes straight to global memory (natural row
+    // order) and into the partial products Inv_j * rhs_j.
     double* O = inv + (int64_t)j * n * ld;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-      int i = e / n, col = e - i * n;
-      O[(int64_t)i * ld + col] = S[i * SLD + col];
+    double pu[PRL];
+#pragma unroll
+    for (int t = 0; t < PRL; ++t) pu[t] = 0.0;
+#pragma unroll 1
+    for (int h = 0; h < NCH; ++h) {
+      const int c0 = warp * RPW + h * CB;
+      const int cbw = min(min(CB, RPW - h * CB), n - c0);
+      if (cbw <= 0) break;
+      double x[PRL][CB];
+      int kmin = n;
+#pragma unroll
+      for (int cc = 0; cc < CB; ++cc) {
+        const int q = cc < cbw ? qinv[c0 + cc] : n;
+        kmin = min(kmin, q);
+#pragma unroll
+        for (int t = 0; t < PRL; ++t) x[t][cc] = (lane + 32 * t == q) ? 1.0 : 0.0;
+      }
+      // forward: steps k of segment sg = k / 32 are owned by slot sg (compile time)
+#pragma unroll
+      for (int sg = 0; sg < PRL; ++sg) {
+        const int ke = min(n - 1, 32 * sg + 32);
+        for (int k = max(kmin, 32 * sg); k < ke; ++k) {
+          const int owner = k & 31;
+          double xk[CB];
+#pragma unroll
+          for (int cc = 0; cc < CB; ++cc) xk[cc] = __shfl_sync(FULL, x[sg][cc], owner);
+#pragma unroll
+          for (int t = sg; t < PRL; ++t) {
+            const int i = lane + 32 * t;
+            if (i > k && i < n) {
+              const double l = S[i * SLD + k];
+#pragma unroll
+              for (int cc = 0; cc < CB; ++cc) x[t][cc] = fma(-l, xk[cc], x[t][cc]);
+            }
+          }
+        }
+      }
+      // backward with U, scaling by 1/U_kk as each x_k completes
+#pragma unroll
+      for (int sg = PRL - 1; sg >= 0; --sg) {
+        for (int k = min(n - 1, 32 * sg + 31); k >= 32 * sg; --k) {
+          const int owner = k & 31;
+          const double rd = rdiag[k];
+          double xk[CB];
+#pragma unroll
+          for (int cc = 0; cc < CB; ++cc) xk[cc] = __shfl_sync(FULL, x[sg][cc] * rd, owner);
+          if (lane == owner) {
+#pragma unroll
+            for (int cc = 0; cc < CB; ++cc) x[sg][cc] = xk[cc];
+          }
+#pragma unroll
+          for (int t = 0; t <= sg; ++t) {
+            const int i = lane + 32 * t;
+            if (i < k) {
+              const double u = S[i * SLD + k];
+#pragma unroll
+              for (int cc = 0; cc < CB; ++cc) x[t][cc] = fma(-u, xk[cc], x[t][cc]);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < PRL; ++t) {
+        const int i = lane + 32 * t;
+        if (i < n) {
+#pragma unroll
+          for (int cc = 0; cc < CB; ++cc) {
+            if (cc < cbw) {
+              const double v = x[t][cc];
+              if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
+              O[(int64_t)i * ld + c0 + cc] = v;
+              pu[t] = fma(v, vec[c0 + cc], pu[t]);
+            }
+          }
+        }
+      }
     }
+    double* part = Pn0;   // [NW][NP] partial products of the forward sweep (Pn0..Pn1)
+    if (rhs) {
+#pragma unroll
+      for (int t = 0; t < PRL; ++t) {
+        const int i = lane + 32 * t;
+        if (i < n) part[warp * NP + i] = pu[t];
+      }
+    }
+    __syncthreads();   // Inv_j complete in global memory; partial products staged
     // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
     if (rhs && j + 1 < nz) {
-      double* u = Pn0;
-      for (int i = warp; i < n; i += NW) {
-        double s = 0.0;
-        for (int m = lane; m < n; m += 32) s += S[i * SLD + m] * vec[m];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
-        if (lane == 0) u[i] = s;
-      }
-      __syncthreads();
+      const int nwu = min(NW, (n + RPW - 1) / RPW);
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double v = rhs[(int64_t)(j + 1) * n + i] - subn[(int64_t)j * n + i] * u[i];
+        double u = part[i];
+        for (int w = 1; w < nwu; ++w) u += part[w * NP + i];
+        const double v = rhs[(int64_t)(j + 1) * n + i] - subn[(int64_t)j * n + i] * u;
         rhs[(int64_t)(j + 1) * n + i] = v;
         vec[i] = v;
       }
@@ -391,8 +420,8 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   if (st_local) atomicOr(status, st_local);
 }
 
-template <int NP, int NW, int PW>
-__global__ void __launch_bounds__(NW * 32, 1)
+template <int NP, int NW, int PW, int MB>
+__global__ void __launch_bounds__(NW * 32, MB)
 factor_kernel(Batch B, double* __restrict__ ws, int32_t* __restrict__ status, int with_rhs) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
@@ -574,21 +603,39 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, c
   return cudaGetLastError();
 }
 
-template <int NP, int NW, int PW>
+template <int NP, int NW, int PW, int MB = 1>
 static cudaError_t launch_factor_t(const Batch& B, double* ws, int32_t* status, int with_rhs,
                                    cudaStream_t st) {
   size_t sm = LUK<NP, NW, PW>::smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW, PW>,
+  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW, PW, MB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  factor_kernel<NP, NW, PW><<<B.count, NW * 32, sm, st>>>(B, ws, status, with_rhs);
+  factor_kernel<NP, NW, PW, MB><<<B.count, NW * 32, sm, st>>>(B, ws, status, with_rhs);
   return cudaGetLastError();
+}
+
+// SM count of the current device (the factor's layout depends on how many
+// atmospheres share an SM).
+static int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+    return 148;
+  return n;
 }
 
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st) {
   if (B.ni <= 32) return launch_factor_t<32, 8, 8>(B, ws, status, with_rhs, st);
   if (B.ni <= 64) return launch_factor_t<64, 16, 8>(B, ws, status, with_rhs, st);
-  if (B.ni <= 96) return launch_factor_t<96, 16, 8>(B, ws, status, with_rhs, st);
+  if (B.ni <= 96) {
+    // Up to one atmosphere per SM: 12 warps per CTA give the shortest chain per
+    // layer. Beyond that, two 8-warp CTAs share an SM so that one atmosphere's
+    // pivot chain fills the other's idle issue slots (measured on B200 for
+    // ni=69, nz=120: 12.9 ms vs 16.0 ms at 1 atmosphere, 26.2 ms vs 19.7 ms
+    // at 296).
+    if (B.count <= sm_count()) return launch_factor_t<96, 12, 8, 1>(B, ws, status, with_rhs, st);
+    return launch_factor_t<96, 8, 8, 2>(B, ws, status, with_rhs, st);
+  }
   return launch_factor_t<128, 16, 8>(B, ws, status, with_rhs, st);
 }
 

@@ -133,6 +133,30 @@ def test_batched_step_equals_single_steps():
         check_step(s1.cpu(), d1.cpu(), sref, dref)
 
 
+def test_batch_beyond_sm_count():
+    """More atmospheres than SMs (the factor then runs two CTAs per SM with a
+    different warp layout): sampled atmospheres against the oracle and against
+    the same atmosphere stepped alone."""
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    B = n_sm + 4
+    net = syn.make_network(43, 69, 700)
+    dn = chem.to_device(net.tables)
+    cases = [syn.make_case(seed=(900 + b,), net=net, nz=8, mild=True, k_range=(-40.0, 4.0)) for b in range(B)]
+    Y = np.stack([c.y for c in cases])
+    K = np.stack([c.k for c in cases])
+    dts = np.full(B, 1e-6)
+    A = {kk: (np.stack([c.atm[kk] for c in cases]) if not isinstance(cases[0].atm[kk], bool)
+              else cases[0].atm[kk]) for kk in cases[0].atm}
+    sol_b, delta_b = jstep.jax_ros2_step(Y, K, dts, atm_of(A), dn)
+    sol_b, delta_b = sol_b.cpu().numpy(), delta_b.cpu().numpy()
+    for b in (0, 1, n_sm - 1, n_sm, B - 1):
+        c = cases[b]
+        sref, dref = orc.ros2_step(c.y, c.k, dts[b], c.atm, c.net.tables)
+        check_step(sol_b[b], delta_b[b], sref, dref)
+        s1, d1 = jstep.jax_ros2_step(c.y, c.k, dts[b], atm_of(c.atm), dn)
+        check_step(sol_b[b], delta_b[b], s1.cpu().numpy(), d1.cpu().numpy())
+
+
 def test_block_thomas_reference_systems():
     g = golden("thomas.npz")
     x = solver.block_thomas_diag_offdiag(g["diag_small_diag"], g["diag_small_sup"], g["diag_small_sub"],
