@@ -137,7 +137,7 @@ __device__ __noinline__ void panel_lu(double* Pn, int n, int k0, int kw, unsigne
 //    solves for the RPW columns w*RPW.. of X = A'^{-1} with warp-synchronous
 //    column-oriented substitution (no block barrier), so X lands in natural
 //    row order.
-template <int NP, int NW, int PW>
+template <int NP, int NW, int PW, int MB>
 __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ inv,
                                   const double* __restrict__ supn, const double* __restrict__ subn,
                                   double* __restrict__ rhs, int32_t* status, char* smem_raw) {
@@ -272,25 +272,40 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       // (d) rank-kw update A[i, C] += M[i, K] V[K, C] (C = columns right of the
       //     panel): unpivoted rows get the Schur update, pivot rows become
       //     U[K, C] = L_KK^{-1} V; rows pivoted in earlier panels are final.
+      //     The pivot rows of this lane's columns are read from shared memory
+      //     once per panel (all column slots when registers allow, else one
+      //     slot at a time).
+      constexpr int VC = (MB == 1 && (RPW + PW) * CPL <= 48) ? CPL : 1;   // column slots held at once
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) {
-        const int i = warp * RPW + r;
-        const int q = qinv[i];
-        if (q >= 0 && q < k0) continue;
-        double mi[PW];
+      for (int c0s = 0; c0s < CPL; c0s += VC) {
+        if (32 * (c0s + VC) - 1 < k0) continue;   // these column slots are left of the panel
+        double vv[PW][VC];
 #pragma unroll
-        for (int t = 0; t < PW; ++t) mi[t] = Mb[i * PLD + t];
+        for (int t = 0; t < PW; ++t)
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          const int col = lane + 32 * c;
-          if (col >= k0 && col < k0 + PW) {
-            a[r][c] = Pn[i * PLD + (col - k0)];
-          } else if (col >= k0 + PW) {
-            double acc = a[r][c];
+          for (int cv = 0; cv < VC; ++cv) vv[t][cv] = t < kw ? V[t * NP + lane + 32 * (c0s + cv)] : 0.0;
 #pragma unroll
-            for (int t = 0; t < PW; ++t)
-              if (t < kw) acc = fma(mi[t], V[t * NP + col], acc);
-            a[r][c] = acc;
+        for (int r = 0; r < RPW; ++r) {
+          const int i = warp * RPW + r;
+          if (i >= n) break;
+          const int q = qinv[i];
+          if (q >= 0 && q < k0) continue;
+          double mi[PW];
+#pragma unroll
+          for (int t = 0; t < PW; ++t) mi[t] = Mb[i * PLD + t];
+#pragma unroll
+          for (int cv = 0; cv < VC; ++cv) {
+            const int c = c0s + cv;
+            if (32 * c + 31 < k0) continue;
+            const int col = lane + 32 * c;
+            if (col >= k0 && col < k0 + PW) {
+              a[r][c] = Pn[i * PLD + (col - k0)];
+            } else if (col >= k0 + PW) {
+              double acc = a[r][c];
+#pragma unroll
+              for (int t = 0; t < PW; ++t) acc = fma(mi[t], vv[t][cv], acc);
+              a[r][c] = acc;
+            }
           }
         }
       }
@@ -427,7 +442,7 @@ factor_kernel(Batch B, double* __restrict__ ws, int32_t* __restrict__ status, in
   const int b = blockIdx.x;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
-  factor_atmosphere<NP, NW, PW>(g.nz, B.ni, B.ld, w.inv, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
+  factor_atmosphere<NP, NW, PW, MB>(g.nz, B.ni, B.ld, w.inv, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
                                 status + b, smem_raw);
 }
 
