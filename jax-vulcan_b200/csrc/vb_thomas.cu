@@ -145,6 +145,8 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   constexpr int RPW = G::RPW, CPL = G::CPL, PRL = G::PRL, SLD = G::SLD, PLD = G::PLD;
   constexpr int CB = RPW > 8 ? (RPW + 1) / 2 : RPW;   // inverse columns per pass
   constexpr int NCH = (RPW + CB - 1) / CB;
+  static_assert(CB % 2 == 0, "x_k is handed over as double2");
+  static_assert(NW * NP + NW * 2 * CB <= 2 * G::PBUF, "broadcast buffers must fit the panel buffers");
   double* S = reinterpret_cast<double*>(smem_raw);          // [NP][SLD]
   double* Pn0 = S + NP * SLD;                               // [PBUF]
   double* Pn1 = Pn0 + G::PBUF;                              // [PBUF]
@@ -333,6 +335,9 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
     // only). Each finished chunk goes straight to global memory (natural row
     // order) and into the partial products Inv_j * rhs_j.
     double* O = inv + (int64_t)j * n * ld;
+    // per-warp double buffer through which the owner lane of step k hands x_k
+    // to the warp (after the rhs partial products in Pn0..Pn1)
+    double* xb = Pn0 + NW * NP + warp * 2 * CB;
     double pu[PRL];
 #pragma unroll
     for (int t = 0; t < PRL; ++t) pu[t] = 0.0;
@@ -356,9 +361,19 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         const int ke = min(n - 1, 32 * sg + 32);
         for (int k = max(kmin, 32 * sg); k < ke; ++k) {
           const int owner = k & 31;
+          double2* slot = reinterpret_cast<double2*>(xb + (k & 1) * CB);
+          if (lane == owner) {
+#pragma unroll
+            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = make_double2(x[sg][cc], x[sg][cc + 1]);
+          }
+          __syncwarp();
           double xk[CB];
 #pragma unroll
-          for (int cc = 0; cc < CB; ++cc) xk[cc] = __shfl_sync(FULL, x[sg][cc], owner);
+          for (int cc = 0; cc < CB; cc += 2) {
+            const double2 v = slot[cc / 2];
+            xk[cc] = v.x;
+            xk[cc + 1] = v.y;
+          }
 #pragma unroll
           for (int t = sg; t < PRL; ++t) {
             const int i = lane + 32 * t;
@@ -375,13 +390,21 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       for (int sg = PRL - 1; sg >= 0; --sg) {
         for (int k = min(n - 1, 32 * sg + 31); k >= 32 * sg; --k) {
           const int owner = k & 31;
-          const double rd = rdiag[k];
+          double2* slot = reinterpret_cast<double2*>(xb + (k & 1) * CB);
+          if (lane == owner) {
+            const double rd = rdiag[k];
+#pragma unroll
+            for (int cc = 0; cc < CB; ++cc) x[sg][cc] = x[sg][cc] * rd;
+#pragma unroll
+            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = make_double2(x[sg][cc], x[sg][cc + 1]);
+          }
+          __syncwarp();
           double xk[CB];
 #pragma unroll
-          for (int cc = 0; cc < CB; ++cc) xk[cc] = __shfl_sync(FULL, x[sg][cc] * rd, owner);
-          if (lane == owner) {
-#pragma unroll
-            for (int cc = 0; cc < CB; ++cc) x[sg][cc] = xk[cc];
+          for (int cc = 0; cc < CB; cc += 2) {
+            const double2 v = slot[cc / 2];
+            xk[cc] = v.x;
+            xk[cc + 1] = v.y;
           }
 #pragma unroll
           for (int t = 0; t <= sg; ++t) {
@@ -394,6 +417,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
           }
         }
       }
+      __syncwarp();   // every lane has read the last hand-over before the next chunk writes one
 #pragma unroll
       for (int t = 0; t < PRL; ++t) {
         const int i = lane + 32 * t;
