@@ -4,6 +4,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -131,15 +132,32 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   csr(loss, lp, le);
   csr(prod, pp, pe);
   csr(jac, jp, je);
-  std::vector<int32_t> lr(le.size()), pr(pe.size()), jidx(je.size());
-  std::vector<double> jcoef(je.size());
-  for (size_t e = 0; e < le.size(); ++e) lr[e] = le[e] / T;
-  for (size_t e = 0; e < pe.size(); ++e) pr[e] = pe[e] / T;
+  // packed term words and the table of distinct coefficients
+  if ((int64_t)R * T > 0xffff) return fail(VB_ERR_ARG, "(nr+1)*max_terms must stay below 65536");
+  std::vector<double> coefs;
+  std::map<uint64_t, int> coef_id;
+  bool too_many = false;
+  auto cid_of = [&](double c) {
+    uint64_t bits;
+    std::memcpy(&bits, &c, sizeof bits);
+    auto it = coef_id.find(bits);
+    if (it != coef_id.end()) return it->second;
+    if ((int)coefs.size() >= vb::MAX_COEF) { too_many = true; return 0; }
+    int id = (int)coefs.size();
+    coefs.push_back(c);
+    coef_id[bits] = id;
+    return id;
+  };
+  std::vector<uint32_t> lw(le.size()), pw(pe.size()), jw(je.size());
+  for (size_t e = 0; e < le.size(); ++e) lw[e] = vb::term_word(le[e] / T, cid_of(r_st[le[e]]));
+  for (size_t e = 0; e < pe.size(); ++e) pw[e] = vb::term_word(pe[e] / T, cid_of(p_st[pe[e]]));
   for (size_t e = 0; e < je.size(); ++e) {
     int fe = je[e], s = fe % T, ro = fe / T, o = ro % (2 * T), r = ro / (2 * T);
-    jidx[e] = r * T + s;
-    jcoef[e] = o < T ? -r_st[(int64_t)r * T + o] : p_st[(int64_t)r * T + (o - T)];
+    double c = o < T ? -r_st[(int64_t)r * T + o] : p_st[(int64_t)r * T + (o - T)];
+    jw[e] = vb::term_word(r * T + s, cid_of(c));
   }
+  if (too_many) return fail(VB_ERR_ARG, "more than 256 distinct stoichiometric coefficients");
+  if (coefs.empty()) coefs.push_back(0.0);
   // destination ranges per thread, balanced by entries (+1 per destination)
   const int NT = vb::LAYER_THREADS;
   std::vector<int32_t> split(NT + 1, ni * ni);
@@ -164,10 +182,9 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
       {ri.data(), ri.size() * 4, 0}, {pi.data(), pi.size() * 4, 0},
       {r_st, (size_t)R * T * 8, 0},  {p_st, (size_t)R * T * 8, 0},
       {three, (size_t)R, 0},         {lp.data(), lp.size() * 4, 0},
-      {le.data(), le.size() * 4, 0}, {lr.data(), lr.size() * 4, 0},
-      {pp.data(), pp.size() * 4, 0}, {pe.data(), pe.size() * 4, 0},
-      {pr.data(), pr.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
-      {jidx.data(), jidx.size() * 4, 0}, {jcoef.data(), jcoef.size() * 8, 0},
+      {lw.data(), lw.size() * 4, 0}, {pp.data(), pp.size() * 4, 0},
+      {pw.data(), pw.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
+      {jw.data(), jw.size() * 4, 0}, {coefs.data(), coefs.size() * 8, 0},
       {split.data(), split.size() * 4, 0}};
   size_t total = 0;
   for (auto& p : parts) { p.off = total; total += (p.bytes + 255) & ~(size_t)255; }
@@ -188,15 +205,14 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   d.p_st = (const double*)(b + parts[3].off);
   d.three = (const uint8_t*)(b + parts[4].off);
   d.loss_ptr = (const int32_t*)(b + parts[5].off);
-  d.loss_ent = (const int32_t*)(b + parts[6].off);
-  d.loss_r = (const int32_t*)(b + parts[7].off);
-  d.prod_ptr = (const int32_t*)(b + parts[8].off);
-  d.prod_ent = (const int32_t*)(b + parts[9].off);
-  d.prod_r = (const int32_t*)(b + parts[10].off);
-  d.jac_ptr = (const int32_t*)(b + parts[11].off);
-  d.jac_idx = (const int32_t*)(b + parts[12].off);
-  d.jac_coef = (const double*)(b + parts[13].off);
-  d.jac_split = (const int32_t*)(b + parts[14].off);
+  d.loss_w = (const uint32_t*)(b + parts[6].off);
+  d.prod_ptr = (const int32_t*)(b + parts[7].off);
+  d.prod_w = (const uint32_t*)(b + parts[8].off);
+  d.jac_ptr = (const int32_t*)(b + parts[9].off);
+  d.jac_w = (const uint32_t*)(b + parts[10].off);
+  d.coef_tab = (const double*)(b + parts[11].off);
+  d.n_coef = (int)coefs.size();
+  d.jac_split = (const int32_t*)(b + parts[12].off);
   net->base = base;
   net->bytes = total;
   *out = net;

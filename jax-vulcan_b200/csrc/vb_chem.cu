@@ -86,19 +86,25 @@ __device__ inline void layer_rates(const NetDev& net, const double* yrow, const 
 // Loss and production sums of every species, each a sequential gather in
 // segment_sum order (one thread per sum): part[2i] = loss_i, part[2i+1] = prod_i.
 // The caller synchronises before reading dy_i/dt = part[2i+1] - part[2i].
-__device__ inline void species_sums(const NetDev& net, const double* rate, double* part) {
+__device__ inline void species_sums(const NetDev& net, const double* coef, const double* rate, double* part) {
   for (int t = threadIdx.x; t < 2 * net.ni; t += blockDim.x) {
     const int i = t >> 1;
+    const int32_t* ptr = (t & 1) ? net.prod_ptr : net.loss_ptr;
+    const uint32_t* w = (t & 1) ? net.prod_w : net.loss_w;
     double acc = 0.0;
-    if (t & 1) {
-      for (int e = net.prod_ptr[i]; e < net.prod_ptr[i + 1]; ++e)
-        acc = acc + net.p_st[net.prod_ent[e]] * rate[net.prod_r[e]];
-    } else {
-      for (int e = net.loss_ptr[i]; e < net.loss_ptr[i + 1]; ++e)
-        acc = acc + net.r_st[net.loss_ent[e]] * rate[net.loss_r[e]];
+    const int e1 = ptr[i + 1];
+#pragma unroll 4
+    for (int e = ptr[i]; e < e1; ++e) {
+      const uint32_t x = w[e];
+      acc = acc + coef[x >> 16] * rate[x & 0xffffu];
     }
     part[t] = acc;
   }
+}
+
+// The coefficient table of the gathers into shared memory (coef[MAX_COEF]).
+__device__ inline void load_coefs(const NetDev& net, double* coef) {
+  for (int c = threadIdx.x; c < net.n_coef; c += blockDim.x) coef[c] = net.coef_tab[c];
 }
 
 // Dense Jacobian of one layer into jac[ni*ni] (chem.py:183-208): each thread
@@ -106,22 +112,26 @@ __device__ inline void species_sums(const NetDev& net, const double* rate, doubl
 // contributions (jac_split), each summed in the reference's scatter order.
 // Requires blockDim.x == LAYER_THREADS.
 template <typename Store>
-__device__ inline void layer_jacobian_each(const NetDev& net, const double* drate, Store store) {
+__device__ inline void layer_jacobian_each(const NetDev& net, const double* coef, const double* drate, Store store) {
   const int d0 = net.jac_split[threadIdx.x], d1 = net.jac_split[threadIdx.x + 1];
   int e = net.jac_ptr[d0];
   int row = d0 / net.ni, col = d0 - row * net.ni;
   for (int d = d0; d < d1; ++d) {
     const int e1 = net.jac_ptr[d + 1];
     double J = 0.0;
-    for (; e < e1; ++e) J = J + net.jac_coef[e] * drate[net.jac_idx[e]];
+#pragma unroll 4
+    for (; e < e1; ++e) {
+      const uint32_t x = net.jac_w[e];
+      J = J + coef[x >> 16] * drate[x & 0xffffu];
+    }
     store(row, col, J);
     if (++col == net.ni) { col = 0; ++row; }
   }
 }
 
-__device__ inline void layer_jacobian(const NetDev& net, const double* drate, double* jac) {
+__device__ inline void layer_jacobian(const NetDev& net, const double* coef, const double* drate, double* jac) {
   const int ni = net.ni;
-  layer_jacobian_each(net, drate, [&](int row, int col, double J) { jac[row * ni + col] = J; });
+  layer_jacobian_each(net, coef, drate, [&](int row, int col, double J) { jac[row * ni + col] = J; });
 }
 
 // Loads state rows j-1..j+1 (stage 2: yk2 = y + k1/r) and their gas sums.
@@ -216,11 +226,13 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   const double r = ros2_r();
   const double c0 = adj ? 0.0 : 1.0 / (r * dt[b]);
 
+  __shared__ double coefs[MAX_COEF];
+  load_coefs(net, coefs);   // visible after the barriers in load_rows
   load_rows(yb, nullptr, a.gas, nz, ni, j, r, false, L);
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
   __shared__ double supb[VB_MAX_NI], subb[VB_MAX_NI];
   __syncthreads();
-  species_sums(net, L.rate, L.part);
+  species_sums(net, coefs, L.rate, L.part);
   layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);
   __syncthreads();
   // the Jacobian gather writes each block entry in its final form
@@ -230,7 +242,7 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   if (adj) {
     // steady_state_grad.py:153-175: diag = J + diag(A_eddy + A_mol) (+ deposition
     // at the bottom), sup_d = B[:-1], sub_d = C[1:] (no c0, not negated)
-    layer_jacobian_each(net, L.drate, [&](int row, int col, double J) {
+    layer_jacobian_each(net, coefs, L.drate, [&](int row, int col, double J) {
       double v = J;
       if (row == col) {
         v = v + L.diagd[row];
@@ -245,7 +257,7 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
     }
     return;
   }
-  layer_jacobian_each(net, L.drate, [&](int row, int col, double J) {
+  layer_jacobian_each(net, coefs, L.drate, [&](int row, int col, double J) {
     double v = (row == col ? c0 : 0.0) - J;
     if (row == col) {
       // jax_step.py:283,288: the deposition term joins diag_d before -diag_d is added
@@ -294,10 +306,12 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   const bool res = resid != nullptr;   // steady-state residual f(y) (steady_state_grad.py:116-130)
   const double dtb = res ? 1.0 : dt[b];
 
+  __shared__ double coefs[MAX_COEF];
+  load_coefs(net, coefs);   // visible after the barriers in load_rows
   load_rows(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
   __syncthreads();
-  species_sums(net, L.rate, L.part);
+  species_sums(net, coefs, L.rate, L.part);
   layer_diffusion(a, nz, ni, j, flags, L, nullptr, nullptr, false);
   __syncthreads();
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
@@ -322,13 +336,15 @@ chem_kernel(NetDev net, int nz, const double* __restrict__ y, const double* __re
   bool want_jac = jac != nullptr;
   LayerSmem L = carve(smem, ni, net.nr, net.T, want_jac, want_jac);
   const double* yrow = y + ((int64_t)b * nz + j) * ni;
+  __shared__ double coefs[MAX_COEF];
+  load_coefs(net, coefs);
   for (int i = threadIdx.x; i <= ni; i += blockDim.x) L.y3[i] = i < ni ? yrow[i] : 1.0;
   __syncthreads();
   layer_rates(net, L.y3, k + (int64_t)b * (net.nr + 1) * nz + j, nz, M[(int64_t)b * nz + j], L.rate,
               L.drate, want_jac);
   __syncthreads();
-  species_sums(net, L.rate, L.part);
-  if (want_jac) layer_jacobian(net, L.drate, L.jac);
+  species_sums(net, coefs, L.rate, L.part);
+  if (want_jac) layer_jacobian(net, coefs, L.drate, L.jac);
   __syncthreads();
   if (dydt)
     for (int i = threadIdx.x; i < ni; i += blockDim.x)

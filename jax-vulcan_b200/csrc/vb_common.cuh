@@ -15,25 +15,34 @@ struct NetDev {
   const double* r_st;            // [nr+1][T]
   const double* p_st;            // [nr+1][T]
   const uint8_t* three;          // [nr+1]
-  // RHS gather tables: for species i, the (r*T+s) slots whose reactant (loss)
-  // or product (prod) index is i, in increasing flat order (segment_sum order).
+  // Gather tables, one 32-bit word per term: the low 16 bits index a rate
+  // (loss / prod: reaction r) or a drate slot (Jacobian: r*T+s), the high 16
+  // bits a coefficient in coef_tab (the distinct stoichiometries, <= 256).
+  // RHS: for species i, the (r*T+s) slots whose reactant (loss) or product
+  // (prod) index is i, in increasing flat order (segment_sum order); the
+  // coefficient is r_st[r*T+s] or p_st[r*T+s].
   const int32_t* loss_ptr;       // [ni+1]
-  const int32_t* loss_ent;       // slot r*T+s (its stoichiometry is r_st[r*T+s])
-  const int32_t* loss_r;         // reaction r of the slot
+  const uint32_t* loss_w;
   const int32_t* prod_ptr;       // [ni+1]
-  const int32_t* prod_ent;
-  const int32_t* prod_r;
-  // Jacobian gather table: for destination d = row*ni+col, the contributions
-  // (r, o, s) in increasing flat order (r*2T + o)*T + s (chem.py:193-207 scatter
-  // order), each stored as its drate slot r*T+s and signed stoichiometry.
+  const uint32_t* prod_w;
+  // Jacobian: for destination d = row*ni+col, the contributions (r, o, s) in
+  // increasing flat order (r*2T + o)*T + s (chem.py:193-207 scatter order);
+  // the coefficient is -r_st[r][o] (o < T) or p_st[r][o-T].
   const int32_t* jac_ptr;        // [ni*ni+1]
-  const int32_t* jac_idx;        // drate slot r*T+s
-  const double* jac_coef;        // -r_st[r][o] (o < T) or p_st[r][o-T]
+  const uint32_t* jac_w;
+  const double* coef_tab;        // [n_coef]
+  int n_coef;
   // Destination ranges of the LAYER_THREADS threads, balanced by entry count.
   const int32_t* jac_split;      // [LAYER_THREADS+1]
 };
 
 constexpr int LAYER_THREADS = 256;
+constexpr int MAX_COEF = 256;   // distinct stoichiometric coefficients of a network
+
+// Term word of a gather table: index (low 16 bits) and coefficient id.
+__host__ __device__ __forceinline__ uint32_t term_word(int idx, int cid) {
+  return (uint32_t)idx | ((uint32_t)cid << 16);
+}
 
 // Offsets (in doubles) of the fields of one atmosphere in the atm blob.
 struct AtmOff {
