@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -158,20 +159,19 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   }
   if (too_many) return fail(VB_ERR_ARG, "more than 256 distinct stoichiometric coefficients");
   if (coefs.empty()) coefs.push_back(0.0);
-  // destination ranges per thread, balanced by entries (+1 per destination)
-  const int NT = vb::LAYER_THREADS;
-  std::vector<int32_t> split(NT + 1, ni * ni);
+  // destinations in decreasing term count (ties: increasing index); threads
+  // take them in rank bands (thread t: ranks t, t + LAYER_THREADS, ...) so the
+  // lanes of a warp sum lists of similar length. Word: d | row << 16 | col << 24.
+  std::vector<uint32_t> order((size_t)ni * ni);
   {
-    int64_t nd = (int64_t)ni * ni;
-    int64_t total = jp[nd] + nd;
-    int64_t target = (total + NT - 1) / NT, acc = 0;
-    int t = 0;
-    split[0] = 0;
-    for (int64_t d = 0; d < nd; ++d) {
-      acc += (jp[d + 1] - jp[d]) + 1;
-      if (acc >= target * (t + 1) && t + 1 < NT) split[++t] = (int32_t)(d + 1);
+    std::vector<int32_t> perm((size_t)ni * ni);
+    for (size_t d = 0; d < perm.size(); ++d) perm[d] = (int32_t)d;
+    std::stable_sort(perm.begin(), perm.end(),
+                     [&](int32_t x, int32_t y) { return jp[x + 1] - jp[x] > jp[y + 1] - jp[y]; });
+    for (size_t q = 0; q < perm.size(); ++q) {
+      const uint32_t d = (uint32_t)perm[q];
+      order[q] = d | ((d / (uint32_t)ni) << 16) | ((d % (uint32_t)ni) << 24);
     }
-    for (int k = t + 1; k <= NT; ++k) split[k] = (int32_t)nd;
   }
   std::vector<int32_t> ri(R * T), pi(R * T);
   for (int e = 0; e < R * T; ++e) { ri[e] = (int32_t)r_idx[e]; pi[e] = (int32_t)p_idx[e]; }
@@ -185,7 +185,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
       {lw.data(), lw.size() * 4, 0}, {pp.data(), pp.size() * 4, 0},
       {pw.data(), pw.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
       {jw.data(), jw.size() * 4, 0}, {coefs.data(), coefs.size() * 8, 0},
-      {split.data(), split.size() * 4, 0}};
+      {order.data(), order.size() * 4, 0}};
   size_t total = 0;
   for (auto& p : parts) { p.off = total; total += (p.bytes + 255) & ~(size_t)255; }
   void* base = nullptr;
@@ -212,7 +212,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   d.jac_w = (const uint32_t*)(b + parts[10].off);
   d.coef_tab = (const double*)(b + parts[11].off);
   d.n_coef = (int)coefs.size();
-  d.jac_split = (const int32_t*)(b + parts[12].off);
+  d.jac_order = (const uint32_t*)(b + parts[12].off);
   net->base = base;
   net->bytes = total;
   *out = net;

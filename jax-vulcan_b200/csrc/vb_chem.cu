@@ -63,7 +63,7 @@ __device__ inline void layer_rates(const NetDev& net, const double* yrow, const 
     }
     double prod = f[0];
     for (int s = 1; s < T; ++s) prod = prod * f[s];
-    double kr = kcol[(int64_t)r * kstride];
+    double kr = __ldcg(kcol + (int64_t)r * kstride);   // L2 only: the strided column would flush the tables from L1
     double rt = kr * prod;
     bool three = net.three[r] != 0;
     if (three) rt = rt * M;
@@ -107,25 +107,24 @@ __device__ inline void load_coefs(const NetDev& net, double* coef) {
   for (int c = threadIdx.x; c < net.n_coef; c += blockDim.x) coef[c] = net.coef_tab[c];
 }
 
-// Dense Jacobian of one layer into jac[ni*ni] (chem.py:183-208): each thread
-// owns a contiguous run of destinations holding about the same number of
-// contributions (jac_split), each summed in the reference's scatter order.
-// Requires blockDim.x == LAYER_THREADS.
+// Dense Jacobian of one layer (chem.py:183-208), each entry summed in the
+// reference's scatter order. Threads take the destinations in rank bands of
+// decreasing term count (jac_order), so the lanes of a warp run loops of
+// similar length.
 template <typename Store>
 __device__ inline void layer_jacobian_each(const NetDev& net, const double* coef, const double* drate, Store store) {
-  const int d0 = net.jac_split[threadIdx.x], d1 = net.jac_split[threadIdx.x + 1];
-  int e = net.jac_ptr[d0];
-  int row = d0 / net.ni, col = d0 - row * net.ni;
-  for (int d = d0; d < d1; ++d) {
+  const int nd = net.ni * net.ni;
+  for (int q = threadIdx.x; q < nd; q += blockDim.x) {
+    const uint32_t o = net.jac_order[q];
+    const int d = (int)(o & 0xffffu);
     const int e1 = net.jac_ptr[d + 1];
     double J = 0.0;
 #pragma unroll 4
-    for (; e < e1; ++e) {
+    for (int e = net.jac_ptr[d]; e < e1; ++e) {
       const uint32_t x = net.jac_w[e];
       J = J + coef[x >> 16] * drate[x & 0xffffu];
     }
-    store(row, col, J);
-    if (++col == net.ni) { col = 0; ++row; }
+    store((int)((o >> 16) & 0xffu), (int)(o >> 24), J);
   }
 }
 

@@ -32,8 +32,8 @@ struct NetDev {
   const uint32_t* jac_w;
   const double* coef_tab;        // [n_coef]
   int n_coef;
-  // Destination ranges of the LAYER_THREADS threads, balanced by entry count.
-  const int32_t* jac_split;      // [LAYER_THREADS+1]
+  // Destinations in decreasing term count: d | row << 16 | col << 24.
+  const uint32_t* jac_order;     // [ni*ni]
 };
 
 constexpr int LAYER_THREADS = 256;
