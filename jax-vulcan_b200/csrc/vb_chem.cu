@@ -46,40 +46,76 @@ __device__ inline LayerSmem carve(double* s, int ni, int nr, int T, bool jac, bo
   return L;
 }
 
+// Rate (and drate) of reaction slot r with TT terms, in the reference's
+// expression order (chem.py:92-99, 156-182).
+template <int TT>
+__device__ inline void rate_slot(const NetDev& net, int r, const double* yrow, double kr, double M, double* rate,
+                                 double* drate, bool jac) {
+  double f[TT], yr[TT], st[TT];
+#pragma unroll
+  for (int s = 0; s < TT; ++s) {
+    const int idx = net.r_idx[r * TT + s];
+    st[s] = net.r_st[r * TT + s];
+    yr[s] = yrow[idx];
+    f[s] = st[s] > 0.0 ? pow_st(yr[s], st[s]) : 1.0;
+  }
+  double prod = f[0];
+#pragma unroll
+  for (int s = 1; s < TT; ++s) prod = prod * f[s];
+  double rt = kr * prod;
+  const bool three = net.three[r] != 0;
+  if (three) rt = rt * M;
+  rate[r] = rt;
+  if (jac) {
+#pragma unroll
+    for (int s = 0; s < TT; ++s) {
+      double lo = (s == 0) ? 1.0 : f[0];
+#pragma unroll
+      for (int t = 1; t < TT; ++t) lo = lo * ((t == s) ? 1.0 : f[t]);
+      double pm1 = st[s] > 0.0 ? pow_st(yr[s], st[s] - 1.0) : 0.0;
+      double d = st[s] * pm1;
+      d = d * lo;
+      d = d * kr;
+      if (three) d = d * M;
+      drate[r * TT + s] = d;
+    }
+  }
+}
+
+// Rate constants of RU consecutive passes, loaded before any arithmetic so the
+// strided L2 loads overlap (L2 only: the column of k would flush the gather
+// tables from L1).
+template <int TT, int RU>
+__device__ inline void rates_t(const NetDev& net, const double* yrow, const double* kcol, int64_t kstride, double M,
+                               double* rate, double* drate, bool jac) {
+  for (int r0 = threadIdx.x; r0 <= net.nr; r0 += RU * blockDim.x) {
+    double kv[RU];
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int r = r0 + u * blockDim.x;
+      kv[u] = r <= net.nr ? __ldcg(kcol + (int64_t)r * kstride) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int r = r0 + u * blockDim.x;
+      if (r <= net.nr) rate_slot<TT>(net, r, yrow, kv[u], M, rate, drate, jac);
+    }
+  }
+}
+
 // rate[r] = k[r] * prod_s y^st (* M) for every reaction slot of one layer
 // (chem.py:92-99); with jac, also drate[r][s] (chem.py:156-182).
 __device__ inline void layer_rates(const NetDev& net, const double* yrow, const double* kcol,
                                    int64_t kstride, double M, double* rate, double* drate, bool jac) {
-  const int T = net.T;
-  for (int r = threadIdx.x; r <= net.nr; r += blockDim.x) {
-    double f[8];
-    double yr[8];
-    double st[8];
-    for (int s = 0; s < T; ++s) {
-      int idx = net.r_idx[r * T + s];
-      st[s] = net.r_st[r * T + s];
-      yr[s] = yrow[idx];
-      f[s] = st[s] > 0.0 ? pow_st(yr[s], st[s]) : 1.0;
-    }
-    double prod = f[0];
-    for (int s = 1; s < T; ++s) prod = prod * f[s];
-    double kr = __ldcg(kcol + (int64_t)r * kstride);   // L2 only: the strided column would flush the tables from L1
-    double rt = kr * prod;
-    bool three = net.three[r] != 0;
-    if (three) rt = rt * M;
-    rate[r] = rt;
-    if (jac) {
-      for (int s = 0; s < T; ++s) {
-        double lo = (s == 0) ? 1.0 : f[0];
-        for (int t = 1; t < T; ++t) lo = lo * ((t == s) ? 1.0 : f[t]);
-        double pm1 = st[s] > 0.0 ? pow_st(yr[s], st[s] - 1.0) : 0.0;
-        double d = st[s] * pm1;
-        d = d * lo;
-        d = d * kr;
-        if (three) d = d * M;
-        drate[r * T + s] = d;
-      }
-    }
+  switch (net.T) {
+    case 1: rates_t<1, 6>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    case 2: rates_t<2, 6>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    case 3: rates_t<3, 6>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    case 4: rates_t<4, 6>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    case 5: rates_t<5, 4>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    case 6: rates_t<6, 4>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    case 7: rates_t<7, 4>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    default: rates_t<8, 4>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
   }
 }
 
