@@ -135,6 +135,134 @@ class Ros2Step:
         return sol, delta, self.status
 
 
+class RaggedRos2Step:
+    """Ros2 step for atmospheres of one network with different layer counts
+    (the ``zoff`` path of ``vb_ros2_step``).
+
+    State, rates and the atmosphere are packed by layers: atmosphere b holds
+    layers ``zoff[b]..zoff[b+1]-1`` of ``y [L, ni]``, the block
+    ``[nr+1, nz_b]`` at ``k[zoff[b]*(nr+1):]`` and its own atmosphere blob.
+    ``pack`` / ``unpack`` convert from and to per-atmosphere arrays.
+    """
+
+    def __init__(self, net: NetworkArrays, atms):
+        self.net = net
+        atms = list(atms)
+        self.batch = len(atms)
+        blobs = [pack_atm(a)[0] for a in atms]
+        flags = {atm_flags(a) for a in atms}
+        if len(flags) != 1:
+            raise ValueError("all atmospheres of a ragged batch share the four transport flags")
+        self.flags = flags.pop()
+        ni = net.ni
+        self.nzs = [int((b.numel() - 6 * ni) // (8 + 3 * ni)) for b in blobs]
+        if min(self.nzs) < 2:
+            raise ValueError("every atmosphere needs nz >= 2")
+        self.nz_max = max(self.nzs)
+        self.zoff_host = np.concatenate([[0], np.cumsum(self.nzs)]).astype(np.int64)
+        self.zoff = torch.as_tensor(self.zoff_host, device="cuda")
+        self.layers = int(self.zoff_host[-1])
+        self.blob = torch.cat(blobs).contiguous()
+        L = _lib.lib()
+        self.ws_bytes = int(L.vb_ros2_workspace_bytes(self.batch, self.nz_max, ni, self.zoff_host.ctypes.data))
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
+        self.status = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
+
+    def pack(self, ys, ks):
+        """Per-atmosphere y [nz_b, ni] and k [nr+1, nz_b] -> packed device tensors."""
+        y = torch.cat([as_device(v).reshape(-1, self.net.ni) for v in ys]).contiguous()
+        k = torch.cat([as_device(v).reshape(-1) for v in ks]).contiguous()
+        return y, k
+
+    def unpack(self, t):
+        """Packed [L, ni] -> list of [nz_b, ni] views."""
+        return [t[self.zoff_host[b]:self.zoff_host[b + 1]] for b in range(self.batch)]
+
+    def __call__(self, y, k, dt, fix_mask=None, out=None, stream=None):
+        """y [L, ni], k [sum (nr+1)*nz_b], dt [B] -> (sol, delta, status)."""
+        y = as_device(y).reshape(self.layers, self.net.ni)
+        k = as_device(k).reshape(-1)
+        if k.numel() != self.layers * (self.net.nr + 1):
+            raise ValueError("k must hold (nr+1)*nz_b values per atmosphere")
+        dt = as_device(dt).reshape(-1)
+        if dt.numel() == 1 and self.batch > 1:
+            dt = dt.expand(self.batch).contiguous()
+        fm = None if fix_mask is None else as_device(fix_mask, torch.uint8).reshape(self.layers, self.net.ni)
+        if out is None:
+            sol = torch.empty_like(y)
+            delta = torch.empty_like(y)
+        else:
+            sol, delta = out
+        _lib.check(_lib.lib().vb_ros2_step(
+            self.net.handle, self.batch, self.nz_max, _lib.ptr(self.zoff), _lib.ptr(y), _lib.ptr(k), _lib.ptr(dt),
+            _lib.ptr(self.blob), self.flags, _lib.ptr(fm), _lib.ptr(sol), _lib.ptr(delta), _lib.ptr(self.status),
+            _lib.ptr(self.ws), self.ws_bytes, _lib.stream_handle(stream)), "vb_ros2_step")
+        return sol, delta, self.status
+
+
+class MultiNetworkBatch:
+    """One Ros2 step for atmospheres of several networks and uneven layer
+    counts (the batched use of the reference step under ``vmap``, one group
+    per network): the groups run on their own CUDA streams, and ``capture``
+    records the whole batch step as one CUDA graph for replay.
+
+    ``cases``: sequence of ``(net, atm, y, k, dt)`` with ``y [nz, ni]``,
+    ``k [nr+1, nz]``; results come back in the order given.
+    """
+
+    def __init__(self, cases):
+        cases = list(cases)
+        groups = {}
+        for idx, (net, atm, y, k, dt) in enumerate(cases):
+            groups.setdefault(id(net), []).append(idx)
+        self.groups = []
+        for idxs in groups.values():
+            net = cases[idxs[0]][0]
+            step = RaggedRos2Step(net, [cases[i][1] for i in idxs])
+            y, k = step.pack([cases[i][2] for i in idxs], [cases[i][3] for i in idxs])
+            dt = torch.as_tensor(np.array([float(cases[i][4]) for i in idxs]), dtype=torch.float64, device="cuda")
+            sol, delta = torch.empty_like(y), torch.empty_like(y)
+            self.groups.append(dict(idx=idxs, step=step, y=y, k=k, dt=dt, sol=sol, delta=delta,
+                                    stream=torch.cuda.Stream()))
+        self.batch = len(cases)
+        self.graph = None
+
+    def _launch(self):
+        main = torch.cuda.current_stream()
+        for g in self.groups:
+            g["stream"].wait_stream(main)
+            with torch.cuda.stream(g["stream"]):
+                g["step"](g["y"], g["k"], g["dt"], out=(g["sol"], g["delta"]), stream=g["stream"])
+        for g in self.groups:
+            main.wait_stream(g["stream"])
+
+    def step(self):
+        """Steps every atmosphere (replays the graph when captured)."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._launch()
+
+    def capture(self):
+        """Records one batch step (all groups) as a CUDA graph."""
+        self._launch()                     # warm: kernel attributes set outside capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._launch()
+        self.graph = g
+        return g
+
+    def results(self):
+        """(sol, delta, status) per atmosphere, in the order of ``cases``."""
+        out = [None] * self.batch
+        for g in self.groups:
+            sols, deltas = g["step"].unpack(g["sol"]), g["step"].unpack(g["delta"])
+            for j, i in enumerate(g["idx"]):
+                out[i] = (sols[j], deltas[j], g["step"].status[j])
+        return out
+
+
 def jax_ros2_step(y, k_arr, dt, atm: AtmStatic, net: NetworkArrays, fix_mask=None):
     """One 2nd-order Rosenbrock step -> (sol, delta_arr) (reference `jax_step.py:249-315`).
 
