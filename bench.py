@@ -186,6 +186,57 @@ def fp64_peak_tflops(lib, torch, stream):
     return best
 
 
+def run_config2(args, torch):
+    """The uneven batch: 256 atmospheres, nz ~ U[60, 200], ni in {30, 69, 89}
+    (three networks), per-atmosphere T offset, Kzz scale and dt, stepped as
+    one CUDA-graph replay of the multi-network batch, next to the same
+    atmospheres stepped one at a time."""
+    syn, chem, jstep = pkg("synthetic"), pkg("chem"), pkg("jax_step")
+    nets, cases = syn.config2_batch(seed=2, batch=args.batch or 256)
+    dev = {id(n): chem.to_device(n.tables) for n in nets.values()}
+    items = [(dev[id(c.net)], jstep.atm_from_dict(c.atm), c.y, c.k, c.dt) for c in cases]
+    batch = jstep.MultiNetworkBatch(items)
+    batch.capture()
+    for _ in range(args.warmup):
+        batch.step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        batch.step()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    # the same atmospheres, one single-instance step after another
+    singles = [(jstep.Ros2Step(it[0], it[1]), torch.as_tensor(it[2], device="cuda"),
+                torch.as_tensor(it[3], device="cuda"), torch.full((1,), it[4], dtype=torch.float64, device="cuda"))
+               for it in items]
+    outs = [(torch.empty_like(y), torch.empty_like(y)) for _, y, _, _ in singles]
+    for (st, y, k, dt), o in zip(singles, outs):
+        st(y, k, dt, out=o)
+    torch.cuda.synchronize()
+    e0.record()
+    for (st, y, k, dt), o in zip(singles, outs):
+        st(y, k, dt, out=o)
+    e1.record()
+    torch.cuda.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    n = len(cases)
+    layers = sum(c.y.shape[0] for c in cases)
+    return {"metric": METRIC, "value": n / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uneven batch; stiff k)",
+            "config": {"workload": f"uneven batch of {n} atmospheres, nz in [60, 200] ({layers} layers), "
+                                   f"ni in {{30, 69, 89}} (370/1400/2000 reactions), one CUDA-graph replay",
+                       "groups": len(batch.groups), "l2": "inputs larger than L2, no flush"},
+            "sequential_single_instance": {"value": n / (seq_ms * 1e-3), "unit": UNIT, "ms_per_pass": seq_ms},
+            "speedup_vs_sequential": seq_ms / ms, "gpu_launches": 6 * len(batch.groups) * args.steps,
+            "clocks": clk}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -195,6 +246,8 @@ def main():
                     help="atmospheres per GPU (default: two per SM, 296 on a B200)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config0", choices=["config0", "config2"],
+                    help="config0: the headline batch (default); config2: the uneven multi-network batch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -212,6 +265,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
+    if args.workload == "config2":
+        if rank == 0:
+            print(json.dumps(run_config2(args, torch)), flush=True)
+        return
     _lib = pkg("_lib")
     chem = pkg("chem")
     jstep = pkg("jax_step")
