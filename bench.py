@@ -39,10 +39,31 @@ def pkg(name):
     return importlib.import_module("jax-vulcan_b200." + name)
 
 
+def rank_seeds(B, rank):
+    """Seeds of the atmospheres a rank steps: disjoint across ranks (replicas
+    over independent atmospheres, no data-path collective)."""
+    return [1000 * rank + b for b in range(B)]
+
+
+def max_over_ranks(x, dist, world, device):
+    """The max of a per-rank timing over all ranks (one all-reduce)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, B, ms):
+    """Whole-job throughput: atmospheres of all ranks per second of the slowest rank."""
+    return world * B / (ms * 1e-3)
+
+
 def make_batch(B, rank, nz=120):
     syn = pkg("synthetic")
     net = syn.make_network(0, 69, 700)
-    cases = [syn.make_case(seed=(1000 * rank + b,), net=net, nz=nz) for b in range(B)]
+    cases = [syn.make_case(seed=(sd,), net=net, nz=nz) for sd in rank_seeds(B, rank)]
     Y = np.stack([c.y for c in cases])
     K = np.stack([c.k for c in cases])
     DT = np.array([c.dt for c in cases])
@@ -305,13 +326,10 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, world, "cuda")
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * B / (ms * 1e-3)
+    value = job_value(world, B, ms)
 
     # per-kernel device times over a separate profiled pass (events on the launch stream)
     L.vb_profile(1)
@@ -351,11 +369,7 @@ def main():
         e2e_step()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, world, "cuda")
     h2d = y_h.numel() * 8 + dt_h.numel() * 8
     d2h = 2 * y_h.numel() * 8
 
@@ -407,7 +421,7 @@ def main():
                        "precision": "fp64", "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 (rates {K.nbytes / 1e6:.0f} MB + solver workspace "
                              f"{step.ws_bytes / 1e6:.0f} MB per GPU), no flush"},
-            "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "e2e": {"value": job_value(world, B, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
                     "note": "y and dt copied in from pinned host memory, sol and delta read back, every step; "
                             "rates and atmosphere stay resident (as in the reference runner's device carry)"},
