@@ -396,9 +396,11 @@ def main():
     achieved = fac_flops / (fac_ms * 1e-3) / 1e12 if fac_ms > 0 else 0.0
     # algorithmic bytes of the factor: read each D_j, write each inverse (ni^2 doubles each)
     fac_bytes = B * nz * 2.0 * ni * ni * 8
-    # DRAM read + write bytes of one factor launch measured by ncu on 32 atmospheres
-    # (dram__bytes_read.sum + dram__bytes_write.sum = 154.9 MB + 92.5 MB), scaled by atmospheres
-    fac_traffic = (154.92e6 + 92.51e6) / 32 * B
+    # DRAM read + write bytes of one factor launch measured by ncu, per atmosphere,
+    # scaled to the batch: 8-warp layout (two atmospheres per SM) on 160 atmospheres
+    # (776.3 MB + 700.8 MB), 12-warp layout on 32 atmospheres (154.9 MB + 96.9 MB)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    fac_traffic = ((776.26e6 + 700.78e6) / 160 if B > n_sm else (154.86e6 + 96.91e6) / 32) * B
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -431,7 +433,7 @@ def main():
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 else None, "traffic": fac_traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one factor "
-                                           "launch on 32 atmospheres, scaled to the batch",
+                                           "launch of the same layout, per atmosphere, scaled to the batch",
                          "peak_source": "measured live: FP64 FMA probe kernel (vb_fp64_probe); "
                                         "MEASURED_PEAKS.json has no FP64 figure",
                          "algorithmic": f"2*ni^3 flops per layer block x {nz} layers x {B} atmospheres",
