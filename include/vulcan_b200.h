@@ -121,6 +121,24 @@ int vb_bt_solve(int batch, int nz, int ni, const void* factors, const double* rh
 int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* rhs, double* x,
                   void* stream);
 
+/* Mixed-precision block solve (the solver of reference solver.py:33-112 with
+ * the demotion inside, same FP64 interface): the diagonal blocks are factored
+ * and inverted in FP32, the solution is refined in FP64 on the full
+ * block-tridiagonal system (r = rhs - M x from the FP64 blocks, x += M~^{-1} r
+ * with the FP32 inverses) until max|correction| <= tol * max|x|, at most
+ * max_refine passes after the first solve. Atmospheres whose refinement
+ * stalls are refactored and solved in FP64 and get VB_STATUS_REFINE_STALL.
+ *   vb_bt_mixed_bytes:  size of the factors buffer (FP64 blocks, FP32 and FP64
+ *                       inverses, per-atmosphere state).
+ *   vb_bt_factor_mixed: diag, sup_d, sub_d as vb_bt_factor -> factors, status.
+ *   vb_bt_solve_mixed:  rhs -> x (must not alias rhs); status |= stall bits;
+ *                       passes [B] (nullable): solve + refinement passes run. */
+size_t vb_bt_mixed_bytes(int batch, int nz, int ni);
+int vb_bt_factor_mixed(int batch, int nz, int ni, const double* diag, const double* sup_d,
+                       const double* sub_d, void* factors, int32_t* status, void* stream);
+int vb_bt_solve_mixed(int batch, int nz, int ni, void* factors, const double* rhs, double* x,
+                      int max_refine, double tol, int32_t* status, int32_t* passes, void* stream);
+
 /* Steady-state residual f(y) = chem_rhs + diffusion (reference
  * steady_state_grad.py:116-130) of a (possibly ragged) batch -> f [B][nz][ni]. */
 int vb_residual(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,

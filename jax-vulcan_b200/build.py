@@ -27,6 +27,7 @@ UNITS = {
     "vb_photo.cu": ["--fmad=false"],
     "vb_adjoint.cu": [],
     "vb_control.cu": ["--fmad=false"],
+    "vb_mixed.cu": [],
 }
 
 

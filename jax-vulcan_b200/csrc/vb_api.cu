@@ -364,6 +364,78 @@ int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* 
   return bt_solve(batch, nz, ni, factors, rhs, x, 1, stream);
 }
 
+// ---- mixed-precision block solve: factors buffer layout (256-byte aligned parts)
+namespace {
+struct MixedLayout {
+  size_t w64, inv32, inv64, state, fallback, passes, total;
+};
+MixedLayout mixed_layout(int batch, int nz, int ni) {
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t L = (size_t)batch * nz, blk = (size_t)ni * vb::round_even(ni);
+  MixedLayout m;
+  m.w64 = 0;
+  m.inv32 = al(L * vb::ws_per_layer(ni, vb::round_even(ni)) * sizeof(double));
+  m.inv64 = m.inv32 + al(L * blk * sizeof(float));
+  m.state = m.inv64 + al(L * blk * sizeof(double));
+  m.fallback = m.state + al((size_t)batch * 4);
+  m.passes = m.fallback + al((size_t)batch * 4);
+  m.total = m.passes + al((size_t)batch * 4);
+  return m;
+}
+}  // namespace
+
+size_t vb_bt_mixed_bytes(int batch, int nz, int ni) {
+  if (batch < 1 || nz < 1 || ni < 1) return 0;
+  return mixed_layout(batch, nz, ni).total;
+}
+
+int vb_bt_factor_mixed(int batch, int nz, int ni, const double* diag, const double* sup_d, const double* sub_d,
+                       void* factors, int32_t* status, void* stream) {
+  if (!diag || !sup_d || !sub_d || !factors || !status) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "bad shape");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = bt_batch(batch, nz, ni);
+  const MixedLayout m = mixed_layout(batch, nz, ni);
+  char* base = (char*)factors;
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  VB_CHECK(vb::launch_pack_blocks(B, diag, sup_d, sub_d, (double*)(base + m.w64), st), "pack");
+  VB_CHECK(vb::launch_factor_into<float>(B, (double*)(base + m.w64), (float*)(base + m.inv32), nullptr, status, st),
+           "fp32 factor");
+  return VB_OK;
+}
+
+int vb_bt_solve_mixed(int batch, int nz, int ni, void* factors, const double* rhs, double* x, int max_refine,
+                      double tol, int32_t* status, int32_t* passes, void* stream) {
+  if (!factors || !rhs || !x || !status) return fail(VB_ERR_ARG, "null argument");
+  if (x == rhs) return fail(VB_ERR_ARG, "x must not alias rhs");
+  if (batch < 1 || nz < 1 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "bad shape");
+  if (max_refine < 1 || max_refine > 8) return fail(VB_ERR_ARG, "max_refine must be in [1, 8]");
+  if (!(tol > 0.0)) return fail(VB_ERR_ARG, "tol must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = bt_batch(batch, nz, ni);
+  const MixedLayout m = mixed_layout(batch, nz, ni);
+  char* base = (char*)factors;
+  double* ws = (double*)(base + m.w64);
+  int32_t* state = (int32_t*)(base + m.state);
+  int32_t* fb = (int32_t*)(base + m.fallback);
+  int32_t* np = (int32_t*)(base + m.passes);
+  VB_CHECK(cudaMemsetAsync(state, 0, sizeof(int32_t) * batch, st), "state reset");
+  VB_CHECK(cudaMemsetAsync(np, 0, sizeof(int32_t) * batch, st), "passes reset");
+  const float* inv32 = (const float*)(base + m.inv32);
+  VB_CHECK(vb::launch_refine<float>(B, ws, inv32, rhs, x, state, np, tol, 1, nullptr, st), "fp32 solve");
+  for (int it = 0; it < max_refine; ++it)
+    VB_CHECK(vb::launch_refine<float>(B, ws, inv32, rhs, x, state, np, tol, 0, nullptr, st), "refinement");
+  VB_CHECK(vb::launch_refine_finalize(batch, state, fb, status, st), "finalize");
+  // FP64 fallback for the atmospheres whose refinement stalled (the others skip)
+  double* inv64 = (double*)(base + m.inv64);
+  VB_CHECK(vb::launch_factor_into<double>(B, ws, inv64, fb, status, st), "fp64 factor");
+  VB_CHECK(vb::launch_refine<double>(B, ws, inv64, rhs, x, state, np, tol, 1, fb, st), "fp64 solve");
+  VB_CHECK(vb::launch_refine<double>(B, ws, inv64, rhs, x, state, np, tol, 0, fb, st), "fp64 refinement");
+  if (passes)
+    VB_CHECK(cudaMemcpyAsync(passes, np, sizeof(int32_t) * batch, cudaMemcpyDeviceToDevice, st), "passes");
+  return VB_OK;
+}
+
 int vb_residual(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
                 const double* atm, int32_t flags, double* f, void* stream) {
   if (!net || !y || !k || !atm || !f) return fail(VB_ERR_ARG, "null argument");

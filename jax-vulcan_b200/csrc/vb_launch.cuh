@@ -50,6 +50,14 @@ cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const
 cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
                            double* J_br_T, double* k, cudaStream_t);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
+template <typename R>
+cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,
+                          int32_t* passes, double tol, int first, const int32_t* only, cudaStream_t st);
+cudaError_t launch_refine_finalize(int batch, const int32_t* state, int32_t* fallback, int32_t* status,
+                                   cudaStream_t st);
+template <typename R>
+cudaError_t launch_factor_into(const Batch& B, double* ws, R* out, const int32_t* only, int32_t* status,
+                               cudaStream_t st);
 cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_t* gas, const double* compo,
                              const double* atom_ini, const double* atm, const uint8_t* fix_mask,
                              const double* fix_y, const double* sol, const double* delta, double* y,

@@ -17,7 +17,7 @@
 
 namespace vb {
 
-template <int NP, int NW, int PW>
+template <int NP, int NW, int PW, typename R = double>
 struct LUK {
   static constexpr int RPW = NP / NW;     // rows per warp
   static constexpr int CPL = NP / 32;     // columns per lane
@@ -34,7 +34,7 @@ struct LUK {
                + (size_t)PW * NP         // V: pivot rows of the current panel
                + 2 * (size_t)NP          // vec, rdiag
                + PW + PW * PW;           // pivot row broadcast, L_KK^{-1}
-    return d * sizeof(double) + sizeof(int) * 2 * NP;
+    return d * sizeof(R) + sizeof(int) * 2 * NP;
   }
 };
 
@@ -43,6 +43,15 @@ __device__ __forceinline__ unsigned long long pivot_key(double v) {
   double a = fabs(v);
   return (a >= 0.0) ? (unsigned long long)__double_as_longlong(a) : 0ull;
 }
+__device__ __forceinline__ unsigned long long pivot_key(float v) {
+  float a = fabsf(v);
+  return (a >= 0.0f) ? ((unsigned long long)__float_as_uint(a) << 32) : 0ull;
+}
+
+// Two values of the factor's element type handed over in one shared-memory access.
+template <typename R> struct Pair;
+template <> struct Pair<double> { using T = double2; };
+template <> struct Pair<float> { using T = float2; };
 
 // Unblocked LU of one PW-column panel by one warp (lane l holds rows
 // l + 32 r in registers): for each column the argmax over unpivoted rows
@@ -50,19 +59,19 @@ __device__ __forceinline__ unsigned long long pivot_key(double v) {
 // row), the pivot row broadcast by shuffles, and the rank-1 update of the
 // panel's remaining columns. Kept out of line so its registers do not compete
 // with the caller's tile.
-template <int PRL, int PW, int PLD>
-__device__ __noinline__ void panel_lu(double* Pn, int n, int k0, int kw, unsigned& usedw_io, int& st_io,
+template <int PRL, int PW, int PLD, typename R>
+__device__ __noinline__ void panel_lu(R* Pn, int n, int k0, int kw, unsigned& usedw_io, int& st_io,
                                       int* pivs, int* qinv, int lane) {
   const unsigned FULL = 0xffffffffu;
   unsigned usedw = usedw_io;
   int st_local = 0;
   // the panel in registers: lane l holds rows l + 32 r, all PW columns
-  double pv[PRL][PW];
+  R pv[PRL][PW];
 #pragma unroll
   for (int r = 0; r < PRL; ++r) {
     const int i = lane + 32 * r;
 #pragma unroll
-    for (int u = 0; u < PW; ++u) pv[r][u] = i < n ? Pn[i * PLD + u] : 0.0;
+    for (int u = 0; u < PW; ++u) pv[r][u] = i < n ? Pn[i * PLD + u] : R(0);
   }
 #pragma unroll
   for (int t = 0; t < PW; ++t) {
@@ -84,22 +93,22 @@ __device__ __noinline__ void panel_lu(double* Pn, int n, int k0, int kw, unsigne
       if ((p & 31) == lane) usedw |= 1u << (p >> 5);
       // broadcast the pivot row (columns t..PW-1) from its owner lane
       const int po = p & 31, pslot = p >> 5;
-      double pr[PW];
+      R pr[PW];
 #pragma unroll
       for (int u = t; u < PW; ++u) {
-        double v = pv[0][u];
+        R v = pv[0][u];
 #pragma unroll
         for (int r = 1; r < PRL; ++r) v = (pslot == r) ? pv[r][u] : v;
         pr[u] = __shfl_sync(FULL, v, po);
       }
-      const double piv = pr[t];
-      if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
-      const double rcp = 1.0 / piv;
+      const R piv = pr[t];
+      if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
+      const R rcp = R(1) / piv;
 #pragma unroll
       for (int r = 0; r < PRL; ++r) {
         const int i = lane + 32 * r;
         if (i < n && !((usedw >> r) & 1u)) {
-          const double l = pv[r][t] * rcp;
+          const R l = pv[r][t] * rcp;
           pv[r][t] = l;
 #pragma unroll
           for (int u = t + 1; u < PW; ++u) pv[r][u] = fma(-l, pr[u], pv[r][u]);
@@ -137,25 +146,26 @@ __device__ __noinline__ void panel_lu(double* Pn, int n, int k0, int kw, unsigne
 //    solves for the RPW columns w*RPW.. of X = A'^{-1} with warp-synchronous
 //    column-oriented substitution (no block barrier), so X lands in natural
 //    row order.
-template <int NP, int NW, int PW, int MB>
-__device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ inv,
+template <int NP, int NW, int PW, int MB, typename R>
+__device__ void factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
                                   const double* __restrict__ supn, const double* __restrict__ subn,
                                   double* __restrict__ rhs, int32_t* status, char* smem_raw) {
-  using G = LUK<NP, NW, PW>;
+  using G = LUK<NP, NW, PW, R>;
+  using R2 = typename Pair<R>::T;
   constexpr int RPW = G::RPW, CPL = G::CPL, PRL = G::PRL, SLD = G::SLD, PLD = G::PLD;
   constexpr int CB = RPW > 8 ? (RPW + 1) / 2 : RPW;   // inverse columns per pass
   constexpr int NCH = (RPW + CB - 1) / CB;
-  static_assert(CB % 2 == 0, "x_k is handed over as double2");
+  static_assert(CB % 2 == 0, "x_k is handed over in pairs");
   static_assert(NW * NP + NW * 2 * CB <= 2 * G::PBUF, "broadcast buffers must fit the panel buffers");
-  double* S = reinterpret_cast<double*>(smem_raw);          // [NP][SLD]
-  double* Pn0 = S + NP * SLD;                               // [PBUF]
-  double* Pn1 = Pn0 + G::PBUF;                              // [PBUF]
-  double* Mb = Pn1 + G::PBUF;                               // [NP][PLD]
-  double* V = Mb + NP * PLD;                                // [PW][NP]
-  double* vec = V + PW * NP;                                // [NP]
-  double* rdiag = vec + NP;                                 // [NP]
-  double* prow_s = rdiag + NP;                              // [PW]
-  double* Linv = prow_s + PW;                               // [PW][PW]
+  R* S = reinterpret_cast<R*>(smem_raw);                    // [NP][SLD]
+  R* Pn0 = S + NP * SLD;                                    // [PBUF]
+  R* Pn1 = Pn0 + G::PBUF;                                   // [PBUF]
+  R* Mb = Pn1 + G::PBUF;                                    // [NP][PLD]
+  R* V = Mb + NP * PLD;                                     // [PW][NP]
+  R* vec = V + PW * NP;                                     // [NP]
+  R* rdiag = vec + NP;                                      // [NP]
+  R* prow_s = rdiag + NP;                                   // [PW]
+  R* Linv = prow_s + PW;                                    // [PW][PW]
   int* pivs = reinterpret_cast<int*>(Linv + PW * PW);       // [NP] pivot row of step k
   int* qinv = pivs + NP;                                    // [NP] step of row i (-1: not yet)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -163,14 +173,14 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   int st_local = 0;
 
   if (rhs) {
-    for (int i = threadIdx.x; i < NP; i += blockDim.x) vec[i] = i < n ? rhs[i] : 0.0;
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) vec[i] = i < n ? (R)rhs[i] : R(0);
   }
   const int npan = (n + PW - 1) / PW;
 
-  double a[RPW][CPL];
+  R a[RPW][CPL];
   for (int j = 0; j < nz; ++j) {
-    const double* D = inv + (int64_t)j * n * ld;
-    const double* Dp = inv + (int64_t)(j > 0 ? j - 1 : 0) * n * ld;   // Inv_{j-1}
+    const double* D = Din + (int64_t)j * n * ld;
+    const R* Dp = out + (int64_t)(j > 0 ? j - 1 : 0) * n * ld;   // Inv_{j-1}
     for (int i = threadIdx.x; i < NP; i += blockDim.x) qinv[i] = -1;
     // ---- load D_j and apply the Hadamard Schur update from Inv_{j-1} (solver.py:47)
 #pragma unroll
@@ -184,10 +194,10 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
           v = D[(int64_t)i * ld + col];
           if (j > 0) {
             double cb = subn[(int64_t)(j - 1) * n + i] * supn[(int64_t)(j - 1) * n + col];
-            v = v - cb * Dp[(int64_t)i * ld + col];
+            v = v - cb * (double)Dp[(int64_t)i * ld + col];
           }
         }
-        a[r][c] = v;
+        a[r][c] = (R)v;
       }
     }
     unsigned usedw = 0;     // warp 0: rows lane + 32*r already pivoted
@@ -195,7 +205,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
     for (int pb = 0; pb < npan; ++pb) {
       const int k0 = pb * PW;
       const int kw = min(PW, n - k0);
-      double* Pn = (pb & 1) ? Pn1 : Pn0;
+      R* Pn = (pb & 1) ? Pn1 : Pn0;
       // (a) owners of the panel columns stage them
 #pragma unroll
       for (int c = 0; c < CPL; ++c) {
@@ -215,7 +225,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         for (int r = 0; r < RPW; ++r)
 #pragma unroll
           for (int c = 0; c < CPL; ++c) Mb[(r * CPL + c) * 32 + lane] = a[r][c];
-        panel_lu<PRL, PW, PLD>(Pn, n, k0, kw, usedw, st_local, pivs, qinv, lane);
+        panel_lu<PRL, PW, PLD, R>(Pn, n, k0, kw, usedw, st_local, pivs, qinv, lane);
 #pragma unroll
         for (int r = 0; r < RPW; ++r)
 #pragma unroll
@@ -224,12 +234,12 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         // L_KK^{-1} (unit lower): lane s builds column s from the pivot rows' multipliers
         if (lane < PW) {
           const int sc = lane;
-          double li[PW];
+          R li[PW];
 #pragma unroll
           for (int t = 0; t < PW; ++t) {
-            double x = (t == sc) ? 1.0 : 0.0;
+            R x = (t == sc) ? R(1) : R(0);
             if (t > sc && t < kw) {
-              const double* lrow = Pn + pivs[k0 + t] * PLD;
+              const R* lrow = Pn + pivs[k0 + t] * PLD;
 #pragma unroll
               for (int m = 0; m < t; ++m)
                 if (m >= sc) x = fma(-lrow[m], li[m], x);
@@ -248,15 +258,15 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         const int r = e / PW, u = e - r * PW;
         const int i = warp * RPW + r;
         const int q = i < n ? qinv[i] : -2;
-        double x = 0.0;
+        R x = R(0);
         if (i < n && q < 0) {
-          const double* row = Pn + i * PLD;
+          const R* row = Pn + i * PLD;
 #pragma unroll
           for (int s2 = 0; s2 < PW; ++s2)
             if (s2 >= u && s2 < kw) x = fma(-row[s2], Linv[s2 * PW + u], x);
         } else if (q >= k0 && q < k0 + kw) {
           const int t = q - k0;
-          x = (u <= t) ? Linv[t * PW + u] - (u == t ? 1.0 : 0.0) : 0.0;
+          x = (u <= t) ? Linv[t * PW + u] - (u == t ? R(1) : R(0)) : R(0);
         }
         Mb[i * PLD + u] = x;
       }
@@ -281,18 +291,18 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
 #pragma unroll
       for (int c0s = 0; c0s < CPL; c0s += VC) {
         if (32 * (c0s + VC) - 1 < k0) continue;   // these column slots are left of the panel
-        double vv[PW][VC];
+        R vv[PW][VC];
 #pragma unroll
         for (int t = 0; t < PW; ++t)
 #pragma unroll
-          for (int cv = 0; cv < VC; ++cv) vv[t][cv] = t < kw ? V[t * NP + lane + 32 * (c0s + cv)] : 0.0;
+          for (int cv = 0; cv < VC; ++cv) vv[t][cv] = t < kw ? V[t * NP + lane + 32 * (c0s + cv)] : R(0);
 #pragma unroll
         for (int r = 0; r < RPW; ++r) {
           const int i = warp * RPW + r;
           if (i >= n) break;
           const int q = qinv[i];
           if (q >= 0 && q < k0) continue;
-          double mi[PW];
+          R mi[PW];
 #pragma unroll
           for (int t = 0; t < PW; ++t) mi[t] = Mb[i * PLD + t];
 #pragma unroll
@@ -303,7 +313,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
             if (col >= k0 && col < k0 + PW) {
               a[r][c] = Pn[i * PLD + (col - k0)];
             } else if (col >= k0 + PW) {
-              double acc = a[r][c];
+              R acc = a[r][c];
 #pragma unroll
               for (int t = 0; t < PW; ++t) acc = fma(mi[t], vv[t][cv], acc);
               a[r][c] = acc;
@@ -324,7 +334,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) rdiag[k] = 1.0 / S[k * SLD + k];
+    for (int k = threadIdx.x; k < n; k += blockDim.x) rdiag[k] = R(1) / S[k * SLD + k];
     __syncthreads();
     // ================================================================ inverse by column blocks
     // X = U^{-1} L^{-1} P (lu_solve(LU, I)), columns split over warps: warp w
@@ -334,26 +344,26 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
     // Lane l holds rows l + 32 t; no block barrier (the factors in S are read
     // only). Each finished chunk goes straight to global memory (natural row
     // order) and into the partial products Inv_j * rhs_j.
-    double* O = inv + (int64_t)j * n * ld;
+    R* O = out + (int64_t)j * n * ld;
     // per-warp double buffer through which the owner lane of step k hands x_k
     // to the warp (after the rhs partial products in Pn0..Pn1)
-    double* xb = Pn0 + NW * NP + warp * 2 * CB;
-    double pu[PRL];
+    R* xb = Pn0 + NW * NP + warp * 2 * CB;
+    R pu[PRL];
 #pragma unroll
-    for (int t = 0; t < PRL; ++t) pu[t] = 0.0;
+    for (int t = 0; t < PRL; ++t) pu[t] = R(0);
 #pragma unroll 1
     for (int h = 0; h < NCH; ++h) {
       const int c0 = warp * RPW + h * CB;
       const int cbw = min(min(CB, RPW - h * CB), n - c0);
       if (cbw <= 0) break;
-      double x[PRL][CB];
+      R x[PRL][CB];
       int kmin = n;
 #pragma unroll
       for (int cc = 0; cc < CB; ++cc) {
         const int q = cc < cbw ? qinv[c0 + cc] : n;
         kmin = min(kmin, q);
 #pragma unroll
-        for (int t = 0; t < PRL; ++t) x[t][cc] = (lane + 32 * t == q) ? 1.0 : 0.0;
+        for (int t = 0; t < PRL; ++t) x[t][cc] = (lane + 32 * t == q) ? R(1) : R(0);
       }
       // forward: steps k of segment sg = k / 32 are owned by slot sg (compile time)
 #pragma unroll
@@ -361,16 +371,16 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         const int ke = min(n - 1, 32 * sg + 32);
         for (int k = max(kmin, 32 * sg); k < ke; ++k) {
           const int owner = k & 31;
-          double2* slot = reinterpret_cast<double2*>(xb + (k & 1) * CB);
+          R2* slot = reinterpret_cast<R2*>(xb + (k & 1) * CB);
           if (lane == owner) {
 #pragma unroll
-            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = make_double2(x[sg][cc], x[sg][cc + 1]);
+            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = R2{x[sg][cc], x[sg][cc + 1]};
           }
           __syncwarp();
-          double xk[CB];
+          R xk[CB];
 #pragma unroll
           for (int cc = 0; cc < CB; cc += 2) {
-            const double2 v = slot[cc / 2];
+            const R2 v = slot[cc / 2];
             xk[cc] = v.x;
             xk[cc + 1] = v.y;
           }
@@ -378,7 +388,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
           for (int t = sg; t < PRL; ++t) {
             const int i = lane + 32 * t;
             if (i > k && i < n) {
-              const double l = S[i * SLD + k];
+              const R l = S[i * SLD + k];
 #pragma unroll
               for (int cc = 0; cc < CB; ++cc) x[t][cc] = fma(-l, xk[cc], x[t][cc]);
             }
@@ -390,19 +400,19 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       for (int sg = PRL - 1; sg >= 0; --sg) {
         for (int k = min(n - 1, 32 * sg + 31); k >= 32 * sg; --k) {
           const int owner = k & 31;
-          double2* slot = reinterpret_cast<double2*>(xb + (k & 1) * CB);
+          R2* slot = reinterpret_cast<R2*>(xb + (k & 1) * CB);
           if (lane == owner) {
-            const double rd = rdiag[k];
+            const R rd = rdiag[k];
 #pragma unroll
             for (int cc = 0; cc < CB; ++cc) x[sg][cc] = x[sg][cc] * rd;
 #pragma unroll
-            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = make_double2(x[sg][cc], x[sg][cc + 1]);
+            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = R2{x[sg][cc], x[sg][cc + 1]};
           }
           __syncwarp();
-          double xk[CB];
+          R xk[CB];
 #pragma unroll
           for (int cc = 0; cc < CB; cc += 2) {
-            const double2 v = slot[cc / 2];
+            const R2 v = slot[cc / 2];
             xk[cc] = v.x;
             xk[cc + 1] = v.y;
           }
@@ -410,7 +420,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
           for (int t = 0; t <= sg; ++t) {
             const int i = lane + 32 * t;
             if (i < k) {
-              const double u = S[i * SLD + k];
+              const R u = S[i * SLD + k];
 #pragma unroll
               for (int cc = 0; cc < CB; ++cc) x[t][cc] = fma(-u, xk[cc], x[t][cc]);
             }
@@ -425,7 +435,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
 #pragma unroll
           for (int cc = 0; cc < CB; ++cc) {
             if (cc < cbw) {
-              const double v = x[t][cc];
+              const R v = x[t][cc];
               if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
               O[(int64_t)i * ld + c0 + cc] = v;
               pu[t] = fma(v, vec[c0 + cc], pu[t]);
@@ -434,7 +444,7 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
         }
       }
     }
-    double* part = Pn0;   // [NW][NP] partial products of the forward sweep (Pn0..Pn1)
+    R* part = Pn0;   // [NW][NP] partial products of the forward sweep (Pn0..Pn1)
     if (rhs) {
 #pragma unroll
       for (int t = 0; t < PRL; ++t) {
@@ -448,10 +458,10 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
       const int nwu = min(NW, (n + RPW - 1) / RPW);
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double u = part[i];
-        for (int w = 1; w < nwu; ++w) u += part[w * NP + i];
+        for (int w = 1; w < nwu; ++w) u += (double)part[w * NP + i];
         const double v = rhs[(int64_t)(j + 1) * n + i] - subn[(int64_t)j * n + i] * u;
         rhs[(int64_t)(j + 1) * n + i] = v;
-        vec[i] = v;
+        vec[i] = (R)v;
       }
     }
     __syncthreads();
@@ -459,15 +469,21 @@ __device__ void factor_atmosphere(int nz, int n, int ld, double* __restrict__ in
   if (st_local) atomicOr(status, st_local);
 }
 
-template <int NP, int NW, int PW, int MB>
+// out == nullptr: the inverses replace the blocks in the workspace (FP64
+// path); otherwise they go to out (layer-major, ni x ld per layer) and the
+// FP64 blocks stay. only != nullptr: atmospheres with only[b] == 0 are skipped.
+template <int NP, int NW, int PW, int MB, typename R>
 __global__ void __launch_bounds__(NW * 32, MB)
-factor_kernel(Batch B, double* __restrict__ ws, int32_t* __restrict__ status, int with_rhs) {
+factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __restrict__ only,
+              int32_t* __restrict__ status, int with_rhs) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
+  if (only && only[b] == 0) return;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
-  factor_atmosphere<NP, NW, PW, MB>(g.nz, B.ni, B.ld, w.inv, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
-                                status + b, smem_raw);
+  R* o = out ? out + g.z0 * B.ni * B.ld : reinterpret_cast<R*>(w.inv);
+  factor_atmosphere<NP, NW, PW, MB, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
+                                       status + b, smem_raw);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -642,14 +658,14 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, c
   return cudaGetLastError();
 }
 
-template <int NP, int NW, int PW, int MB = 1>
+template <int NP, int NW, int PW, int MB = 1, typename R = double>
 static cudaError_t launch_factor_t(const Batch& B, double* ws, int32_t* status, int with_rhs,
-                                   cudaStream_t st) {
-  size_t sm = LUK<NP, NW, PW>::smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW, PW, MB>,
+                                   cudaStream_t st, R* out = nullptr, const int32_t* only = nullptr) {
+  size_t sm = LUK<NP, NW, PW, R>::smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW, PW, MB, R>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  factor_kernel<NP, NW, PW, MB><<<B.count, NW * 32, sm, st>>>(B, ws, status, with_rhs);
+  factor_kernel<NP, NW, PW, MB, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs);
   return cudaGetLastError();
 }
 
@@ -677,6 +693,24 @@ cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_
   }
   return launch_factor_t<128, 16, 8>(B, ws, status, with_rhs, st);
 }
+
+// Factors into a separate inverse region (the workspace keeps the FP64
+// blocks): R = float for the mixed-precision solve, R = double for its FP64
+// fallback (only the atmospheres with only[b] != 0).
+template <typename R>
+cudaError_t launch_factor_into(const Batch& B, double* ws, R* out, const int32_t* only, int32_t* status,
+                               cudaStream_t st) {
+  if (B.ni <= 32) return launch_factor_t<32, 8, 8, 1, R>(B, ws, status, 0, st, out, only);
+  if (B.ni <= 64) return launch_factor_t<64, 16, 8, 1, R>(B, ws, status, 0, st, out, only);
+  if (B.ni <= 96) {
+    if (B.count <= sm_count()) return launch_factor_t<96, 12, 8, 1, R>(B, ws, status, 0, st, out, only);
+    return launch_factor_t<96, 8, 8, 2, R>(B, ws, status, 0, st, out, only);
+  }
+  return launch_factor_t<128, 16, 8, 1, R>(B, ws, status, 0, st, out, only);
+}
+template cudaError_t launch_factor_into<float>(const Batch&, double*, float*, const int32_t*, int32_t*, cudaStream_t);
+template cudaError_t launch_factor_into<double>(const Batch&, double*, double*, const int32_t*, int32_t*,
+                                                cudaStream_t);
 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {
   int stages = SWEEP_MAX_STAGES;

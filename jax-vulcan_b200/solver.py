@@ -70,3 +70,45 @@ def block_thomas_diag_offdiag(diag, sup_d, sub_d, rhs, stream=None):
     """Factor + solve (reference `solver.py:115-126`)."""
     return solve_block_thomas_diag_offdiag(factor_block_thomas_diag_offdiag(diag, sup_d, sub_d, stream), rhs,
                                            stream)
+
+
+class MixedFactors(NamedTuple):
+    buf: torch.Tensor       # opaque device buffer (vb_bt_mixed_bytes)
+    batch: int
+    nz: int
+    ni: int
+    status: torch.Tensor    # [batch] int32 status words
+    single: bool
+
+
+def factor_block_thomas_mixed(diag, sup_d, sub_d, stream=None) -> MixedFactors:
+    """Mixed-precision factorisation: FP32 LU and inverses of the eliminated
+    diagonal blocks, the FP64 blocks kept for the refinement residual."""
+    d = as_device(diag)
+    single = d.dim() == 3
+    if single:
+        d = d.unsqueeze(0)
+    B, nz, ni, _ = d.shape
+    su = as_device(sup_d).reshape(B, max(nz - 1, 0), ni)
+    sb = as_device(sub_d).reshape(B, max(nz - 1, 0), ni)
+    L = _lib.lib()
+    buf = torch.empty(int(L.vb_bt_mixed_bytes(B, nz, ni)), dtype=torch.uint8, device=d.device)
+    status = torch.zeros(B, dtype=torch.int32, device=d.device)
+    _lib.check(L.vb_bt_factor_mixed(B, nz, ni, _lib.ptr(d), _lib.ptr(su) if su.numel() else _lib.ptr(d),
+                                    _lib.ptr(sb) if sb.numel() else _lib.ptr(d), _lib.ptr(buf), _lib.ptr(status),
+                                    _lib.stream_handle(stream)), "vb_bt_factor_mixed")
+    return MixedFactors(buf, B, nz, ni, status, single)
+
+
+def solve_block_thomas_mixed(factors: MixedFactors, rhs, max_refine: int = 3, tol: float = 1e-13, stream=None):
+    """Solve with FP64 iterative refinement over the FP32 factors; atmospheres
+    whose refinement stalls are refactored and solved in FP64
+    (VB_STATUS_REFINE_STALL in ``factors.status``). Returns (x, passes)."""
+    r = as_device(rhs).reshape(factors.batch, factors.nz, factors.ni).contiguous()
+    x = torch.empty_like(r)
+    passes = torch.zeros(factors.batch, dtype=torch.int32, device=r.device)
+    _lib.check(_lib.lib().vb_bt_solve_mixed(factors.batch, factors.nz, factors.ni, _lib.ptr(factors.buf),
+                                            _lib.ptr(r), _lib.ptr(x), int(max_refine), float(tol),
+                                            _lib.ptr(factors.status), _lib.ptr(passes),
+                                            _lib.stream_handle(stream)), "vb_bt_solve_mixed")
+    return (x[0] if factors.single else x), passes
