@@ -258,6 +258,70 @@ def run_config2(args, torch):
             "clocks": clk}
 
 
+def run_config3(args, torch):
+    """The mixed-precision block solve at the SNCHO shape (ni=89, 2000
+    reactions, nz=150, B=128): FP32 factor + FP64 refinement (<= 3 passes)
+    with FP64 fallback, against the FP64 factor + solve, on the specified
+    stiff rate constants (k in [1e-45, 1e-6]) and on order-scaled
+    (well-conditioned) ones of the same shapes."""
+    syn, chem, jstep, solver = pkg("synthetic"), pkg("chem"), pkg("jax_step"), pkg("solver")
+    B = args.batch or 128
+    net = syn.config3_case().net
+    dn = chem.to_device(net.tables)
+    out = {}
+    for label, mild in (("stiff", False), ("well_conditioned", True)):
+        cases = [syn.make_case(seed=(3000 + b,), ni=89, n_fwd=1000, nz=150, elements=("C", "H", "O", "N", "S"),
+                               k_range=(-45.0, -6.0) if not mild else (-45.0, 4.0), mild=mild, net=net)
+                 for b in range(B)]
+        Y = torch.as_tensor(np.stack([c.y for c in cases]), device="cuda")
+        K = torch.as_tensor(np.stack([c.k for c in cases]), device="cuda")
+        A = {kk: (v if isinstance(v, bool) else np.stack([c.atm[kk] for c in cases])) for kk, v in cases[0].atm.items()}
+        M = torch.as_tensor(A["M"], device="cuda")
+        # the stage-1 system of the Ros2 step: c0 I - J - diag(diag_d), negated off-diagonals
+        J = chem.chem_jac_analytical(Y, M, K, dn)
+        diff, diag_d, sup_d, sub_d = jstep.diffusion(Y, jstep.atm_from_dict(A))
+        dt = torch.as_tensor(np.array([c.dt for c in cases]), device="cuda")
+        c0 = 1.0 / ((1.0 + 1.0 / np.sqrt(2.0)) * dt)
+        eye = torch.eye(89, dtype=torch.float64, device="cuda")
+        diag = c0[:, None, None, None] * eye - J - torch.diag_embed(diag_d)
+        rhs = chem.chem_rhs(Y, M, K, dn) + diff
+        sup_n, sub_n = -sup_d, -sub_d
+
+        def timed(fn, reps=3):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                res = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps, res
+
+        t64, x64 = timed(lambda: solver.block_thomas_diag_offdiag(diag, sup_n, sub_n, rhs))
+        tf64, _ = timed(lambda: solver.factor_block_thomas_diag_offdiag(diag, sup_n, sub_n))
+        tf32, _ = timed(lambda: solver.factor_block_thomas_mixed(diag, sup_n, sub_n))
+
+        def mixed():
+            f = solver.factor_block_thomas_mixed(diag, sup_n, sub_n)
+            x, passes = solver.solve_block_thomas_mixed(f, rhs, max_refine=3, tol=1e-13)
+            return x, passes, f.status
+
+        tmx, (xm, passes, status) = timed(mixed)
+        rel = ((xm - x64).abs() / x64.abs().clamp_min(1e-30)).amax(dim=(0, 1)).cpu().numpy()
+        st = status.cpu().numpy()
+        out[label] = {"fp64_ms": t64, "mixed_ms": tmx, "speedup": t64 / tmx,
+                      "fp64_factor_ms": tf64, "fp32_factor_ms": tf32,
+                      "fallback_fraction": float(((st & 4) != 0).mean()),
+                      "passes_max": int(passes.max().item()),
+                      "max_rel_err_vs_fp64": float(rel.max()),
+                      "per_species_max_rel_err_vs_fp64": [float(v) for v in rel]}
+    return {"metric": "mixed-precision block solve vs FP64 (SNCHO shape)", "unit": "ms per batch solve",
+            "higher_is_better": False, "config": {"workload": f"block solve of {B} SNCHO-shaped stage-1 systems "
+                                                              f"(ni=89, nz=150)", "batch": B},
+            "results": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -267,8 +331,9 @@ def main():
                     help="atmospheres per GPU (default: two per SM, 296 on a B200)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config0", choices=["config0", "config2"],
-                    help="config0: the headline batch (default); config2: the uneven multi-network batch")
+    ap.add_argument("--workload", default="config0", choices=["config0", "config2", "config3"],
+                    help="config0: the headline batch (default); config2: the uneven multi-network batch; "
+                         "config3: the mixed-precision block solve against FP64")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -286,9 +351,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    if args.workload == "config2":
+    if args.workload in ("config2", "config3"):
         if rank == 0:
-            print(json.dumps(run_config2(args, torch)), flush=True)
+            run = run_config2 if args.workload == "config2" else run_config3
+            print(json.dumps(run(args, torch)), flush=True)
         return
     _lib = pkg("_lib")
     chem = pkg("chem")
