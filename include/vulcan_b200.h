@@ -201,6 +201,17 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
                  double* y, double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
                  double* dt, VbLoopScalars* scalars, void* stream);
 
+/* Cotangents of every transport leaf of the steady-state residual
+ * (reference steady_state_grad.py:36-59 SteadyStateInputs leaves Kzz, Dzz,
+ * dzi, vz, Hpi, Ti, Tco, g, ms, alpha, vm, vs, top_flux, bot_flux, bot_vdep;
+ * the VJP of steady_state_grad.py:224-233): given lambda [B][nz][ni] (from
+ * vb_adjoint), g_atm = -lambda . d diffusion / d leaf, written in the layout
+ * of the atmosphere blob ([B][VB_ATM_DOUBLES(nz, ni)], same field order; the
+ * M and gas-mask slots and the unused last slot of interface arrays are 0:
+ * M's cotangent is vb_adjoint's g_M). With zoff the caller zeroes g_atm. */
+int vb_adjoint_atm(int batch, int nz, int ni, const int64_t* zoff, const double* y_star, const double* atm,
+                   int32_t atm_flags, const double* lambda, double* g_atm, void* stream);
+
 /* Photochemistry (reference photo.py). Cross sections and branch tables are
  * device arrays shared by the batch, except the temperature-dependent tables
  * absp_T_cross [n_abs_T][nz][nbin] and cross_J_T [n_br_T][nz][nbin], which

@@ -50,6 +50,7 @@ SIGNATURES = {
     "vb_profile_read": (_i, [_p, _p, _i]),
     "vb_fp64_probe": (_i, [_p, _i, _i, _i, _p]),
     "vb_ros2_step_static": (_i, [_p, _i, _i, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _p]),
+    "vb_adjoint_atm": (_i, [_i, _i, _i, _p, _p, _p, _i32, _p, _p, _p]),
     "vb_bt_mixed_bytes": (_sz, [_i, _i, _i]),
     "vb_bt_factor_mixed": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_bt_solve_mixed": (_i, [_i, _i, _i, _p, _p, _p, _i, C.c_double, _p, _p, _p]),

@@ -104,6 +104,108 @@ vjp_transport_kernel(Batch B, const double* __restrict__ y, const double* __rest
   }
 }
 
+// ---- cotangents of every transport leaf of the atmosphere blob
+// Fields of the blob in VB_ATM_DOUBLES order that the diffusion depends on.
+enum AtmField { F_KZZ, F_DZI, F_VZ, F_HPI, F_TI, F_TCO, F_G, F_DZZ, F_VM, F_VS, F_MS, F_ALPHA, F_TOP, F_BOT,
+                F_VDEP, N_FIELDS };
+
+// Reads of an atmosphere as Duals with the derivative seeded on one element
+// (field f, flat element e of that field).
+struct SeedAcc {
+  AtmRef a;
+  int ni, f;
+  int64_t e;
+  __device__ Dual s(int fld, int64_t idx, double v) const { return {v, (fld == f && idx == e) ? 1.0 : 0.0}; }
+  __device__ Dual Kzz(int m) const { return s(F_KZZ, m, a.Kzz[m]); }
+  __device__ Dual dzi(int m) const { return s(F_DZI, m, a.dzi[m]); }
+  __device__ Dual vz(int m) const { return s(F_VZ, m, a.vz[m]); }
+  __device__ Dual Hpi(int m) const { return s(F_HPI, m, a.Hpi[m]); }
+  __device__ Dual Ti(int m) const { return s(F_TI, m, a.Ti[m]); }
+  __device__ Dual Tco(int m) const { return s(F_TCO, m, a.Tco[m]); }
+  __device__ Dual g(int m) const { return s(F_G, m, a.g[m]); }
+  __device__ Dual Dzz(int m, int i) const { return s(F_DZZ, (int64_t)m * ni + i, a.Dzz[(int64_t)m * ni + i]); }
+  __device__ Dual vm(int m, int i) const { return s(F_VM, (int64_t)m * ni + i, a.vm[(int64_t)m * ni + i]); }
+  __device__ Dual vs(int m, int i) const { return s(F_VS, (int64_t)m * ni + i, a.vs[(int64_t)m * ni + i]); }
+  __device__ Dual ms(int i) const { return s(F_MS, i, a.ms[i]); }
+  __device__ Dual alpha(int i) const { return s(F_ALPHA, i, a.alpha[i]); }
+  __device__ Dual top(int i) const { return s(F_TOP, i, a.top[i]); }
+  __device__ Dual bot(int i) const { return s(F_BOT, i, a.bot[i]); }
+  __device__ Dual vdep(int i) const { return s(F_VDEP, i, a.vdep[i]); }
+};
+
+// diff[j][i] with boundary fluxes (jax_step.py:223-246), the terms of the
+// forward kernels' layer_diffusion, as a Dual.
+__device__ inline Dual diff_entry(const SeedAcc& acc, const double* yb, double ysm, double ys0, double ysp, int nz,
+                                  int ni, int j, int i, int flags) {
+  const double use_vm = (flags & VB_USE_VM_MOL) ? 1.0 : 0.0;
+  const double use_set = (flags & VB_USE_SETTLING) ? 1.0 : 0.0;
+  Dual Ae, Be, Ce, Am, Bm, Cm;
+  eddy_row_t<Dual>(acc, nz, j, ysm, ys0, ysp, Ae, Be, Ce);
+  mol_row_t<Dual>(acc, nz, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
+  const Dual At = Ae + Am, Bt = Be + Bm, Ct = Ce + Cm;
+  const double y0 = yb[(int64_t)j * ni + i];
+  Dual d;
+  if (j == 0) {
+    d = At * y0 + Bt * yb[(int64_t)(j + 1) * ni + i];
+  } else if (j == nz - 1) {
+    d = At * y0 + Ct * yb[(int64_t)(j - 1) * ni + i];
+  } else {
+    d = At * y0 + Bt * yb[(int64_t)(j + 1) * ni + i] + Ct * yb[(int64_t)(j - 1) * ni + i];
+  }
+  if (j == nz - 1 && (flags & VB_USE_TOPFLUX)) d = d + acc.top(i) / acc.dzi(nz - 2);
+  if (j == 0 && (flags & VB_USE_BOTFLUX)) d = d + (acc.bot(i) - y0 * acc.vdep(i)) / acc.dzi(0);
+  return d;
+}
+
+// One thread per leaf element: g = -sum over the stencil rows (and species)
+// the element enters of lambda . d diff / d leaf, written at the element's
+// place in the cotangent blob. Grid: (element blocks, atmospheres).
+__global__ void __launch_bounds__(128)
+vjp_atm_kernel(Batch B, const double* __restrict__ y, const double* __restrict__ atm, int flags,
+               const double* __restrict__ lam, double* __restrict__ g_atm) {
+  const int b = blockIdx.y;
+  const Geo g = geo_of(B, b);
+  const int ni = B.ni, nz = g.nz;
+  const int64_t NI = ni, NZ = nz;
+  const int64_t cnt[N_FIELDS] = {NZ - 1, NZ - 1, NZ - 1, NZ - 1, NZ - 1, NZ, NZ, (NZ - 1) * NI, NZ * NI,
+                                 (NZ - 1) * NI, NI, NI, NI, NI, NI};
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int f = 0;
+  while (f < N_FIELDS && q >= cnt[f]) q -= cnt[f++];
+  if (f >= N_FIELDS) return;
+  const double* blob = atm + g.atm;
+  SeedAcc acc{atm_ref(blob, nz, ni), ni, f, q};
+  const double* yb = y + g.z0 * ni;
+  const double* lb = lam + g.z0 * ni;
+  int lo = 0, hi = nz - 1, i0 = 0, i1 = ni - 1;
+  if (f <= F_TI) { lo = (int)q - 1; hi = (int)q + 2; }                           // interface m = q
+  else if (f == F_TCO || f == F_G) { lo = (int)q - 1; hi = (int)q + 1; }          // layer q
+  else if (f == F_DZZ || f == F_VS) { const int m = (int)(q / ni); i0 = i1 = (int)(q % ni); lo = m - 1; hi = m + 2; }
+  else if (f == F_VM) { const int l = (int)(q / ni); i0 = i1 = (int)(q % ni); lo = l - 1; hi = l + 1; }
+  else if (f == F_MS || f == F_ALPHA) { i0 = i1 = (int)q; }
+  else if (f == F_TOP) { i0 = i1 = (int)q; lo = hi = nz - 1; }
+  else { i0 = i1 = (int)q; lo = hi = 0; }                                         // bot_flux, bot_vdep
+  lo = max(lo, 0);
+  hi = min(hi, nz - 1);
+  double gsum = 0.0;
+  for (int j = lo; j <= hi; ++j) {
+    // gas sums of rows j-1, j, j+1 (0 outside the column, as the forward kernels)
+    double ys3[3];
+    for (int w = 0; w < 3; ++w) {
+      const int jj = j - 1 + w;
+      ys3[w] = (jj >= 0 && jj < nz) ? pairwise_sum_masked(yb + (int64_t)jj * ni, acc.a.gas, ni) : 0.0;
+    }
+    for (int i = i0; i <= i1; ++i) {
+      const Dual d = diff_entry(acc, yb, ys3[0], ys3[1], ys3[2], nz, ni, j, i, flags);
+      gsum += lb[(int64_t)j * ni + i] * d.d;
+    }
+  }
+  const AtmOff o = atm_offsets(nz, ni);
+  const int64_t field_off[N_FIELDS] = {o.Kzz, o.dzi, o.vz, o.Hpi, o.Ti, o.Tco, o.g, o.Dzz, o.vm, o.vs,
+                                       o.ms, o.alpha, o.top, o.bot, o.vdep};
+  g_atm[g.atm + field_off[f] + q] = -gsum;
+}
+
 __global__ void gather_k1_kernel(Batch B, double* __restrict__ ws, double* __restrict__ out) {
   const int b = blockIdx.y, j = blockIdx.x;
   Geo g = geo_of(B, b);
@@ -116,6 +218,15 @@ cudaError_t launch_gather_k1(const Batch& B, double* ws, double* out, cudaStream
   if (!out) return cudaSuccess;
   dim3 grid(B.nz, B.count);
   gather_k1_kernel<<<grid, 128, 0, st>>>(B, ws, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vjp_atm(const Batch& B, const double* y, const double* atm, int flags, const double* lam,
+                           double* g_atm, cudaStream_t st) {
+  const int64_t NZ = B.nz, NI = B.ni;
+  const int64_t per = 5 * (NZ - 1) + 2 * NZ + 2 * (NZ - 1) * NI + NZ * NI + 5 * NI;
+  dim3 grid((unsigned)((per + 127) / 128), B.count);
+  vjp_atm_kernel<<<grid, 128, 0, st>>>(B, y, atm, flags, lam, g_atm);
   return cudaGetLastError();
 }
 

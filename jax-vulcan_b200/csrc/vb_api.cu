@@ -561,6 +561,19 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
   return VB_OK;
 }
 
+int vb_adjoint_atm(int batch, int nz, int ni, const int64_t* zoff, const double* y_star, const double* atm,
+                   int32_t flags, const double* lambda, double* g_atm, void* stream) {
+  if (!y_star || !atm || !lambda || !g_atm) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "batch >= 1, nz >= 2, 1 <= ni <= 128");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = bt_batch(batch, nz, ni);
+  B.zoff = zoff;
+  const size_t total = zoff ? 0 : (size_t)batch * VB_ATM_DOUBLES(nz, ni);
+  if (total) VB_CHECK(cudaMemsetAsync(g_atm, 0, total * sizeof(double), st), "clear");
+  VB_CHECK(vb::launch_vjp_atm(B, y_star, atm, flags, lambda, g_atm, st), "vjp atm");
+  return VB_OK;
+}
+
 int vb_ros2_step_static(const VbNet* net, int batch, int nz, const double* y, const double* k, const double* dt,
                         const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol, double* delta,
                         int32_t* status, void* stream) {

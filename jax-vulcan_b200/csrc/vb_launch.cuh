@@ -29,6 +29,8 @@ cudaError_t launch_stage2(const NetDev&, const Batch&, const double* y, const do
                           const double* atm, int flags, const uint8_t* fix_mask, double* ws, cudaStream_t,
                           double* resid = nullptr);
 // Cotangents from lambda held in the workspace's k1 rows (see vb_adjoint).
+cudaError_t launch_vjp_atm(const Batch& B, const double* y, const double* atm, int flags, const double* lam,
+                           double* g_atm, cudaStream_t st);
 cudaError_t launch_vjp(const NetDev&, const Batch&, const double* y, const double* k, const double* atm, int flags,
                        double* ws, double* g_k, double* g_M, double* g_Kzz, double* g_top, double* g_bot,
                        double* g_vdep, cudaStream_t);

@@ -82,109 +82,161 @@ __device__ __forceinline__ AtmRef atm_ref(const double* blob, int nz, int ni) {
   return a;
 }
 
+// Number types of the stencil formulas: double (the forward kernels) or
+// Dual (value + one derivative, for the adjoint's leaf cotangents).
+struct Dual {
+  double v, d;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+  return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)};
+}
+__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+__device__ __forceinline__ Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
+__device__ __forceinline__ double value_of(double x) { return x; }
+__device__ __forceinline__ double value_of(Dual x) { return x.v; }
+template <typename T> __device__ __forceinline__ T pos_part_t(T v) { return (value_of(v) > 0.0 ? 1.0 : 0.0) * v; }
+template <typename T> __device__ __forceinline__ T neg_part_t(T v) { return (value_of(v) < 0.0 ? 1.0 : 0.0) * v; }
+
+// Plain reads of an atmosphere (the forward kernels).
+struct AtmPtrAcc {
+  const AtmRef& a;
+  int ni;
+  __device__ double Kzz(int m) const { return a.Kzz[m]; }
+  __device__ double dzi(int m) const { return a.dzi[m]; }
+  __device__ double vz(int m) const { return a.vz[m]; }
+  __device__ double Hpi(int m) const { return a.Hpi[m]; }
+  __device__ double Ti(int m) const { return a.Ti[m]; }
+  __device__ double Tco(int m) const { return a.Tco[m]; }
+  __device__ double g(int m) const { return a.g[m]; }
+  __device__ double Dzz(int m, int i) const { return a.Dzz[(int64_t)m * ni + i]; }
+  __device__ double vm(int m, int i) const { return a.vm[(int64_t)m * ni + i]; }
+  __device__ double vs(int m, int i) const { return a.vs[(int64_t)m * ni + i]; }
+  __device__ double ms(int i) const { return a.ms[i]; }
+  __device__ double alpha(int i) const { return a.alpha[i]; }
+};
+
 // Eddy coefficients of stencil row j (reference jax_step.py:167-193).
-__device__ inline void eddy_row(const AtmRef& a, int nz, int j, double ysm, double ys0, double ysp,
-                                double& A, double& Bc, double& C) {
-  const double* Kzz = a.Kzz;
-  const double* dzi = a.dzi;
-  const double* vz = a.vz;
+template <typename T, typename Acc>
+__device__ inline void eddy_row_t(const Acc& a, int nz, int j, double ysm, double ys0, double ysp, T& A, T& Bc,
+                                  T& C) {
   if (j == 0) {
-    A = -1.0 / dzi[0] * (Kzz[0] / dzi[0]) * (ysp + ys0) / 2.0 / ys0;
-    A = A - pos_part(vz[0]) / dzi[0];
-    Bc = 1.0 / dzi[0] * (Kzz[0] / dzi[0]) * (ysp + ys0) / 2.0 / ysp;
-    Bc = Bc - neg_part(vz[0]) / dzi[0];
-    C = 0.0;
+    A = -1.0 / a.dzi(0) * (a.Kzz(0) / a.dzi(0)) * (ysp + ys0) / 2.0 / ys0;
+    A = A - pos_part_t(a.vz(0)) / a.dzi(0);
+    Bc = 1.0 / a.dzi(0) * (a.Kzz(0) / a.dzi(0)) * (ysp + ys0) / 2.0 / ysp;
+    Bc = Bc - neg_part_t(a.vz(0)) / a.dzi(0);
+    C = T{};
   } else if (j == nz - 1) {
     int t = nz - 2;
-    A = -1.0 / dzi[t] * (Kzz[t] / dzi[t]) * (ys0 + ysm) / 2.0 / ys0;
-    A = A + neg_part(vz[t]) / dzi[t];
-    C = 1.0 / dzi[t] * (Kzz[t] / dzi[t]) * (ys0 + ysm) / 2.0 / ysm;
-    C = C + pos_part(vz[t]) / dzi[t];
-    Bc = 0.0;
+    A = -1.0 / a.dzi(t) * (a.Kzz(t) / a.dzi(t)) * (ys0 + ysm) / 2.0 / ys0;
+    A = A + neg_part_t(a.vz(t)) / a.dzi(t);
+    C = 1.0 / a.dzi(t) * (a.Kzz(t) / a.dzi(t)) * (ys0 + ysm) / 2.0 / ysm;
+    C = C + pos_part_t(a.vz(t)) / a.dzi(t);
+    Bc = T{};
   } else {
-    double dz_ave = 0.5 * (dzi[j - 1] + dzi[j]);
+    const auto dz_ave = 0.5 * (a.dzi(j - 1) + a.dzi(j));
     A = -1.0 / dz_ave *
-        (Kzz[j] / dzi[j] * (ysp + ys0) / 2.0 + Kzz[j - 1] / dzi[j - 1] * (ys0 + ysm) / 2.0) / ys0;
-    Bc = 1.0 / dz_ave * Kzz[j] / dzi[j] * (ysp + ys0) / 2.0 / ysp;
-    C = 1.0 / dz_ave * Kzz[j - 1] / dzi[j - 1] * (ys0 + ysm) / 2.0 / ysm;
-    A = A - (pos_part(vz[j]) - neg_part(vz[j - 1])) / dz_ave;
-    Bc = Bc - neg_part(vz[j]) / dz_ave;
-    C = C + pos_part(vz[j - 1]) / dz_ave;
+        (a.Kzz(j) / a.dzi(j) * (ysp + ys0) / 2.0 + a.Kzz(j - 1) / a.dzi(j - 1) * (ys0 + ysm) / 2.0) / ys0;
+    Bc = 1.0 / dz_ave * a.Kzz(j) / a.dzi(j) * (ysp + ys0) / 2.0 / ysp;
+    C = 1.0 / dz_ave * a.Kzz(j - 1) / a.dzi(j - 1) * (ys0 + ysm) / 2.0 / ysm;
+    A = A - (pos_part_t(a.vz(j)) - neg_part_t(a.vz(j - 1))) / dz_ave;
+    Bc = Bc - neg_part_t(a.vz(j)) / dz_ave;
+    C = C + pos_part_t(a.vz(j - 1)) / dz_ave;
   }
+}
+
+__device__ inline void eddy_row(const AtmRef& a, int nz, int j, double ysm, double ys0, double ysp,
+                                double& A, double& Bc, double& C) {
+  eddy_row_t<double>(AtmPtrAcc{a, 0}, nz, j, ysm, ys0, ysp, A, Bc, C);
 }
 
 // Gravity/thermal-diffusion factor of compute_diff_grav (jax_step.py:80-87):
 // -1/Hpi[h] + ms*g[gi]/(Navo*kb*Ti[h]) + alpha/Ti[h]*(Tco[t1]-Tco[t0])/dzi[h].
-__device__ __forceinline__ double grav_fac(const AtmRef& a, int i, int h, int gi, int t1, int t0) {
-  return -1.0 / a.Hpi[h] + a.ms[i] * a.g[gi] / (NAVO * KB * a.Ti[h]) +
-         a.alpha[i] / a.Ti[h] * (a.Tco[t1] - a.Tco[t0]) / a.dzi[h];
+template <typename T, typename Acc>
+__device__ __forceinline__ T grav_fac_t(const Acc& a, int i, int h, int gi, int t1, int t0) {
+  return -1.0 / a.Hpi(h) + a.ms(i) * a.g(gi) / (NAVO * KB * a.Ti(h)) +
+         a.alpha(i) / a.Ti(h) * (a.Tco(t1) - a.Tco(t0)) / a.dzi(h);
 }
 
 // Molecular-diffusion coefficients of species i on stencil row j, including the
 // y-independent gravity / vm / settling pieces (jax_step.py:67-147, 195-218).
+template <typename T, typename Acc>
+__device__ inline void mol_row_t(const Acc& a, int nz, int j, int i, double ysm, double ys0, double ysp,
+                                 double use_vm, double use_set, T& A, T& Bc, T& C) {
+  if (j == 0) {
+    const T D0 = a.Dzz(0, i);
+    const T g0 = 1.0 / a.dzi(0) * D0 / 2.0 * grav_fac_t<T>(a, i, 0, 0, 1, 0);
+    const T vm0 = a.vm(0, i);
+    const T vs0 = a.vs(0, i);
+    const T b0_vm = -pos_part_t(vm0) / a.dzi(0);
+    const T b0_vm_B = -neg_part_t(vm0) / a.dzi(0);
+    const T b0_vs = -pos_part_t(vs0) / a.dzi(0);
+    const T b0_vs_B = -neg_part_t(vs0) / a.dzi(0);
+    const T bA = (1.0 - use_vm) * g0 + use_vm * b0_vm + use_set * b0_vs;
+    const T bB = (1.0 - use_vm) * g0 + use_vm * b0_vm_B + use_set * b0_vs_B;
+    A = -1.0 / a.dzi(0) * (D0 / a.dzi(0)) * (ysp + ys0) / 2.0 / ys0 + bA;
+    Bc = 1.0 / a.dzi(0) * (D0 / a.dzi(0)) * (ysp + ys0) / 2.0 / ysp + bB;
+    C = T{};
+  } else if (j == nz - 1) {
+    const int t = nz - 2;
+    const T Dt = a.Dzz(t, i);
+    const T gt = -1.0 / a.dzi(t) * Dt / 2.0 * grav_fac_t<T>(a, i, t, nz - 1, nz - 1, nz - 2);
+    const T vmt = a.vm(nz - 1, i);
+    const T vst = a.vs(t, i);
+    const T bt_vm = neg_part_t(vmt) / a.dzi(t);
+    const T bt_vm_C = pos_part_t(vmt) / a.dzi(t);
+    const T bt_vs = neg_part_t(vst) / a.dzi(t);
+    const T bt_vs_C = pos_part_t(vst) / a.dzi(t);
+    const T bA = (1.0 - use_vm) * gt + use_vm * bt_vm + use_set * bt_vs;
+    const T bC = (1.0 - use_vm) * gt + use_vm * bt_vm_C + use_set * bt_vs_C;
+    A = -1.0 / a.dzi(t) * (Dt / a.dzi(t)) * (ys0 + ysm) / 2.0 / ys0 + bA;
+    C = 1.0 / a.dzi(t) * (Dt / a.dzi(t)) * (ys0 + ysm) / 2.0 / ysm + bC;
+    Bc = T{};
+  } else {
+    const T dz_ave = 0.5 * (a.dzi(j - 1) + a.dzi(j));
+    const T Dj = a.Dzz(j, i);
+    const T Dm = a.Dzz(j - 1, i);
+    const T gj = grav_fac_t<T>(a, i, j, j, j + 1, j);
+    const T gjm = grav_fac_t<T>(a, i, j - 1, j, j, j - 1);
+    const T gjpb = grav_fac_t<T>(a, i, j, j + 1, j + 1, j);
+    const T gjmc = grav_fac_t<T>(a, i, j - 1, j - 1, j, j - 1);
+    const T inv2 = 1.0 / (2.0 * dz_ave);
+    const T Ag = inv2 * (Dj * gj - Dm * gjm);
+    const T Bg = inv2 * Dj * gjpb;
+    const T Cg = -inv2 * Dm * gjmc;
+    const T vmj = a.vm(j, i), vmm = a.vm(j - 1, i);
+    const T vsj = a.vs(j, i), vsm = a.vs(j - 1, i);
+    const T Avm = -(pos_part_t(vmj) - neg_part_t(vmm)) / dz_ave;
+    const T Bvm = -neg_part_t(vmj) / dz_ave;
+    const T Cvm = pos_part_t(vmm) / dz_ave;
+    const T Avs = -(pos_part_t(vsj) - neg_part_t(vsm)) / dz_ave;
+    const T Bvs = -neg_part_t(vsj) / dz_ave;
+    const T Cvs = pos_part_t(vsm) / dz_ave;
+    const T Ax = (1.0 - use_vm) * Ag + use_vm * Avm + use_set * Avs;
+    const T Bx = (1.0 - use_vm) * Bg + use_vm * Bvm + use_set * Bvs;
+    const T Cx = (1.0 - use_vm) * Cg + use_vm * Cvm + use_set * Cvs;
+    A = -1.0 / dz_ave * (Dj / a.dzi(j) * (ysp + ys0) / 2.0 + Dm / a.dzi(j - 1) * (ys0 + ysm) / 2.0) / ys0;
+    A = A + Ax;
+    Bc = 1.0 / dz_ave * Dj / a.dzi(j) * (ysp + ys0) / 2.0 / ysp;
+    Bc = Bc + Bx;
+    C = 1.0 / dz_ave * Dm / a.dzi(j - 1) * (ys0 + ysm) / 2.0 / ysm;
+    C = C + Cx;
+  }
+}
+
 __device__ inline void mol_row(const AtmRef& a, int nz, int ni, int j, int i, double ysm, double ys0,
                                double ysp, double use_vm, double use_set, double& A, double& Bc,
                                double& C) {
-  const double* dzi = a.dzi;
-  if (j == 0) {
-    double D0 = a.Dzz[i];
-    double g0 = 1.0 / dzi[0] * D0 / 2.0 * grav_fac(a, i, 0, 0, 1, 0);
-    double vm0 = a.vm[i];
-    double vs0 = a.vs[i];
-    double b0_vm = -pos_part(vm0) / dzi[0];
-    double b0_vm_B = -neg_part(vm0) / dzi[0];
-    double b0_vs = -pos_part(vs0) / dzi[0];
-    double b0_vs_B = -neg_part(vs0) / dzi[0];
-    double bA = (1.0 - use_vm) * g0 + use_vm * b0_vm + use_set * b0_vs;
-    double bB = (1.0 - use_vm) * g0 + use_vm * b0_vm_B + use_set * b0_vs_B;
-    A = -1.0 / dzi[0] * (D0 / dzi[0]) * (ysp + ys0) / 2.0 / ys0 + bA;
-    Bc = 1.0 / dzi[0] * (D0 / dzi[0]) * (ysp + ys0) / 2.0 / ysp + bB;
-    C = 0.0;
-  } else if (j == nz - 1) {
-    int t = nz - 2;
-    double Dt = a.Dzz[(int64_t)t * ni + i];
-    double gt = -1.0 / dzi[t] * Dt / 2.0 * grav_fac(a, i, t, nz - 1, nz - 1, nz - 2);
-    double vmt = a.vm[(int64_t)(nz - 1) * ni + i];
-    double vst = a.vs[(int64_t)t * ni + i];
-    double bt_vm = neg_part(vmt) / dzi[t];
-    double bt_vm_C = pos_part(vmt) / dzi[t];
-    double bt_vs = neg_part(vst) / dzi[t];
-    double bt_vs_C = pos_part(vst) / dzi[t];
-    double bA = (1.0 - use_vm) * gt + use_vm * bt_vm + use_set * bt_vs;
-    double bC = (1.0 - use_vm) * gt + use_vm * bt_vm_C + use_set * bt_vs_C;
-    A = -1.0 / dzi[t] * (Dt / dzi[t]) * (ys0 + ysm) / 2.0 / ys0 + bA;
-    C = 1.0 / dzi[t] * (Dt / dzi[t]) * (ys0 + ysm) / 2.0 / ysm + bC;
-    Bc = 0.0;
-  } else {
-    double dz_ave = 0.5 * (dzi[j - 1] + dzi[j]);
-    double Dj = a.Dzz[(int64_t)j * ni + i];
-    double Dm = a.Dzz[(int64_t)(j - 1) * ni + i];
-    double gj = grav_fac(a, i, j, j, j + 1, j);
-    double gjm = grav_fac(a, i, j - 1, j, j, j - 1);
-    double gjpb = grav_fac(a, i, j, j + 1, j + 1, j);
-    double gjmc = grav_fac(a, i, j - 1, j - 1, j, j - 1);
-    double inv2 = 1.0 / (2.0 * dz_ave);
-    double Ag = inv2 * (Dj * gj - Dm * gjm);
-    double Bg = inv2 * Dj * gjpb;
-    double Cg = -inv2 * Dm * gjmc;
-    double vmj = a.vm[(int64_t)j * ni + i], vmm = a.vm[(int64_t)(j - 1) * ni + i];
-    double vsj = a.vs[(int64_t)j * ni + i], vsm = a.vs[(int64_t)(j - 1) * ni + i];
-    double Avm = -(pos_part(vmj) - neg_part(vmm)) / dz_ave;
-    double Bvm = -neg_part(vmj) / dz_ave;
-    double Cvm = pos_part(vmm) / dz_ave;
-    double Avs = -(pos_part(vsj) - neg_part(vsm)) / dz_ave;
-    double Bvs = -neg_part(vsj) / dz_ave;
-    double Cvs = pos_part(vsm) / dz_ave;
-    double Ax = (1.0 - use_vm) * Ag + use_vm * Avm + use_set * Avs;
-    double Bx = (1.0 - use_vm) * Bg + use_vm * Bvm + use_set * Bvs;
-    double Cx = (1.0 - use_vm) * Cg + use_vm * Cvm + use_set * Cvs;
-    A = -1.0 / dz_ave * (Dj / dzi[j] * (ysp + ys0) / 2.0 + Dm / dzi[j - 1] * (ys0 + ysm) / 2.0) / ys0;
-    A = A + Ax;
-    Bc = 1.0 / dz_ave * Dj / dzi[j] * (ysp + ys0) / 2.0 / ysp;
-    Bc = Bc + Bx;
-    C = 1.0 / dz_ave * Dm / dzi[j - 1] * (ys0 + ysm) / 2.0 / ysm;
-    C = C + Cx;
-  }
+  mol_row_t<double>(AtmPtrAcc{a, ni}, nz, j, i, ysm, ys0, ysp, use_vm, use_set, A, Bc, C);
 }
 
 }  // namespace vb

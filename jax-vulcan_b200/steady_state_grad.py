@@ -57,10 +57,34 @@ def validate_steady_state_solution(y_star, k_arr, atm, net, residual_rtol=1e-6, 
     return resid_inf
 
 
+def unpack_atm_cotangents(g_atm, nz, ni):
+    """Blob of cotangents ([B][VB_ATM_DOUBLES]) -> the reference leaf arrays
+    (interface arrays [B][nz-1], layer arrays [B][nz], per-species [B][ni])."""
+    B = g_atm.shape[0]
+    o, out = 0, {}
+    for name in ("Kzz", "dzi", "vz", "Hpi", "Ti", "Tco", "g", "M"):
+        out[name] = g_atm[:, o:o + nz]
+        o += nz
+    for name in ("Dzz", "vm", "vs"):
+        out[name] = g_atm[:, o:o + nz * ni].reshape(B, nz, ni)
+        o += nz * ni
+    for name in ("ms", "alpha", "top_flux", "bot_flux", "bot_vdep"):
+        out[name] = g_atm[:, o:o + ni]
+        o += ni
+    for name in ("Kzz", "dzi", "vz", "Hpi", "Ti", "Dzz", "vs"):   # interface arrays: nz-1 used
+        out[name] = out[name][:, :nz - 1]
+    del out["M"]          # the chemistry's M cotangent comes from vb_adjoint
+    out["Kzz_transport"] = out.pop("Kzz")   # the same cotangent as vb_adjoint's Kzz, by differentiation
+    return out
+
+
 def implicit_cotangents(y_star, k_arr, atm: AtmStatic, net: NetworkArrays, v, stream=None):
     """Cotangents -lambda . df/dtheta with lambda = J_y^{-T} v (reference `_ssi_bwd`,
-    `steady_state_grad.py:214-230`). Returns a dict with ``lambda``, ``k_arr``, ``M``,
-    ``Kzz``, ``top_flux``, ``bot_flux``, ``bot_vdep`` and ``status``."""
+    `steady_state_grad.py:214-230`) for every leaf of the reference
+    `SteadyStateInputs` (`steady_state_grad.py:36-59`): a dict with ``lambda``,
+    ``k_arr``, ``M``, ``Kzz``, ``Dzz``, ``dzi``, ``vz``, ``Hpi``, ``Ti``, ``Tco``,
+    ``g``, ``ms``, ``alpha``, ``vm``, ``vs``, ``top_flux``, ``bot_flux``,
+    ``bot_vdep`` and ``status``."""
     yt, kt, single = _batch(y_star, k_arr)
     B, nz, ni = yt.shape
     vt = as_device(v).reshape(B, nz, ni)
@@ -87,6 +111,11 @@ def implicit_cotangents(y_star, k_arr, atm: AtmStatic, net: NetworkArrays, v, st
                             _lib.ptr(out["bot_vdep"]), _lib.ptr(out["status"]), _lib.ptr(ws), ws_bytes,
                             _lib.stream_handle(stream)), "vb_adjoint")
     out["Kzz"] = kzz_full[:, :nz - 1]
+    # every other transport leaf, from the blob of cotangents (vb_adjoint_atm)
+    g_atm = torch.empty_like(blob)
+    _lib.check(L.vb_adjoint_atm(B, nz, ni, None, _lib.ptr(yt), _lib.ptr(blob), atm_flags(atm), _lib.ptr(out["lambda"]),
+                                _lib.ptr(g_atm), _lib.stream_handle(stream)), "vb_adjoint_atm")
+    out.update(unpack_atm_cotangents(g_atm, nz, ni))
     if single:
         out = {kk: (vv[0] if kk != "status" else vv) for kk, vv in out.items()}
     return out
