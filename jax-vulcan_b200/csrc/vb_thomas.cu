@@ -715,6 +715,9 @@ template cudaError_t launch_factor_into<double>(const Batch&, double*, double*, 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {
   int stages = SWEEP_MAX_STAGES;
   while (stages > 1 && sweep_smem_bytes(B.ni, stages) > 220 * 1024) --stages;
+  // more atmospheres than SMs: a shallower ring lets two CTAs share an SM (one wave)
+  if (B.count > sm_count())
+    while (stages > 2 && 2 * sweep_smem_bytes(B.ni, stages) > 224 * 1024) --stages;
   size_t sm = sweep_smem_bytes(B.ni, stages);
   cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
