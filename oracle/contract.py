@@ -149,3 +149,59 @@ def attempt(s, k, atm, net, compo, atom_ini, p, **kw):
     """One attempt: the Ros2 step from ``s["y"]`` then ``body_update``."""
     sol, delta_arr = ros2.ros2_step(s["y"], k, s["dt"], atm, net, fix_mask=kw.get("fix_mask"))
     return body_update(s, sol, delta_arr, atm["M"], compo, atom_ini, p, **kw)
+
+
+CONV_FIELDS = ["longdy", "longdydt", "longdy_seen_min", "count_since_new_min"]
+
+
+def conv_update(s, ring_y, ring_t, n_0, p, ignore=None, do_accept=True):
+    """Ring append and convergence diagnostics after one attempt (the state
+    ``s`` is the post-attempt state: y, ymix, t, accept_count and the carried
+    longdy fields). Follows `outer_loop.py:918-928` (ring slot
+    ``max(accept_count - 1, 0) % conv_step`` rewritten with (y, t)),
+    `_conv_jax` `:633-670` (lookback to the ring entry nearest ``t *
+    st_factor``, the newest slot excluded; longdy = max over the masked
+    relative change), `:944-989` (longdy / longdydt kept only on accept; the
+    stall counter restarts on a 5 % drop). ``p``: conv_step, st_factor,
+    mtol_conv, atol. Rings are updated in place; returns the new fields."""
+    conv = p["conv_step"]
+    acc = int(s["accept_count"])
+    idx = max(acc - 1, 0) % conv
+    ring_y[idx] = s["y"]
+    ring_t[idx] = s["t"]
+    diffs = np.abs(ring_t - s["t"] * p["st_factor"])
+    diffs[idx] = np.inf
+    k = int(np.argmin(diffs))
+    la = np.abs((s["y"] - ring_y[k]) / n_0[:, None])
+    la = np.where(s["ymix"] < p["mtol_conv"], 0.0, la)
+    la = np.where(s["y"] < p["atol"], 0.0, la)
+    if ignore is not None:
+        la = np.where(np.asarray(ignore, bool)[None, :], 0.0, la)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = np.where(s["ymix"] > 0, la / np.maximum(s["ymix"], 1e-300), 0.0)
+    ld_new = np.max(ratio)
+    ldt_new = ld_new / max(s["t"] - ring_t[k], 1e-300)
+    out = {}
+    out["longdy"] = ld_new if do_accept else s["longdy"]
+    out["longdydt"] = ldt_new if do_accept else s["longdydt"]
+    drop = do_accept and out["longdy"] < s["longdy_seen_min"] * 0.95
+    out["longdy_seen_min"] = out["longdy"] if drop else s["longdy_seen_min"]
+    out["count_since_new_min"] = 0 if drop else (s["count_since_new_min"] + 1 if do_accept else
+                                                 s["count_since_new_min"])
+    return out
+
+
+def loop_continues(s, p, slope_min, aflux_change=0.0):
+    """`cond_fn` (`outer_loop.py:672-713`) without the chunk cap: False once the
+    run is too long, has too many accepted steps, or is ready and converged
+    (or stalled). ``p``: runtime, count_max, trun_min, count_min, yconv_cri,
+    slope_cri, yconv_min, flux_cri, conv_stall_window."""
+    too_long = s["t"] > p["runtime"]
+    too_many = s["accept_count"] > p["count_max"]
+    conv = (((s["longdy"] < p["yconv_cri"]) and (s["longdydt"] < p["slope_cri"]))
+            or ((s["longdy"] < p["yconv_min"]) and (s["longdydt"] < slope_min)))
+    conv = conv and aflux_change < p["flux_cri"]
+    stalled = (s["count_since_new_min"] > p["conv_stall_window"] and s["longdy_seen_min"] < p["yconv_min"]
+               and s["longdy"] < p["yconv_min"] and aflux_change < p["flux_cri"])
+    ready = s["t"] > p["trun_min"] and s["accept_count"] > p["count_min"]
+    return not (too_long or too_many or (ready and (conv or stalled)))

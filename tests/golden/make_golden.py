@@ -329,6 +329,45 @@ def body_fixture(mods, syn, ref, shim):
     np.savez_compressed(os.path.join(HERE, "body.npz"), **out)
     print("body: ok")
 
+    # convergence chain: ring buffer, longdy / longdydt, stall detector and the
+    # loop condition cond_fn (outer_loop.py:614-713, 919-989), recorded after
+    # every attempt of the reference body
+    cond_log = []
+
+    def while_once(cond, fn, init):
+        res = fn(init)
+        cond_log.append(bool(cond(res)))
+        return res
+
+    ns["jax"].lax.while_loop = while_once
+    conv_over = dict(count_min=2, yconv_cri=0.3, yconv_min=1.0, slope_cri=1e30, conv_stall_window=3,
+                     trun_min=0.0, flux_cri=0.1, st_factor=0.5, mtol_conv=1e-20)
+    p = dict(BODY_PARAMS)
+    p.update(conv_over)
+    runner = ns["_make_runner"](net, statics(p), False, J(gas_all), False, J(np.zeros((nz, ni), bool)), False,
+                                1e30, 1e30)
+    s = state(y0, mix(y0), 1e-6, 0.05, accept_count=np.int32(0), delta_count=np.int32(0), nega_count=np.int32(0),
+              loss_count=np.int32(0), t=np.float64(0.0))
+    conv_fields = ["accept_count", "retry_count", "t", "dt", "longdy", "longdydt", "longdy_seen_min",
+                   "count_since_new_min"]
+    cv = dict(conv_in_y=np.asarray(s.y), conv_in_ymix=np.asarray(s.ymix), conv_in_atom_loss=np.asarray(s.atom_loss),
+              conv_n=np.array(40), conv_slope_min=np.array(1e-8))
+    for k2, v in conv_over.items():
+        cv["conv_param_" + k2] = np.array(v)
+    rec = {f: [] for f in conv_fields}
+    for _ in range(40):
+        s = runner(s, atm)
+        for f_ in conv_fields:
+            rec[f_].append(np.asarray(getattr(s, f_)))
+    for f_ in conv_fields:
+        cv["conv_" + f_] = np.array(rec[f_])
+    cv["conv_cond"] = np.array(cond_log)
+    cv["conv_y_ring"] = np.asarray(s.y_time_ring)
+    cv["conv_t_ring"] = np.asarray(s.t_time_ring)
+    cv["conv_y"] = np.asarray(s.y)
+    np.savez_compressed(os.path.join(HERE, "conv.npz"), **cv)
+    print("conv: accepts", [int(a) for a in rec["accept_count"]], "cond", cond_log)
+
 
 def photo_fixture(mods, syn):
     photo = mods["photo"]

@@ -130,6 +130,33 @@ def test_loop_body_attempts():
         check_body_state(s, c["out"], 1e-13)
 
 
+def test_convergence_chain():
+    """Ring buffer, longdy / longdydt, stall detector and the loop condition
+    against 40 attempts of the reference runner (``tests/golden/conv.npz``)."""
+    net, atm, compo, atom_ini, k, params, cases = golden_body()
+    g = golden("conv.npz")
+    cp = {kk[len("conv_param_"):]: g[kk].item() for kk in g if kk.startswith("conv_param_")}
+    p = dict(params, **cp)
+    p.update(runtime=1e30, count_max=10 ** 6, conv_step=4, use_adapt_rtol=False)
+    al = g["conv_in_atom_loss"]
+    s = dict(y=g["conv_in_y"], y_prev=g["conv_in_y"], ymix=g["conv_in_ymix"], dt=1e-6, t=0.0, delta=0.0,
+             accept_count=0, retry_count=0, atom_loss=al, atom_loss_prev=al, nega_count=0, loss_count=0,
+             delta_count=0, small_y=1.5, nega_y=2.5, rtol=0.05, loss_criteria=1e-3, longdy=1.0, longdydt=1.0,
+             longdy_seen_min=np.inf, count_since_new_min=0)
+    nz, ni = s["y"].shape
+    ring_y, ring_t = np.zeros((4, nz, ni)), np.zeros(4)
+    for a in range(int(g["conv_n"])):
+        s = oc.attempt(s, k, atm, net, compo, atom_ini, p)
+        s.update(oc.conv_update(s, ring_y, ring_t, atm["M"], p, do_accept=s["_accept"] or s["_force"]))
+        for f in ("accept_count", "retry_count", "count_since_new_min"):
+            assert int(s[f]) == int(g["conv_" + f][a]), (a, f)
+        for f in ("t", "dt", "longdy", "longdydt", "longdy_seen_min"):
+            close(s[f], g["conv_" + f][a], 1e-12, floor=1e-300)
+        assert oc.loop_continues(s, p, float(g["conv_slope_min"])) == bool(g["conv_cond"][a]), a
+    close(ring_y, g["conv_y_ring"], 1e-12, floor=1e-30)
+    close(ring_t, g["conv_t_ring"], 1e-12)
+
+
 def _ph(g):
     return {k[3:]: (g[k].item() if g[k].ndim == 0 else g[k]) for k in g if k.startswith("ph_")}
 
