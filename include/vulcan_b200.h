@@ -164,7 +164,8 @@ int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const d
  * rebalance (:844-853), next state (:899-917), counters (:1062-1066),
  * adaptive rtol (:990-1020) and the next dt (:181-193, :1022-1031), per
  * atmosphere, on the device. Photo, condensation, atmosphere refresh, ion
- * balance, bottom pins and the convergence ring are not part of it. */
+ * balance and bottom pins are not part of it; the convergence ring and the
+ * loop condition are vb_loop_converge. */
 #define VB_LOOP_MAX_ATOMS 16
 #define VB_LOOP_HYDRO_PARTIAL 1  /* rebalance gas species only (use_condense) */
 #define VB_LOOP_ZERO_BOT_ROW 2   /* drop the bottom layer from the error norm */
@@ -187,6 +188,24 @@ typedef struct VbLoopScalars {
   double t, delta, small_y, nega_y, rtol, loss_criteria;
   int32_t accept_count, retry_count, nega_count, loss_count, delta_count, last_decision;
 } VbLoopScalars;
+/* Convergence and termination knobs (reference _Statics, outer_loop.py:420-460;
+ * defaults in vulcan_cfg). conv_step >= 2 is the ring length. */
+typedef struct VbConvParams {
+  int32_t conv_step, count_min, count_max, conv_stall_window;
+  int32_t use_photo, final_update_photo_frq, reserved0, reserved1;
+  double st_factor, mtol_conv, atol, yconv_cri, yconv_min, slope_cri, flux_cri, trun_min, runtime;
+  double photo_switch_longdy, photo_switch_longdydt;
+} VbConvParams;
+/* Per-atmosphere convergence carry (JaxIntegState fields of the same names),
+ * device memory, updated in place by vb_loop_converge. Start: longdy =
+ * longdydt = 1, longdy_seen_min = +inf, count_since_new_min = 0, done = 0,
+ * update_photo_frq = the initial photo frequency. aflux_change is written by
+ * vb_photo_update. done = 1 once the loop condition stops the atmosphere;
+ * vb_loop_body and vb_loop_converge then leave it alone. */
+typedef struct VbConvState {
+  double longdy, longdydt, longdy_seen_min, aflux_change;
+  int32_t count_since_new_min, done, update_photo_frq, is_final_photo_frq;
+} VbConvState;
 /* Device arrays: gas_mask [ni] uint8 or NULL (non-gas species present: the
  * ysums of clip and mix run over gas species), compo [ni][n_atoms],
  * atom_ini [B][n_atoms], fix_mask [B][nz][ni] uint8 and fix_y [B][nz][ni]
@@ -194,12 +213,32 @@ typedef struct VbLoopScalars {
  * must not alias the state), state: y, y_prev, ymix [B][nz][ni] (y may equal
  * y_prev), atom_loss, atom_loss_prev [B][n_atoms], dt [B], scalars [B]. The layer
  * densities n_0 are the atmosphere blob's M. zoff as in vb_ros2_step (nz is
- * then the maximum layer count). */
+ * then the maximum layer count). conv [B] (nullable): atmospheres whose record
+ * has done set are skipped. */
 int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopParams* params,
                  const double* atm, const uint8_t* gas_mask, const double* compo, const double* atom_ini,
                  const uint8_t* fix_mask, const double* fix_y, const double* sol, const double* delta_arr,
                  double* y, double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
-                 double* dt, VbLoopScalars* scalars, void* stream);
+                 double* dt, VbLoopScalars* scalars, const VbConvState* conv, void* stream);
+
+/* Convergence part of the adaptive runner, after vb_loop_body: writes (y, t)
+ * into ring slot max(accept_count - 1, 0) % conv_step (outer_loop.py:918-928),
+ * finds the ring entry nearest t * st_factor (the slot just written excluded),
+ * computes longdy = max masked |y - y_old| / n_0 / ymix and longdydt =
+ * longdy / (t - t_old) (_conv_jax, :633-670), keeps them only after an
+ * accepted step, runs the stall counter (:944-989) and the photo-frequency
+ * switch (:1040-1050), and evaluates cond_fn (:672-713) into conv[b].done.
+ * Device arrays: slope_min [B] (cond_fn's slope floor), ignore_mask [ni]
+ * uint8 or NULL (species left out of longdy), y, ymix [B][nz][ni],
+ * scalars [B], ring_y [B][conv_step][nz][ni], ring_t [B][conv_step],
+ * conv [B], photo_due [B] int32 or NULL (set to 1 where the next attempt
+ * should run the photo branch: not done, use_photo, retry_count == 0 and
+ * accept_count % update_photo_frq == 0, as outer_loop.py:716-724). With zoff,
+ * atmosphere b's ring starts at zoff[b] * ni * conv_step. */
+int vb_loop_converge(int batch, int nz, int ni, const int64_t* zoff, const VbConvParams* params, const double* atm,
+                     const double* slope_min, const uint8_t* ignore_mask, const double* y, const double* ymix,
+                     const VbLoopScalars* scalars, double* ring_y, double* ring_t, VbConvState* conv,
+                     int32_t* photo_due, void* stream);
 
 /* Cotangents of every transport leaf of the steady-state residual
  * (reference steady_state_grad.py:36-59 SteadyStateInputs leaves Kzz, Dzz,

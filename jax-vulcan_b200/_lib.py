@@ -54,7 +54,8 @@ SIGNATURES = {
     "vb_bt_mixed_bytes": (_sz, [_i, _i, _i]),
     "vb_bt_factor_mixed": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_bt_solve_mixed": (_i, [_i, _i, _i, _p, _p, _p, _i, C.c_double, _p, _p, _p]),
-    "vb_loop_body": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "vb_loop_body": (_i, [_i, _i, _i] + [_p] * 19),
+    "vb_loop_converge": (_i, [_i, _i, _i] + [_p] * 13),
 }
 
 PROFILE_SITES = ["stage1_assembly", "factor", "back_sweep_1", "stage2_assembly", "forward_sweep_2",

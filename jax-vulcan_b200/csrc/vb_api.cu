@@ -538,7 +538,7 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
                  const uint8_t* gas_mask, const double* compo, const double* atom_ini, const uint8_t* fix_mask,
                  const double* fix_y, const double* sol, const double* delta_arr, double* y, double* y_prev,
                  double* ymix, double* atom_loss, double* atom_loss_prev, double* dt, VbLoopScalars* scalars,
-                 void* stream) {
+                 const VbConvState* conv, void* stream) {
   if (!params || !atm || !compo || !atom_ini || !sol || !delta_arr || !y || !y_prev || !ymix || !atom_loss ||
       !atom_loss_prev || !dt || !scalars)
     return fail(VB_ERR_ARG, "null argument");
@@ -556,8 +556,24 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
   B.ld = vb::round_even(ni);
   B.zoff = zoff;
   VB_CHECK(vb::launch_loop_body(B, p, gas_mask, compo, atom_ini, atm, fix_mask, fix_y, sol, delta_arr, y, y_prev,
-                                ymix, atom_loss, atom_loss_prev, dt, scalars, (cudaStream_t)stream),
+                                ymix, atom_loss, atom_loss_prev, dt, scalars, conv, (cudaStream_t)stream),
            "loop body");
+  return VB_OK;
+}
+
+int vb_loop_converge(int batch, int nz, int ni, const int64_t* zoff, const VbConvParams* params, const double* atm,
+                     const double* slope_min, const uint8_t* ignore_mask, const double* y, const double* ymix,
+                     const VbLoopScalars* scalars, double* ring_y, double* ring_t, VbConvState* conv,
+                     int32_t* photo_due, void* stream) {
+  if (!params || !atm || !slope_min || !y || !ymix || !scalars || !ring_y || !ring_t || !conv)
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2 || ni < 1 || ni > VB_MAX_NI) return fail(VB_ERR_ARG, "batch >= 1, nz >= 2, 1 <= ni <= 128");
+  if (params->conv_step < 2) return fail(VB_ERR_ARG, "conv_step must be >= 2");
+  vb::Batch B = bt_batch(batch, nz, ni);
+  B.zoff = zoff;
+  VB_CHECK(vb::launch_loop_conv(B, *params, atm, slope_min, ignore_mask, y, ymix, scalars, ring_y, ring_t, conv,
+                                photo_due, (cudaStream_t)stream),
+           "loop convergence");
   return VB_OK;
 }
 

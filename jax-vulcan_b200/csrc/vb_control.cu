@@ -5,7 +5,11 @@
 // force-accept (:745-756), reject counters (:758-764), time (:766-768),
 // hydrostatic rebalance (:844-853), next y / ymix / atom loss (:899-917),
 // adaptive rtol (:990-1020) and the next dt (_step_size :181-193,
-// :1022-1031).
+// :1022-1031). An atmosphere whose convergence record is done is skipped.
+//
+// loop_conv_kernel, after the body: ring buffer of (y, t), the lookback and
+// the relative change longdy / longdydt, the stall counter, the
+// photo-frequency switch and the loop condition, per atmosphere.
 //
 // One CTA per atmosphere, one warp per layer (lanes over species, ni <= 128).
 // Phase A clips and reduces (error norm, sign flags, clipped mass, per-layer
@@ -68,13 +72,14 @@ loop_body_kernel(Batch B, VbLoopParams p, const uint8_t* __restrict__ gas, const
                  const double* __restrict__ atom_ini, const double* __restrict__ atm, ElemIn E,
                  double* y, double* y_prev, double* ymix,  // may alias one another (y == y_prev)
                  double* __restrict__ atom_loss, double* __restrict__ atom_loss_prev, double* __restrict__ dtp,
-                 VbLoopScalars* __restrict__ st) {
+                 VbLoopScalars* __restrict__ st, const VbConvState* __restrict__ conv) {
   extern __shared__ double ys[];  // [2][nz]: ysum of the clipped and of the rebalanced state
   __shared__ double red[BODY_WARPS][4 + 2 * VB_LOOP_MAX_ATOMS];
   __shared__ int flags_s[BODY_WARPS][2];
   __shared__ int decision;  // 0 reject, 1 accept, 2 force-accept
 
   const int b = blockIdx.x;
+  if (conv && conv[b].done) return;  // stopped by the loop condition: frozen
   const Geo g = geo_of(B, b);
   const int ni = B.ni, nz = g.nz, na = p.n_atoms;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -288,7 +293,7 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
                              const double* atom_ini, const double* atm, const uint8_t* fix_mask,
                              const double* fix_y, const double* sol, const double* delta, double* y,
                              double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
-                             double* dt, VbLoopScalars* st, cudaStream_t stream) {
+                             double* dt, VbLoopScalars* st, const VbConvState* conv, cudaStream_t stream) {
   ElemIn E;
   E.sol = sol;
   E.delta = delta;
@@ -304,7 +309,123 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
     if (e != cudaSuccess) return e;
   }
   loop_body_kernel<<<B.count, BODY_THREADS, smem, stream>>>(B, p, gas, compo, atom_ini, atm, E, y, y_prev, ymix,
-                                                            atom_loss, atom_loss_prev, dt, st);
+                                                            atom_loss, atom_loss_prev, dt, st, conv);
+  return cudaGetLastError();
+}
+
+// Convergence after the body (one CTA per atmosphere). Ring slot
+// max(accept_count - 1, 0) % conv_step takes (y, t) (outer_loop.py:918-928);
+// the lookback entry is the first slot, the one just written excluded, whose
+// t is nearest t * st_factor (_conv_jax, :633-670); longdy is the largest
+// |y - y_old| / n_0 / ymix over the entries with ymix >= mtol_conv,
+// y >= atol and the species not ignored, longdydt = longdy / (t - t_old);
+// both kept only after an accepted (or force-accepted) step, with the stall
+// counter restarting on a 5 % drop below the lowest longdy seen (:944-989);
+// photo-frequency switch (:1040-1050); cond_fn (:672-713) -> done.
+__global__ void __launch_bounds__(BODY_THREADS)
+loop_conv_kernel(Batch B, VbConvParams p, const double* __restrict__ atm, const double* __restrict__ slope_min,
+                 const uint8_t* __restrict__ ignore, const double* __restrict__ y, const double* __restrict__ ymix,
+                 const VbLoopScalars* __restrict__ st, double* __restrict__ ring_y, double* __restrict__ ring_t,
+                 VbConvState* __restrict__ conv, int32_t* __restrict__ photo_due) {
+  __shared__ double red[BODY_WARPS];
+  __shared__ int k_s;
+  const int b = blockIdx.x;
+  if (conv[b].done) {
+    if (photo_due && threadIdx.x == 0) photo_due[b] = 0;
+    return;
+  }
+  const Geo g = geo_of(B, b);
+  const int ni = B.ni, nz = g.nz, n = nz * ni;
+  const int64_t o = g.z0 * ni;
+  const VbLoopScalars s = st[b];
+  const int cs = p.conv_step;
+  const int idx = (s.accept_count > 0 ? s.accept_count - 1 : 0) % cs;
+  double* ry = ring_y + o * cs;
+  double* rt = ring_t + (int64_t)b * cs;
+  const double* M = atm + g.atm + atm_offsets(nz, ni).M;
+  const double* yb = y + o;
+  const double* xb = ymix + o;
+  if (threadIdx.x == 0) {
+    rt[idx] = s.t;
+    const double target = s.t * p.st_factor;
+    int k = -1;
+    double best = 0.0;
+    for (int q = 0; q < cs; ++q) {
+      const double dq = q == idx ? INFINITY : fabs(rt[q] - target);
+      if (k < 0 || dq < best) {
+        k = q;
+        best = dq;
+      }
+    }
+    k_s = k;
+  }
+  __syncthreads();
+  const int k = k_s;
+  const double* yo = ry + (int64_t)k * n;
+  double mx = 0.0;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int j = e / ni, i = e - j * ni;
+    const double yv = yb[e], xv = xb[e];
+    double la = fabs((yv - yo[e]) / M[j]);
+    if (xv < p.mtol_conv) la = 0.0;
+    if (yv < p.atol) la = 0.0;
+    if (ignore && ignore[i]) la = 0.0;
+    const double ratio = xv > 0.0 ? la / fmax(xv, 1e-300) : 0.0;
+    mx = jmax(mx, ratio);
+  }
+  __syncthreads();  // every thread has read the lookback entry before the slot is rewritten
+  double* slot = ry + (int64_t)idx * n;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) slot[e] = yb[e];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = jmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ld_new = red[0];
+    for (int w = 1; w < BODY_WARPS; ++w) ld_new = jmax(ld_new, red[w]);
+    const double ldt_new = ld_new / fmax(s.t - rt[k], 1e-300);
+    VbConvState c = conv[b];
+    const bool take = s.last_decision != 0;
+    if (take) {
+      c.longdy = ld_new;
+      c.longdydt = ldt_new;
+    }
+    const bool drop = take && (c.longdy < c.longdy_seen_min * 0.95);
+    if (drop) {
+      c.longdy_seen_min = c.longdy;
+      c.count_since_new_min = 0;
+    } else if (take) {
+      c.count_since_new_min += 1;
+    }
+    if (p.use_photo && !c.is_final_photo_frq && c.longdy < p.photo_switch_longdy &&
+        c.longdydt < p.photo_switch_longdydt) {
+      c.update_photo_frq = p.final_update_photo_frq;
+      c.is_final_photo_frq = 1;
+    }
+    const bool too_long = s.t > p.runtime;
+    const bool too_many = s.accept_count > p.count_max;
+    bool converged = ((c.longdy < p.yconv_cri) && (c.longdydt < p.slope_cri)) ||
+                     ((c.longdy < p.yconv_min) && (c.longdydt < slope_min[b]));
+    converged = converged && (c.aflux_change < p.flux_cri);
+    const bool stalled = (c.count_since_new_min > p.conv_stall_window) && (c.longdy_seen_min < p.yconv_min) &&
+                         (c.longdy < p.yconv_min) && (c.aflux_change < p.flux_cri);
+    const bool ready = (s.t > p.trun_min) && (s.accept_count > p.count_min);
+    c.done = (too_long || too_many || (ready && (converged || stalled))) ? 1 : 0;
+    conv[b] = c;
+    if (photo_due)
+      photo_due[b] = (!c.done && p.use_photo && c.update_photo_frq > 0 && s.retry_count == 0 &&
+                      s.accept_count % c.update_photo_frq == 0)
+                         ? 1
+                         : 0;
+  }
+}
+
+cudaError_t launch_loop_conv(const Batch& B, const VbConvParams& p, const double* atm, const double* slope_min,
+                             const uint8_t* ignore, const double* y, const double* ymix, const VbLoopScalars* st,
+                             double* ring_y, double* ring_t, VbConvState* conv, int32_t* photo_due,
+                             cudaStream_t stream) {
+  loop_conv_kernel<<<B.count, BODY_THREADS, 0, stream>>>(B, p, atm, slope_min, ignore, y, ymix, st, ring_y, ring_t,
+                                                         conv, photo_due);
   return cudaGetLastError();
 }
 

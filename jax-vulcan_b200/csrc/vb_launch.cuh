@@ -64,6 +64,10 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
                              const double* atom_ini, const double* atm, const uint8_t* fix_mask,
                              const double* fix_y, const double* sol, const double* delta, double* y,
                              double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
-                             double* dt, VbLoopScalars* st, cudaStream_t stream);
+                             double* dt, VbLoopScalars* st, const VbConvState* conv, cudaStream_t stream);
+cudaError_t launch_loop_conv(const Batch& B, const VbConvParams& p, const double* atm, const double* slope_min,
+                             const uint8_t* ignore, const double* y, const double* ymix, const VbLoopScalars* st,
+                             double* ring_y, double* ring_t, VbConvState* conv, int32_t* photo_due,
+                             cudaStream_t stream);
 
 }  // namespace vb

@@ -5,10 +5,12 @@
 per-atmosphere carry of `JaxIntegState` (`outer_loop.py:45-135`) that the
 body updates (y, y_prev, ymix, dt, t, delta, counters, atom losses, rtol,
 loss_criteria) as device tensors. ``loop_body`` runs one body update after a
-step; ``AdaptiveRunner`` chains ``vb_ros2_step`` and ``vb_loop_body`` on one
-stream, so N attempts of N atmospheres run with no host round trip (each
-atmosphere accepts, rejects or force-accepts on its own, as the vmapped
-reference runner does).
+step; ``ConvStatics`` and ``loop_converge`` add the convergence ring, the
+convergence diagnostics and the loop condition (`outer_loop.py:633-713`,
+`:918-989`). ``AdaptiveRunner`` chains ``vb_ros2_step``, ``vb_loop_body``
+and ``vb_loop_converge`` on one stream, so N attempts of N atmospheres run
+with no host round trip (each atmosphere accepts, rejects, force-accepts and
+stops on its own, as the vmapped reference runner does).
 """
 from __future__ import annotations
 
@@ -43,6 +45,59 @@ SCALARS_DTYPE = np.dtype([("t", "<f8"), ("delta", "<f8"), ("small_y", "<f8"), ("
                           ("retry_count", "<i4"), ("nega_count", "<i4"), ("loss_count", "<i4"),
                           ("delta_count", "<i4"), ("last_decision", "<i4")])
 assert SCALARS_DTYPE.itemsize == 72
+
+# VbConvState, one record per atmosphere (48 bytes)
+CONV_DTYPE = np.dtype([("longdy", "<f8"), ("longdydt", "<f8"), ("longdy_seen_min", "<f8"), ("aflux_change", "<f8"),
+                       ("count_since_new_min", "<i4"), ("done", "<i4"), ("update_photo_frq", "<i4"),
+                       ("is_final_photo_frq", "<i4")])
+assert CONV_DTYPE.itemsize == 48
+
+
+class VbConvParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("conv_step", "count_min", "count_max", "conv_stall_window", "use_photo",
+                                         "final_update_photo_frq", "reserved0", "reserved1")] + \
+               [(n, C.c_double) for n in ("st_factor", "mtol_conv", "atol", "yconv_cri", "yconv_min", "slope_cri",
+                                          "flux_cri", "trun_min", "runtime", "photo_switch_longdy",
+                                          "photo_switch_longdydt")]
+
+
+@dataclass
+class ConvStatics:
+    """Convergence and termination knobs of the reference `_Statics`
+    (`outer_loop.py:420-460`), with the defaults of `vulcan_cfg.py`."""
+    conv_step: int = 500
+    count_min: int = 120
+    count_max: int = 10000
+    conv_stall_window: int = 200
+    st_factor: float = 0.5
+    mtol_conv: float = 1e-20
+    atol: float = 0.1
+    yconv_cri: float = 0.01
+    yconv_min: float = 0.1
+    slope_cri: float = 1e-4
+    flux_cri: float = 0.1
+    trun_min: float = 1e2
+    runtime: float = 1e22
+    use_photo: bool = False
+    final_update_photo_frq: int = 5
+    photo_switch_longdy: float = 0.0
+    photo_switch_longdydt: float = 0.0
+
+    def params(self) -> VbConvParams:
+        p = VbConvParams()
+        for n, ctype in VbConvParams._fields_:
+            if hasattr(self, n):
+                v = getattr(self, n)
+                setattr(p, n, float(v) if ctype is C.c_double else int(v))
+        return p
+
+
+def slope_min_of(Kzz, Hp):
+    """cond_fn's slope floor (`outer_loop.py:678-683`), per atmosphere:
+    max(min(min(Kzz / (0.1 Hp[:-1])^2), 1e-8), 1e-10)."""
+    Kzz, Hp = np.atleast_2d(np.asarray(Kzz)), np.atleast_2d(np.asarray(Hp))
+    v = np.min(Kzz / (0.1 * Hp[:, :-1]) ** 2, axis=1)
+    return np.maximum(np.minimum(v, 1e-8), 1e-10)
 
 
 @dataclass
@@ -110,6 +165,26 @@ class LoopState:
         for k, v in (counters or {}).items():
             rec[k] = v
         self.scalars = torch.from_numpy(rec.view(np.uint8).copy()).cuda()
+        self.conv = None
+
+    def enable_convergence(self, conv_step, longdy=1.0, longdydt=1.0, update_photo_frq=0, photo_due=False):
+        """Allocates the ring buffers and the convergence carry, with the
+        reference's initial values (longdy = longdydt = 1, longdy_seen_min =
+        inf). ``photo_due``: whether the first attempt runs the photo branch
+        (the reference's first attempt has accept_count = 0, so it does
+        whenever photochemistry is on)."""
+        B, nz, ni = self.y.shape
+        self.conv_step = int(conv_step)
+        self.ring_y = torch.zeros((B, self.conv_step, nz, ni), dtype=torch.float64, device="cuda")
+        self.ring_t = torch.zeros((B, self.conv_step), dtype=torch.float64, device="cuda")
+        rec = np.zeros(B, CONV_DTYPE)
+        rec["longdy"], rec["longdydt"], rec["longdy_seen_min"] = longdy, longdydt, np.inf
+        rec["update_photo_frq"] = update_photo_frq
+        self.conv = torch.from_numpy(rec.view(np.uint8).copy()).cuda()
+        self.photo_due = torch.full((B,), int(bool(photo_due)), dtype=torch.int32, device="cuda")
+
+    def conv_host(self) -> np.ndarray:
+        return self.conv.cpu().numpy().view(CONV_DTYPE)
 
     @property
     def batch(self) -> int:
@@ -146,17 +221,39 @@ def loop_body(state: LoopState, sol, delta_arr, atm_blob, compo, atom_ini, stati
         B, nz, ni, _lib.ptr(zoff), C.addressof(p), _lib.ptr(atm_blob), _lib.ptr(gm), _lib.ptr(compo),
         _lib.ptr(atom_ini), _lib.ptr(fm), _lib.ptr(fy), _lib.ptr(sol), _lib.ptr(delta_arr), _lib.ptr(state.y),
         _lib.ptr(state.y_prev), _lib.ptr(state.ymix), _lib.ptr(state.atom_loss), _lib.ptr(state.atom_loss_prev),
-        _lib.ptr(state.dt), _lib.ptr(state.scalars), _lib.stream_handle(stream)), "vb_loop_body")
+        _lib.ptr(state.dt), _lib.ptr(state.scalars), _lib.ptr(state.conv), _lib.stream_handle(stream)),
+        "vb_loop_body")
+
+
+def loop_converge(state: LoopState, atm_blob, statics: ConvStatics, slope_min, ignore_mask=None, zoff=None,
+                  stream=None):
+    """Ring append, convergence diagnostics and the loop condition after a
+    body update (device, in place; atmospheres that stop are frozen)."""
+    B, nz, ni = state.y.shape
+    p = statics.params()
+    sm = as_device(np.broadcast_to(np.asarray(slope_min, np.float64), (B,)).copy())
+    ig = None if ignore_mask is None else as_device(np.asarray(ignore_mask, np.uint8), torch.uint8)
+    _lib.check(_lib.lib().vb_loop_converge(
+        B, nz, ni, _lib.ptr(zoff), C.addressof(p), _lib.ptr(atm_blob), _lib.ptr(sm), _lib.ptr(ig), _lib.ptr(state.y),
+        _lib.ptr(state.ymix), _lib.ptr(state.scalars), _lib.ptr(state.ring_y), _lib.ptr(state.ring_t),
+        _lib.ptr(state.conv), _lib.ptr(state.photo_due), _lib.stream_handle(stream)), "vb_loop_converge")
 
 
 class AdaptiveRunner:
     """Attempts of the reference loop body (`outer_loop.py:715-1100`, without
-    photo, condensation, refresh or the convergence ring) for a batch of
-    atmospheres: each attempt is one ``vb_ros2_step`` from ``state.y`` with
-    ``state.dt`` followed by ``vb_loop_body``; both stay on one stream."""
+    the photo update, condensation or refresh) for a batch of atmospheres:
+    each attempt is one ``vb_ros2_step`` from ``state.y`` with ``state.dt``
+    followed by ``vb_loop_body`` and, given ``conv``, ``vb_loop_converge``
+    (ring buffer, convergence diagnostics, loop condition); all on one
+    stream. ``slope_min``: cond_fn's slope floor per atmosphere
+    (``slope_min_of``)."""
 
     def __init__(self, net: NetworkArrays, atm: AtmStatic, statics: LoopStatics, compo, atom_ini,
-                 batch: int | None = None, gas_mask=None):
+                 batch: int | None = None, gas_mask=None, conv: ConvStatics | None = None, slope_min=1e-8,
+                 ignore_mask=None):
+        self.conv = conv
+        self.slope_min = slope_min
+        self.ignore_mask = ignore_mask
         self.step = Ros2Step(net, atm, batch)
         self.statics = statics
         self.compo = as_device(compo).contiguous()
@@ -170,9 +267,34 @@ class AdaptiveRunner:
         self.step(state.y, k, state.dt, fix_mask=fix_mask, out=(self.sol, self.delta), stream=stream)
         loop_body(state, self.sol, self.delta, self.step.blob, self.compo, self.atom_ini, self.statics,
                   gas_mask=self.gas_mask, fix_mask=fix_mask, fix_y=fix_y, stream=stream)
+        if self.conv is not None:
+            if state.conv is None:
+                state.enable_convergence(self.conv.conv_step)
+            loop_converge(state, self.step.blob, self.conv, self.slope_min, self.ignore_mask, stream=stream)
 
     def run(self, state: LoopState, k, n_attempts: int, fix_mask=None, fix_y=None, stream=None):
         k = as_device(k).contiguous()
         for _ in range(int(n_attempts)):
             self.attempt(state, k, fix_mask, fix_y, stream)
         return state
+
+    def run_to_convergence(self, state: LoopState, k, max_attempts: int, check_every: int = 50, fix_mask=None,
+                           fix_y=None, stream=None) -> int:
+        """Attempts until the loop condition stops every atmosphere
+        (converged, stalled, too long or too many steps) or ``max_attempts``
+        have run; the done flags are read back every ``check_every``
+        attempts only, and stopped atmospheres stay frozen meanwhile.
+        Returns the number of attempts run."""
+        if self.conv is None:
+            raise ValueError("the runner was built without ConvStatics")
+        if state.conv is None:
+            state.enable_convergence(self.conv.conv_step)
+        k = as_device(k).contiguous()
+        n = 0
+        while n < max_attempts:
+            for _ in range(min(check_every, max_attempts - n)):
+                self.attempt(state, k, fix_mask, fix_y, stream)
+                n += 1
+            if state.conv_host()["done"].all():
+                break
+        return n

@@ -159,8 +159,8 @@ def test_loop_body_rejects_bad_arguments():
     import ctypes as C
     dummy = C.c_void_p(16)  # never dereferenced: argument checks come first
     rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, None, None, dummy, dummy,
-                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None)
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None)
     assert rc == 1 and b"n_atoms" in L.vb_last_error()
     rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, dummy, None, dummy, dummy,
-                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None)
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None)
     assert rc == 1 and b"fix_mask" in L.vb_last_error()
