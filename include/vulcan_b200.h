@@ -291,6 +291,19 @@ int vb_photo_flux(int batch, int nz, int ni, const VbPhoto* photo, const double*
  * (photo.py:455-478). */
 int vb_photo_j(int batch, int nz, int nr, const VbPhoto* photo, const double* aflux, double* J_br,
                double* J_br_T, double* k, void* stream);
+/* The photo branch of the adaptive loop (reference outer_loop.py:283-350,
+ * gated as outer_loop.py:716-724): tau -> flux -> J -> photolysis rows of k
+ * for the atmospheres with due[b] != 0 (due NULL: all); the others are left
+ * untouched. dflux_u [B][nz+1][nbin] holds the previous call's upward flux on
+ * entry and the new one on return. With conv != NULL, conv[b].aflux_change of
+ * each updated atmosphere becomes the largest |aflux_new - aflux_old| /
+ * |aflux_new| over the entries with aflux_new > flux_atol (0 if none), where
+ * aflux_old is what `aflux` held on entry. J_br / J_br_T nullable; k as
+ * vb_ros2_step's [B][nr+1][nz]. */
+int vb_photo_update(int batch, int nz, int ni, int nr, const VbPhoto* photo, const int32_t* due, const double* y,
+                    const double* dz, const double* ymix, double* tau, double* aflux, double* sflux,
+                    double* dflux_d, double* dflux_u, double* J_br, double* J_br_T, double* k, double flux_atol,
+                    VbConvState* conv, void* stream);
 
 /* Profiling: while enabled, every kernel launch of vb_ros2_step is bracketed
  * by CUDA events recorded on the launching stream (launch sites:

@@ -477,7 +477,7 @@ int vb_photo_tau(int batch, int nz, int ni, const VbPhoto* photo, const double* 
                  double* tau, void* stream) {
   if (!photo || !y || !dz || !tau) return fail(VB_ERR_ARG, "null argument");
   if (batch < 1 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
-  VB_CHECK(vb::launch_photo_tau(batch, nz, ni, *photo, y, dz, tau, (cudaStream_t)stream), "photo tau");
+  VB_CHECK(vb::launch_photo_tau(batch, nz, ni, *photo, y, dz, tau, nullptr, nullptr, (cudaStream_t)stream), "photo tau");
   return VB_OK;
 }
 
@@ -488,7 +488,7 @@ int vb_photo_flux(int batch, int nz, int ni, const VbPhoto* photo, const double*
     return fail(VB_ERR_ARG, "null argument");
   if (batch < 1 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
   VB_CHECK(vb::launch_photo_flux(batch, nz, ni, *photo, tau, ymix, dflux_u_prev, aflux, sflux, dflux_d, dflux_u,
-                                 (cudaStream_t)stream),
+                                 nullptr, 0.0, nullptr, (cudaStream_t)stream),
            "photo flux");
   return VB_OK;
 }
@@ -498,7 +498,26 @@ int vb_photo_j(int batch, int nz, int nr, const VbPhoto* photo, const double* af
   if (!photo || !aflux) return fail(VB_ERR_ARG, "null argument");
   if (batch < 1 || nz < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
     return fail(VB_ERR_ARG, "bad shape");
-  VB_CHECK(vb::launch_photo_j(batch, nz, nr, *photo, aflux, J_br, J_br_T, k, (cudaStream_t)stream), "photo J");
+  VB_CHECK(vb::launch_photo_j(batch, nz, nr, *photo, aflux, J_br, J_br_T, k, nullptr, (cudaStream_t)stream),
+           "photo J");
+  return VB_OK;
+}
+
+int vb_photo_update(int batch, int nz, int ni, int nr, const VbPhoto* photo, const int32_t* due, const double* y,
+                    const double* dz, const double* ymix, double* tau, double* aflux, double* sflux,
+                    double* dflux_d, double* dflux_u, double* J_br, double* J_br_T, double* k, double flux_atol,
+                    VbConvState* conv, void* stream) {
+  if (!photo || !y || !dz || !ymix || !tau || !aflux || !sflux || !dflux_d || !dflux_u || !k)
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || ni < 1 || nr < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
+    return fail(VB_ERR_ARG, "bad shape");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* achg = conv ? &conv[0].aflux_change : nullptr;
+  VB_CHECK(vb::launch_photo_tau(batch, nz, ni, *photo, y, dz, tau, due, achg, st), "photo tau");
+  VB_CHECK(vb::launch_photo_flux(batch, nz, ni, *photo, tau, ymix, dflux_u, aflux, sflux, dflux_d, dflux_u, due,
+                                 flux_atol, achg, st),
+           "photo flux");
+  VB_CHECK(vb::launch_photo_j(batch, nz, nr, *photo, aflux, J_br, J_br_T, k, due, st), "photo J");
   return VB_OK;
 }
 

@@ -44,13 +44,14 @@ cudaError_t launch_sweep(const Batch&, double* ws, const SweepArgs&, cudaStream_
 cudaError_t launch_pack_blocks(const Batch&, const double* diag, const double* sup_d, const double* sub_d,
                                double* ws, cudaStream_t);
 
+// due (nullable): per-atmosphere mask; achg (nullable): &conv[0].aflux_change
 cudaError_t launch_photo_tau(int batch, int nz, int ni, const VbPhoto& P, const double* y, const double* dz,
-                             double* tau, cudaStream_t);
+                             double* tau, const int32_t* due, double* achg, cudaStream_t);
 cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const double* tau, const double* ymix,
                               const double* du_prev, double* aflux, double* sflux, double* dd, double* du,
-                              cudaStream_t);
+                              const int32_t* due, double flux_atol, double* achg, cudaStream_t);
 cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
-                           double* J_br_T, double* k, cudaStream_t);
+                           double* J_br_T, double* k, const int32_t* due, cudaStream_t);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
 template <typename R>
 cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,

@@ -7,6 +7,11 @@
 //   j_kernel     J-rates, a block reduction over bins per (layer, branch) with
 //                the two-resolution trapezoid correction, fused with the write
 //                of the photolysis rows of k (photo.py:309-351, 455-478).
+// Each kernel takes an optional per-atmosphere mask `due` (atmospheres with
+// due[b] == 0 are left alone: the photo branch of the adaptive loop runs only
+// where its cadence says so, outer_loop.py:716-724), and the flux kernel an
+// optional per-atmosphere accumulator of the actinic-flux change
+// (outer_loop.py:327-336), which the tau kernel of the same update zeroes.
 // Compiled with --fmad=false: products and sums round as the reference's
 // element-wise expressions do.
 #include <cuda_runtime.h>
@@ -17,12 +22,18 @@
 namespace vb {
 
 constexpr int PHOTO_THREADS = 128;
+// achg points at VbConvState::aflux_change of atmosphere 0; the records are
+// VbConvState-sized apart
+constexpr int64_t ACHG_STRIDE = sizeof(VbConvState) / sizeof(double);
+static_assert(sizeof(VbConvState) % sizeof(double) == 0, "VbConvState size");
 
 __global__ void __launch_bounds__(PHOTO_THREADS)
 tau_kernel(int nz, int ni, VbPhoto P, const double* __restrict__ y, const double* __restrict__ dz,
-           double* __restrict__ tau) {
+           double* __restrict__ tau, const int32_t* __restrict__ due, double* __restrict__ achg) {
   const int b = blockIdx.y;
   const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (due && due[b] == 0) return;
+  if (achg && bin == 0) achg[(int64_t)b * ACHG_STRIDE] = 0.0;
   if (bin >= P.nbin) return;
   const int nbin = P.nbin;
   const double* yb = y + (int64_t)b * nz * ni;
@@ -115,10 +126,14 @@ __device__ inline TwoStream two_stream(const VbPhoto& P, const double* __restric
 
 __global__ void __launch_bounds__(PHOTO_THREADS)
 flux_kernel(int nz, int ni, VbPhoto P, const double* __restrict__ tau, const double* __restrict__ ymix,
-            const double* __restrict__ du_prev, double* __restrict__ aflux, double* __restrict__ sflux,
-            double* __restrict__ dd, double* __restrict__ du) {
+            const double* du_prev, double* __restrict__ aflux, double* __restrict__ sflux,
+            double* __restrict__ dd, double* du, const int32_t* __restrict__ due, double flux_atol,
+            double* __restrict__ achg) {
+  // du_prev and du may be one buffer: each thread reads its bin of du_prev in
+  // the down recursion before the up recursion overwrites it.
   const int b = blockIdx.y;
   const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (due && due[b] == 0) return;
   if (bin >= P.nbin) return;
   const int nbin = P.nbin;
   const int64_t zb = (int64_t)b * (nz + 1) * nbin;
@@ -151,6 +166,7 @@ flux_kernel(int nz, int ni, VbPhoto P, const double* __restrict__ tau, const dou
   double u_prev = 0.0;
   dub[bin] = 0.0;
   const double conv = P.hc / P.bins[bin];
+  double change = 0.0;  // largest relative aflux change of this bin (entries above flux_atol)
   for (int j = 1; j <= nz; ++j) {
     const double t0 = tb[(int64_t)(j - 1) * nbin + bin], t1 = tb[(int64_t)j * nbin + bin];
     TwoStream c = two_stream(P, xT, nz, ni, ym + (int64_t)(j - 1) * ni, j - 1, bin, t0 - t1);
@@ -161,17 +177,28 @@ flux_kernel(int nz, int ni, VbPhoto P, const double* __restrict__ tau, const dou
     dub[(int64_t)j * nbin + bin] = v;
     const double ave = 0.5 * (sb[(int64_t)(j - 1) * nbin + bin] + sb[(int64_t)j * nbin + bin]);
     const double tot = ave + 0.5 * (u_prev + v + ddb[(int64_t)j * nbin + bin] + ddb[(int64_t)(j - 1) * nbin + bin]) / P.edd;
-    ab[(int64_t)(j - 1) * nbin + bin] = tot / conv;
+    const double an = tot / conv;
+    if (achg && an > flux_atol) {
+      const double r = fabs(an - ab[(int64_t)(j - 1) * nbin + bin]) / fmax(fabs(an), 1e-300);
+      change = (r > change || r != r) ? r : change;
+    }
+    ab[(int64_t)(j - 1) * nbin + bin] = an;
     u_prev = v;
   }
+  // the ratios are >= 0 or NaN, so their bit patterns order as their values
+  // do and a NaN wins the maximum, as it does in the reference's max
+  if (achg && change != 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(achg + (int64_t)b * ACHG_STRIDE),
+              static_cast<unsigned long long>(__double_as_longlong(change)));
 }
 
 // J of one (layer, branch): trapezoid over the two bin resolutions
 // (photo.py:316-349), then the k row (photo.py:465-478).
 __global__ void __launch_bounds__(PHOTO_THREADS)
 j_kernel(int nz, int nr, VbPhoto P, const double* __restrict__ aflux, double* __restrict__ J_br,
-         double* __restrict__ J_br_T, double* __restrict__ k) {
+         double* __restrict__ J_br_T, double* __restrict__ k, const int32_t* __restrict__ due) {
   const int j = blockIdx.x, br = blockIdx.y, b = blockIdx.z;
+  if (due && due[b] == 0) return;
   const int nbin = P.nbin, d12 = P.din12;
   const bool is_T = br >= P.n_br;
   const int brl = is_T ? br - P.n_br : br;
@@ -219,25 +246,26 @@ j_kernel(int nz, int nr, VbPhoto P, const double* __restrict__ aflux, double* __
 }
 
 cudaError_t launch_photo_tau(int batch, int nz, int ni, const VbPhoto& P, const double* y, const double* dz,
-                             double* tau, cudaStream_t st) {
+                             double* tau, const int32_t* due, double* achg, cudaStream_t st) {
   dim3 grid((P.nbin + PHOTO_THREADS - 1) / PHOTO_THREADS, batch);
-  tau_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, ni, P, y, dz, tau);
+  tau_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, ni, P, y, dz, tau, due, achg);
   return cudaGetLastError();
 }
 
 cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const double* tau, const double* ymix,
                               const double* du_prev, double* aflux, double* sflux, double* dd, double* du,
-                              cudaStream_t st) {
+                              const int32_t* due, double flux_atol, double* achg, cudaStream_t st) {
   dim3 grid((P.nbin + PHOTO_THREADS - 1) / PHOTO_THREADS, batch);
-  flux_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, ni, P, tau, ymix, du_prev, aflux, sflux, dd, du);
+  flux_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, ni, P, tau, ymix, du_prev, aflux, sflux, dd, du, due, flux_atol,
+                                              achg);
   return cudaGetLastError();
 }
 
 cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
-                           double* J_br_T, double* k, cudaStream_t st) {
+                           double* J_br_T, double* k, const int32_t* due, cudaStream_t st) {
   if (P.n_br + P.n_br_T == 0) return cudaSuccess;
   dim3 grid(nz, P.n_br + P.n_br_T, batch);
-  j_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, nr, P, aflux, J_br, J_br_T, k);
+  j_kernel<<<grid, PHOTO_THREADS, 0, st>>>(nz, nr, P, aflux, J_br, J_br_T, k, due);
   return cudaGetLastError();
 }
 

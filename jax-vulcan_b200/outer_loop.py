@@ -79,6 +79,7 @@ class ConvStatics:
     trun_min: float = 1e2
     runtime: float = 1e22
     use_photo: bool = False
+    ini_update_photo_frq: int = 100
     final_update_photo_frq: int = 5
     photo_switch_longdy: float = 0.0
     photo_switch_longdydt: float = 0.0
@@ -246,11 +247,25 @@ class AdaptiveRunner:
     followed by ``vb_loop_body`` and, given ``conv``, ``vb_loop_converge``
     (ring buffer, convergence diagnostics, loop condition); all on one
     stream. ``slope_min``: cond_fn's slope floor per atmosphere
-    (``slope_min_of``)."""
+    (``slope_min_of``).
+
+    With ``photo`` (a ``photo.PhotoDevice``; needs ``conv`` with
+    ``use_photo``), each attempt first runs the photo branch for the
+    atmospheres whose photo-due flag is set (reference `outer_loop.py:716-724`:
+    no retry pending and ``accept_count % update_photo_frq == 0``), which
+    rewrites their photolysis rows of ``k`` in place and their actinic-flux
+    change; ``dz`` [B, nz] or [nz] is the layer thickness of the photo grid
+    and ``photo_carry`` (a ``photo.PhotoCarry``) the photo fields of the
+    carry."""
 
     def __init__(self, net: NetworkArrays, atm: AtmStatic, statics: LoopStatics, compo, atom_ini,
                  batch: int | None = None, gas_mask=None, conv: ConvStatics | None = None, slope_min=1e-8,
-                 ignore_mask=None):
+                 ignore_mask=None, photo=None, dz=None, flux_atol=1.0, photo_carry=None):
+        if photo is not None and (conv is None or not conv.use_photo):
+            raise ValueError("the photo branch needs ConvStatics with use_photo")
+        self.photo = photo
+        self.dz = None if dz is None else as_device(dz)
+        self.flux_atol = float(flux_atol)
         self.conv = conv
         self.slope_min = slope_min
         self.ignore_mask = ignore_mask
@@ -262,14 +277,30 @@ class AdaptiveRunner:
         B, nz, ni = self.step.batch, self.step.nz, net.ni
         self.sol = torch.empty((B, nz, ni), dtype=torch.float64, device="cuda")
         self.delta = torch.empty_like(self.sol)
+        if photo is not None:
+            from .photo import PhotoCarry
+            self.photo_carry = photo_carry if photo_carry is not None else PhotoCarry(photo, B, nz)
+
+    def start(self, state: LoopState):
+        """Gives ``state`` its convergence carry (first attempt photo-due
+        when photochemistry is on, as in the reference)."""
+        c = self.conv
+        state.enable_convergence(c.conv_step, update_photo_frq=c.ini_update_photo_frq if c.use_photo else 0,
+                                 photo_due=c.use_photo)
 
     def attempt(self, state: LoopState, k, fix_mask=None, fix_y=None, stream=None):
+        if self.conv is not None and state.conv is None:
+            self.start(state)
+        if self.photo is not None:
+            from .photo import photo_branch
+            if not (isinstance(k, torch.Tensor) and k.is_cuda and k.dtype == torch.float64 and k.is_contiguous()):
+                raise TypeError("with the photo branch, k must be a contiguous float64 CUDA tensor (updated in place)")
+            photo_branch(self.photo_carry, state.y, state.ymix, self.dz, k, self.photo, due=state.photo_due,
+                         flux_atol=self.flux_atol, conv=state.conv, stream=stream)
         self.step(state.y, k, state.dt, fix_mask=fix_mask, out=(self.sol, self.delta), stream=stream)
         loop_body(state, self.sol, self.delta, self.step.blob, self.compo, self.atom_ini, self.statics,
                   gas_mask=self.gas_mask, fix_mask=fix_mask, fix_y=fix_y, stream=stream)
         if self.conv is not None:
-            if state.conv is None:
-                state.enable_convergence(self.conv.conv_step)
             loop_converge(state, self.step.blob, self.conv, self.slope_min, self.ignore_mask, stream=stream)
 
     def run(self, state: LoopState, k, n_attempts: int, fix_mask=None, fix_y=None, stream=None):
@@ -288,7 +319,7 @@ class AdaptiveRunner:
         if self.conv is None:
             raise ValueError("the runner was built without ConvStatics")
         if state.conv is None:
-            state.enable_convergence(self.conv.conv_step)
+            self.start(state)
         k = as_device(k).contiguous()
         n = 0
         while n < max_attempts:

@@ -5,6 +5,9 @@
 cross-section tables in device memory once (the reference's ``PhotoData`` and
 ``PhotoJData``) and ``photo_update`` runs the in-loop photo branch
 (tau -> flux -> J -> k rows, reference `outer_loop.py:283-350`).
+``PhotoCarry`` holds the photo fields of the loop carry for a batch and
+``photo_branch`` runs that branch for the atmospheres a device mask selects,
+with the actinic-flux change the loop condition reads.
 """
 from __future__ import annotations
 
@@ -190,3 +193,45 @@ def photo_update(y, ymix, dz, k_arr, photo: PhotoDevice, dflux_u_prev, stream=No
     aflux, sflux, dd, du = compute_flux_jax(tau, ymix, photo, dflux_u_prev, stream=stream)
     update_k_with_J(k_arr, aflux, photo, stream)
     return aflux, du
+
+
+class PhotoCarry:
+    """Photo fields of the loop carry for a batch of atmospheres (reference
+    `JaxIntegState` tau, aflux, sflux, dflux_d, dflux_u, J_br, J_br_T,
+    `outer_loop.py:66-80`), device tensors updated in place."""
+
+    def __init__(self, photo: PhotoDevice, batch: int, nz: int, aflux=None, dflux_u=None):
+        nbin = photo.nbin
+        dev = dict(dtype=torch.float64, device="cuda")
+        self.tau = torch.zeros((batch, nz + 1, nbin), **dev)
+        self.aflux = (torch.zeros((batch, nz, nbin), **dev) if aflux is None
+                      else as_device(aflux).reshape(batch, nz, nbin).clone())
+        self.sflux = torch.zeros((batch, nz + 1, nbin), **dev)
+        self.dflux_d = torch.zeros((batch, nz + 1, nbin), **dev)
+        self.dflux_u = (torch.zeros((batch, nz + 1, nbin), **dev) if dflux_u is None
+                        else as_device(dflux_u).reshape(batch, nz + 1, nbin).clone())
+        s = photo.struct
+        self.J_br = torch.zeros((batch, s.n_br, nz), **dev)
+        self.J_br_T = torch.zeros((batch, s.n_br_T, nz), **dev)
+
+
+def photo_branch(carry: PhotoCarry, y, ymix, dz, k_arr, photo: PhotoDevice, due=None, flux_atol=1.0, conv=None,
+                 stream=None):
+    """The photo branch of the adaptive loop for the atmospheres with
+    ``due[b] != 0`` (all when ``due`` is None): tau -> flux -> J -> photolysis
+    rows of ``k_arr`` [B, nr+1, nz] in place (reference `outer_loop.py:283-350`).
+    With ``conv`` (the loop's ``VbConvState`` records), the actinic-flux
+    change of each updated atmosphere is written to its record."""
+    B, nz, ni = y.shape
+    nr = k_arr.shape[1] - 1
+    dzt = as_device(dz).reshape(-1, nz)
+    if dzt.shape[0] == 1 and B > 1:
+        dzt = dzt.expand(B, nz)
+    dzt = dzt.contiguous()
+    _lib.check(_lib.lib().vb_photo_update(
+        B, nz, ni, nr, C.addressof(photo.struct), _lib.ptr(due), _lib.ptr(y), _lib.ptr(dzt), _lib.ptr(ymix),
+        _lib.ptr(carry.tau), _lib.ptr(carry.aflux), _lib.ptr(carry.sflux), _lib.ptr(carry.dflux_d),
+        _lib.ptr(carry.dflux_u), _lib.ptr(carry.J_br) if carry.J_br.numel() else None,
+        _lib.ptr(carry.J_br_T) if carry.J_br_T.numel() else None, _lib.ptr(k_arr), float(flux_atol), _lib.ptr(conv),
+        _lib.stream_handle(stream)), "vb_photo_update")
+    return carry

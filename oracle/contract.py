@@ -13,6 +13,10 @@ Restates, from reference `outer_loop.py`:
   `body_fn` (`:715-1100`): accept / reject / force-accept, hydrostatic
   rebalance, counters, adaptive rtol and dt, for a run without photo,
   condensation, atmosphere refresh, ion balance or bottom pins.
+* ``conv_update`` / ``loop_continues`` -> the convergence ring and
+  diagnostics (`:633-670`, `:918-989`) and `cond_fn` (`:672-713`)
+* ``photo_switch`` / ``photo_due`` -> the photo-frequency switch
+  (`:1040-1050`) and the photo cadence (`:716-724`)
 """
 from __future__ import annotations
 
@@ -205,3 +209,20 @@ def loop_continues(s, p, slope_min, aflux_change=0.0):
                and s["longdy"] < p["yconv_min"] and aflux_change < p["flux_cri"])
     ready = s["t"] > p["trun_min"] and s["accept_count"] > p["count_min"]
     return not (too_long or too_many or (ready and (conv or stalled)))
+
+
+def photo_switch(s, p):
+    """Photo-frequency switch from the initial to the final cadence once
+    longdy and longdydt (after this attempt's update) drop below their
+    thresholds (reference `outer_loop.py:1040-1050`). ``p``: use_photo,
+    photo_switch_longdy, photo_switch_longdydt, final_update_photo_frq."""
+    sw = (bool(p["use_photo"]) and not s["is_final_photo_frq"] and s["longdy"] < p["photo_switch_longdy"]
+          and s["longdydt"] < p["photo_switch_longdydt"])
+    return dict(update_photo_frq=p["final_update_photo_frq"] if sw else s["update_photo_frq"],
+                is_final_photo_frq=bool(s["is_final_photo_frq"] or sw))
+
+
+def photo_due(s, p):
+    """Whether the next attempt runs the photo branch: no retry pending and
+    ``accept_count % update_photo_frq == 0`` (reference `outer_loop.py:716-724`)."""
+    return bool(p["use_photo"]) and s["retry_count"] == 0 and s["accept_count"] % s["update_photo_frq"] == 0

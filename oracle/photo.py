@@ -7,6 +7,7 @@ baseline of ``bench.py``; never by the product path.
 * ``compute_flux``   -> `photo.py:126-245`
 * ``compute_J``      -> `photo.py:309-351` (``_compute_J_inner``)
 * ``update_k_with_J`` -> `photo.py:455-478`
+* ``aflux_change``   -> `outer_loop.py:327-336`
 """
 from __future__ import annotations
 
@@ -148,3 +149,14 @@ def photo_update(y, ymix, dz, k_arr, ph, dflux_u_prev):
     k_new = update_k_with_J(k_arr, J_br, J_br_T, ph["branch_re_idx"], np.ones(nb, bool),
                             ph["branch_T_re_idx"], np.ones(nbT, bool), ph["f_diurnal"])
     return k_new, aflux, dflux_u
+
+
+def aflux_change(aflux_new, aflux_old, flux_atol):
+    """Largest relative change of the actinic flux over the entries above
+    ``flux_atol``; 0 when none is (reference `outer_loop.py:327-336`)."""
+    mask = aflux_new > flux_atol
+    if not mask.any():
+        return 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = np.where(mask, np.abs(aflux_new - aflux_old) / np.maximum(np.abs(aflux_new), 1e-300), 0.0)
+    return float(np.max(ratio))

@@ -121,3 +121,78 @@ def test_loop_converge_rejects_bad_arguments():
                             dummy, None, None)
     assert rc == 1 and b"null" in L.vb_last_error()
     torch.cuda.synchronize()
+
+
+def test_photo_branch_inside_the_loop_matches_oracle_chain():
+    """Ten attempts with photochemistry on (30 species, 10 photolysis
+    branches, nz=12, 1700 bins): the photo cadence (first attempt due, then
+    ``accept_count % update_photo_frq == 0`` with no retry pending), the
+    switch from the initial (3) to the final (2) frequency, the photolysis
+    rows of k, the actinic-flux change and the state, against the oracle
+    chain of the same attempts (photo kernels, body, convergence). The chain
+    accepts, rejects and skips due photo updates behind retries. The
+    actinic-flux change (here ~1e-6, a ratio of differences of fluxes good to
+    ~1e-12) is held to 1e-10 absolute plus 1e-8 relative."""
+    from oracle import contract as oc
+    from oracle import photo as op
+    photo = load_pkg("photo")
+    syn = load_pkg("synthetic")
+    net = syn.make_network(7, 30, 185, n_photo=10)
+    case = syn.make_case(seed=7, net=net, nz=12, mild=True, k_range=(-20.0, -2.0))
+    bins, din12 = syn.make_bins(bin_max=402.0)
+    ph = dict(syn.make_photo(7, net, case.atm["Tco"], bins, din12), f_diurnal=1e-3)
+    tables, atm, dz = net.tables, case.atm, case.extra["dz"]
+    nz, nbin = case.y.shape[0], bins.shape[0]
+    compo = net.compo
+    y0 = case.y
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * (1 + 1e-7)
+    al0 = (np.einsum("zi,ia->a", y0, compo) - atom_ini) / atom_ini
+    ymix0 = y0 / y0.sum(axis=1, keepdims=True)
+    body = dict(loss_eps=0.1, pos_cut=0.0, nega_cut=-1.0, mtol=1e-22, atol=0.1, dt_var_min=0.5, dt_var_max=2.0,
+                dt_min=1e-14, dt_max=1e4, batch_max_retries=8, rtol_min=0.02, rtol_max=1.0,
+                adapt_rtol_dec_period=5, adapt_rtol_inc_period=10, adapt_rtol_dec=0.5, adapt_rtol_inc=1.5,
+                adapt_rtol_loss_mul=10.0, adapt_rtol_inc_loss_thresh=1e-3)
+    cs = loop.ConvStatics(conv_step=4, count_min=10 ** 6, use_photo=True, ini_update_photo_frq=3,
+                          final_update_photo_frq=2, photo_switch_longdy=1e300, photo_switch_longdydt=1e300)
+    p = dict(body, use_adapt_rtol=False, **{f: getattr(cs, f) for f in (
+        "conv_step", "count_min", "count_max", "conv_stall_window", "st_factor", "mtol_conv", "yconv_cri",
+        "yconv_min", "slope_cri", "flux_cri", "trun_min", "runtime", "use_photo", "final_update_photo_frq",
+        "photo_switch_longdy", "photo_switch_longdydt")})
+    dev = photo.PhotoDevice(ph, nz)
+    runner = loop.AdaptiveRunner(chem.to_device(tables), jstep.atm_from_dict(atm), loop.LoopStatics(**body), compo,
+                                 atom_ini, conv=cs, slope_min=1e-8, photo=dev, dz=dz, flux_atol=1.0)
+    state = loop.LoopState(y0[None], ymix0[None], 1e-6, al0[None], rtol=0.05)
+    runner.start(state)
+    k = torch.as_tensor(case.k[None], device="cuda").contiguous()
+
+    s = dict(y=y0, y_prev=y0, ymix=ymix0, dt=1e-6, t=0.0, delta=0.0, accept_count=0, retry_count=0,
+             atom_loss=al0, atom_loss_prev=al0, nega_count=0, loss_count=0, delta_count=0, small_y=0.0, nega_y=0.0,
+             rtol=0.05, loss_criteria=1e-3, longdy=1.0, longdydt=1.0, longdy_seen_min=np.inf,
+             count_since_new_min=0, update_photo_frq=3, is_final_photo_frq=False, aflux_change=0.0)
+    kr, aflux, du = case.k.copy(), np.zeros((nz, nbin)), np.zeros((nz + 1, nbin))
+    ring_y, ring_t = np.zeros((4, nz, tables.ni)), np.zeros(4)
+    due, n_photo = True, 0
+    for a in range(10):
+        assert int(state.photo_due.cpu()[0]) == int(due), a
+        if due:
+            n_photo += 1
+            kr, anew, du = op.photo_update(s["y"], s["ymix"], dz, kr, ph, du)
+            s["aflux_change"] = op.aflux_change(anew, aflux, 1.0)
+            aflux = anew
+        s = oc.attempt(s, kr, atm, tables, compo, atom_ini, p)
+        s.update(oc.conv_update(s, ring_y, ring_t, atm["M"], p, do_accept=s["_accept"] or s["_force"]))
+        s.update(oc.photo_switch(s, p))
+        done = not oc.loop_continues(s, p, 1e-8, s["aflux_change"])
+        due = (not done) and oc.photo_due(s, p)
+        runner.attempt(state, k)
+        sc, cv = state.scalars_host()[0], state.conv_host()[0]
+        assert rel(k[0].cpu().numpy(), kr, 1e-300) <= TOL, a
+        assert abs(cv["aflux_change"] - s["aflux_change"]) <= 1e-10 + TOL * s["aflux_change"], \
+            (a, cv["aflux_change"], s["aflux_change"])
+        for f in ("accept_count", "retry_count", "count_since_new_min", "update_photo_frq"):
+            assert int(sc[f] if f in sc.dtype.names else cv[f]) == int(s[f]), (a, f)
+        assert int(cv["is_final_photo_frq"]) == int(s["is_final_photo_frq"]) and int(cv["done"]) == int(done)
+        assert rel(state.y.cpu().numpy()[0], s["y"], 1e-30) <= TOL, a
+        assert rel(sc["t"], s["t"]) <= TOL and rel(cv["longdy"], s["longdy"]) <= TOL, a
+    assert rel(runner.photo_carry.aflux[0].cpu().numpy(), aflux, 1e-300) <= TOL
+    assert n_photo >= 3

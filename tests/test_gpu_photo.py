@@ -75,3 +75,62 @@ def test_photo_update_config1_size():
     assert rel_bin(aflux.cpu().numpy(), aflux_ref) <= 1e-11
     assert rel_bin(du.cpu().numpy(), du_ref) <= 1e-11
     assert rel(kt.cpu().numpy(), k_ref) <= 1e-11
+
+
+def photo_batch_case(nbin_max=402.0, nz=12):
+    net = syn.make_network(7, 30, 185, n_photo=10)
+    atm, extra = syn.make_atmosphere(7, net, nz=nz)
+    bins, din12 = syn.make_bins(bin_max=nbin_max)
+    ph = syn.make_photo(7, net, atm["Tco"], bins, din12)
+    return net, atm, extra, ph
+
+
+def test_photo_branch_masked_with_aflux_change():
+    """vb_photo_update on three atmospheres with due = [1, 0, 1]: the due
+    ones bit for bit equal to the separate tau / flux / J calls (which read
+    the previous upward flux from another buffer: the in-place update of
+    dflux_u must not change a bit) and against the oracle (tau -> flux -> J ->
+    k rows, aflux change against the aflux held on entry); the other bit for
+    bit untouched. Tolerances as above, except the upward flux: on this grid
+    (12 optically thick layers) a relative change of 4e-16 in y moves dflux_u
+    by 1e-11 of its bin maximum (measured with the oracle), so the 1e-12 of
+    tau allows ~1e-8 there. The aflux change (a ratio of differences of order
+    1e-2 .. 1) within 1e-9 relative."""
+    net, atm, extra, ph = photo_batch_case()
+    nz, nbin = extra["y"].shape[0], ph["bins"].shape[0]
+    rng = np.random.default_rng(3)
+    ys = [extra["y"] * s for s in (1.0, 0.5, 2.0)]
+    ymix = extra["ymix"]
+    k0 = syn.make_rates(7, net, nz)
+    prev = np.abs(rng.normal(0, 1, (3, nz + 1, nbin))) * 1e3
+    dev = photo.PhotoDevice(ph, nz)
+    carry = photo.PhotoCarry(dev, 3, nz, dflux_u=prev)
+    refs = [op.photo_update(ys[b], ymix, extra["dz"], k0, ph, prev[b]) for b in range(3)]
+    old = np.stack([refs[0][1] * (1.0 + 0.05 * rng.standard_normal((nz, nbin))),
+                    np.full((nz, nbin), 7.0), np.zeros((nz, nbin))])
+    carry.aflux.copy_(torch.as_tensor(old))
+    loop = load_pkg("outer_loop")
+    rec = np.zeros(3, loop.CONV_DTYPE)
+    rec["aflux_change"] = [-1.0, 0.25, -1.0]
+    conv = torch.from_numpy(rec.view(np.uint8).copy()).cuda()
+    k = torch.as_tensor(np.stack([k0] * 3), device="cuda").contiguous()
+    due = torch.tensor([1, 0, 1], dtype=torch.int32, device="cuda")
+    y = torch.as_tensor(np.stack(ys), device="cuda")
+    x = torch.as_tensor(np.stack([ymix] * 3), device="cuda")
+    photo.photo_branch(carry, y, x, extra["dz"], k, dev, due=due, flux_atol=1.0, conv=conv)
+    got = conv.cpu().numpy().view(loop.CONV_DTYPE)
+    for b in (0, 2):
+        k1 = torch.as_tensor(k0, device="cuda").clone()
+        a1, du1 = photo.photo_update(ys[b], ymix, extra["dz"], k1, dev, prev[b])
+        assert torch.equal(carry.aflux[b], a1) and torch.equal(carry.dflux_u[b], du1) and torch.equal(k[b], k1)
+        k_ref, a_ref, du_ref = refs[b]
+        assert rel_bin(carry.aflux[b].cpu().numpy(), a_ref) <= 1e-11
+        assert rel_bin(carry.dflux_u[b].cpu().numpy(), du_ref) <= 1e-8
+        assert rel(k[b].cpu().numpy(), k_ref) <= 1e-11
+        want = op.aflux_change(a_ref, old[b], 1.0)
+        assert abs(got["aflux_change"][b] - want) <= 1e-9 * abs(want), (b, got["aflux_change"][b], want)
+    assert got["aflux_change"][2] == 1.0          # from zeros: every entry above flux_atol changed fully
+    assert got["aflux_change"][1] == 0.25
+    assert np.array_equal(carry.aflux[1].cpu().numpy(), old[1])
+    assert np.array_equal(carry.dflux_u[1].cpu().numpy(), prev[1])
+    assert np.array_equal(k[1].cpu().numpy(), k0)
