@@ -322,6 +322,86 @@ def run_config3(args, torch):
             "results": out}
 
 
+def run_config1(args, torch):
+    """The adaptive loop with photochemistry at the config-1 shapes (ni=69,
+    700+700 reactions plus 40 photolysis branches, nz=120, 2500 bins over
+    2-800 nm): every attempt is one Ros2 step, the loop body, the
+    convergence update and, on the reference cadence, the photo branch of
+    the atmospheres that are due, all on the device. Timed for one
+    atmosphere (the latency of an adaptive step) and for a batch of
+    atmospheres with their own initial states, each taking its own accept /
+    reject / photo path. Rate constants are order-scaled (pseudo-first-order
+    1e-12 .. 1e4 /s): with the stiff config-0 constants the reference
+    contract force-accepts at dt_min with the state unchanged."""
+    syn, chem, jstep, loop, photo = pkg("synthetic"), pkg("chem"), pkg("jax_step"), pkg("outer_loop"), pkg("photo")
+    net = syn.make_network(0, 69, 700, n_photo=40)
+    dn = chem.to_device(net.tables)
+    bins, din12 = syn.make_bins()
+    nz = 120
+
+    def setup(B):
+        atms, extras = zip(*[syn.make_atmosphere((b,), net, nz=nz) for b in range(B)])
+        A = {kk: (v if isinstance(v, bool) else np.stack([a[kk] for a in atms])) for kk, v in atms[0].items()}
+        ph = syn.make_photo(0, net, atms[0]["Tco"], bins, din12)       # Tco is the same profile for every seed
+        K = np.stack([syn.make_rates((b,), net, nz, -12.0, 4.0, n_ref=float(e["n"].max()))
+                      for b, e in enumerate(extras)])
+        y0 = np.stack([e["y"] for e in extras])
+        atom_ini = np.einsum("bzi,ia->ba", y0, net.compo)
+        sm = np.concatenate([loop.slope_min_of(a["Kzz"], e["Hp"]) for a, e in zip(atms, extras)])
+        runner = loop.AdaptiveRunner(dn, jstep.atm_from_dict(A), loop.LoopStatics(dt_max=1e17), net.compo, atom_ini,
+                                     batch=B, conv=loop.ConvStatics(use_photo=True), slope_min=sm,
+                                     photo=photo.PhotoDevice(ph, nz), dz=np.stack([e["dz"] for e in extras]),
+                                     flux_atol=1.0)
+        state = loop.LoopState(y0, np.stack([e["ymix"] for e in extras]), 1e-10, np.zeros_like(atom_ini), rtol=0.2)
+        runner.start(state)
+        return runner, state, torch.as_tensor(K, device="cuda").contiguous()
+
+    def timed(B, attempts):
+        runner, state, k = setup(B)
+        for _ in range(args.warmup):
+            runner.attempt(state, k)
+        torch.cuda.synchronize()
+        n_photo = torch.zeros((), dtype=torch.int64, device="cuda")
+        acc0 = state.scalars_host()["accept_count"].sum()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(attempts):
+            n_photo += state.photo_due.sum()
+            runner.attempt(state, k)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        # the photo branch alone with every atmosphere due
+        due = torch.ones(B, dtype=torch.int32, device="cuda")
+        e0.record()
+        for _ in range(5):
+            photo.photo_branch(runner.photo_carry, state.y, state.ymix, runner.dz, k.clone(), runner.photo, due=due,
+                               flux_atol=1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        sc = state.scalars_host()
+        return {"batch": B, "attempts": attempts, "ms_per_attempt": ms / attempts,
+                "value": B * attempts / (ms * 1e-3), "accepted": int(sc["accept_count"].sum() - acc0),
+                "photo_updates": int(n_photo.item()), "photo_branch_ms_all_due": e0.elapsed_time(e1) / 5,
+                "max_abs_atom_loss": float(np.abs(state.atom_loss.cpu().numpy()).max())}
+
+    B = args.batch or torch.cuda.get_device_properties(0).multi_processor_count
+    single = timed(1, max(args.steps, 50))
+    clocks = ClockSampler(0)
+    clocks.start()
+    batched = timed(B, args.steps)
+    clk = clocks.stop()
+    return {"metric": "adaptive-loop attempts/s (Ros2 step + body + convergence + photo on cadence)",
+            "value": batched["value"], "unit": "atmosphere-attempts/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": batched["ms_per_attempt"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded config-1 shapes; order-scaled k)",
+            "config": {"workload": f"adaptive loop with photochemistry, {B} atmospheres of ni=69, nz=120, "
+                                   f"2500 bins, 40 branches", "l2": "state larger than L2 at this batch, no flush"},
+            "batched": batched, "single_atmosphere": single,
+            "gpu_launches_per_attempt": "7 (step) + 1 (body) + 1 (convergence) + 3 (photo)", "clocks": clk}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,8 +411,9 @@ def main():
                     help="atmospheres per GPU (default: two per SM, 296 on a B200)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config0", choices=["config0", "config2", "config3"],
-                    help="config0: the headline batch (default); config2: the uneven multi-network batch; "
+    ap.add_argument("--workload", default="config0", choices=["config0", "config1", "config2", "config3"],
+                    help="config0: the headline batch (default); config1: the adaptive loop with "
+                         "photochemistry; config2: the uneven multi-network batch; "
                          "config3: the mixed-precision block solve against FP64")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -351,9 +432,9 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    if args.workload in ("config2", "config3"):
+    if args.workload in ("config1", "config2", "config3"):
         if rank == 0:
-            run = run_config2 if args.workload == "config2" else run_config3
+            run = {"config1": run_config1, "config2": run_config2, "config3": run_config3}[args.workload]
             print(json.dumps(run(args, torch)), flush=True)
         return
     _lib = pkg("_lib")

@@ -81,8 +81,8 @@ class ConvStatics:
     use_photo: bool = False
     ini_update_photo_frq: int = 100
     final_update_photo_frq: int = 5
-    photo_switch_longdy: float = 0.0
-    photo_switch_longdydt: float = 0.0
+    photo_switch_longdy: float = 1.0      # yconv_min * 10
+    photo_switch_longdydt: float = 1e-6
 
     def params(self) -> VbConvParams:
         p = VbConvParams()

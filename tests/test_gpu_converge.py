@@ -196,3 +196,49 @@ def test_photo_branch_inside_the_loop_matches_oracle_chain():
         assert rel(sc["t"], s["t"]) <= TOL and rel(cv["longdy"], s["longdy"]) <= TOL, a
     assert rel(runner.photo_carry.aflux[0].cpu().numpy(), aflux, 1e-300) <= TOL
     assert n_photo >= 3
+
+
+def test_loop_reaches_the_known_steady_state():
+    """The open chain 0 -> A -> B -> 0 of the reference's steady-state tests
+    (k1=1, k3=0.5, k5=0.3, four layers, eddy and molecular diffusion): the
+    device loop (step, body, convergence) runs from a uniform 1:1 state until
+    its own loop condition stops it, and the state it stops at is the
+    reference's Newton steady state (``tests/golden/adjoint.npz``; close to
+    the well-mixed [A] = k1/k3 = 2, [B] = k1/k5 = 10/3, with boundary layers
+    off by ~0.4 %). The body rescales every accepted state to n_0 * ymix, so
+    the layer densities n_0 = M are set to the steady state's layer totals:
+    M enters only three-body chemistry (none here), so this leaves the steady
+    state unchanged and makes it a fixed point of the loop. Stopping rule:
+    longdy < 1e-7 with longdydt < 1e-9 over the lookback window, so the
+    stopped state is within 1e-5 of the steady state."""
+    g = golden("adjoint.npz")
+    NT = load_pkg("network").NetworkTables
+    net = NT(species=("A", "B"), ni=2, nr=6, reactant_idx=g["chain_r_idx"], product_idx=g["chain_p_idx"],
+             reactant_stoich=g["chain_r_st"], product_stoich=g["chain_p_st"], is_three_body=g["chain_three"],
+             is_photo=np.zeros(7, bool))
+    nz, ni = 4, 2
+    n0 = g["chain_y"].sum(axis=1)
+    atm = dict(Kzz=np.full(nz - 1, 1e-2), Dzz=np.full((nz - 1, ni), 1e-3), dzi=np.full(nz - 1, 1.0),
+               vz=np.zeros(nz - 1), Hpi=np.full(nz - 1, 1.0), Ti=np.full(nz - 1, 1500.0), Tco=np.full(nz, 1500.0),
+               g=np.full(nz, 1.0), ms=np.full(ni, 1.0), alpha=np.zeros(ni), M=n0.copy(),
+               vm=np.zeros((nz, ni)), vs=np.zeros((nz - 1, ni)), top_flux=np.zeros(ni), bot_flux=np.zeros(ni),
+               bot_vdep=np.zeros(ni), gas_indx_mask=np.ones(ni, dtype=bool), use_vm_mol=False,
+               use_settling=False, use_topflux=False, use_botflux=False)
+    k = np.zeros((1, 7, nz))
+    k[0, 1], k[0, 3], k[0, 5] = 1.0, 0.5, 0.3
+    y0 = np.repeat((n0 / 2.0)[None, :, None], ni, axis=2)
+    compo = np.ones((ni, 1))
+    atom_ini = y0[0].sum(axis=0) @ compo
+    statics = loop.LoopStatics(loss_eps=1e30, dt_max=1e3)      # open chain: atoms are not conserved
+    conv = loop.ConvStatics(conv_step=50, count_min=100, yconv_cri=1e-7, slope_cri=1e-9, yconv_min=1e-7,
+                            trun_min=1.0, runtime=1e12, count_max=20000)
+    runner = loop.AdaptiveRunner(chem.to_device(net), jstep.atm_from_dict(atm), statics, compo, atom_ini,
+                                 conv=conv, slope_min=1e-10)
+    state = loop.LoopState(y0, np.full_like(y0, 0.5), 1e-3, np.zeros((1, 1)), rtol=0.05)
+    n = runner.run_to_convergence(state, k, max_attempts=20000, check_every=100)
+    sc, cv = state.scalars_host()[0], state.conv_host()[0]
+    assert cv["done"] == 1 and sc["accept_count"] < 20000 and sc["t"] < 1e12, (n, sc, cv)
+    assert cv["longdy"] < 1e-7 and cv["longdydt"] < 1e-9      # stopped by convergence, not by a cap
+    y = state.y.cpu().numpy()[0]
+    assert rel(y, g["chain_y"]) <= 1e-5, (y, g["chain_y"])
+    assert rel(y[:, 0], np.full(nz, 2.0)) <= 1e-2 and rel(y[:, 1], np.full(nz, 10.0 / 3.0)) <= 1e-2
