@@ -305,6 +305,40 @@ int vb_photo_update(int batch, int nz, int ni, int nr, const VbPhoto* photo, con
                     double* dflux_d, double* dflux_u, double* J_br, double* J_br_T, double* k, double flux_atol,
                     VbConvState* conv, void* stream);
 
+/* Rate constants on the device (reference rates.py:61-208 and gibbs.py:41-150):
+ * per layer, the forward constant of every forward row (modified Arrhenius
+ * a T^n exp(-E/T); Lindemann k0 / (1 + k0 M / k_inf); the hardcoded Troe of
+ * OH + CH3 + M -> CH3OH + M), the low-temperature caps, the reverse constant
+ * k_f / K_eq with K_eq = exp(sum st g(reactants) - sum st g(products))
+ * (k_B T / 1e6)^(dn) from NASA-9 g/RT, and the removal of listed rows.
+ * code[i] of forward row i (odd): VB_RK_* kind | cap << 2 | VB_RC_* bits. */
+#define VB_RK_NONE 0          /* left at zero (photo, ion, condensation, radiative, ...) */
+#define VB_RK_ARRHENIUS 1
+#define VB_RK_LINDEMANN 2
+#define VB_RK_TROE_OH_CH3 3
+#define VB_RCAP_CH3 1         /* H + CH3 + M -> CH4 + M, T <= 277.5 K */
+#define VB_RCAP_C2H4 2        /* H + C2H4 + M -> C2H5 + M, T <= 300 K */
+#define VB_RCAP_C2H5 3        /* H + C2H5 + M -> C2H6 + M, T <= 200 K */
+#define VB_RC_THERMAL 16      /* K_eq from the Gibbs energies (else K_eq = 1) */
+#define VB_RC_REVERSE 32      /* row i+1 is a reverse row (i+1 < stop_rev_indx); else it stays zero */
+#define VB_RC_DROP_FWD 64     /* row i is removed (zeroed after the reverse fill) */
+#define VB_RC_DROP_REV 128    /* row i+1 is removed */
+#define VB_RATES_LOWT_CAPS 1  /* apply the low-temperature caps */
+typedef struct VbRateTables {
+  int32_t nr, ni, max_terms, reserved;
+  const int32_t* code;        /* [nr+1] (forward rows used) */
+  const double* par;          /* [nr+1][6]: a, n, E, a_inf, n_inf, E_inf */
+  const double* nasa9;        /* [ni][2][10]: low-T (T < 1000 K) and high-T coefficients */
+  const int32_t* r_idx;       /* [nr+1][max_terms] reactant species, padding ni */
+  const int32_t* p_idx;       /* [nr+1][max_terms] product species, padding ni */
+  const double* r_st;         /* [nr+1][max_terms] */
+  const double* p_st;         /* [nr+1][max_terms] */
+} VbRateTables;
+/* T, M [B][nz] -> k [B][nr+1][nz] (row 0 zero); dkdT (nullable, same layout)
+ * = dk/dT at fixed M, by dual numbers through the same formulas. */
+int vb_rates(int batch, int nz, const VbRateTables* tables, const double* T, const double* M, int32_t flags,
+             double* k, double* dkdT, void* stream);
+
 /* Profiling: while enabled, every kernel launch of vb_ros2_step is bracketed
  * by CUDA events recorded on the launching stream (launch sites:
  * 0 stage-1 assembly, 1 factor, 2 back sweep 1, 3 stage-2 assembly,

@@ -28,6 +28,7 @@ UNITS = {
     "vb_adjoint.cu": [],
     "vb_control.cu": ["--fmad=false"],
     "vb_mixed.cu": [],
+    "vb_rates.cu": ["--fmad=false"],
 }
 
 

@@ -547,6 +547,19 @@ int vb_profile_read(double* ms, int64_t* counts, int n) {
   return VB_OK;
 }
 
+int vb_rates(int batch, int nz, const VbRateTables* tables, const double* T, const double* M, int32_t flags,
+             double* k, double* dkdT, void* stream) {
+  if (!tables || !T || !M || !k) return fail(VB_ERR_ARG, "null argument");
+  const VbRateTables& t = *tables;
+  if (!t.code || !t.par || !t.nasa9 || !t.r_idx || !t.p_idx || !t.r_st || !t.p_st)
+    return fail(VB_ERR_ARG, "null rate table");
+  if (batch < 1 || batch > 65535 || nz < 1 || t.nr < 2 || (t.nr & 1) || t.nr / 2 > 65535 || t.ni < 1 ||
+      t.max_terms < 1)
+    return fail(VB_ERR_ARG, "bad shape: batch in [1, 65535], nz >= 1, nr even in [2, 131070], ni >= 1");
+  VB_CHECK(vb::launch_rates(batch, nz, t, T, M, flags, k, dkdT, (cudaStream_t)stream), "rates");
+  return VB_OK;
+}
+
 int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream) {
   if (!out || blocks < 1 || threads < 32 || iters < 1) return fail(VB_ERR_ARG, "bad probe arguments");
   VB_CHECK(vb::launch_fp64_probe(out, blocks, threads, iters, (cudaStream_t)stream), "fp64 probe");

@@ -52,6 +52,8 @@ cudaError_t launch_photo_flux(int batch, int nz, int ni, const VbPhoto& P, const
                               const int32_t* due, double flux_atol, double* achg, cudaStream_t);
 cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const double* aflux, double* J_br,
                            double* J_br_T, double* k, const int32_t* due, cudaStream_t);
+cudaError_t launch_rates(int batch, int nz, const VbRateTables& t, const double* T, const double* M, int flags,
+                         double* k, double* dkdT, cudaStream_t st);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
 template <typename R>
 cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,

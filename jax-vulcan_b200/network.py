@@ -16,7 +16,13 @@ stoichiometry tables as the reference parser (`network.py:197-491`):
 * `M` is dropped from the slots and recorded per direction as a three-body flag
   (`:286-291`, `:424-425`);
 * unused slots hold the padding index ``ni`` with stoichiometry 0 (`:377-385`);
-* species are numbered by first appearance in the file (`:223-229`).
+* species are numbered by first appearance in the file (`:223-229`);
+* the leading numeric columns give the rate parameters: ``a n E`` in the
+  two-body and both three-body sections, plus ``a_inf n_inf E_inf`` in the
+  three-body section with high-pressure rates (`:444-451`); every row of a
+  section carries its flag (`:427-443`); ``stop_rev_indx`` is the row of the
+  `# reverse stops` marker, else the first photo row, else ``nr + 1``
+  (`:252-253`, `:353-356`).
 
 Config-named extra species (reference `network.py:157-194`) are not appended:
 the synthetic networks name every species in their reactions.
@@ -59,6 +65,21 @@ class NetworkTables:
     is_photo: np.ndarray         # bool [nr+1]
     pho_rate_index: dict = field(default_factory=dict)  # (species, branch) -> row
     photo_sp: tuple = ()
+    # rate parameters and section flags ([nr+1]; None for tables built by hand)
+    a: np.ndarray = None
+    n: np.ndarray = None
+    E: np.ndarray = None
+    a_inf: np.ndarray = None
+    n_inf: np.ndarray = None
+    E_inf: np.ndarray = None
+    is_forward: np.ndarray = None
+    has_kinf: np.ndarray = None
+    is_special: np.ndarray = None
+    is_conden: np.ndarray = None
+    is_radiative: np.ndarray = None
+    is_ion: np.ndarray = None
+    stop_rev_indx: int = 0
+    Rf: dict = field(default_factory=dict)              # forward row -> "A + B -> C + D"
 
     @property
     def max_terms(self) -> int:
@@ -113,12 +134,19 @@ def parse_network_text(text: str) -> NetworkTables:
             order.append(sp)
 
     row = 1
+    stop_rev = None
+    photo_row = None
     for raw in text.splitlines():
         if not raw.strip():
             continue
         sec = _section_of(raw)
         if sec is not None:
             section = sec
+            if sec == PHOTO and photo_row is None:
+                photo_row = row
+            continue
+        if raw.lstrip().startswith("# reverse stops"):
+            stop_rev = row
             continue
         if raw.lstrip().startswith("#"):
             continue
@@ -142,9 +170,15 @@ def parse_network_text(text: str) -> NetworkTables:
             return acc
 
         cols = tail.split()
+        nums = []
+        for c in cols:
+            try:
+                nums.append(float(c))
+            except ValueError:
+                break
         rec = dict(row=row, section=section, reac=collapse(reac), prod=collapse(prod),
                    m_reac=any(sp == "M" for _, sp in reac),
-                   m_prod=any(sp == "M" for _, sp in prod))
+                   m_prod=any(sp == "M" for _, sp in prod), eq=eq, nums=nums)
         records.append(rec)
         if section == PHOTO:
             target = cols[0] if cols else eq.split()[0]
@@ -163,6 +197,12 @@ def parse_network_text(text: str) -> NetworkTables:
     p_st = np.zeros((nr + 1, T), dtype=np.float64)
     three = np.zeros(nr + 1, dtype=bool)
     photo = np.zeros(nr + 1, dtype=bool)
+    par = {f: np.zeros(nr + 1) for f in ("a", "n", "E", "a_inf", "n_inf", "E_inf")}
+    flag = {f: np.zeros(nr + 1, dtype=bool) for f in ("is_forward", "has_kinf", "is_special", "is_conden",
+                                                      "is_radiative", "is_ion")}
+    sec_flag = {THREE_BODY_KINF: "has_kinf", SPECIAL: "is_special", CONDEN: "is_conden",
+                RADIATIVE: "is_radiative"}
+    Rf = {}
     for rec in records:
         i = rec["row"]
         for s, (sp, st) in enumerate(rec["reac"].items()):
@@ -173,11 +213,27 @@ def parse_network_text(text: str) -> NetworkTables:
             r_idx[i + 1, s], r_st[i + 1, s] = sp, st
         three[i] = rec["m_reac"]
         three[i + 1] = rec["m_prod"]
-        photo[i] = rec["section"] == PHOTO
+        sec = rec["section"]
+        photo[i] = sec == PHOTO
+        flag["is_forward"][i] = True
+        if sec in sec_flag:
+            flag[sec_flag[sec]][i] = flag[sec_flag[sec]][i + 1] = True
+        if sec == ION:
+            flag["is_ion"][i] = True
+        cols = rec["nums"]
+        if sec in (TWO_BODY, THREE_BODY_KINF, THREE_BODY_NO_KINF):
+            if len(cols) >= 3:
+                par["a"][i], par["n"][i], par["E"][i] = cols[0], cols[1], cols[2]
+            if sec == THREE_BODY_KINF and len(cols) >= 6:
+                par["a_inf"][i], par["n_inf"][i], par["E_inf"][i] = cols[3], cols[4], cols[5]
+        Rf[i] = rec["eq"]
+    if stop_rev is None:
+        stop_rev = photo_row if photo_row is not None else nr + 1
     return NetworkTables(species=tuple(order), ni=ni, nr=nr, reactant_idx=r_idx,
                          product_idx=p_idx, reactant_stoich=r_st, product_stoich=p_st,
                          is_three_body=three, is_photo=photo,
-                         pho_rate_index=pho_rate_index, photo_sp=tuple(photo_sp))
+                         pho_rate_index=pho_rate_index, photo_sp=tuple(photo_sp),
+                         stop_rev_indx=int(stop_rev), Rf=Rf, **par, **flag)
 
 
 def parse_network(path) -> NetworkTables:

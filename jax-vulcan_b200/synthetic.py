@@ -471,3 +471,90 @@ def make_photo(seed, net: SyntheticNetwork, Tco, bins, din12, dbin1=0.125, dbin2
         bins=bins, sflux_top=sflux_top, mu_zenith=float(np.cos(48.0 / 180.0 * 3.14159)),
         edd=0.5, ag0=0.0, hc=hc, f_diurnal=1.0,
     )
+
+
+def _eq_of(tables, row):
+    """Reaction text of a parsed row (reactants -> products, M restored)."""
+    sp = tables.species
+
+    def side(idx, st, m):
+        terms = [(sp[i] if s == 1 else f"{int(s)}*{sp[i]}") for i, s in zip(idx, st) if s > 0]
+        return " + ".join(terms + (["M"] if m else []))
+
+    m = bool(tables.is_three_body[row])
+    return f"{side(tables.reactant_idx[row], tables.reactant_stoich[row], m)} -> " \
+           f"{side(tables.product_idx[row], tables.product_stoich[row], m)}"
+
+
+def make_rate_network(seed=0, ni=30, n_fwd=120, n_kinf=24, n_nokinf=12, n_photo=6) -> str:
+    """Network text exercising every rate form of the rate build: two-body
+    modified Arrhenius (``a n E``), three-body with high-pressure rates
+    (Lindemann, ``a n E a_inf n_inf E_inf``), three-body without, the three
+    low-temperature-cap reactions (reference `rates.py:30-33`), the special
+    ``OH + CH3 + M -> CH3OH + M`` (hardcoded Troe), `# reverse stops` and a
+    photo section. Reactions come from a seeded balanced network; parameters
+    are seeded log-uniform / uniform draws written with 4 significant digits."""
+    rng = _rng(seed, 17)
+    base = make_network(seed, ni, n_fwd, n_photo=n_photo)
+    t = base.tables
+    rows = [r for r in range(1, t.nr + 1, 2) if not t.is_photo[r]]
+    n2 = len(rows) - n_kinf - n_nokinf
+    lines = ["# rate-build test network (written by jax-vulcan_b200.synthetic)", "# Two-body Reactions"]
+    fid = 1
+
+    def put(eq, cols):
+        nonlocal fid
+        lines.append(f"{fid:5d} [ {eq} ]  " + "  ".join(cols))
+        fid += 2
+
+    def e(x):
+        return f"{x:.3E}"
+
+    for r in rows[:n2]:
+        put(_eq_of(t, r), [e(10 ** rng.uniform(-14, -9)), f"{rng.uniform(-2, 2):.3f}",
+                           f"{rng.uniform(-300, 20000):.1f}"])
+    lines.append("# 3-body and Disscoiation Reactions")
+    for r in rows[n2:n2 + n_kinf]:
+        eq = _eq_of(t, r)
+        if " + M" not in eq:
+            lhs, rhs = eq.split(" -> ")
+            eq = f"{lhs} + M -> {rhs} + M"
+        put(eq, [e(10 ** rng.uniform(-33, -26)), f"{rng.uniform(-4, 1):.3f}", f"{rng.uniform(0, 5000):.1f}",
+                 e(10 ** rng.uniform(-12, -9)), f"{rng.uniform(-1, 1):.3f}", f"{rng.uniform(0, 3000):.1f}"])
+    for eq in ("H + CH3 + M -> CH4 + M", "H + C2H4 + M -> C2H5 + M", "H + C2H5 + M -> C2H6 + M"):
+        put(eq, [e(10 ** rng.uniform(-30, -24)), f"{rng.uniform(-3, 0):.3f}", f"{rng.uniform(0, 700):.1f}",
+                 e(10 ** rng.uniform(-11, -9)), f"{rng.uniform(-0.5, 1.5):.3f}", f"{rng.uniform(0, 600):.1f}"])
+    lines.append("# 3-body reactions without high-pressure rates")
+    for r in rows[n2 + n_kinf:]:
+        eq = _eq_of(t, r)
+        if " + M" not in eq:
+            lhs, rhs = eq.split(" -> ")
+            eq = f"{lhs} + M -> {rhs} + M"
+        put(eq, [e(10 ** rng.uniform(-34, -28)), f"{rng.uniform(-3, 0):.3f}", f"{rng.uniform(0, 1000):.1f}"])
+    lines.append("# special cases")
+    put("OH + CH3 + M -> CH3OH + M", [])
+    lines.append("# reverse stops")
+    lines.append("# photo disscoiation (no reversals)")
+    for sp, br, row in base.photo_branches:
+        put(_eq_of(t, row), [sp, str(br)])
+    return "\n".join(lines) + "\n"
+
+
+def make_nasa9(seed, ni):
+    """Seeded NASA-9 coefficients [ni, 2, 10] (low-T and high-T branches,
+    reference `gibbs.py:16-38` layout): magnitudes of real species' fits,
+    with the enthalpy constant a8 within +-1e4 K so that g/RT stays within
+    a few hundred down to 150 K."""
+    rng = _rng(seed, 19)
+    c = np.zeros((ni, 2, 10))
+    for j in range(2):
+        c[:, j, 0] = rng.uniform(-5e4, 5e4, ni)
+        c[:, j, 1] = rng.uniform(-500.0, 500.0, ni)
+        c[:, j, 2] = rng.uniform(2.0, 6.0, ni)
+        c[:, j, 3] = rng.uniform(-5e-3, 5e-3, ni)
+        c[:, j, 4] = rng.uniform(-5e-6, 5e-6, ni)
+        c[:, j, 5] = rng.uniform(-3e-9, 3e-9, ni)
+        c[:, j, 6] = rng.uniform(-5e-13, 5e-13, ni)
+        c[:, j, 8] = rng.uniform(-1e4, 1e4, ni)
+        c[:, j, 9] = rng.uniform(-10.0, 20.0, ni)
+    return c

@@ -6,7 +6,8 @@ Run in the build container (the reference sources are not on the GPU box):
 
 JAX is not installed, so the unmodified reference modules (`network.py`,
 `chem.py`, `solver.py`, `jax_step.py`, `photo.py`, `integrate.py`,
-`steady_state_grad.py`, and the caller-contract functions of `outer_loop.py`)
+`steady_state_grad.py`, `rates.py`, `gibbs.py`, and the caller-contract
+functions of `outer_loop.py`)
 are imported with ``_jax_numpy_shim`` standing in for ``jax``. A stub
 ``vulcan_cfg`` with no species lists is installed first so the reference
 parser does not append config-named species (reference `network.py:157-194`).
@@ -477,6 +478,43 @@ def adjoint_fixture(mods, syn):
     print("adjoint: ok, chain Newton iterations", it)
 
 
+RATE_T = np.array([150.0, 180.0, 199.99, 200.0, 250.0, 277.5, 277.6, 300.0, 300.1, 420.0, 650.0, 800.0,
+                   999.9, 1000.0, 1000.1, 1300.0, 1700.0, 2100.0, 2600.0, 3000.0])
+
+
+def rates_fixture(mods, syn):
+    """Reference rates.py / gibbs.py (plain NumPy, imported unmodified) on a
+    seeded network with every rate form and seeded NASA-9 coefficients:
+    forward constants, low-T caps, g/RT, K_eq, reverse fill, removal, the
+    end-to-end build_rate_array, and the parser's rate columns and flags."""
+    rates, gibbs = importlib.import_module("rates"), importlib.import_module("gibbs")
+    text = syn.make_rate_network(0)
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(text)
+        path = f.name
+    rn = mods["network"].parse_network(path)
+    os.unlink(path)
+    coeffs = syn.make_nasa9(0, rn.ni)
+    T = RATE_T
+    M = 10.0 ** np.linspace(19.0, 10.0, T.shape[0])
+    remove = [3, 8, 101, 250]
+    k_fwd = rates.compute_forward_k(rn, T, M)
+    k_caps = rates.apply_lowT_caps(rn, k_fwd, T, M)
+    g = gibbs.gibbs_sp_vector(coeffs, T)
+    K = gibbs.K_eq_array(rn, g, T)
+    k_nocap = gibbs.fill_reverse_k(rn, k_fwd, K, remove_list=None)
+    cfg = types.SimpleNamespace(use_lowT_limit_rates=True, remove_list=remove)
+    atm = types.SimpleNamespace(Tco=T, M=M)
+    k_all = rates.build_rate_array(cfg, rn, atm, coeffs)
+    out = dict(net_text=np.array(text), coeffs=coeffs, T=T, M=M, remove=np.array(remove), k_fwd=k_fwd,
+               k_caps=k_caps, g=g, K=K, k_nocap=k_nocap, k_all=k_all, stop_rev_indx=np.array(rn.stop_rev_indx))
+    for f in ("a", "n", "E", "a_inf", "n_inf", "E_inf", "is_forward", "has_kinf", "is_special", "is_conden",
+              "is_radiative", "is_photo", "is_ion"):
+        out["net_" + f] = np.asarray(getattr(rn, f))
+    np.savez_compressed(os.path.join(HERE, "rates.npz"), **out)
+    print("rates: ok", k_all.shape, "nonzero", int((k_all != 0).sum()))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE", "/root/reference"))
@@ -489,8 +527,10 @@ def main():
         for name in sorted(only):
             if name == "body":
                 body_fixture(mods, syn, args.reference, shim)
+            elif name == "rates":
+                rates_fixture(mods, syn)
             else:
-                raise SystemExit(f"--only supports: body (got {name})")
+                raise SystemExit(f"--only supports: body, rates (got {name})")
         return
     mild = dict(mild=True, k_range=(-40.0, 4.0))
     step_fixture(mods, "plain", syn.make_case(seed=5, ni=12, n_fwd=30, nz=10, **mild), n_steps=3)
@@ -511,6 +551,7 @@ def main():
     photo_fixture(mods, syn)
     adjoint_fixture(mods, syn)
     body_fixture(mods, syn, args.reference, shim)
+    rates_fixture(mods, syn)
 
 
 if __name__ == "__main__":

@@ -252,3 +252,40 @@ def k_gradient_scale(y, M, lam, net):
     s = (np.abs(net.product_stoich)[None] * lp[:, net.product_idx]).sum(2) + \
         (np.abs(net.reactant_stoich)[None] * lp[:, net.reactant_idx]).sum(2)
     return (np.abs(Pp) * s).T
+
+
+def _rates_case():
+    g = golden("rates.npz")
+    net = load_pkg("network").parse_network_text(str(g["net_text"]))
+    return g, net
+
+
+def test_rate_build_matches_reference():
+    """Reference rates.py / gibbs.py (tests/golden/rates.npz): this package's
+    parser reads the same rate columns and flags, and the oracle reproduces
+    every stage bit for bit; its complex-step dk/dT agrees with central
+    differences (h = 1e-4 K) to their truncation error, away from the
+    branch switches at 200, 277.5, 300 and 1000 K."""
+    from oracle import rates as orr
+    g, net = _rates_case()
+    for f in ("a", "n", "E", "a_inf", "n_inf", "E_inf", "is_forward", "has_kinf", "is_special", "is_conden",
+              "is_radiative", "is_photo", "is_ion"):
+        np.testing.assert_array_equal(getattr(net, f), g["net_" + f], err_msg=f)
+    assert net.stop_rev_indx == int(g["stop_rev_indx"])
+    T, M, c, rm = g["T"], g["M"], g["coeffs"], list(g["remove"])
+    kf = orr.compute_forward_k(net, T, M)
+    np.testing.assert_array_equal(kf, g["k_fwd"])
+    np.testing.assert_array_equal(orr.apply_lowT_caps(net, kf, T, M), g["k_caps"])
+    gs = orr.gibbs_sp_vector(c, T)
+    np.testing.assert_array_equal(gs, g["g"])
+    K = orr.K_eq_array(net, gs, T)
+    np.testing.assert_array_equal(K, g["K"])
+    np.testing.assert_array_equal(orr.fill_reverse_k(net, kf, K), g["k_nocap"])
+    k = orr.build_rate_array(net, c, T, M, lowT_caps=True, remove_list=rm)
+    np.testing.assert_array_equal(k, g["k_all"])
+    d = orr.dk_dT(net, c, T, M, lowT_caps=True, remove_list=rm)
+    h = 1e-4
+    fd = (orr.build_rate_array(net, c, T + h, M, True, rm) - orr.build_rate_array(net, c, T - h, M, True, rm)) / (2 * h)
+    ok = np.all([np.abs(T - t) > 1e-3 for t in (200.0, 277.5, 300.0, 1000.0)], axis=0)
+    scale = np.maximum(np.abs(fd[:, ok]), 1e-12 * np.abs(k[:, ok]) + 1e-300)
+    assert np.max(np.abs(d[:, ok] - fd[:, ok]) / scale) < 1e-4
