@@ -402,6 +402,80 @@ def run_config1(args, torch):
             "gpu_launches_per_attempt": "7 (step) + 1 (body) + 1 (convergence) + 3 (photo)", "clocks": clk}
 
 
+def run_config4(args, torch):
+    """The implicit steady-state adjoint, batched: for B atmospheres of the
+    config-1 shape (ni=69, 700+700 Arrhenius / Lindemann reactions with NASA-9
+    reverse rates plus 40 photolysis rows, nz=120, molecular diffusion and
+    boundary fluxes on), the loss sum of seeded weights times log ymix at 10
+    layers, and its gradient with respect to log k, T (through the rate
+    constants, Tco and Ti), log Kzz and the boundary fluxes: one rate build
+    with dk/dT, the block factor + transposed solve + VJP kernels, the
+    transport-leaf VJP and the composition, per batch."""
+    from types import SimpleNamespace
+    syn, chem, jstep, ssg, rates, network = (pkg("synthetic"), pkg("chem"), pkg("jax_step"),
+                                             pkg("steady_state_grad"), pkg("rates"), pkg("network"))
+    net = network.parse_network_text(syn.make_rate_network(0, ni=69, n_fwd=700, n_kinf=60, n_nokinf=20, n_photo=40,
+                                                           special=False))
+    coeffs = syn.make_nasa9(0, net.ni)
+    dn = chem.to_device(net)
+    rt = rates.RateTables(net, coeffs)
+    ms = np.random.default_rng(0).uniform(2.0, 60.0, net.ni)
+    layers = np.random.default_rng(1).choice(120, 10, replace=False)
+
+    def setup(B):
+        atms, extras = zip(*[syn.make_atmosphere((b,), SimpleNamespace(tables=net, ms=ms), nz=120, moldiff=True,
+                                                 fluxes=True) for b in range(B)])
+        A = {kk: (v if isinstance(v, bool) else np.stack([a[kk] for a in atms])) for kk, v in atms[0].items()}
+        y = torch.as_tensor(np.stack([e["y"] for e in extras]), device="cuda")
+        w = torch.as_tensor(np.random.default_rng(2).normal(0.0, 1.0, (B, 10, net.ni)), device="cuda")
+        return jstep.atm_from_dict(A), A, y, w
+
+    def gradient(atm, A, y, w):
+        T = torch.as_tensor(A["Tco"], device="cuda")
+        M = torch.as_tensor(A["M"], device="cuda")
+        k, dkdT = rt(T, M, with_dkdT=True)
+        yv = y.clone().requires_grad_(True)
+        ymix = yv[:, layers] / yv[:, layers].sum(dim=2, keepdim=True)
+        (v,) = torch.autograd.grad((w * torch.log(ymix)).sum(), [yv])
+        cot = ssg.implicit_cotangents(y, k, atm, dn, v)
+        return dict(log_k=cot["k_arr"] * k, T=ssg.temperature_cotangent(cot, dkdT),
+                    log_Kzz=cot["Kzz"] * torch.as_tensor(A["Kzz"], device="cuda"),
+                    top_flux=cot["top_flux"], bot_flux=cot["bot_flux"], bot_vdep=cot["bot_vdep"],
+                    status=cot["status"])
+
+    def timed(B, reps):
+        atm, A, y, w = setup(B)
+        for _ in range(args.warmup):
+            g = gradient(atm, A, y, w)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            g = gradient(atm, A, y, w)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_ = e0.elapsed_time(e1) / reps
+        finite = all(bool(torch.isfinite(v).all()) for kk, v in g.items() if kk != "status")
+        return {"batch": B, "ms_per_batch_gradient": ms_, "value": B / (ms_ * 1e-3), "finite": finite,
+                "nonzero_status": int((g["status"] != 0).sum())}
+
+    B = args.batch or 64
+    reps = max(3, min(args.steps, 20))
+    single = timed(1, reps)
+    clocks = ClockSampler(0)
+    clocks.start()
+    batched = timed(B, reps)
+    clk = clocks.stop()
+    return {"metric": "implicit steady-state gradients/s (log k, T, log Kzz, boundary fluxes)",
+            "value": batched["value"], "unit": "atmosphere-gradients/s", "n_gpus": 1, "steps": reps,
+            "warmup": args.warmup, "ms_per_step": batched["ms_per_batch_gradient"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded config-1 shapes, rates from NASA-9; states not converged)",
+            "config": {"workload": f"adjoint of {B} atmospheres, ni={net.ni}, nr={net.nr}, nz=120, loss over 10 "
+                                   f"layers", "l2": "per-batch inputs larger than L2 at B=64, no flush"},
+            "batched": batched, "single_atmosphere": single, "clocks": clk}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,10 +485,12 @@ def main():
                     help="atmospheres per GPU (default: two per SM, 296 on a B200)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config0", choices=["config0", "config1", "config2", "config3"],
+    ap.add_argument("--workload", default="config0", choices=["config0", "config1", "config2", "config3",
+                                                             "config4"],
                     help="config0: the headline batch (default); config1: the adaptive loop with "
                          "photochemistry; config2: the uneven multi-network batch; "
-                         "config3: the mixed-precision block solve against FP64")
+                         "config3: the mixed-precision block solve against FP64; config4: the batched "
+                         "implicit adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -432,9 +508,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    if args.workload in ("config1", "config2", "config3"):
+    if args.workload in ("config1", "config2", "config3", "config4"):
         if rank == 0:
-            run = {"config1": run_config1, "config2": run_config2, "config3": run_config3}[args.workload]
+            run = {"config1": run_config1, "config2": run_config2, "config3": run_config3,
+                   "config4": run_config4}[args.workload]
             print(json.dumps(run(args, torch)), flush=True)
         return
     _lib = pkg("_lib")

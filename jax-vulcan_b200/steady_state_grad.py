@@ -3,10 +3,10 @@
 
 At a steady state f(y*, theta) = 0, so dL/dtheta = -(J_y^{-T} dL/dy*) . df/dtheta.
 ``implicit_cotangents`` assembles J_y, solves the transposed block-tridiagonal
-system with the block-Thomas factors and applies the VJP kernels. Supported
-leaves: ``k_arr`` (and ``M``), ``Kzz``, ``top_flux``, ``bot_flux``,
-``bot_vdep``; the reference's molecular-diffusion leaves (Dzz, Hpi, Ti, Tco,
-g, ms, alpha, vm, vs, vz, dzi) are not differentiated here.
+system with the block-Thomas factors and applies the VJP kernels to every
+leaf of the reference `SteadyStateInputs`. ``temperature_cotangent`` adds the
+path through the rate constants (dk/dT from ``rates``) to the temperature
+leaves.
 
 ``DifferentiableSteadyState`` is the ``torch.autograd.Function`` counterpart of
 the reference's ``differentiable_steady_state`` custom_vjp (`:284-330`):
@@ -119,6 +119,21 @@ def implicit_cotangents(y_star, k_arr, atm: AtmStatic, net: NetworkArrays, v, st
     if single:
         out = {kk: (vv[0] if kk != "status" else vv) for kk, vv in out.items()}
     return out
+
+
+def temperature_cotangent(cot, dkdT=None):
+    """dL/dT per layer [B, nz] (or [nz]) at fixed M: the Tco leaf, the
+    interface temperatures Ti = (T_j + T_{j+1}) / 2 (reference
+    `atm_setup.py:371`) and, given ``dkdT`` [B, nr+1, nz] from
+    ``rates.build_rate_array(..., with_dkdT=True)``, the rate constants:
+    g_T[j] = g_Tco[j] + (g_Ti[j-1] + g_Ti[j]) / 2 + sum_r g_k[r, j] dk_r/dT[j]."""
+    gT = cot["Tco"].clone()
+    gTi = cot["Ti"]
+    gT[..., :-1] += 0.5 * gTi
+    gT[..., 1:] += 0.5 * gTi
+    if dkdT is not None:
+        gT += (cot["k_arr"] * dkdT.reshape(cot["k_arr"].shape)).sum(dim=-2)
+    return gT
 
 
 class DifferentiableSteadyState(torch.autograd.Function):

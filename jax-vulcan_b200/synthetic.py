@@ -486,14 +486,16 @@ def _eq_of(tables, row):
            f"{side(tables.product_idx[row], tables.product_stoich[row], m)}"
 
 
-def make_rate_network(seed=0, ni=30, n_fwd=120, n_kinf=24, n_nokinf=12, n_photo=6) -> str:
+def make_rate_network(seed=0, ni=30, n_fwd=120, n_kinf=24, n_nokinf=12, n_photo=6, special=True) -> str:
     """Network text exercising every rate form of the rate build: two-body
     modified Arrhenius (``a n E``), three-body with high-pressure rates
     (Lindemann, ``a n E a_inf n_inf E_inf``), three-body without, the three
     low-temperature-cap reactions (reference `rates.py:30-33`), the special
     ``OH + CH3 + M -> CH3OH + M`` (hardcoded Troe), `# reverse stops` and a
     photo section. Reactions come from a seeded balanced network; parameters
-    are seeded log-uniform / uniform draws written with 4 significant digits."""
+    are seeded log-uniform / uniform draws written with 4 significant digits.
+    ``special=False`` leaves out the cap and special reactions (and their
+    named species), so the network has exactly ``ni`` species."""
     rng = _rng(seed, 17)
     base = make_network(seed, ni, n_fwd, n_photo=n_photo)
     t = base.tables
@@ -521,7 +523,7 @@ def make_rate_network(seed=0, ni=30, n_fwd=120, n_kinf=24, n_nokinf=12, n_photo=
             eq = f"{lhs} + M -> {rhs} + M"
         put(eq, [e(10 ** rng.uniform(-33, -26)), f"{rng.uniform(-4, 1):.3f}", f"{rng.uniform(0, 5000):.1f}",
                  e(10 ** rng.uniform(-12, -9)), f"{rng.uniform(-1, 1):.3f}", f"{rng.uniform(0, 3000):.1f}"])
-    for eq in ("H + CH3 + M -> CH4 + M", "H + C2H4 + M -> C2H5 + M", "H + C2H5 + M -> C2H6 + M"):
+    for eq in ("H + CH3 + M -> CH4 + M", "H + C2H4 + M -> C2H5 + M", "H + C2H5 + M -> C2H6 + M")[:3 * special]:
         put(eq, [e(10 ** rng.uniform(-30, -24)), f"{rng.uniform(-3, 0):.3f}", f"{rng.uniform(0, 700):.1f}",
                  e(10 ** rng.uniform(-11, -9)), f"{rng.uniform(-0.5, 1.5):.3f}", f"{rng.uniform(0, 600):.1f}"])
     lines.append("# 3-body reactions without high-pressure rates")
@@ -531,8 +533,9 @@ def make_rate_network(seed=0, ni=30, n_fwd=120, n_kinf=24, n_nokinf=12, n_photo=
             lhs, rhs = eq.split(" -> ")
             eq = f"{lhs} + M -> {rhs} + M"
         put(eq, [e(10 ** rng.uniform(-34, -28)), f"{rng.uniform(-3, 0):.3f}", f"{rng.uniform(0, 1000):.1f}"])
-    lines.append("# special cases")
-    put("OH + CH3 + M -> CH3OH + M", [])
+    if special:
+        lines.append("# special cases")
+        put("OH + CH3 + M -> CH3OH + M", [])
     lines.append("# reverse stops")
     lines.append("# photo disscoiation (no reversals)")
     for sp, br, row in base.photo_branches:

@@ -113,3 +113,44 @@ def test_residual_gate():
     assert r < 1e-9
     with pytest.raises(ValueError):
         ssg.validate_steady_state_solution(g["chain_y"] * 1.5, k, jstep.atm_from_dict(atm), dn)
+
+
+def test_temperature_gradient_through_rates_and_transport():
+    """dL/dT per layer = the Tco leaf + the interface-temperature leaf (Ti the
+    mean of its two layers) + sum_r g_k dk_r/dT (vb_rates' dual-number dk/dT),
+    against central differences (h = 0.1 K) of phi(T) = -lambda . f(y,
+    k(T), atm(T)) on the oracle, with lambda from the GPU adjoint: the
+    adjoint identity g_theta = -lambda . df/dtheta holds at any state.
+    Network with Arrhenius and Lindemann rates and NASA-9 reverse rates
+    (12 species, 30 + 30 reactions), molecular diffusion with thermal
+    diffusion on, 10 layers from 800 to 2000 K. Tolerance 1e-5 of the
+    largest |dphi/dT| (the FD truncation error is ~1e-6 of it)."""
+    from types import SimpleNamespace
+    from oracle import rates as orr
+    rates = load_pkg("rates")
+    net_tab = load_pkg("network").parse_network_text(
+        syn.make_rate_network(3, ni=12, n_fwd=30, n_kinf=6, n_nokinf=3, n_photo=0, special=False))
+    coeffs = syn.make_nasa9(3, net_tab.ni)
+    rng = np.random.default_rng(3)
+    ms = rng.uniform(2.0, 60.0, net_tab.ni)
+    atm, extra = syn.make_atmosphere(3, SimpleNamespace(tables=net_tab, ms=ms), nz=10, moldiff=True)
+    T, M = atm["Tco"].copy(), atm["M"]
+    assert np.all(np.abs(T - 1000.0) > 1.0)            # no NASA-9 branch switch inside the differences
+    k = orr.build_rate_array(net_tab, coeffs, T, M)
+    y = extra["y"]
+    v = rng.normal(0.0, 1.0, y.shape) / np.abs(y)
+    dn = chem.to_device(net_tab)
+    cot = ssg.implicit_cotangents(y, k, jstep.atm_from_dict(atm), dn, v)
+    _, dkdT = rates.RateTables(net_tab, coeffs)(T, M, with_dkdT=True)
+    gT = ssg.temperature_cotangent(cot, dkdT).cpu().numpy()
+    lam = cot["lambda"].cpu().numpy()
+
+    def phi(Tz):
+        a = dict(atm, Tco=Tz, Ti=0.5 * (Tz[1:] + Tz[:-1]))
+        return -float(np.sum(lam * oa.residual(y, orr.build_rate_array(net_tab, coeffs, Tz, M), a, net_tab)))
+
+    h = 0.1
+    fd = np.array([(phi(T + h * np.eye(10)[z]) - phi(T - h * np.eye(10)[z])) / (2 * h) for z in range(10)])
+    err = np.max(np.abs(gT - fd)) / np.max(np.abs(fd))
+    print(f"dL/dT vs central differences: {err:.2e}")
+    assert err <= 1e-5, (gT, fd)
