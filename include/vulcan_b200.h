@@ -339,6 +339,46 @@ typedef struct VbRateTables {
 int vb_rates(int batch, int nz, const VbRateTables* tables, const double* T, const double* M, int32_t flags,
              double* k, double* dkdT, void* stream);
 
+/* Atmosphere refresh (reference atm_refresh.py:36-122), uniform batches:
+ * mu = ymix . mol_mass per layer; the hydrostatic integration upward from
+ * the reference layer pref_indx (zco[pref] = zco_pref, g = gs there) and
+ * downward below it, g = gs (Rp / (Rp + zco))^2, Hp = kb T / (mu / Navo g),
+ * dz = Hp ln(pico[j] / pico[j+1]); dzi, Hpi the means of adjacent layers;
+ * the diffusion-limited escape flux at the top of each esc_idx species,
+ * -Dzz_top y_top (1/Hp_top - ms g_top / (Navo kb T_top)), floored at
+ * -max_flux. g, dzi, Hpi and those top_flux entries are written into the
+ * atmosphere blob (the splice of outer_loop.py:729-730); Tco, ms and Dzz
+ * (its last interface row) are read from it. Device arrays: pico
+ * [B][nz+1], mol_mass [ni], esc_idx [n_esc], y, ymix [B][nz][ni]; outputs
+ * (each nullable) mu, Hp, dz [B][nz], zco [B][nz+1]. */
+typedef struct VbRefreshParams {
+  int32_t pref_indx, n_esc;
+  double zco_pref, gs, Rp, kb, Navo, max_flux;
+} VbRefreshParams;
+int vb_atm_refresh(int batch, int nz, int ni, const VbRefreshParams* params, const double* pico,
+                   const double* mol_mass, const int32_t* esc_idx, const double* y, const double* ymix, double* atm,
+                   double* mu, double* Hp, double* dz, double* zco, void* stream);
+/* Condensation rates (reference conden.py:55-71): rate = Dg coeff (y[sp] -
+ * sat_n) for each condensation reaction r; k[re_idx[r]] = max(rate, 0),
+ * k[re_idx[r] + 1] = max(-rate, 0). Dg, sat_n [B][n_re][nz], coeff [n_re],
+ * re_idx, sp_idx [n_re], y [B][nz][ni], k [B][nr+1][nz]. */
+int vb_conden_rates(int batch, int nz, int ni, int nr, int n_re, const int32_t* re_idx, const int32_t* sp_idx,
+                    const double* coeff, const double* Dg, const double* sat_n, const double* y, double* k,
+                    void* stream);
+/* Cold-trap relaxation of one condensing species (reference conden.py:74-160):
+ * implicit Euler toward saturation, mass moved between species sp and its
+ * condensate sp_l_s, then y = ymix * (gas sum of y before the update) for
+ * every species. conden_top >= 0 clamps condensation to layers <=
+ * conden_top and clips the condensate's ymix at 0 (the NH3 form); -1 is
+ * the H2O form. Dg, sat [B][nz], dt [B]; n_0 and the gas mask are the
+ * blob's M and gas slots; y, ymix [B][nz][ni] updated in place. */
+typedef struct VbRelaxParams {
+  int32_t sp, sp_l_s, conden_top, reserved;
+  double m_over_rho_r2;
+} VbRelaxParams;
+int vb_conden_relax(int batch, int nz, int ni, const VbRelaxParams* params, const double* Dg, const double* sat,
+                    const double* atm, const double* dt, double* y, double* ymix, void* stream);
+
 /* Profiling: while enabled, every kernel launch of vb_ros2_step is bracketed
  * by CUDA events recorded on the launching stream (launch sites:
  * 0 stage-1 assembly, 1 factor, 2 back sweep 1, 3 stage-2 assembly,

@@ -48,6 +48,9 @@ SIGNATURES = {
     "vb_photo_j": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_photo_update": (_i, [_i, _i, _i, _i] + [_p] * 13 + [C.c_double, _p, _p]),
     "vb_rates": (_i, [_i, _i, _p, _p, _p, C.c_int32, _p, _p, _p]),
+    "vb_atm_refresh": (_i, [_i, _i, _i] + [_p] * 12),
+    "vb_conden_rates": (_i, [_i, _i, _i, _i, _i] + [_p] * 8),
+    "vb_conden_relax": (_i, [_i, _i, _i] + [_p] * 8),
     "vb_profile": (_i, [_i]),
     "vb_profile_read": (_i, [_p, _p, _i]),
     "vb_fp64_probe": (_i, [_p, _i, _i, _i, _p]),

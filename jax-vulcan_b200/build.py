@@ -29,6 +29,7 @@ UNITS = {
     "vb_control.cu": ["--fmad=false"],
     "vb_mixed.cu": [],
     "vb_rates.cu": ["--fmad=false"],
+    "vb_refresh.cu": ["--fmad=false"],
 }
 
 

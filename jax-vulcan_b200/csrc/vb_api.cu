@@ -560,6 +560,46 @@ int vb_rates(int batch, int nz, const VbRateTables* tables, const double* T, con
   return VB_OK;
 }
 
+int vb_atm_refresh(int batch, int nz, int ni, const VbRefreshParams* params, const double* pico,
+                   const double* mol_mass, const int32_t* esc_idx, const double* y, const double* ymix, double* atm,
+                   double* mu, double* Hp, double* dz, double* zco, void* stream) {
+  if (!params || !pico || !mol_mass || !y || !ymix || !atm || (params->n_esc > 0 && !esc_idx))
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2 || ni < 1 || params->n_esc < 0)
+    return fail(VB_ERR_ARG, "batch >= 1, nz >= 2, ni >= 1, n_esc >= 0");
+  if (params->pref_indx < 0 || params->pref_indx >= nz) return fail(VB_ERR_ARG, "pref_indx must be in [0, nz)");
+  if ((5 * (size_t)nz + 1) * sizeof(double) > 200 * 1024) return fail(VB_ERR_ARG, "nz too large for the refresh");
+  VB_CHECK(vb::launch_atm_refresh(batch, nz, ni, *params, pico, mol_mass, esc_idx, y, ymix, atm, mu, Hp, dz, zco,
+                                  (cudaStream_t)stream),
+           "atm refresh");
+  return VB_OK;
+}
+
+int vb_conden_rates(int batch, int nz, int ni, int nr, int n_re, const int32_t* re_idx, const int32_t* sp_idx,
+                    const double* coeff, const double* Dg, const double* sat_n, const double* y, double* k,
+                    void* stream) {
+  if (n_re == 0) return VB_OK;
+  if (!re_idx || !sp_idx || !coeff || !Dg || !sat_n || !y || !k) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || batch > 65535 || nz < 1 || ni < 1 || nr < 2 || n_re < 0 || n_re > 65535)
+    return fail(VB_ERR_ARG, "bad shape");
+  VB_CHECK(vb::launch_conden_rates(batch, nz, ni, nr, n_re, re_idx, sp_idx, coeff, Dg, sat_n, y, k,
+                                   (cudaStream_t)stream),
+           "conden rates");
+  return VB_OK;
+}
+
+int vb_conden_relax(int batch, int nz, int ni, const VbRelaxParams* params, const double* Dg, const double* sat,
+                    const double* atm, const double* dt, double* y, double* ymix, void* stream) {
+  if (!params || !Dg || !sat || !atm || !dt || !y || !ymix) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 1 || ni < 1) return fail(VB_ERR_ARG, "bad shape");
+  const VbRelaxParams& p = *params;
+  if (p.sp < 0 || p.sp >= ni || p.sp_l_s < 0 || p.sp_l_s >= ni || p.sp == p.sp_l_s)
+    return fail(VB_ERR_ARG, "sp and sp_l_s must be distinct species in [0, ni)");
+  VB_CHECK(vb::launch_conden_relax(batch, nz, ni, p, Dg, sat, atm, dt, y, ymix, (cudaStream_t)stream),
+           "conden relax");
+  return VB_OK;
+}
+
 int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream) {
   if (!out || blocks < 1 || threads < 32 || iters < 1) return fail(VB_ERR_ARG, "bad probe arguments");
   VB_CHECK(vb::launch_fp64_probe(out, blocks, threads, iters, (cudaStream_t)stream), "fp64 probe");

@@ -54,6 +54,15 @@ cudaError_t launch_photo_j(int batch, int nz, int nr, const VbPhoto& P, const do
                            double* J_br_T, double* k, const int32_t* due, cudaStream_t);
 cudaError_t launch_rates(int batch, int nz, const VbRateTables& t, const double* T, const double* M, int flags,
                          double* k, double* dkdT, cudaStream_t st);
+cudaError_t launch_atm_refresh(int batch, int nz, int ni, const VbRefreshParams& p, const double* pico,
+                               const double* mol_mass, const int32_t* esc, const double* y, const double* ymix,
+                               double* atm, double* mu, double* Hp, double* dz, double* zco, cudaStream_t st);
+cudaError_t launch_conden_rates(int batch, int nz, int ni, int nr, int n_re, const int32_t* re_idx,
+                                const int32_t* sp_idx, const double* coeff, const double* Dg, const double* sat,
+                                const double* y, double* k, cudaStream_t st);
+cudaError_t launch_conden_relax(int batch, int nz, int ni, const VbRelaxParams& p, const double* Dg,
+                                const double* sat, const double* atm, const double* dt, double* y, double* ymix,
+                                cudaStream_t st);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
 template <typename R>
 cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,

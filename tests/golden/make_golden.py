@@ -6,8 +6,8 @@ Run in the build container (the reference sources are not on the GPU box):
 
 JAX is not installed, so the unmodified reference modules (`network.py`,
 `chem.py`, `solver.py`, `jax_step.py`, `photo.py`, `integrate.py`,
-`steady_state_grad.py`, `rates.py`, `gibbs.py`, and the caller-contract
-functions of `outer_loop.py`)
+`steady_state_grad.py`, `rates.py`, `gibbs.py`, `atm_refresh.py`,
+`conden.py`, and the caller-contract functions of `outer_loop.py`)
 are imported with ``_jax_numpy_shim`` standing in for ``jax``. A stub
 ``vulcan_cfg`` with no species lists is installed first so the reference
 parser does not append config-named species (reference `network.py:157-194`).
@@ -515,6 +515,69 @@ def rates_fixture(mods, syn):
     print("rates: ok", k_all.shape, "nonzero", int((k_all != 0).sum()))
 
 
+def refresh_fixture(mods):
+    """Reference atm_refresh.py (update_mu_dz_jax with a reference layer
+    inside the column, update_phi_esc_jax with the flux floor active for one
+    species) and conden.py (update_conden_rates, apply_h2o_relax_jax,
+    apply_nh3_relax_jax with condensing and evaporating layers) through the
+    stand-in, on seeded inputs."""
+    import _jax_numpy_shim as shim
+    ar, cd = importlib.import_module("atm_refresh"), importlib.import_module("conden")
+    rng = np.random.default_rng(21)
+    nz, ni = 16, 12
+    J = lambda a: np.asarray(a, dtype=np.float64).view(shim.JArr)  # noqa: E731
+    ymix = 10.0 ** rng.uniform(-8, 0, (nz, ni))
+    ymix /= ymix.sum(axis=1, keepdims=True)
+    Tco = np.linspace(1800.0, 700.0, nz)
+    pico = np.logspace(8.0, 0.0, nz + 1)
+    n_0 = 0.5 * (pico[:-1] + pico[1:]) / (1.380649e-16 * Tco)
+    y = ymix * n_0[:, None]
+    mol_mass = rng.uniform(2.0, 60.0, ni)
+    ms = mol_mass / 6.02214076e23
+    Dzz_top = 10.0 ** rng.uniform(5.0, 9.0, ni)
+    esc = np.array([0, 3, 7], dtype=np.int32)
+    kb, Navo, gs, Rp = 1.38064852e-16, 6.02214086e23, 2140.0, 7.1492e9
+    top_flux = rng.normal(0.0, 1e6, ni)
+    pref = 5
+    max_flux = float(np.sort(np.abs(Dzz_top[esc] * y[-1, esc] / 1e7))[1])   # floors one of the three
+    st = ar.AtmRefreshStatic(Tco=J(Tco), pico=J(pico), mol_mass=J(mol_mass), ms=J(ms), Dzz_top=J(Dzz_top),
+                             diff_esc_idx=esc, pref_indx=pref, zco_pref=0.0, gs=gs, Rp=Rp, kb=kb, Navo=Navo,
+                             max_flux=max_flux, nz=nz, ni=ni)
+    mu, g, Hp, dz, zco, dzi, Hpi = (np.asarray(v) for v in ar.update_mu_dz_jax(J(ymix), st))
+    tf = np.asarray(ar.update_phi_esc_jax(J(y), J(g), J(Hp), J(top_flux), st))
+    # condensation: two condensing species (H2O-like at 1, NH3-like at 4) with condensates 2 and 5
+    nr = 20
+    k = 10.0 ** rng.uniform(-20, -10, (nr + 1, nz))
+    re_idx = np.array([11, 15], dtype=np.int32)
+    sp_idx = np.array([1, 4], dtype=np.int32)
+    Dg = 10.0 ** rng.uniform(-2, 1, (2, nz))
+    sat_n = y[:, sp_idx].T * rng.uniform(0.5, 1.5, (2, nz))
+    coeff = np.array([3.0e-9, 0.0])
+    gas = np.ones(ni, dtype=bool)
+    gas[[2, 5]] = False
+    h2o_Dg, nh3_Dg = Dg[0], Dg[1]
+    h2o_sat, nh3_sat = sat_n[0], sat_n[1]
+    y[:, 2] = y[:, 1] * rng.uniform(0.0, 0.5, nz)
+    y[:, 5] = y[:, 4] * rng.uniform(0.0, 0.5, nz)
+    dt = 3.0e4
+    cst = cd.CondenStatic(conden_re_idx=re_idx, conden_sp_idx=sp_idx, Dg_per_re=J(Dg), sat_n_per_re=J(sat_n),
+                          coeff_per_re=J(coeff), h2o_active=True, h2o_idx=1, h2o_l_s_idx=2, h2o_Dg=J(h2o_Dg),
+                          h2o_sat=J(h2o_sat), h2o_m_over_rho_r2=0.7, nh3_active=True, nh3_idx=4, nh3_l_s_idx=5,
+                          nh3_Dg=J(nh3_Dg), nh3_sat=J(nh3_sat), nh3_m_over_rho_r2=0.3, nh3_conden_top=9,
+                          n_0=J(n_0), gas_indx_mask=gas)
+    k_new = np.asarray(cd.update_conden_rates(J(k), J(y), cst))
+    y1, x1 = cd.apply_h2o_relax_jax(J(y), J(ymix), dt, cst)
+    y2, x2 = cd.apply_nh3_relax_jax(y1, x1, dt, cst)
+    out = dict(ymix=ymix, Tco=Tco, pico=pico, mol_mass=mol_mass, ms=ms, Dzz_top=Dzz_top, esc=esc, pref=np.array(pref),
+               consts=np.array([kb, Navo, gs, Rp, max_flux]), top_flux=top_flux, y=y, n_0=n_0, mu=mu, g=g, Hp=Hp,
+               dz=dz, zco=zco, dzi=dzi, Hpi=Hpi, top_flux_new=tf, k=k, re_idx=re_idx, sp_idx=sp_idx, Dg=Dg,
+               sat_n=sat_n, coeff=coeff, gas=gas, dt=np.array(dt), k_new=k_new, y_h2o=np.asarray(y1),
+               ymix_h2o=np.asarray(x1), y_nh3=np.asarray(y2), ymix_nh3=np.asarray(x2))
+    np.savez_compressed(os.path.join(HERE, "refresh.npz"), **out)
+    tau_h2o = 1.0 / (h2o_Dg * 0.7 * (y[:, 1] - h2o_sat))
+    print("refresh: ok; h2o condensing layers", int((tau_h2o > 0).sum()), "of", nz)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE", "/root/reference"))
@@ -529,8 +592,10 @@ def main():
                 body_fixture(mods, syn, args.reference, shim)
             elif name == "rates":
                 rates_fixture(mods, syn)
+            elif name == "refresh":
+                refresh_fixture(mods)
             else:
-                raise SystemExit(f"--only supports: body, rates (got {name})")
+                raise SystemExit(f"--only supports: body, rates, refresh (got {name})")
         return
     mild = dict(mild=True, k_range=(-40.0, 4.0))
     step_fixture(mods, "plain", syn.make_case(seed=5, ni=12, n_fwd=30, nz=10, **mild), n_steps=3)
@@ -552,6 +617,7 @@ def main():
     adjoint_fixture(mods, syn)
     body_fixture(mods, syn, args.reference, shim)
     rates_fixture(mods, syn)
+    refresh_fixture(mods)
 
 
 if __name__ == "__main__":
