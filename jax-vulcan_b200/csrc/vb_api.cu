@@ -476,7 +476,7 @@ int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const d
 int vb_photo_tau(int batch, int nz, int ni, const VbPhoto* photo, const double* y, const double* dz,
                  double* tau, void* stream) {
   if (!photo || !y || !dz || !tau) return fail(VB_ERR_ARG, "null argument");
-  if (batch < 1 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
+  if (batch < 1 || batch > 65535 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
   VB_CHECK(vb::launch_photo_tau(batch, nz, ni, *photo, y, dz, tau, nullptr, nullptr, (cudaStream_t)stream), "photo tau");
   return VB_OK;
 }
@@ -486,7 +486,7 @@ int vb_photo_flux(int batch, int nz, int ni, const VbPhoto* photo, const double*
                   void* stream) {
   if (!photo || !tau || !ymix || !dflux_u_prev || !aflux || !sflux || !dflux_d || !dflux_u)
     return fail(VB_ERR_ARG, "null argument");
-  if (batch < 1 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
+  if (batch < 1 || batch > 65535 || nz < 1 || ni < 1 || photo->nbin < 1) return fail(VB_ERR_ARG, "bad shape");
   VB_CHECK(vb::launch_photo_flux(batch, nz, ni, *photo, tau, ymix, dflux_u_prev, aflux, sflux, dflux_d, dflux_u,
                                  nullptr, 0.0, nullptr, (cudaStream_t)stream),
            "photo flux");
@@ -496,7 +496,7 @@ int vb_photo_flux(int batch, int nz, int ni, const VbPhoto* photo, const double*
 int vb_photo_j(int batch, int nz, int nr, const VbPhoto* photo, const double* aflux, double* J_br,
                double* J_br_T, double* k, void* stream) {
   if (!photo || !aflux) return fail(VB_ERR_ARG, "null argument");
-  if (batch < 1 || nz < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
+  if (batch < 1 || batch > 65535 || nz < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
     return fail(VB_ERR_ARG, "bad shape");
   VB_CHECK(vb::launch_photo_j(batch, nz, nr, *photo, aflux, J_br, J_br_T, k, nullptr, (cudaStream_t)stream),
            "photo J");
@@ -509,7 +509,7 @@ int vb_photo_update(int batch, int nz, int ni, int nr, const VbPhoto* photo, con
                     VbConvState* conv, void* stream) {
   if (!photo || !y || !dz || !ymix || !tau || !aflux || !sflux || !dflux_d || !dflux_u || !k)
     return fail(VB_ERR_ARG, "null argument");
-  if (batch < 1 || nz < 1 || ni < 1 || nr < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
+  if (batch < 1 || batch > 65535 || nz < 1 || ni < 1 || nr < 1 || photo->nbin < 1 || photo->din12 < 0 || photo->din12 > photo->nbin)
     return fail(VB_ERR_ARG, "bad shape");
   cudaStream_t st = (cudaStream_t)stream;
   double* achg = conv ? &conv[0].aflux_change : nullptr;
