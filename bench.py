@@ -402,6 +402,73 @@ def run_config1(args, torch):
             "gpu_launches_per_attempt": "7 (step) + 1 (body) + 1 (convergence) + 3 (photo)", "clocks": clk}
 
 
+def run_photo(args, torch):
+    """The photo update alone at the config-1 shapes (nz=120, 2500 bins, 19
+    absorbers of which 4 temperature dependent, 2 scatterers, 40 branches of
+    which 10 temperature dependent) for B atmospheres: tau, flux and J timed
+    separately with CUDA events, each against the HBM roofline of its
+    algorithmic bytes (per-atmosphere arrays read / written once, the shared
+    cross-section tables once per launch)."""
+    import ctypes as C
+    syn, photo, _lib = pkg("synthetic"), pkg("photo"), pkg("_lib")
+    net = syn.make_network(0, 69, 700, n_photo=40)
+    atm, extra = syn.make_atmosphere(0, net, nz=120)
+    bins, din12 = syn.make_bins()
+    dev = photo.PhotoDevice(syn.make_photo(0, net, atm["Tco"], bins, din12), 120)
+    s = dev.struct
+    B = args.batch or torch.cuda.get_device_properties(0).multi_processor_count
+    nz, ni, nbin, nr = 120, 69, s.nbin, net.tables.nr
+    y = torch.as_tensor(np.stack([extra["y"]] * B), device="cuda").contiguous()
+    x = torch.as_tensor(np.stack([extra["ymix"]] * B), device="cuda").contiguous()
+    dz = torch.as_tensor(np.stack([extra["dz"]] * B), device="cuda").contiguous()
+    tau = torch.empty((B, nz + 1, nbin), dtype=torch.float64, device="cuda")
+    af = torch.empty((B, nz, nbin), dtype=torch.float64, device="cuda")
+    sf, dd, du = torch.empty_like(tau), torch.empty_like(tau), torch.zeros_like(tau)
+    k = torch.zeros((B, nr + 1, nz), dtype=torch.float64, device="cuda")
+    L = _lib.lib()
+    sh = _lib.stream_handle()
+    launches = {
+        "tau": lambda: L.vb_photo_tau(B, nz, ni, C.addressof(s), y.data_ptr(), dz.data_ptr(), tau.data_ptr(), sh),
+        "flux": lambda: L.vb_photo_flux(B, nz, ni, C.addressof(s), tau.data_ptr(), x.data_ptr(), du.data_ptr(),
+                                        af.data_ptr(), sf.data_ptr(), dd.data_ptr(), du.data_ptr(), sh),
+        "J": lambda: L.vb_photo_j(B, nz, nr, C.addressof(s), af.data_ptr(), None, None, k.data_ptr(), sh)}
+    per_atm = {"tau": 8 * (nz * ni + nz + (nz + 1) * nbin),
+               "flux": 8 * ((nz + 1) * nbin * 2 + nz * ni + nz * nbin + 3 * (nz + 1) * nbin),
+               "J": 8 * (nz * nbin + (s.n_br + s.n_br_T) * nz)}
+    shared = {"tau": 8 * nbin * (s.n_abs + s.n_scat + s.n_abs_T * nz),
+              "flux": 8 * nbin * (s.n_abs + s.n_scat + s.n_abs_T * nz + 2),
+              "J": 8 * nbin * (s.n_br + s.n_br_T * nz)}
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    for _ in range(args.warmup):
+        for f in launches.values():
+            f()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, f in launches.items():
+        e0.record()
+        for _ in range(args.steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        bytes_ = B * per_atm[name] + shared[name]
+        out[name] = {"ms_per_launch": ms, "algorithmic_bytes": bytes_, "achieved_gbs": bytes_ / (ms * 1e-3) / 1e9,
+                     "hbm_frac": bytes_ / (ms * 1e-3) / 1e9 / peak}
+    clk = clocks.stop()
+    total = sum(v["ms_per_launch"] for v in out.values())
+    return {"metric": "photo updates/s (tau + two-stream flux + J-rates into k)", "value": B / (total * 1e-3),
+            "unit": "atmosphere-photo-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded config-1 photochemistry)",
+            "config": {"workload": f"photo update of {B} atmospheres, nz=120, 2500 bins, 40 branches",
+                       "l2": "flux arrays larger than L2 at B >= 8, no flush"},
+            "kernels": out, "hbm_peak_gbs": peak, "clocks": clk}
+
+
 def run_config4(args, torch):
     """The implicit steady-state adjoint, batched: for B atmospheres of the
     config-1 shape (ni=69, 700+700 Arrhenius / Lindemann reactions with NASA-9
@@ -486,11 +553,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="config0", choices=["config0", "config1", "config2", "config3",
-                                                             "config4"],
+                                                             "config4", "photo"],
                     help="config0: the headline batch (default); config1: the adaptive loop with "
                          "photochemistry; config2: the uneven multi-network batch; "
                          "config3: the mixed-precision block solve against FP64; config4: the batched "
-                         "implicit adjoint")
+                         "implicit adjoint; photo: the photo kernels against HBM")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -508,10 +575,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    if args.workload in ("config1", "config2", "config3", "config4"):
+    if args.workload in ("config1", "config2", "config3", "config4", "photo"):
         if rank == 0:
             run = {"config1": run_config1, "config2": run_config2, "config3": run_config3,
-                   "config4": run_config4}[args.workload]
+                   "config4": run_config4, "photo": run_photo}[args.workload]
             print(json.dumps(run(args, torch)), flush=True)
         return
     _lib = pkg("_lib")
