@@ -214,12 +214,16 @@ typedef struct VbConvState {
  * y_prev), atom_loss, atom_loss_prev [B][n_atoms], dt [B], scalars [B]. The layer
  * densities n_0 are the atmosphere blob's M. zoff as in vb_ros2_step (nz is
  * then the maximum layer count). conv [B] (nullable): atmospheres whose record
- * has done set are skipped. */
+ * has done set are skipped. pre_y, pre_ymix [B][nz][ni] (nullable, together):
+ * for an accepted or force-accepted attempt, the attempt's clipped state
+ * (sol_clip and ymix_new, outer_loop.py:740), the input of the atmosphere
+ * refresh (vb_loop_refresh). */
 int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopParams* params,
                  const double* atm, const uint8_t* gas_mask, const double* compo, const double* atom_ini,
                  const uint8_t* fix_mask, const double* fix_y, const double* sol, const double* delta_arr,
                  double* y, double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
-                 double* dt, VbLoopScalars* scalars, const VbConvState* conv, void* stream);
+                 double* dt, VbLoopScalars* scalars, const VbConvState* conv, double* pre_y, double* pre_ymix,
+                 void* stream);
 
 /* Convergence part of the adaptive runner, after vb_loop_body: writes (y, t)
  * into ring slot max(accept_count - 1, 0) % conv_step (outer_loop.py:918-928),
@@ -358,6 +362,16 @@ typedef struct VbRefreshParams {
 int vb_atm_refresh(int batch, int nz, int ni, const VbRefreshParams* params, const double* pico,
                    const double* mol_mass, const int32_t* esc_idx, const double* y, const double* ymix, double* atm,
                    double* mu, double* Hp, double* dz, double* zco, void* stream);
+/* The refresh inside the adaptive loop (outer_loop.py:813-840), after
+ * vb_loop_body: for each atmosphere whose attempt was taken (accepted or
+ * force-accepted, scalars[b].last_decision != 0) with a pre-increment
+ * accept count that is a multiple of update_frq, and that is not done
+ * (conv nullable), vb_atm_refresh of the attempt's clipped state (the
+ * body's pre_y, pre_ymix); the others are left untouched. */
+int vb_loop_refresh(int batch, int nz, int ni, const VbRefreshParams* params, int32_t update_frq,
+                    const VbLoopScalars* scalars, const VbConvState* conv, const double* pico,
+                    const double* mol_mass, const int32_t* esc_idx, const double* pre_y, const double* pre_ymix,
+                    double* atm, double* mu, double* Hp, double* dz, double* zco, void* stream);
 /* Condensation rates (reference conden.py:55-71): rate = Dg coeff (y[sp] -
  * sat_n) for each condensation reaction r; k[re_idx[r]] = max(rate, 0),
  * k[re_idx[r] + 1] = max(-rate, 0). Dg, sat_n [B][n_re][nz], coeff [n_re],

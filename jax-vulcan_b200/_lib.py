@@ -49,6 +49,7 @@ SIGNATURES = {
     "vb_photo_update": (_i, [_i, _i, _i, _i] + [_p] * 13 + [C.c_double, _p, _p]),
     "vb_rates": (_i, [_i, _i, _p, _p, _p, C.c_int32, _p, _p, _p]),
     "vb_atm_refresh": (_i, [_i, _i, _i] + [_p] * 12),
+    "vb_loop_refresh": (_i, [_i, _i, _i, _p, C.c_int32] + [_p] * 12),
     "vb_conden_rates": (_i, [_i, _i, _i, _i, _i] + [_p] * 8),
     "vb_conden_relax": (_i, [_i, _i, _i] + [_p] * 8),
     "vb_profile": (_i, [_i]),
@@ -59,7 +60,7 @@ SIGNATURES = {
     "vb_bt_mixed_bytes": (_sz, [_i, _i, _i]),
     "vb_bt_factor_mixed": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_bt_solve_mixed": (_i, [_i, _i, _i, _p, _p, _p, _i, C.c_double, _p, _p, _p]),
-    "vb_loop_body": (_i, [_i, _i, _i] + [_p] * 19),
+    "vb_loop_body": (_i, [_i, _i, _i] + [_p] * 21),
     "vb_loop_converge": (_i, [_i, _i, _i] + [_p] * 13),
 }
 

@@ -570,8 +570,25 @@ int vb_atm_refresh(int batch, int nz, int ni, const VbRefreshParams* params, con
   if (params->pref_indx < 0 || params->pref_indx >= nz) return fail(VB_ERR_ARG, "pref_indx must be in [0, nz)");
   if ((5 * (size_t)nz + 1) * sizeof(double) > 200 * 1024) return fail(VB_ERR_ARG, "nz too large for the refresh");
   VB_CHECK(vb::launch_atm_refresh(batch, nz, ni, *params, pico, mol_mass, esc_idx, y, ymix, atm, mu, Hp, dz, zco,
-                                  (cudaStream_t)stream),
+                                  nullptr, 1, nullptr, (cudaStream_t)stream),
            "atm refresh");
+  return VB_OK;
+}
+
+int vb_loop_refresh(int batch, int nz, int ni, const VbRefreshParams* params, int32_t update_frq,
+                    const VbLoopScalars* scalars, const VbConvState* conv, const double* pico,
+                    const double* mol_mass, const int32_t* esc_idx, const double* pre_y, const double* pre_ymix,
+                    double* atm, double* mu, double* Hp, double* dz, double* zco, void* stream) {
+  if (!params || !scalars || !pico || !mol_mass || !pre_y || !pre_ymix || !atm || (params->n_esc > 0 && !esc_idx))
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2 || ni < 1 || params->n_esc < 0)
+    return fail(VB_ERR_ARG, "batch >= 1, nz >= 2, ni >= 1, n_esc >= 0");
+  if (update_frq < 1) return fail(VB_ERR_ARG, "update_frq must be >= 1");
+  if (params->pref_indx < 0 || params->pref_indx >= nz) return fail(VB_ERR_ARG, "pref_indx must be in [0, nz)");
+  if ((5 * (size_t)nz + 1) * sizeof(double) > 200 * 1024) return fail(VB_ERR_ARG, "nz too large for the refresh");
+  VB_CHECK(vb::launch_atm_refresh(batch, nz, ni, *params, pico, mol_mass, esc_idx, pre_y, pre_ymix, atm, mu, Hp, dz,
+                                  zco, scalars, update_frq, conv, (cudaStream_t)stream),
+           "loop refresh");
   return VB_OK;
 }
 
@@ -610,7 +627,8 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
                  const uint8_t* gas_mask, const double* compo, const double* atom_ini, const uint8_t* fix_mask,
                  const double* fix_y, const double* sol, const double* delta_arr, double* y, double* y_prev,
                  double* ymix, double* atom_loss, double* atom_loss_prev, double* dt, VbLoopScalars* scalars,
-                 const VbConvState* conv, void* stream) {
+                 const VbConvState* conv, double* pre_y, double* pre_ymix, void* stream) {
+  if ((pre_y == nullptr) != (pre_ymix == nullptr)) return fail(VB_ERR_ARG, "pre_y and pre_ymix go together");
   if (!params || !atm || !compo || !atom_ini || !sol || !delta_arr || !y || !y_prev || !ymix || !atom_loss ||
       !atom_loss_prev || !dt || !scalars)
     return fail(VB_ERR_ARG, "null argument");
@@ -628,7 +646,8 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
   B.ld = vb::round_even(ni);
   B.zoff = zoff;
   VB_CHECK(vb::launch_loop_body(B, p, gas_mask, compo, atom_ini, atm, fix_mask, fix_y, sol, delta_arr, y, y_prev,
-                                ymix, atom_loss, atom_loss_prev, dt, scalars, conv, (cudaStream_t)stream),
+                                ymix, atom_loss, atom_loss_prev, dt, scalars, conv, pre_y, pre_ymix,
+                                (cudaStream_t)stream),
            "loop body");
   return VB_OK;
 }

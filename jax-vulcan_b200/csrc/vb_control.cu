@@ -72,7 +72,8 @@ loop_body_kernel(Batch B, VbLoopParams p, const uint8_t* __restrict__ gas, const
                  const double* __restrict__ atom_ini, const double* __restrict__ atm, ElemIn E,
                  double* y, double* y_prev, double* ymix,  // may alias one another (y == y_prev)
                  double* __restrict__ atom_loss, double* __restrict__ atom_loss_prev, double* __restrict__ dtp,
-                 VbLoopScalars* __restrict__ st, const VbConvState* __restrict__ conv) {
+                 VbLoopScalars* __restrict__ st, const VbConvState* __restrict__ conv, double* __restrict__ pre_y,
+                 double* __restrict__ pre_ymix) {
   extern __shared__ double ys[];  // [2][nz]: ysum of the clipped and of the rebalanced state
   __shared__ double red[BODY_WARPS][4 + 2 * VB_LOOP_MAX_ATOMS];
   __shared__ int flags_s[BODY_WARPS][2];
@@ -262,6 +263,21 @@ loop_body_kernel(Batch B, VbLoopParams p, const uint8_t* __restrict__ gas, const
   double* yb = y + o;
   double* ypb = y_prev + o;
   double* xb = ymix + o;
+  // the attempt's clipped state (sol_clip, ymix_new of outer_loop.py:740),
+  // which the atmosphere refresh of an accepted or force-accepted attempt
+  // reads (outer_loop.py:818-826); written before the state is overwritten
+  if (pre_y && dec != 0) {
+    for (int j = warp; j < nz; j += BODY_WARPS) {
+      const double sc = ysc[j];
+      for (int i = lane; i < ni; i += 32) {
+        const int64_t e = (int64_t)j * ni + i;
+        double v, d;
+        const double c = clip_elem(Eb, e, v, d);
+        pre_y[o + e] = c;
+        pre_ymix[o + e] = c / sc;
+      }
+    }
+  }
   if (dec == 1) {
     for (int j = warp; j < nz; j += BODY_WARPS) {
       const double sc = ysc[j], sb = ysb[j], Mj = M[j];
@@ -293,7 +309,8 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
                              const double* atom_ini, const double* atm, const uint8_t* fix_mask,
                              const double* fix_y, const double* sol, const double* delta, double* y,
                              double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
-                             double* dt, VbLoopScalars* st, const VbConvState* conv, cudaStream_t stream) {
+                             double* dt, VbLoopScalars* st, const VbConvState* conv, double* pre_y,
+                             double* pre_ymix, cudaStream_t stream) {
   ElemIn E;
   E.sol = sol;
   E.delta = delta;
@@ -309,7 +326,8 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
     if (e != cudaSuccess) return e;
   }
   loop_body_kernel<<<B.count, BODY_THREADS, smem, stream>>>(B, p, gas, compo, atom_ini, atm, E, y, y_prev, ymix,
-                                                            atom_loss, atom_loss_prev, dt, st, conv);
+                                                            atom_loss, atom_loss_prev, dt, st, conv, pre_y,
+                                                            pre_ymix);
   return cudaGetLastError();
 }
 

@@ -56,7 +56,9 @@ cudaError_t launch_rates(int batch, int nz, const VbRateTables& t, const double*
                          double* k, double* dkdT, cudaStream_t st);
 cudaError_t launch_atm_refresh(int batch, int nz, int ni, const VbRefreshParams& p, const double* pico,
                                const double* mol_mass, const int32_t* esc, const double* y, const double* ymix,
-                               double* atm, double* mu, double* Hp, double* dz, double* zco, cudaStream_t st);
+                               double* atm, double* mu, double* Hp, double* dz, double* zco,
+                               const VbLoopScalars* loop_st, int update_frq, const VbConvState* conv,
+                               cudaStream_t st);
 cudaError_t launch_conden_rates(int batch, int nz, int ni, int nr, int n_re, const int32_t* re_idx,
                                 const int32_t* sp_idx, const double* coeff, const double* Dg, const double* sat,
                                 const double* y, double* k, cudaStream_t st);
@@ -76,7 +78,8 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
                              const double* atom_ini, const double* atm, const uint8_t* fix_mask,
                              const double* fix_y, const double* sol, const double* delta, double* y,
                              double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
-                             double* dt, VbLoopScalars* st, const VbConvState* conv, cudaStream_t stream);
+                             double* dt, VbLoopScalars* st, const VbConvState* conv, double* pre_y,
+                             double* pre_ymix, cudaStream_t stream);
 cudaError_t launch_loop_conv(const Batch& B, const VbConvParams& p, const double* atm, const double* slope_min,
                              const uint8_t* ignore, const double* y, const double* ymix, const VbLoopScalars* st,
                              double* ring_y, double* ring_t, VbConvState* conv, int32_t* photo_due,

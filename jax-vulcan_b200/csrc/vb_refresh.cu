@@ -1,6 +1,7 @@
 // Atmosphere refresh and condensation (reference atm_refresh.py, conden.py).
 //
-// refresh_kernel (CTA per atmosphere): mean molecular mass per layer, then
+// refresh_kernel (CTA per atmosphere; inside the loop, only the atmospheres
+//   whose taken attempt falls on the refresh cadence): mean molecular mass per layer, then
 //   the hydrostatic integration, a true serial recurrence in z
 //   (zco[j+1] = zco[j] + dz[j]), run by one thread upward from the reference
 //   layer and downward below it; the interface means and the escape fluxes
@@ -27,8 +28,14 @@ __global__ void __launch_bounds__(REFRESH_THREADS)
 refresh_kernel(int nz, int ni, VbRefreshParams p, const double* __restrict__ pico, const double* __restrict__ mol_mass,
                const int32_t* __restrict__ esc, const double* __restrict__ y, const double* __restrict__ ymix,
                double* __restrict__ atm, double* __restrict__ mu_o, double* __restrict__ Hp_o,
-               double* __restrict__ dz_o, double* __restrict__ zco_o) {
+               double* __restrict__ dz_o, double* __restrict__ zco_o, const VbLoopScalars* __restrict__ st,
+               int update_frq, const VbConvState* __restrict__ conv) {
   extern __shared__ double sm[];
+  if (st) {   // inside the loop: taken attempts on the refresh cadence only (outer_loop.py:813-818)
+    const VbLoopScalars s = st[blockIdx.x];
+    const bool done = conv && conv[blockIdx.x].done;
+    if (done || s.last_decision == 0 || (s.accept_count - 1) % update_frq != 0) return;
+  }
   double* mu = sm;            // [nz]
   double* g = mu + nz;        // [nz]
   double* Hp = g + nz;        // [nz]
@@ -162,13 +169,16 @@ relax_kernel(int nz, int ni, VbRelaxParams p, const double* __restrict__ Dg, con
 
 cudaError_t launch_atm_refresh(int batch, int nz, int ni, const VbRefreshParams& p, const double* pico,
                                const double* mol_mass, const int32_t* esc, const double* y, const double* ymix,
-                               double* atm, double* mu, double* Hp, double* dz, double* zco, cudaStream_t st) {
+                               double* atm, double* mu, double* Hp, double* dz, double* zco,
+                               const VbLoopScalars* loop_st, int update_frq, const VbConvState* conv,
+                               cudaStream_t st) {
   const size_t smem = (5 * (size_t)nz + 1) * sizeof(double);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(refresh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  refresh_kernel<<<batch, REFRESH_THREADS, smem, st>>>(nz, ni, p, pico, mol_mass, esc, y, ymix, atm, mu, Hp, dz, zco);
+  refresh_kernel<<<batch, REFRESH_THREADS, smem, st>>>(nz, ni, p, pico, mol_mass, esc, y, ymix, atm, mu, Hp, dz, zco,
+                                                       loop_st, update_frq, conv);
   return cudaGetLastError();
 }
 

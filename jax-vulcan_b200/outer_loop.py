@@ -205,8 +205,10 @@ class LoopState:
 
 
 def loop_body(state: LoopState, sol, delta_arr, atm_blob, compo, atom_ini, statics: LoopStatics,
-              gas_mask=None, fix_mask=None, fix_y=None, zoff=None, stream=None):
-    """One body update of every atmosphere after a step (device, in place)."""
+              gas_mask=None, fix_mask=None, fix_y=None, zoff=None, stream=None, pre=None):
+    """One body update of every atmosphere after a step (device, in place).
+    ``pre`` (optional pair of [B, nz, ni] tensors) receives the clipped state
+    of taken attempts, the input of the loop's atmosphere refresh."""
     B, nz, ni = state.y.shape
     compo = as_device(compo).contiguous()
     n_atoms = compo.shape[1]
@@ -222,8 +224,8 @@ def loop_body(state: LoopState, sol, delta_arr, atm_blob, compo, atom_ini, stati
         B, nz, ni, _lib.ptr(zoff), C.addressof(p), _lib.ptr(atm_blob), _lib.ptr(gm), _lib.ptr(compo),
         _lib.ptr(atom_ini), _lib.ptr(fm), _lib.ptr(fy), _lib.ptr(sol), _lib.ptr(delta_arr), _lib.ptr(state.y),
         _lib.ptr(state.y_prev), _lib.ptr(state.ymix), _lib.ptr(state.atom_loss), _lib.ptr(state.atom_loss_prev),
-        _lib.ptr(state.dt), _lib.ptr(state.scalars), _lib.ptr(state.conv), _lib.stream_handle(stream)),
-        "vb_loop_body")
+        _lib.ptr(state.dt), _lib.ptr(state.scalars), _lib.ptr(state.conv), _lib.ptr(pre[0] if pre else None),
+        _lib.ptr(pre[1] if pre else None), _lib.stream_handle(stream)), "vb_loop_body")
 
 
 def loop_converge(state: LoopState, atm_blob, statics: ConvStatics, slope_min, ignore_mask=None, zoff=None,
@@ -256,11 +258,19 @@ class AdaptiveRunner:
     rewrites their photolysis rows of ``k`` in place and their actinic-flux
     change; ``dz`` [B, nz] or [nz] is the layer thickness of the photo grid
     and ``photo_carry`` (a ``photo.PhotoCarry``) the photo fields of the
-    carry."""
+    carry.
+
+    With ``refresh`` (an ``atm_refresh.AtmRefreshStatic``), every taken
+    attempt whose pre-increment accept count is a multiple of ``update_frq``
+    refreshes the atmosphere from the attempt's clipped state (reference
+    `outer_loop.py:813-840`): g, dzi, Hpi and the escape fluxes go into the
+    packed atmosphere the next step reads, and ``self.dz`` (the photo grid)
+    follows the refreshed layer thicknesses."""
 
     def __init__(self, net: NetworkArrays, atm: AtmStatic, statics: LoopStatics, compo, atom_ini,
                  batch: int | None = None, gas_mask=None, conv: ConvStatics | None = None, slope_min=1e-8,
-                 ignore_mask=None, photo=None, dz=None, flux_atol=1.0, photo_carry=None):
+                 ignore_mask=None, photo=None, dz=None, flux_atol=1.0, photo_carry=None, refresh=None,
+                 update_frq: int = 1):
         if photo is not None and (conv is None or not conv.use_photo):
             raise ValueError("the photo branch needs ConvStatics with use_photo")
         self.photo = photo
@@ -280,6 +290,25 @@ class AdaptiveRunner:
         if photo is not None:
             from .photo import PhotoCarry
             self.photo_carry = photo_carry if photo_carry is not None else PhotoCarry(photo, B, nz)
+        self.refresh = refresh
+        self.update_frq = int(update_frq)
+        if refresh is not None:
+            if update_frq < 1:
+                raise ValueError("update_frq must be >= 1")
+            self.pre = (torch.empty((B, nz, ni), dtype=torch.float64, device="cuda"),
+                        torch.empty((B, nz, ni), dtype=torch.float64, device="cuda"))
+            self.mu = torch.empty((B, nz), dtype=torch.float64, device="cuda")
+            self.Hp = torch.empty_like(self.mu)
+            if self.dz is None:
+                self.dz = torch.zeros((B, nz), dtype=torch.float64, device="cuda")
+            else:
+                self.dz = self.dz.reshape(-1, nz).expand(B, nz).contiguous().clone()
+            self.zco = torch.empty((B, nz + 1), dtype=torch.float64, device="cuda")
+            pico = as_device(refresh.pico).reshape(-1, nz + 1)
+            self.pico = pico.expand(B, nz + 1).contiguous()
+            self.mol_mass = as_device(refresh.mol_mass)
+            self.esc = as_device(np.asarray(refresh.diff_esc_idx, np.int32), torch.int32)
+            self.refresh_params = refresh.params()
 
     def start(self, state: LoopState):
         """Gives ``state`` its convergence carry (first attempt photo-due
@@ -299,7 +328,16 @@ class AdaptiveRunner:
                          flux_atol=self.flux_atol, conv=state.conv, stream=stream)
         self.step(state.y, k, state.dt, fix_mask=fix_mask, out=(self.sol, self.delta), stream=stream)
         loop_body(state, self.sol, self.delta, self.step.blob, self.compo, self.atom_ini, self.statics,
-                  gas_mask=self.gas_mask, fix_mask=fix_mask, fix_y=fix_y, stream=stream)
+                  gas_mask=self.gas_mask, fix_mask=fix_mask, fix_y=fix_y, stream=stream,
+                  pre=self.pre if self.refresh is not None else None)
+        if self.refresh is not None:
+            B, nz, ni = state.y.shape
+            _lib.check(_lib.lib().vb_loop_refresh(
+                B, nz, ni, C.addressof(self.refresh_params), self.update_frq, _lib.ptr(state.scalars),
+                _lib.ptr(state.conv), _lib.ptr(self.pico), _lib.ptr(self.mol_mass),
+                _lib.ptr(self.esc) if self.esc.numel() else None, _lib.ptr(self.pre[0]), _lib.ptr(self.pre[1]),
+                _lib.ptr(self.step.blob), _lib.ptr(self.mu), _lib.ptr(self.Hp), _lib.ptr(self.dz),
+                _lib.ptr(self.zco), _lib.stream_handle(stream)), "vb_loop_refresh")
         if self.conv is not None:
             loop_converge(state, self.step.blob, self.conv, self.slope_min, self.ignore_mask, stream=stream)
 

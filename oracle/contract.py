@@ -146,6 +146,7 @@ def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partia
     dt_force = step_size(p["dt_min"], delta, rtol, p["dt_var_min"], p["dt_var_max"], p["dt_min"], p["dt_max"])
     out.update(dt=float(dt_force if force else (dt_norm if accept else next_reject)), rtol=rtol, loss_criteria=lc)
     out["_accept"], out["_force"] = accept, force
+    out["_sol_clip"], out["_ymix_new"] = sol_clip, ymix_new   # the refresh's inputs (outer_loop.py:818-826)
     return out
 
 

@@ -159,8 +159,64 @@ def test_loop_body_rejects_bad_arguments():
     import ctypes as C
     dummy = C.c_void_p(16)  # never dereferenced: argument checks come first
     rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, None, None, dummy, dummy,
-                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None)
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None, None, None)
     assert rc == 1 and b"n_atoms" in L.vb_last_error()
     rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, dummy, None, dummy, dummy,
-                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None)
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None, None, None)
     assert rc == 1 and b"fix_mask" in L.vb_last_error()
+
+
+def test_loop_refresh_matches_oracle_chain():
+    """The atmosphere refresh inside the loop (reference `outer_loop.py:813-840`):
+    ten attempts with a refresh on every second taken attempt (pre-increment
+    accept count divisible by 2) from the attempt's clipped state, g, dzi,
+    Hpi and two species' escape fluxes (floored at -max_flux) written into
+    the atmosphere the next step reads; against the oracle chain of the same
+    attempts. Decisions equal; y and the refreshed fields within 1e-9
+    relative (the step bound carried through the chain)."""
+    from oracle import refresh as orf
+    ar = load_pkg("atm_refresh")
+    case = syn.make_case(seed=41, ni=12, n_fwd=30, nz=10, mild=True, k_range=(-40.0, 4.0), moldiff=True,
+                         fluxes=True)
+    tables, extra = case.net.tables, case.extra
+    compo = case.net.compo
+    y0 = case.y
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * (1 + 1e-7)
+    al0 = (np.einsum("zi,ia->a", y0, compo) - atom_ini) / atom_ini
+    ymix0 = y0 / y0.sum(axis=1, keepdims=True)
+    esc, max_flux = np.array([0, 3]), 1e6
+    st = ar.AtmRefreshStatic(pico=extra["pico"], mol_mass=case.net.ms, diff_esc_idx=esc, pref_indx=0, zco_pref=0.0,
+                             gs=syn.GS, Rp=syn.RP, max_flux=max_flux)
+    p = oc_params()
+    runner = loop.AdaptiveRunner(chem.to_device(tables), jstep.atm_from_dict(case.atm), loop.LoopStatics(**p), compo,
+                                 atom_ini, conv=loop.ConvStatics(conv_step=4, count_min=10 ** 6), refresh=st,
+                                 update_frq=2, dz=extra["dz"])
+    state = loop.LoopState(y0[None], ymix0[None], 1e-8, al0[None], rtol=0.2)
+    atm = dict(case.atm)
+    s = dict(y=y0, y_prev=y0, ymix=ymix0, dt=1e-8, t=0.0, delta=0.0, atom_loss=al0, atom_loss_prev=al0,
+             small_y=0.0, nega_y=0.0, rtol=0.2, loss_criteria=1e-3, accept_count=0, retry_count=0, nega_count=0,
+             loss_count=0, delta_count=0)
+    refreshed = 0
+    for a in range(10):
+        s = oc.attempt(s, case.k, atm, tables, compo, atom_ini, dict(p, use_adapt_rtol=False))
+        take = s["_accept"] or s["_force"]
+        if take and (s["accept_count"] - 1) % 2 == 0:
+            mu, g, Hp, dz, zco, dzi, Hpi = orf.update_mu_dz(s["_ymix_new"], atm["Tco"], extra["pico"], case.net.ms,
+                                                            0, 0.0, syn.GS, syn.RP, st.kb, st.Navo)
+            tf = orf.update_phi_esc(s["_sol_clip"], g, Hp, atm["top_flux"], atm["Tco"], atm["Dzz"][-1], atm["ms"],
+                                    esc, st.kb, st.Navo, max_flux)
+            atm.update(g=g, dzi=dzi, Hpi=Hpi, top_flux=tf)
+            refreshed += 1
+            last_dz = dz
+        runner.attempt(state, case.k[None])
+        dec = int(state.scalars_host()["last_decision"][0])
+        assert dec == (2 if s["_force"] else (1 if s["_accept"] else 0)), (a, dec)
+    assert refreshed >= 4
+    got = state.snapshot()
+    assert np.max(np.abs(got["y"][0] - s["y"]) / np.maximum(np.abs(s["y"]), 1e-30)) <= 1e-9
+    f = ar.blob_fields(runner.step.blob, 10, 12)
+    for name in ("g", "dzi", "Hpi", "top_flux"):
+        ref = np.asarray(atm[name])
+        e = np.max(np.abs(f[name][0].cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-300))
+        assert e <= 1e-9, (name, e)
+    assert np.max(np.abs(runner.dz[0].cpu().numpy() - last_dz) / np.abs(last_dz)) <= 1e-9
