@@ -262,15 +262,16 @@ class AdaptiveRunner:
 
     With ``refresh`` (an ``atm_refresh.AtmRefreshStatic``), every taken
     attempt whose pre-increment accept count is a multiple of ``update_frq``
-    refreshes the atmosphere from the attempt's clipped state (reference
-    `outer_loop.py:813-840`): g, dzi, Hpi and the escape fluxes go into the
+    (default 100, the reference's `update_frq`) refreshes the atmosphere from
+    the attempt's clipped state (reference `outer_loop.py:813-840`): g, dzi,
+    Hpi and the escape fluxes go into the
     packed atmosphere the next step reads, and ``self.dz`` (the photo grid)
     follows the refreshed layer thicknesses."""
 
     def __init__(self, net: NetworkArrays, atm: AtmStatic, statics: LoopStatics, compo, atom_ini,
                  batch: int | None = None, gas_mask=None, conv: ConvStatics | None = None, slope_min=1e-8,
                  ignore_mask=None, photo=None, dz=None, flux_atol=1.0, photo_carry=None, refresh=None,
-                 update_frq: int = 1):
+                 update_frq: int = 100):
         if photo is not None and (conv is None or not conv.use_photo):
             raise ValueError("the photo branch needs ConvStatics with use_photo")
         self.photo = photo
