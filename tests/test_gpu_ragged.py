@@ -76,3 +76,76 @@ def test_multi_network_batch_and_graph_replay():
         torch.cuda.synchronize()
         for (s, d, st), (s0, d0) in zip(batch.results(), eager):
             assert torch.equal(s, s0) and torch.equal(d, d0) and int(st) == 0
+
+
+def test_loop_body_and_convergence_on_a_ragged_batch():
+    """vb_loop_body and vb_loop_converge with zoff: atmospheres of 12, 7 and
+    10 layers packed by layers in one launch (state, rings and records at
+    per-atmosphere offsets) equal the same atmospheres run alone, bit for
+    bit."""
+    import ctypes as C
+    loop = load_pkg("outer_loop")
+    _lib = load_pkg("_lib")
+    L = _lib.lib()
+    net = syn.make_network(51, 30, 185)
+    dn = chem.to_device(net.tables)
+    ni = net.tables.ni
+    nzs = [12, 7, 10]
+    cases = [syn.make_case(seed=(560 + b,), net=net, nz=nz, mild=True, k_range=(-40.0, 4.0), moldiff=True)
+             for b, nz in enumerate(nzs)]
+    dts = np.array([1e-6, 3e-6, 1e-7])
+    rstep = jstep.RaggedRos2Step(dn, [jstep.atm_from_dict(c.atm) for c in cases])
+    y, k = rstep.pack([c.y for c in cases], [c.k for c in cases])
+    sol, delta, status = rstep(y, k, torch.as_tensor(dts, device="cuda"))
+    compo = net.compo
+    na = compo.shape[1]
+    atom_ini = np.stack([np.einsum("zi,ia->a", c.y, compo) * (1 + 1e-7) for c in cases])
+    al0 = np.stack([(np.einsum("zi,ia->a", c.y, compo) - atom_ini[b]) / atom_ini[b] for b, c in enumerate(cases)])
+    ymix = [c.y / c.y.sum(axis=1, keepdims=True) for c in cases]
+    Y, YP = y.clone(), y.clone()
+    X = torch.as_tensor(np.concatenate(ymix), device="cuda").contiguous()
+    DT = torch.as_tensor(dts, device="cuda").clone()
+    AL = torch.as_tensor(al0, device="cuda").contiguous()
+    ALP = AL.clone()
+    rec = np.zeros(3, loop.SCALARS_DTYPE)
+    rec["rtol"], rec["loss_criteria"] = 0.05, 1e-3
+    SC = torch.from_numpy(rec.view(np.uint8).copy()).cuda()
+    p = loop.LoopStatics().params(na)
+    compo_d = torch.as_tensor(compo, device="cuda")
+    ini_d = torch.as_tensor(atom_ini, device="cuda")
+    sh = _lib.stream_handle()
+    assert L.vb_loop_body(3, rstep.nz_max, ni, rstep.zoff.data_ptr(), C.addressof(p), rstep.blob.data_ptr(), None,
+                          compo_d.data_ptr(), ini_d.data_ptr(), None, None, sol.data_ptr(), delta.data_ptr(),
+                          Y.data_ptr(), YP.data_ptr(), X.data_ptr(), AL.data_ptr(), ALP.data_ptr(), DT.data_ptr(),
+                          SC.data_ptr(), None, None, None, sh) == 0
+    cs = 4
+    cp = loop.ConvStatics(conv_step=cs).params()
+    ring_y = torch.zeros((rstep.layers * cs, ni), dtype=torch.float64, device="cuda")
+    ring_t = torch.zeros((3, cs), dtype=torch.float64, device="cuda")
+    crec = np.zeros(3, loop.CONV_DTYPE)
+    crec["longdy"], crec["longdydt"], crec["longdy_seen_min"] = 1.0, 1.0, np.inf
+    CV = torch.from_numpy(crec.view(np.uint8).copy()).cuda()
+    sm = torch.full((3,), 1e-8, dtype=torch.float64, device="cuda")
+    assert L.vb_loop_converge(3, rstep.nz_max, ni, rstep.zoff.data_ptr(), C.addressof(cp), rstep.blob.data_ptr(),
+                              sm.data_ptr(), None, Y.data_ptr(), X.data_ptr(), SC.data_ptr(), ring_y.data_ptr(),
+                              ring_t.data_ptr(), CV.data_ptr(), None, sh) == 0
+    torch.cuda.synchronize()
+    z = rstep.zoff_host
+    sc_all = SC.cpu().numpy().view(loop.SCALARS_DTYPE)
+    cv_all = CV.cpu().numpy().view(loop.CONV_DTYPE)
+    for b, c in enumerate(cases):
+        step1 = jstep.Ros2Step(dn, jstep.atm_from_dict(c.atm))
+        s1, d1, _ = step1(c.y, c.k, dts[b])
+        st1 = loop.LoopState(c.y[None], ymix[b][None], dts[b], al0[b][None], rtol=0.05)
+        loop.loop_body(st1, s1.reshape(1, *c.y.shape), d1.reshape(1, *c.y.shape), step1.blob, compo, atom_ini[b],
+                       loop.LoopStatics())
+        st1.enable_convergence(cs)
+        loop.loop_converge(st1, step1.blob, loop.ConvStatics(conv_step=cs), 1e-8)
+        torch.cuda.synchronize()
+        sl = slice(int(z[b]), int(z[b + 1]))
+        assert torch.equal(Y[sl], st1.y[0]) and torch.equal(YP[sl], st1.y_prev[0]) and torch.equal(X[sl], st1.ymix[0]), b
+        assert torch.equal(AL[b], st1.atom_loss[0]) and torch.equal(DT[b], st1.dt[0]), b
+        assert sc_all[b].tobytes() == st1.scalars_host()[0].tobytes(), b
+        assert cv_all[b].tobytes() == st1.conv_host()[0].tobytes(), b
+        rs = slice(int(z[b]) * cs, int(z[b + 1]) * cs)
+        assert torch.equal(ring_y[rs].reshape(cs, -1, ni), st1.ring_y[0]) and torch.equal(ring_t[b], st1.ring_t[0]), b
