@@ -217,13 +217,14 @@ typedef struct VbConvState {
  * has done set are skipped. pre_y, pre_ymix [B][nz][ni] (nullable, together):
  * for an accepted or force-accepted attempt, the attempt's clipped state
  * (sol_clip and ymix_new, outer_loop.py:740), the input of the atmosphere
- * refresh (vb_loop_refresh). */
+ * refresh (vb_loop_refresh) and the condensation (vb_loop_condense). pre_td
+ * [B][2] (nullable): the attempt's start time t and step dt. */
 int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopParams* params,
                  const double* atm, const uint8_t* gas_mask, const double* compo, const double* atom_ini,
                  const uint8_t* fix_mask, const double* fix_y, const double* sol, const double* delta_arr,
                  double* y, double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
                  double* dt, VbLoopScalars* scalars, const VbConvState* conv, double* pre_y, double* pre_ymix,
-                 void* stream);
+                 double* pre_td, void* stream);
 
 /* Convergence part of the adaptive runner, after vb_loop_body: writes (y, t)
  * into ring slot max(accept_count - 1, 0) % conv_step (outer_loop.py:918-928),
@@ -372,6 +373,36 @@ int vb_loop_refresh(int batch, int nz, int ni, const VbRefreshParams* params, in
                     const VbLoopScalars* scalars, const VbConvState* conv, const double* pico,
                     const double* mol_mass, const int32_t* esc_idx, const double* pre_y, const double* pre_ymix,
                     double* atm, double* mu, double* Hp, double* dz, double* zco, void* stream);
+/* Condensation inside the adaptive loop (reference outer_loop.py:770-800), after
+ * vb_loop_body (with pre_y, pre_ymix, pre_td) and before vb_loop_refresh:
+ * for each atmosphere whose attempt was taken with a start time t >=
+ * start_conden_time (and that is not done), the condensation rows of k from
+ * the attempt's clipped state (conden.py:55-71), then the H2O and NH3
+ * cold-trap relaxations with the attempt's dt (conden.py:74-160) applied to
+ * that state; for an accepted attempt the hydrostatic rebalance of the body
+ * (outer_loop.py:844-917) is redone from the relaxed state: y, y_prev, ymix,
+ * atom_loss and atom_loss_prev. The fixed-species switch that the reference
+ * couples to the end of the window is not part of it. Device arrays in the
+ * table: re_idx, sp_idx, coeff [n_re]; Dg_re, sat_re [B][n_re][nz];
+ * h2o_Dg, h2o_sat, nh3_Dg, nh3_sat [B][nz] (nullable when inactive). */
+typedef struct VbCondenLoop {
+  int32_t n_re, h2o_active, h2o_sp, h2o_l_s, nh3_active, nh3_sp, nh3_l_s, nh3_conden_top;
+  double start_conden_time, h2o_m_over_rho_r2, nh3_m_over_rho_r2;
+  const int32_t* re_idx;
+  const int32_t* sp_idx;
+  const double* coeff;
+  const double* Dg_re;
+  const double* sat_re;
+  const double* h2o_Dg;
+  const double* h2o_sat;
+  const double* nh3_Dg;
+  const double* nh3_sat;
+} VbCondenLoop;
+int vb_loop_condense(int batch, int nz, int ni, int nr, const VbCondenLoop* conden, const VbLoopParams* params,
+                     const double* atm, const uint8_t* gas_mask, const double* compo, const double* atom_ini,
+                     const VbLoopScalars* scalars, const VbConvState* conv, const double* pre_td, double* pre_y,
+                     double* pre_ymix, double* y, double* y_prev, double* ymix, double* atom_loss,
+                     double* atom_loss_prev, double* k, void* stream);
 /* Condensation rates (reference conden.py:55-71): rate = Dg coeff (y[sp] -
  * sat_n) for each condensation reaction r; k[re_idx[r]] = max(rate, 0),
  * k[re_idx[r] + 1] = max(-rate, 0). Dg, sat_n [B][n_re][nz], coeff [n_re],

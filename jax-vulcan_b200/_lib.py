@@ -60,7 +60,8 @@ SIGNATURES = {
     "vb_bt_mixed_bytes": (_sz, [_i, _i, _i]),
     "vb_bt_factor_mixed": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _p]),
     "vb_bt_solve_mixed": (_i, [_i, _i, _i, _p, _p, _p, _i, C.c_double, _p, _p, _p]),
-    "vb_loop_body": (_i, [_i, _i, _i] + [_p] * 21),
+    "vb_loop_body": (_i, [_i, _i, _i] + [_p] * 22),
+    "vb_loop_condense": (_i, [_i, _i, _i, _i] + [_p] * 18),
     "vb_loop_converge": (_i, [_i, _i, _i] + [_p] * 13),
 }
 

@@ -7,6 +7,9 @@ layers at or below ``nh3_conden_top`` and clips the condensate), keeping the
 reference names. ``CondenStatic`` holds the reference's static fields as
 device tensors (batched: Dg and saturation arrays [B, ...]); the total
 density n_0 and the gas mask are read from the packed atmosphere.
+``CondenStatic.loop_table`` gives the ``VbCondenLoop`` table with which
+``outer_loop.AdaptiveRunner(conden=...)`` runs condensation inside the loop
+(``vb_loop_condense``, reference `outer_loop.py:770-800`).
 """
 from __future__ import annotations
 
@@ -18,6 +21,15 @@ import torch
 
 from . import _lib
 from .chem import as_device
+
+
+class VbCondenLoop(C.Structure):
+    """Mirror of ``VbCondenLoop`` in include/vulcan_b200.h."""
+    _fields_ = [(n, C.c_int32) for n in ("n_re", "h2o_active", "h2o_sp", "h2o_l_s", "nh3_active", "nh3_sp",
+                                         "nh3_l_s", "nh3_conden_top")] + \
+               [(n, C.c_double) for n in ("start_conden_time", "h2o_m_over_rho_r2", "nh3_m_over_rho_r2")] + \
+               [(n, C.c_void_p) for n in ("re_idx", "sp_idx", "coeff", "Dg_re", "sat_re", "h2o_Dg", "h2o_sat",
+                                          "nh3_Dg", "nh3_sat")]
 
 
 class VbRelaxParams(C.Structure):
@@ -50,6 +62,42 @@ class CondenStatic:
     nh3_sat: object = None
     nh3_m_over_rho_r2: float = 0.0
     nh3_conden_top: int = 0
+    start_conden_time: float = 0.0
+
+    def loop_table(self, batch: int, nz: int):
+        """The ``VbCondenLoop`` table (device copies kept on the object)."""
+        keep = self.__dict__.setdefault("_keep", {})
+        re = np.asarray(self.conden_re_idx, np.int32)
+        n_re = int(re.size)
+        t = VbCondenLoop()
+        t.n_re = n_re
+        t.start_conden_time = float(self.start_conden_time)
+
+        def dev(name, x, dtype=torch.float64, shape=None):
+            a = as_device(np.asarray(x) if not torch.is_tensor(x) else x, dtype)
+            if shape is not None:
+                a = a.reshape(shape).contiguous()
+            keep[name] = a
+            return a.data_ptr() if a.numel() else None
+
+        if n_re:
+            t.re_idx = dev("re_idx", re, torch.int32)
+            t.sp_idx = dev("sp_idx", np.asarray(self.conden_sp_idx, np.int32), torch.int32)
+            t.coeff = dev("coeff", self.coeff_per_re)
+            t.Dg_re = dev("Dg_re", self.Dg_per_re, shape=(batch, n_re, nz))
+            t.sat_re = dev("sat_re", self.sat_n_per_re, shape=(batch, n_re, nz))
+        if self.h2o_active:
+            t.h2o_active, t.h2o_sp, t.h2o_l_s = 1, int(self.h2o_idx), int(self.h2o_l_s_idx)
+            t.h2o_m_over_rho_r2 = float(self.h2o_m_over_rho_r2)
+            t.h2o_Dg = dev("h2o_Dg", self.h2o_Dg, shape=(batch, nz))
+            t.h2o_sat = dev("h2o_sat", self.h2o_sat, shape=(batch, nz))
+        if self.nh3_active:
+            t.nh3_active, t.nh3_sp, t.nh3_l_s = 1, int(self.nh3_idx), int(self.nh3_l_s_idx)
+            t.nh3_conden_top = int(self.nh3_conden_top)
+            t.nh3_m_over_rho_r2 = float(self.nh3_m_over_rho_r2)
+            t.nh3_Dg = dev("nh3_Dg", self.nh3_Dg, shape=(batch, nz))
+            t.nh3_sat = dev("nh3_sat", self.nh3_sat, shape=(batch, nz))
+        return t
 
 
 def update_conden_rates(k_arr, y, st: CondenStatic, stream=None):

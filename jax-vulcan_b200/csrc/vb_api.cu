@@ -617,6 +617,29 @@ int vb_conden_relax(int batch, int nz, int ni, const VbRelaxParams* params, cons
   return VB_OK;
 }
 
+int vb_loop_condense(int batch, int nz, int ni, int nr, const VbCondenLoop* conden, const VbLoopParams* params,
+                     const double* atm, const uint8_t* gas_mask, const double* compo, const double* atom_ini,
+                     const VbLoopScalars* scalars, const VbConvState* conv, const double* pre_td, double* pre_y,
+                     double* pre_ymix, double* y, double* y_prev, double* ymix, double* atom_loss,
+                     double* atom_loss_prev, double* k, void* stream) {
+  if (!conden || !params || !atm || !compo || !atom_ini || !scalars || !pre_td || !pre_y || !pre_ymix || !y ||
+      !y_prev || !ymix || !atom_loss || !atom_loss_prev || !k)
+    return fail(VB_ERR_ARG, "null argument");
+  const VbCondenLoop& c = *conden;
+  if (batch < 1 || nz < 1 || ni < 1 || ni > VB_MAX_NI || nr < 2 || c.n_re < 0)
+    return fail(VB_ERR_ARG, "bad shape");
+  if (params->n_atoms < 1 || params->n_atoms > VB_LOOP_MAX_ATOMS) return fail(VB_ERR_ARG, "n_atoms must be in [1, 16]");
+  if (c.n_re > 0 && (!c.re_idx || !c.sp_idx || !c.coeff || !c.Dg_re || !c.sat_re))
+    return fail(VB_ERR_ARG, "condensation rows need re_idx, sp_idx, coeff, Dg_re and sat_re");
+  if ((c.h2o_active && (!c.h2o_Dg || !c.h2o_sat)) || (c.nh3_active && (!c.nh3_Dg || !c.nh3_sat)))
+    return fail(VB_ERR_ARG, "an active relaxation needs its Dg and saturation arrays");
+  VB_CHECK(vb::launch_loop_condense(batch, nz, ni, nr, c, *params, atm, gas_mask, compo, atom_ini, scalars, conv,
+                                    pre_td, pre_y, pre_ymix, y, y_prev, ymix, atom_loss, atom_loss_prev, k,
+                                    (cudaStream_t)stream),
+           "loop condensation");
+  return VB_OK;
+}
+
 int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream) {
   if (!out || blocks < 1 || threads < 32 || iters < 1) return fail(VB_ERR_ARG, "bad probe arguments");
   VB_CHECK(vb::launch_fp64_probe(out, blocks, threads, iters, (cudaStream_t)stream), "fp64 probe");
@@ -627,7 +650,7 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
                  const uint8_t* gas_mask, const double* compo, const double* atom_ini, const uint8_t* fix_mask,
                  const double* fix_y, const double* sol, const double* delta_arr, double* y, double* y_prev,
                  double* ymix, double* atom_loss, double* atom_loss_prev, double* dt, VbLoopScalars* scalars,
-                 const VbConvState* conv, double* pre_y, double* pre_ymix, void* stream) {
+                 const VbConvState* conv, double* pre_y, double* pre_ymix, double* pre_td, void* stream) {
   if ((pre_y == nullptr) != (pre_ymix == nullptr)) return fail(VB_ERR_ARG, "pre_y and pre_ymix go together");
   if (!params || !atm || !compo || !atom_ini || !sol || !delta_arr || !y || !y_prev || !ymix || !atom_loss ||
       !atom_loss_prev || !dt || !scalars)
@@ -646,7 +669,7 @@ int vb_loop_body(int batch, int nz, int ni, const int64_t* zoff, const VbLoopPar
   B.ld = vb::round_even(ni);
   B.zoff = zoff;
   VB_CHECK(vb::launch_loop_body(B, p, gas_mask, compo, atom_ini, atm, fix_mask, fix_y, sol, delta_arr, y, y_prev,
-                                ymix, atom_loss, atom_loss_prev, dt, scalars, conv, pre_y, pre_ymix,
+                                ymix, atom_loss, atom_loss_prev, dt, scalars, conv, pre_y, pre_ymix, pre_td,
                                 (cudaStream_t)stream),
            "loop body");
   return VB_OK;

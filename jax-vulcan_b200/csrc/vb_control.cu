@@ -73,7 +73,7 @@ loop_body_kernel(Batch B, VbLoopParams p, const uint8_t* __restrict__ gas, const
                  double* y, double* y_prev, double* ymix,  // may alias one another (y == y_prev)
                  double* __restrict__ atom_loss, double* __restrict__ atom_loss_prev, double* __restrict__ dtp,
                  VbLoopScalars* __restrict__ st, const VbConvState* __restrict__ conv, double* __restrict__ pre_y,
-                 double* __restrict__ pre_ymix) {
+                 double* __restrict__ pre_ymix, double* __restrict__ pre_td) {
   extern __shared__ double ys[];  // [2][nz]: ysum of the clipped and of the rebalanced state
   __shared__ double red[BODY_WARPS][4 + 2 * VB_LOOP_MAX_ATOMS];
   __shared__ int flags_s[BODY_WARPS][2];
@@ -196,6 +196,10 @@ loop_body_kernel(Batch B, VbLoopParams p, const uint8_t* __restrict__ gas, const
     }
     VbLoopScalars s = st[b];
     const double dt = dtp[b];
+    if (pre_td) {   // the attempt's start time and step, which condensation reads
+      pre_td[2 * (int64_t)b] = s.t;
+      pre_td[2 * (int64_t)b + 1] = dt;
+    }
     double* alb = atom_loss + (int64_t)b * na;
     double* alp = atom_loss_prev + (int64_t)b * na;
     const double* ini = atom_ini + (int64_t)b * na;
@@ -310,7 +314,7 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
                              const double* fix_y, const double* sol, const double* delta, double* y,
                              double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
                              double* dt, VbLoopScalars* st, const VbConvState* conv, double* pre_y,
-                             double* pre_ymix, cudaStream_t stream) {
+                             double* pre_ymix, double* pre_td, cudaStream_t stream) {
   ElemIn E;
   E.sol = sol;
   E.delta = delta;
@@ -327,7 +331,7 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
   }
   loop_body_kernel<<<B.count, BODY_THREADS, smem, stream>>>(B, p, gas, compo, atom_ini, atm, E, y, y_prev, ymix,
                                                             atom_loss, atom_loss_prev, dt, st, conv, pre_y,
-                                                            pre_ymix);
+                                                            pre_ymix, pre_td);
   return cudaGetLastError();
 }
 

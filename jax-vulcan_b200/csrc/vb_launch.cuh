@@ -79,7 +79,12 @@ cudaError_t launch_loop_body(const Batch& B, const VbLoopParams& p, const uint8_
                              const double* fix_y, const double* sol, const double* delta, double* y,
                              double* y_prev, double* ymix, double* atom_loss, double* atom_loss_prev,
                              double* dt, VbLoopScalars* st, const VbConvState* conv, double* pre_y,
-                             double* pre_ymix, cudaStream_t stream);
+                             double* pre_ymix, double* pre_td, cudaStream_t stream);
+cudaError_t launch_loop_condense(int batch, int nz, int ni, int nr, const VbCondenLoop& c, const VbLoopParams& p,
+                                 const double* atm, const uint8_t* gas, const double* compo, const double* atom_ini,
+                                 const VbLoopScalars* st, const VbConvState* conv, const double* pre_td,
+                                 double* pre_y, double* pre_ymix, double* y, double* y_prev, double* ymix,
+                                 double* atom_loss, double* atom_loss_prev, double* k, cudaStream_t stream);
 cudaError_t launch_loop_conv(const Batch& B, const VbConvParams& p, const double* atm, const double* slope_min,
                              const uint8_t* ignore, const double* y, const double* ymix, const VbLoopScalars* st,
                              double* ring_y, double* ring_t, VbConvState* conv, int32_t* photo_due,

@@ -118,6 +118,46 @@ __global__ void conden_rates_kernel(int nz, int ni, int nr, int n_re, const int3
   kb[(int64_t)(re_idx[r] + 1) * nz + z] = neg;
 }
 
+// One layer of the cold-trap relaxation of one species (conden.py:74-160),
+// by one warp: lane 0 forms the scalar updates of the species and its
+// condensate, every lane re-projects y = ymix * (gas sum of y before the
+// update) over the row.
+__device__ inline void relax_layer(int lane, int j, int ni, const VbRelaxParams& p, double Dg, double s, double n0,
+                                   const double* gasm, double dt, double* yr, double* xr) {
+  const int sp = p.sp, ls = p.sp_l_s;
+  double ysum = 0.0, x_sp = 0.0, x_ls = 0.0;
+  if (lane == 0) {
+    ysum = pairwise_sum_masked(yr, gasm, ni);
+    double denom = Dg * p.m_over_rho_r2 * (yr[sp] - s);
+    if (fabs(denom) < 1e-300) denom = 1e-300;
+    const double tau = 1.0 / denom;
+    const double sat_mix = s / n0;
+    const double y_conden = (xr[sp] + dt / tau * sat_mix) / (1.0 + dt / tau);
+    double ice = (yr[sp] - s) * dt / tau;
+    ice = fmin(yr[ls], ice);
+    bool conden = tau > 0.0;
+    if (p.conden_top >= 0) conden = conden && (j <= p.conden_top);
+    const double dc = conden ? xr[sp] - y_conden : 0.0;
+    const double de = tau < 0.0 ? ice / n0 : 0.0;
+    x_ls = xr[ls] + dc;
+    x_sp = xr[sp] + (-dc);
+    x_sp = x_sp + de;
+    x_ls = x_ls + (-de);
+    if (p.conden_top >= 0) x_ls = fmax(x_ls, 0.0);
+  }
+  ysum = __shfl_sync(0xffffffffu, ysum, 0);
+  x_sp = __shfl_sync(0xffffffffu, x_sp, 0);
+  x_ls = __shfl_sync(0xffffffffu, x_ls, 0);
+  for (int i = lane; i < ni; i += 32) {
+    double x = xr[i];
+    if (i == sp) x = x_sp;
+    if (i == ls) x = x_ls;
+    xr[i] = x;
+    yr[i] = x * ysum;
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(RELAX_THREADS)
 relax_kernel(int nz, int ni, VbRelaxParams p, const double* __restrict__ Dg, const double* __restrict__ sat,
              const double* __restrict__ atm, const double* __restrict__ dtp, double* __restrict__ y,
@@ -127,43 +167,109 @@ relax_kernel(int nz, int ni, VbRelaxParams p, const double* __restrict__ Dg, con
   const AtmOff off = atm_offsets(nz, ni);
   const double* A = atm + (int64_t)b * VB_ATM_DOUBLES(nz, ni);
   const double dt = dtp[b];
-  const int sp = p.sp, ls = p.sp_l_s;
-  for (int j = warp; j < nz; j += RELAX_THREADS / 32) {
-    double* yr = y + ((int64_t)b * nz + j) * ni;
-    double* xr = ymix + ((int64_t)b * nz + j) * ni;
-    double ysum = 0.0, x_sp = 0.0, x_ls = 0.0;
-    if (lane == 0) {
-      ysum = pairwise_sum_masked(yr, A + off.gas, ni);
-      const double n0 = A[off.M + j];
-      const double s = sat[(int64_t)b * nz + j];
-      double denom = Dg[(int64_t)b * nz + j] * p.m_over_rho_r2 * (yr[sp] - s);
-      if (fabs(denom) < 1e-300) denom = 1e-300;
-      const double tau = 1.0 / denom;
-      const double sat_mix = s / n0;
-      const double y_conden = (xr[sp] + dt / tau * sat_mix) / (1.0 + dt / tau);
-      double ice = (yr[sp] - s) * dt / tau;
-      ice = fmin(yr[ls], ice);
-      bool conden = tau > 0.0;
-      if (p.conden_top >= 0) conden = conden && (j <= p.conden_top);
-      const double dc = conden ? xr[sp] - y_conden : 0.0;
-      const double de = tau < 0.0 ? ice / n0 : 0.0;
-      x_ls = xr[ls] + dc;
-      x_sp = xr[sp] + (-dc);
-      x_sp = x_sp + de;
-      x_ls = x_ls + (-de);
-      if (p.conden_top >= 0) x_ls = fmax(x_ls, 0.0);
+  for (int j = warp; j < nz; j += RELAX_THREADS / 32)
+    relax_layer(lane, j, ni, p, Dg[(int64_t)b * nz + j], sat[(int64_t)b * nz + j], A[off.M + j], A + off.gas, dt,
+                y + ((int64_t)b * nz + j) * ni, ymix + ((int64_t)b * nz + j) * ni);
+}
+
+// Condensation inside the adaptive loop (outer_loop.py:770-800), CTA per
+// atmosphere: the condensation rows of k from the attempt's clipped state,
+// the H2O and NH3 relaxations of that state with the attempt's dt, and for
+// an accepted attempt the hydrostatic rebalance of the body redone from the
+// relaxed state (the same per-element expressions as loop_body_kernel).
+__global__ void __launch_bounds__(RELAX_THREADS)
+loop_condense_kernel(int nz, int ni, int nr, VbCondenLoop c, VbLoopParams p, const double* __restrict__ atm,
+                     const uint8_t* __restrict__ gas, const double* __restrict__ compo,
+                     const double* __restrict__ atom_ini, const VbLoopScalars* __restrict__ st,
+                     const VbConvState* __restrict__ conv, const double* __restrict__ pre_td,
+                     double* __restrict__ pre_y, double* __restrict__ pre_ymix,
+                     double* y, double* y_prev, double* ymix,   // may alias one another (y == y_prev)
+                     double* __restrict__ atom_loss, double* __restrict__ atom_loss_prev, double* __restrict__ k) {
+  constexpr int W = RELAX_THREADS / 32;
+  __shared__ double red[W][VB_LOOP_MAX_ATOMS];
+  const int b = blockIdx.x;
+  if (conv && conv[b].done) return;                                   // the body left it alone
+  const int dec = st[b].last_decision;
+  if (dec == 0 || !(pre_td[2 * (int64_t)b] >= c.start_conden_time)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const AtmOff off = atm_offsets(nz, ni);
+  const double* A = atm + (int64_t)b * VB_ATM_DOUBLES(nz, ni);
+  const double* M = A + off.M;
+  const double dt = pre_td[2 * (int64_t)b + 1];
+  double* py = pre_y + (int64_t)b * nz * ni;
+  double* px = pre_ymix + (int64_t)b * nz * ni;
+  // condensation rows of k (conden.py:55-71) from the clipped state
+  double* kb = k + (int64_t)b * (nr + 1) * nz;
+  for (int e = threadIdx.x; e < c.n_re * nz; e += RELAX_THREADS) {
+    const int r = e / nz, z = e - r * nz;
+    const int64_t o = ((int64_t)b * c.n_re + r) * nz + z;
+    const double rate = c.Dg_re[o] * c.coeff[r] * (py[(int64_t)z * ni + c.sp_idx[r]] - c.sat_re[o]);
+    kb[(int64_t)c.re_idx[r] * nz + z] = (rate != rate) ? rate : fmax(rate, 0.0);
+    kb[(int64_t)(c.re_idx[r] + 1) * nz + z] = (rate != rate) ? rate : fmax(-rate, 0.0);
+  }
+  __syncthreads();   // the rates read the clipped state before the relaxation rewrites it
+  // H2O, then NH3 (conden.py:74-160)
+  for (int j = warp; j < nz; j += W) {
+    double* yr = py + (int64_t)j * ni;
+    double* xr = px + (int64_t)j * ni;
+    if (c.h2o_active) {
+      VbRelaxParams q{c.h2o_sp, c.h2o_l_s, -1, 0, c.h2o_m_over_rho_r2};
+      relax_layer(lane, j, ni, q, c.h2o_Dg[(int64_t)b * nz + j], c.h2o_sat[(int64_t)b * nz + j], M[j], A + off.gas,
+                  dt, yr, xr);
     }
-    ysum = __shfl_sync(0xffffffffu, ysum, 0);
-    x_sp = __shfl_sync(0xffffffffu, x_sp, 0);
-    x_ls = __shfl_sync(0xffffffffu, x_ls, 0);
+    if (c.nh3_active) {
+      VbRelaxParams q{c.nh3_sp, c.nh3_l_s, c.nh3_conden_top, 0, c.nh3_m_over_rho_r2};
+      relax_layer(lane, j, ni, q, c.nh3_Dg[(int64_t)b * nz + j], c.nh3_sat[(int64_t)b * nz + j], M[j], A + off.gas,
+                  dt, yr, xr);
+    }
+  }
+  if (dec != 1) return;   // a force-accepted attempt keeps y_prev (outer_loop.py:903-906)
+  __syncthreads();
+  // hydrostatic rebalance from the relaxed state (outer_loop.py:846-853, 899-917)
+  const bool hydro = (p.flags & VB_LOOP_HYDRO_PARTIAL) != 0;
+  const int na = p.n_atoms;
+  double pb[VB_LOOP_MAX_ATOMS];
+#pragma unroll
+  for (int a = 0; a < VB_LOOP_MAX_ATOMS; ++a) pb[a] = 0.0;
+  double* yb = y + (int64_t)b * nz * ni;
+  double* ypb = y_prev + (int64_t)b * nz * ni;
+  double* xb = ymix + (int64_t)b * nz * ni;
+  for (int j = warp; j < nz; j += W) {
+    double bs = 0.0;
     for (int i = lane; i < ni; i += 32) {
-      double x = xr[i];
-      if (i == sp) x = x_sp;
-      if (i == ls) x = x_ls;
-      xr[i] = x;
-      yr[i] = x * ysum;
+      const bool gi = !gas || gas[i];
+      const double bv = (hydro && !gi) ? py[(int64_t)j * ni + i] : M[j] * px[(int64_t)j * ni + i];
+      if (gi) bs += bv;
+      yb[(int64_t)j * ni + i] = bv;
+      ypb[(int64_t)j * ni + i] = bv;
+#pragma unroll
+      for (int a = 0; a < VB_LOOP_MAX_ATOMS; ++a)
+        if (a < na) pb[a] += compo[i * na + a] * bv;
     }
+#pragma unroll
+    for (int off2 = 16; off2 > 0; off2 >>= 1) bs += __shfl_xor_sync(0xffffffffu, bs, off2);
     __syncwarp();
+    for (int i = lane; i < ni; i += 32) xb[(int64_t)j * ni + i] = yb[(int64_t)j * ni + i] / bs;
+  }
+#pragma unroll
+  for (int a = 0; a < VB_LOOP_MAX_ATOMS; ++a) {
+    if (a < na) {
+#pragma unroll
+      for (int off2 = 16; off2 > 0; off2 >>= 1) pb[a] += __shfl_xor_sync(0xffffffffu, pb[a], off2);
+    }
+  }
+  if (lane == 0)
+    for (int a = 0; a < na; ++a) red[warp][a] = pb[a];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int a = 0; a < na; ++a) {
+      double sb = red[0][a];
+      for (int w = 1; w < W; ++w) sb += red[w][a];
+      const double ini = atom_ini[(int64_t)b * na + a];
+      const double al = (sb - ini) / ini;
+      atom_loss[(int64_t)b * na + a] = al;
+      atom_loss_prev[(int64_t)b * na + a] = al;
+    }
   }
 }
 
@@ -197,4 +303,17 @@ cudaError_t launch_conden_relax(int batch, int nz, int ni, const VbRelaxParams& 
   return cudaGetLastError();
 }
 
+}  // namespace vb
+
+namespace vb {
+cudaError_t launch_loop_condense(int batch, int nz, int ni, int nr, const VbCondenLoop& c, const VbLoopParams& p,
+                                 const double* atm, const uint8_t* gas, const double* compo, const double* atom_ini,
+                                 const VbLoopScalars* st, const VbConvState* conv, const double* pre_td,
+                                 double* pre_y, double* pre_ymix, double* y, double* y_prev, double* ymix,
+                                 double* atom_loss, double* atom_loss_prev, double* k, cudaStream_t stream) {
+  loop_condense_kernel<<<batch, RELAX_THREADS, 0, stream>>>(nz, ni, nr, c, p, atm, gas, compo, atom_ini, st, conv,
+                                                            pre_td, pre_y, pre_ymix, y, y_prev, ymix, atom_loss,
+                                                            atom_loss_prev, k);
+  return cudaGetLastError();
+}
 }  // namespace vb

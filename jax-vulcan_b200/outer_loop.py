@@ -207,8 +207,9 @@ class LoopState:
 def loop_body(state: LoopState, sol, delta_arr, atm_blob, compo, atom_ini, statics: LoopStatics,
               gas_mask=None, fix_mask=None, fix_y=None, zoff=None, stream=None, pre=None):
     """One body update of every atmosphere after a step (device, in place).
-    ``pre`` (optional pair of [B, nz, ni] tensors) receives the clipped state
-    of taken attempts, the input of the loop's atmosphere refresh."""
+    ``pre`` (optional (pre_y, pre_ymix[, pre_td]) tensors) receives the
+    clipped state of taken attempts (and each attempt's start time and
+    step), the input of the loop's condensation and refresh."""
     B, nz, ni = state.y.shape
     compo = as_device(compo).contiguous()
     n_atoms = compo.shape[1]
@@ -225,7 +226,8 @@ def loop_body(state: LoopState, sol, delta_arr, atm_blob, compo, atom_ini, stati
         _lib.ptr(atom_ini), _lib.ptr(fm), _lib.ptr(fy), _lib.ptr(sol), _lib.ptr(delta_arr), _lib.ptr(state.y),
         _lib.ptr(state.y_prev), _lib.ptr(state.ymix), _lib.ptr(state.atom_loss), _lib.ptr(state.atom_loss_prev),
         _lib.ptr(state.dt), _lib.ptr(state.scalars), _lib.ptr(state.conv), _lib.ptr(pre[0] if pre else None),
-        _lib.ptr(pre[1] if pre else None), _lib.stream_handle(stream)), "vb_loop_body")
+        _lib.ptr(pre[1] if pre else None), _lib.ptr(pre[2] if pre and len(pre) > 2 else None),
+        _lib.stream_handle(stream)), "vb_loop_body")
 
 
 def loop_converge(state: LoopState, atm_blob, statics: ConvStatics, slope_min, ignore_mask=None, zoff=None,
@@ -271,7 +273,7 @@ class AdaptiveRunner:
     def __init__(self, net: NetworkArrays, atm: AtmStatic, statics: LoopStatics, compo, atom_ini,
                  batch: int | None = None, gas_mask=None, conv: ConvStatics | None = None, slope_min=1e-8,
                  ignore_mask=None, photo=None, dz=None, flux_atol=1.0, photo_carry=None, refresh=None,
-                 update_frq: int = 100):
+                 update_frq: int = 100, conden=None):
         if photo is not None and (conv is None or not conv.use_photo):
             raise ValueError("the photo branch needs ConvStatics with use_photo")
         self.photo = photo
@@ -293,11 +295,17 @@ class AdaptiveRunner:
             self.photo_carry = photo_carry if photo_carry is not None else PhotoCarry(photo, B, nz)
         self.refresh = refresh
         self.update_frq = int(update_frq)
+        self.conden = conden
+        if refresh is not None or conden is not None:
+            self.pre = (torch.empty((B, nz, ni), dtype=torch.float64, device="cuda"),
+                        torch.empty((B, nz, ni), dtype=torch.float64, device="cuda"),
+                        torch.empty((B, 2), dtype=torch.float64, device="cuda"))
+        if conden is not None:
+            self.conden_table = conden.loop_table(B, nz)
+            self.gas_mask_d = None if gas_mask is None else as_device(np.asarray(gas_mask, np.uint8), torch.uint8)
         if refresh is not None:
             if update_frq < 1:
                 raise ValueError("update_frq must be >= 1")
-            self.pre = (torch.empty((B, nz, ni), dtype=torch.float64, device="cuda"),
-                        torch.empty((B, nz, ni), dtype=torch.float64, device="cuda"))
             self.mu = torch.empty((B, nz), dtype=torch.float64, device="cuda")
             self.Hp = torch.empty_like(self.mu)
             if self.dz is None:
@@ -330,7 +338,20 @@ class AdaptiveRunner:
         self.step(state.y, k, state.dt, fix_mask=fix_mask, out=(self.sol, self.delta), stream=stream)
         loop_body(state, self.sol, self.delta, self.step.blob, self.compo, self.atom_ini, self.statics,
                   gas_mask=self.gas_mask, fix_mask=fix_mask, fix_y=fix_y, stream=stream,
-                  pre=self.pre if self.refresh is not None else None)
+                  pre=self.pre if (self.refresh is not None or self.conden is not None) else None)
+        if self.conden is not None:
+            if not (isinstance(k, torch.Tensor) and k.is_cuda and k.dtype == torch.float64 and k.is_contiguous()):
+                raise TypeError("with condensation, k must be a contiguous float64 CUDA tensor (updated in place)")
+            B, nz, ni = state.y.shape
+            p = self.statics.params(self.compo.shape[1])
+            ini = self.atom_ini.reshape(-1, self.compo.shape[1])
+            ini = (ini.expand(B, -1) if ini.shape[0] == 1 else ini).contiguous()
+            _lib.check(_lib.lib().vb_loop_condense(
+                B, nz, ni, k.shape[1] - 1, C.addressof(self.conden_table), C.addressof(p), _lib.ptr(self.step.blob),
+                _lib.ptr(self.gas_mask_d), _lib.ptr(self.compo), _lib.ptr(ini), _lib.ptr(state.scalars),
+                _lib.ptr(state.conv), _lib.ptr(self.pre[2]), _lib.ptr(self.pre[0]), _lib.ptr(self.pre[1]),
+                _lib.ptr(state.y), _lib.ptr(state.y_prev), _lib.ptr(state.ymix), _lib.ptr(state.atom_loss),
+                _lib.ptr(state.atom_loss_prev), _lib.ptr(k), _lib.stream_handle(stream)), "vb_loop_condense")
         if self.refresh is not None:
             B, nz, ni = state.y.shape
             _lib.check(_lib.lib().vb_loop_refresh(

@@ -74,7 +74,7 @@ def mix_from_y(y, gas=None):
 
 
 def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partial=False,
-                zero_bot_row=False, fix_mask=None, fix_y=None):
+                zero_bot_row=False, fix_mask=None, fix_y=None, conden=None):
     """State after one attempt of the reference loop body given the step's
     (sol, delta_arr): fixed species (`outer_loop.py:733-739`), clip, atom loss,
     error norm (`:741-743`), accept / force-accept (`:745-756`), reject
@@ -107,6 +107,16 @@ def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partia
     too_big = bool(delta > rtol)
     any_neg = bool(np.any(sol_clip < 0))
     t_next = s["t"] + (p["dt_min"] if force else s["dt"]) if do_acc else s["t"]
+
+    # condensation (outer_loop.py:770-800): on a taken attempt inside the time
+    # window, ``conden(sol_clip, ymix_new, dt)`` (the relaxation of
+    # conden.py:74-160 with the attempt's dt) replaces the clipped state
+    # before the hydrostatic rebalance; the caller rewrites the condensation
+    # rows of k from the clipped state before it (``_sol_clip_raw``)
+    sol_clip_raw, fired = sol_clip, False
+    if conden is not None and do_acc and s["t"] >= conden["start_time"]:
+        sol_clip, ymix_new = conden["fn"](sol_clip, ymix_new, s["dt"])
+        fired = True
 
     bal_full = M[:, None] * ymix_new
     if hydro_partial:
@@ -147,6 +157,7 @@ def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partia
     out.update(dt=float(dt_force if force else (dt_norm if accept else next_reject)), rtol=rtol, loss_criteria=lc)
     out["_accept"], out["_force"] = accept, force
     out["_sol_clip"], out["_ymix_new"] = sol_clip, ymix_new   # the refresh's inputs (outer_loop.py:818-826)
+    out["_sol_clip_raw"], out["_conden_fired"] = sol_clip_raw, fired
     return out
 
 

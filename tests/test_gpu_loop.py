@@ -159,10 +159,10 @@ def test_loop_body_rejects_bad_arguments():
     import ctypes as C
     dummy = C.c_void_p(16)  # never dereferenced: argument checks come first
     rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, None, None, dummy, dummy,
-                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None, None, None)
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None, None, None, None)
     assert rc == 1 and b"n_atoms" in L.vb_last_error()
     rc = L.vb_loop_body(2, 10, 12, None, C.addressof(p), dummy, None, dummy, dummy, dummy, None, dummy, dummy,
-                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None, None, None)
+                        dummy, dummy, dummy, dummy, dummy, dummy, dummy, None, None, None, None, None)
     assert rc == 1 and b"fix_mask" in L.vb_last_error()
 
 
@@ -220,3 +220,62 @@ def test_loop_refresh_matches_oracle_chain():
         e = np.max(np.abs(f[name][0].cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-300))
         assert e <= 1e-9, (name, e)
     assert np.max(np.abs(runner.dz[0].cpu().numpy() - last_dz) / np.abs(last_dz)) <= 1e-9
+
+
+def test_loop_condensation_matches_oracle_chain():
+    """Condensation inside the loop (reference `outer_loop.py:770-800`): eight
+    accepted attempts, each inside the time window, so each rewrites the
+    condensation rows of k (here a photolysis row, unused with photochemistry
+    off) from the attempt's clipped state and relaxes species 1 toward
+    saturation into species 2 with the attempt's dt, before the hydrostatic
+    rebalance; against the oracle chain with the same hook. The relaxation
+    moves the state by 3-25 % per attempt. Decisions equal; y, ymix and the
+    atom losses within 1e-9, the condensation rows within 1e-9 relative."""
+    from oracle import refresh as orf
+    cd = load_pkg("conden")
+    case = syn.make_case(seed=43, ni=12, n_fwd=30, nz=10, mild=True, k_range=(-40.0, 4.0), moldiff=True, n_photo=2)
+    tables, compo, y0, atm = case.net.tables, case.net.compo, case.y, dict(case.atm)
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * (1 + 1e-7)
+    al0 = (np.einsum("zi,ia->a", y0, compo) - atom_ini) / atom_ini
+    ymix0 = y0 / y0.sum(axis=1, keepdims=True)
+    rng = np.random.default_rng(43)
+    nz = 10
+    sat = y0[:, 1] * rng.uniform(0.5, 1.5, nz)
+    Dg = 10 ** rng.uniform(-2, 1, nz)
+    row = case.net.photo_branches[0][2]
+    re_idx, sp_idx, coeff = np.array([row]), np.array([3]), np.array([1e-30])
+    Dg_re = 10 ** rng.uniform(-2, 1, (1, nz))
+    sat_re = y0[:, 3][None] * rng.uniform(0.5, 1.5, (1, nz))
+    m = 1e-2 / (1e-8 * np.max(Dg) * np.max(y0[:, 1]))
+    st = cd.CondenStatic(conden_re_idx=re_idx, conden_sp_idx=sp_idx, Dg_per_re=Dg_re[None], sat_n_per_re=sat_re[None],
+                         coeff_per_re=coeff, atm_blob=None, h2o_active=True, h2o_idx=1, h2o_l_s_idx=2,
+                         h2o_Dg=Dg[None], h2o_sat=sat[None], h2o_m_over_rho_r2=m, start_conden_time=0.0)
+    p = oc_params()
+    runner = loop.AdaptiveRunner(chem.to_device(tables), jstep.atm_from_dict(atm), loop.LoopStatics(**p), compo,
+                                 atom_ini, conv=loop.ConvStatics(conv_step=4, count_min=10 ** 6), conden=st)
+    state = loop.LoopState(y0[None], ymix0[None], 1e-8, al0[None], rtol=0.2)
+    k = torch.as_tensor(case.k[None], device="cuda").contiguous()
+    fn = lambda y, x, dt: orf.apply_relax(y, x, dt, 1, 2, Dg, sat, m, atm["M"], atm["gas_indx_mask"])  # noqa: E731
+    s = dict(y=y0, y_prev=y0, ymix=ymix0, dt=1e-8, t=0.0, delta=0.0, atom_loss=al0, atom_loss_prev=al0,
+             small_y=0.0, nega_y=0.0, rtol=0.2, loss_criteria=1e-3, accept_count=0, retry_count=0, nega_count=0,
+             loss_count=0, delta_count=0)
+    k_o = case.k.copy()
+    fired = 0
+    for a in range(8):
+        s = oc.attempt(s, k_o, atm, tables, compo, atom_ini, dict(p, use_adapt_rtol=False),
+                       conden=dict(start_time=0.0, fn=fn))
+        if s["_conden_fired"]:
+            k_o = orf.update_conden_rates(k_o, s["_sol_clip_raw"], re_idx, sp_idx, Dg_re, sat_re, coeff)
+            fired += 1
+        runner.attempt(state, k)
+        dec = int(state.scalars_host()["last_decision"][0])
+        assert dec == (2 if s["_force"] else (1 if s["_accept"] else 0)), (a, dec)
+    assert fired == 8
+    got = state.snapshot()
+    for f in ("y", "ymix", "y_prev"):
+        e = np.max(np.abs(got[f][0] - s[f]) / np.maximum(np.abs(s[f]), 1e-30))
+        assert e <= 1e-9, (f, e)
+    assert np.max(np.abs(got["atom_loss"][0] - s["atom_loss"])) <= 1e-9
+    kd = k[0].cpu().numpy()
+    for r in (row, row + 1):
+        assert np.max(np.abs(kd[r] - k_o[r]) / np.maximum(np.abs(k_o[r]), 1e-300)) <= 1e-9, r

@@ -117,7 +117,7 @@ def test_loop_body_and_convergence_on_a_ragged_batch():
     assert L.vb_loop_body(3, rstep.nz_max, ni, rstep.zoff.data_ptr(), C.addressof(p), rstep.blob.data_ptr(), None,
                           compo_d.data_ptr(), ini_d.data_ptr(), None, None, sol.data_ptr(), delta.data_ptr(),
                           Y.data_ptr(), YP.data_ptr(), X.data_ptr(), AL.data_ptr(), ALP.data_ptr(), DT.data_ptr(),
-                          SC.data_ptr(), None, None, None, sh) == 0
+                          SC.data_ptr(), None, None, None, None, sh) == 0
     cs = 4
     cp = loop.ConvStatics(conv_step=cs).params()
     ring_y = torch.zeros((rstep.layers * cs, ni), dtype=torch.float64, device="cuda")
