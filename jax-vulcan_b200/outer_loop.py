@@ -187,6 +187,42 @@ class LoopState:
     def conv_host(self) -> np.ndarray:
         return self.conv.cpu().numpy().view(CONV_DTYPE)
 
+    _FIELDS = ("y", "y_prev", "ymix", "dt", "atom_loss", "atom_loss_prev", "scalars", "conv", "ring_y", "ring_t",
+               "photo_due")
+
+    def save(self, path, **extra):
+        """Checkpoint of the carry (and of any device tensors the run owns,
+        given by name: k, the packed atmosphere, the photo carry, dz) to one
+        ``.npz``; ``load`` restores it bit for bit, so a run continues as if
+        it had not stopped."""
+        arrays = {}
+        for f in self._FIELDS:
+            t = getattr(self, f, None)
+            if t is not None:
+                arrays["state_" + f] = t.detach().cpu().numpy()
+        arrays["state_y_prev_is_y"] = np.array(self.y_prev is self.y)
+        if self.conv is not None:
+            arrays["state_conv_step"] = np.array(self.conv_step)
+        for name, t in extra.items():
+            arrays["extra_" + name] = t.detach().cpu().numpy() if torch.is_tensor(t) else np.asarray(t)
+        np.savez(path, **arrays)
+
+    @classmethod
+    def load(cls, path):
+        """(state, extras) from a ``save`` checkpoint: the state's tensors and
+        the named extras on the current CUDA device."""
+        d = np.load(path)
+        st = cls.__new__(cls)
+        for f in cls._FIELDS:
+            key = "state_" + f
+            setattr(st, f, torch.from_numpy(d[key].copy()).cuda() if key in d else None)
+        if bool(d["state_y_prev_is_y"]):
+            st.y_prev = st.y
+        if "state_conv_step" in d:
+            st.conv_step = int(d["state_conv_step"])
+        extras = {k[len("extra_"):]: torch.from_numpy(d[k].copy()).cuda() for k in d.files if k.startswith("extra_")}
+        return st, extras
+
     @property
     def batch(self) -> int:
         return self.y.shape[0]

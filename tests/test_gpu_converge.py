@@ -242,3 +242,62 @@ def test_loop_reaches_the_known_steady_state():
     y = state.y.cpu().numpy()[0]
     assert rel(y, g["chain_y"]) <= 1e-5, (y, g["chain_y"])
     assert rel(y[:, 0], np.full(nz, 2.0)) <= 1e-2 and rel(y[:, 1], np.full(nz, 10.0 / 3.0)) <= 1e-2
+
+
+def test_checkpoint_resume_is_bit_exact(tmp_path):
+    """Checkpoint and resume of the device loop: a run with photochemistry
+    and convergence stops after 6 attempts, is saved (carry, records, rings,
+    photo-due flags, k, the packed atmosphere, the photo carry), and a fresh
+    runner that loads the checkpoint continues 6 attempts to the same bits
+    as the original run continuing without a stop."""
+    photo = load_pkg("photo")
+    syn = load_pkg("synthetic")
+    net = syn.make_network(7, 30, 185, n_photo=10)
+    case = syn.make_case(seed=7, net=net, nz=12, mild=True, k_range=(-20.0, -2.0))
+    bins, din12 = syn.make_bins(bin_max=402.0)
+    ph = dict(syn.make_photo(7, net, case.atm["Tco"], bins, din12), f_diurnal=1e-3)
+    compo, y0 = net.compo, case.y
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * (1 + 1e-7)
+    al0 = (np.einsum("zi,ia->a", y0, compo) - atom_ini) / atom_ini
+    ymix0 = y0 / y0.sum(axis=1, keepdims=True)
+    body = dict(loss_eps=0.1, pos_cut=0.0, nega_cut=-1.0, mtol=1e-22, atol=0.1, dt_var_min=0.5, dt_var_max=2.0,
+                dt_min=1e-14, dt_max=1e4, batch_max_retries=8, rtol_min=0.02, rtol_max=1.0,
+                adapt_rtol_dec_period=5, adapt_rtol_inc_period=10, adapt_rtol_dec=0.5, adapt_rtol_inc=1.5,
+                adapt_rtol_loss_mul=10.0, adapt_rtol_inc_loss_thresh=1e-3)
+    cs = loop.ConvStatics(conv_step=4, count_min=10 ** 6, use_photo=True, ini_update_photo_frq=3,
+                          final_update_photo_frq=2, photo_switch_longdy=1e300, photo_switch_longdydt=1e300)
+
+    def make_runner():
+        return loop.AdaptiveRunner(chem.to_device(net.tables), jstep.atm_from_dict(case.atm),
+                                   loop.LoopStatics(**body), compo, atom_ini, conv=cs, slope_min=1e-8,
+                                   photo=photo.PhotoDevice(ph, 12), dz=case.extra["dz"], flux_atol=1.0)
+
+    carry_fields = ("tau", "aflux", "sflux", "dflux_d", "dflux_u", "J_br", "J_br_T")
+    ra = make_runner()
+    sa = loop.LoopState(y0[None], ymix0[None], 1e-6, al0[None], rtol=0.05)
+    ra.start(sa)
+    ka = torch.as_tensor(case.k[None], device="cuda").contiguous()
+    for _ in range(6):
+        ra.attempt(sa, ka)
+    path = tmp_path / "loop.npz"
+    sa.save(path, k=ka, blob=ra.step.blob, **{f: getattr(ra.photo_carry, f) for f in carry_fields})
+    for _ in range(6):
+        ra.attempt(sa, ka)
+    torch.cuda.synchronize()
+
+    rb = make_runner()
+    sb, extra = loop.LoopState.load(path)
+    kb = extra["k"].contiguous()
+    rb.step.blob.copy_(extra["blob"])
+    for f in carry_fields:
+        getattr(rb.photo_carry, f).copy_(extra[f])
+    for _ in range(6):
+        rb.attempt(sb, kb)
+    torch.cuda.synchronize()
+    for f in ("y", "y_prev", "ymix", "dt", "atom_loss", "atom_loss_prev", "scalars", "conv", "ring_y", "ring_t",
+              "photo_due"):
+        assert torch.equal(getattr(sa, f), getattr(sb, f)), f
+    assert torch.equal(ka, kb)
+    for f in carry_fields:
+        assert torch.equal(getattr(ra.photo_carry, f), getattr(rb.photo_carry, f)), f
+    assert int(sa.scalars_host()["accept_count"][0]) >= 8
