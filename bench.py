@@ -713,7 +713,7 @@ def main():
 
     peak64 = fp64_peak_tflops(L, torch, sh)
     ni, nz = net.tables.ni, Y.shape[1]
-    # LU with partial pivoting + inverse of every layer block: 2*ni^3 flops counted
+    # Gauss-Jordan inverse of every layer block: ni^3 FMAs = 2*ni^3 flops counted
     fac_flops = B * nz * 2.0 * ni ** 3
     fac_ms = per_kernel["factor"]["ms_per_launch"]
     achieved = fac_flops / (fac_ms * 1e-3) / 1e12 if fac_ms > 0 else 0.0
@@ -753,8 +753,8 @@ def main():
                             "step i-1's results come down while the steps compute); rates and atmosphere stay "
                             "resident (as in the reference runner's device carry)"},
             "gpu_launches": 6 * args.steps,
-            "roofline": {"bound": "fp64", "kernel": "factor (LU with partial pivoting + inverse of each "
-                                                    "layer block, serial in z, one CTA per atmosphere)",
+            "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan inverse with partial pivoting of "
+                                                    "each layer block, serial in z, one CTA per atmosphere)",
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 else None, "traffic": fac_traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one factor "

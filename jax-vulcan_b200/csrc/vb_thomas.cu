@@ -4,39 +4,18 @@
 // factor: for each layer j (serial in z)
 //     A'_j  = D_j - (sub_d[j-1] sup_d[j-1]^T) o A'_{j-1}^{-1}     (solver.py:47)
 //     Inv_j = A'_j^{-1}                                            (solver.py:46,48)
-// Each A'_j is factored by LU with partial pivoting on a register-resident
-// tile (implicit row pivoting: no row exchanges, the factors are stored in
-// pivot order), then inverted column block by column block, one block per
-// warp, by substitution with the factors. The forward sweep of the first
-// right-hand side rides along (solver.py:73-88). The stored inverses turn
-// every later solve into matrix-vector products (solver.py:91-111).
+// Each A'_j is inverted in place by Gauss-Jordan elimination with partial
+// pivoting on a register-resident tile (implicit pivoting: no row exchanges),
+// one serial chain of ni pivot steps per layer with one block barrier each.
+// The forward sweep of the first right-hand side rides along
+// (solver.py:73-88). The stored inverses turn every later solve into
+// matrix-vector products (solver.py:91-111).
 #include <cuda_runtime.h>
 
 #include "vb_common.cuh"
 #include "vb_launch.cuh"
 
 namespace vb {
-
-template <int NP, int NW, int PW, typename R = double>
-struct LUK {
-  static constexpr int RPW = NP / NW;     // rows per warp
-  static constexpr int CPL = NP / 32;     // columns per lane
-  static constexpr int PRL = NP / 32;     // panel rows per lane of the panel warp
-  static constexpr int SLD = NP + 1;      // smem row stride of S (doubles)
-  static constexpr int PLD = PW + 1;      // smem row stride of a panel buffer
-  static constexpr int PBUF = (NP * PLD > RPW * NP) ? NP * PLD : RPW * NP;
-  static_assert(NW * NP <= 2 * PBUF, "partial products of the rhs sweep must fit the panel buffers");
-  static_assert(RPW * CPL * 32 <= NP * PLD + PW * NP, "warp 0's tile must fit Mb..V while it factors a panel");
-  static size_t smem_bytes() {
-    size_t d = (size_t)NP * SLD          // S: LU factors in pivot order
-               + 2 * (size_t)PBUF        // panel buffers / triangular-solve row buffers
-               + (size_t)NP * PLD        // M: update multipliers of the current panel
-               + (size_t)PW * NP         // V: pivot rows of the current panel
-               + 2 * (size_t)NP          // vec, rdiag
-               + PW + PW * PW;           // pivot row broadcast, L_KK^{-1}
-    return d * sizeof(R) + sizeof(int) * 2 * NP;
-  }
-};
 
 // Pivot key of a candidate: |v| as an order-preserving 64-bit pattern (NaN -> 0).
 __device__ __forceinline__ unsigned long long pivot_key(double v) {
@@ -48,423 +27,320 @@ __device__ __forceinline__ unsigned long long pivot_key(float v) {
   return (a >= 0.0f) ? ((unsigned long long)__float_as_uint(a) << 32) : 0ull;
 }
 
+// Correctly rounded reciprocal (the value of 1 / x).
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+
 // Two values of the factor's element type handed over in one shared-memory access.
 template <typename R> struct Pair;
 template <> struct Pair<double> { using T = double2; };
 template <> struct Pair<float> { using T = float2; };
 
-// Unblocked LU of one PW-column panel by one warp (lane l holds rows
-// l + 32 r in registers): for each column the argmax over unpivoted rows
-// (three redux.sync reductions of the 64-bit |v| key, ties to the lowest
-// row), the pivot row broadcast by shuffles, and the rank-1 update of the
-// panel's remaining columns. Kept out of line so its registers do not compete
-// with the caller's tile.
-template <int PRL, int PW, int PLD, typename R>
-__device__ __noinline__ void panel_lu(R* Pn, int n, int k0, int kw, unsigned& usedw_io, int& st_io,
-                                      int* pivs, int* qinv, int lane) {
-  const unsigned FULL = 0xffffffffu;
-  unsigned usedw = usedw_io;
-  int st_local = 0;
-  // the panel in registers: lane l holds rows l + 32 r, all PW columns
-  R pv[PRL][PW];
-#pragma unroll
-  for (int r = 0; r < PRL; ++r) {
-    const int i = lane + 32 * r;
-#pragma unroll
-    for (int u = 0; u < PW; ++u) pv[r][u] = i < n ? Pn[i * PLD + u] : R(0);
+// ---------------------------------------------------------------- Gauss-Jordan factor
+// Shared-memory plan of gj_factor_atmosphere (carved in this order, each
+// piece on a 16-byte boundary).
+template <int RPL, int CPW, int NW, typename R>
+struct GJK {
+  static constexpr int NPR = 32 * RPL;          // row capacity (lane l holds rows l + 32 r)
+  static constexpr int NPC = CPW * NW;          // column capacity (warp w holds columns w*CPW + c)
+  __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
+  static size_t smem_bytes(int n, int ld, bool dpf) {
+    const size_t blk = (size_t)n * ld;
+    return al(blk * sizeof(R))                        // Ib: the inverse of the layer (natural order)
+           + (dpf ? al(blk * sizeof(double)) : 0)     // Db: the next diagonal block, prefetched
+           + al(2 * NPR * sizeof(R))                  // colb: multipliers of the next step (2 parities)
+           + al(NPR * sizeof(R))                      // rps: 1 / pivot of each row
+           + al(2 * NPR * sizeof(double))             // rsb: the next layer's rhs and sub_d rows
+           + al(2 * NPR * sizeof(double))             // vecs: right-hand side ping-pong
+           + al(NPC * sizeof(int))                    // pivs: pivot row of each step
+           + al(2 * sizeof(int))                      // pb: pivot row of the next step (2 parities)
+           + 16;                                      // mbarrier of the prefetch
   }
-#pragma unroll
-  for (int t = 0; t < PW; ++t) {
-    if (t < kw) {
-      unsigned long long bk = 0ull;
-      unsigned brow = 0xffffffffu;
-#pragma unroll
-      for (int r = 0; r < PRL; ++r) {
-        const int i = lane + 32 * r;
-        if (i < n && !((usedw >> r) & 1u)) {
-          unsigned long long kk = pivot_key(pv[r][t]);
-          if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
-        }
-      }
-      const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-      const unsigned m1 = __reduce_max_sync(FULL, hi);
-      const unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
-      const int p = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
-      if ((p & 31) == lane) usedw |= 1u << (p >> 5);
-      // broadcast the pivot row (columns t..PW-1) from its owner lane
-      const int po = p & 31, pslot = p >> 5;
-      R pr[PW];
-#pragma unroll
-      for (int u = t; u < PW; ++u) {
-        R v = pv[0][u];
-#pragma unroll
-        for (int r = 1; r < PRL; ++r) v = (pslot == r) ? pv[r][u] : v;
-        pr[u] = __shfl_sync(FULL, v, po);
-      }
-      const R piv = pr[t];
-      if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
-      const R rcp = R(1) / piv;
-#pragma unroll
-      for (int r = 0; r < PRL; ++r) {
-        const int i = lane + 32 * r;
-        if (i < n && !((usedw >> r) & 1u)) {
-          const R l = pv[r][t] * rcp;
-          pv[r][t] = l;
-#pragma unroll
-          for (int u = t + 1; u < PW; ++u) pv[r][u] = fma(-l, pr[u], pv[r][u]);
-        }
-      }
-      if (lane == 0) { pivs[k0 + t] = p; qinv[p] = k0 + t; }
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < PRL; ++r) {
-    const int i = lane + 32 * r;
-    if (i < n) {
-#pragma unroll
-      for (int u = 0; u < PW; ++u) Pn[i * PLD + u] = pv[r][u];
-    }
-  }
-  usedw_io = usedw;
-  st_io |= st_local;
-}
+};
 
-// Factor all layers of one atmosphere. On entry inv[j] holds D_j (row stride
-// ld); on exit inv[j] holds A'_j^{-1}. With rhs != nullptr the first sweep of
-// the right-hand side rhs[nz][ni] is done in place (solver.py:73-88).
+// Factor all layers of one atmosphere by Gauss-Jordan inversion of each
+// Schur-updated diagonal block. On entry Din[j] holds D_j (row stride ld); on
+// exit out[j] holds A'_j^{-1}; with rhs != nullptr the first sweep of the
+// right-hand side rhs[nz][ni] is done in place (solver.py:73-88).
 //
-// Each diagonal block is inverted as the reference does (solver.py:46-48):
-// LU with partial pivoting (lu_factor), then the inverse by forward and back
-// substitution on the identity (lu_solve(LU, I)).
-//  * LU: blocked right-looking elimination with implicit row pivoting on a
-//    register-resident tile (warp w owns rows w*RPW.., lane l columns l+32c).
-//    Warp 0 factors each PW-column panel (argmax over unpivoted rows by three
-//    redux.sync reductions, pivot row broadcast through shared memory);
-//    every warp then forms U[K, C] = L_KK^{-1} A[P, C] for its columns and
-//    applies the rank-PW update A[R, C] -= L[R, K] U[K, C] to unpivoted rows.
-//  * The factors are stored in pivot order in shared memory; warp w then
-//    solves for the RPW columns w*RPW.. of X = A'^{-1} with warp-synchronous
-//    column-oriented substitution (no block barrier), so X lands in natural
-//    row order.
-template <int NP, int NW, int PW, int MB, typename R>
-__device__ void factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
-                                  const double* __restrict__ supn, const double* __restrict__ subn,
-                                  double* __restrict__ rhs, int32_t* status, char* smem_raw) {
-  using G = LUK<NP, NW, PW, R>;
+// The reference inverts each block by lu_factor then lu_solve(LU, I)
+// (solver.py:46-48). Here the inverse comes from one serial chain of ni
+// Gauss-Jordan steps instead of three (factor, forward and back
+// substitution). The elimination runs on the transposed block A'^T with
+// partial pivoting (so on A' it pivots within a row): the inverse of A'^T
+// then has a small left residual, i.e. X = A'^{-1} has a small right residual
+// |A' X - I| as the reference's lu_solve(LU, I) columns do, which is what the
+// later solves x = X b need (Gauss-Jordan on A' itself only bounds |X A' - I|;
+// on the stiff config-0 draw that left the block solve's normwise backward
+// error at 4e-12 instead of 7e-15).
+//  * Tile in registers: lane l holds rows l + 32 r (r < RPL), warp w columns
+//    w*CPW + c (c < CPW) of A'^T. No row exchanges: row p_k is the pivot row
+//    of step k. Pivot rows are not normalised during the elimination (row i
+//    carries the factor piv_i of its own step), so every element update is
+//    one FMA
+//        S[i][:] -= m_i S[p][:],   m_i = S[i][k] / piv_k  (m_p = 0),
+//    column k becomes -m_i (row p: 1), and each row is scaled by 1/piv_i at
+//    the end. The stored result T satisfies (A'^T)^{-1}[q(i)][p_m] = T[i][m]
+//    (q(i): the step whose pivot row is i), so A'^{-1}[p_m][q(i)] = T[i][m],
+//    applied by the scatter into Ib.
+//  * One block barrier per step. During step k the owner warp of column
+//    k+1 updates that column first, takes its argmax (three redux.sync on the
+//    64-bit |v| key, ties to the lowest row, as LAPACK's idamax), inverts the
+//    pivot and publishes p_{k+1} with the scaled multipliers; the other warps
+//    update meanwhile. A warp takes its part of the pivot row from the owner
+//    lane by shuffles (no block barrier).
+//  * Layer j's Schur update reads Inv_{j-1} from Ib (shared), D_j from Db
+//    (bulk-prefetched during layer j-1) when DPF, else from global memory.
+template <int RPL, int CPW, int NW, bool DPF, typename R>
+__device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
+                                                     const double* __restrict__ supn,
+                                                     const double* __restrict__ subn, double* rhs,
+                                                     int32_t* status, char* smem_raw) {
+  using G = GJK<RPL, CPW, NW, R>;
   using R2 = typename Pair<R>::T;
-  constexpr int RPW = G::RPW, CPL = G::CPL, PRL = G::PRL, SLD = G::SLD, PLD = G::PLD;
-  constexpr int CB = RPW > 8 ? (RPW + 1) / 2 : RPW;   // inverse columns per pass
-  constexpr int NCH = (RPW + CB - 1) / CB;
-  static_assert(CB % 2 == 0, "x_k is handed over in pairs");
-  static_assert(NW * NP + NW * 2 * CB <= 2 * G::PBUF, "broadcast buffers must fit the panel buffers");
-  R* S = reinterpret_cast<R*>(smem_raw);                    // [NP][SLD]
-  R* Pn0 = S + NP * SLD;                                    // [PBUF]
-  R* Pn1 = Pn0 + G::PBUF;                                   // [PBUF]
-  R* Mb = Pn1 + G::PBUF;                                    // [NP][PLD]
-  R* V = Mb + NP * PLD;                                     // [PW][NP]
-  R* vec = V + PW * NP;                                     // [NP]
-  R* rdiag = vec + NP;                                      // [NP]
-  R* prow_s = rdiag + NP;                                   // [PW]
-  R* Linv = prow_s + PW;                                    // [PW][PW]
-  int* pivs = reinterpret_cast<int*>(Linv + PW * PW);       // [NP] pivot row of step k
-  int* qinv = pivs + NP;                                    // [NP] step of row i (-1: not yet)
+  constexpr int NPR = G::NPR;
+  // value of slot s (warp-uniform) of a per-lane row array
+  auto pick = [](const R* v, int s) {
+    R x = v[0];
+#pragma unroll
+    for (int r = 1; r < RPL; ++r) x = (s == r) ? v[r] : x;
+    return x;
+  };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned FULL = 0xffffffffu;
+  const int blk = n * ld;
+  char* sp = smem_raw;
+  auto take = [&](size_t bytes) {
+    char* q = sp;
+    sp += G::al(bytes);
+    return q;
+  };
+  R* Ib = reinterpret_cast<R*>(take((size_t)blk * sizeof(R)));
+  double* Db = DPF ? reinterpret_cast<double*>(take((size_t)blk * sizeof(double))) : nullptr;
+  R* colb = reinterpret_cast<R*>(take(2 * NPR * sizeof(R)));
+  R* rps = reinterpret_cast<R*>(take(NPR * sizeof(R)));
+  double* rsb = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
+  double* vecs = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
+  int* pivs = reinterpret_cast<int*>(take(G::NPC * sizeof(int)));
+  int* pb = reinterpret_cast<int*>(take(2 * sizeof(int)));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(take(16));
+  const uint32_t dbytes = (uint32_t)(blk * sizeof(double));
   int st_local = 0;
 
-  if (rhs) {
-    for (int i = threadIdx.x; i < NP; i += blockDim.x) vec[i] = i < n ? (R)rhs[i] : R(0);
+  for (int e = threadIdx.x; e < blk; e += blockDim.x) Ib[e] = R(0);   // the padding column stays 0
+  if (rhs)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) vecs[i] = rhs[i];
+  if (DPF && threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (DPF && threadIdx.x == 0) {
+    mbar_expect_tx(bar, dbytes);
+    bulk_g2s(Db, Din, dbytes, bar);
   }
-  const int npan = (n + PW - 1) / PW;
 
-  R a[RPW][CPL];
+  // argmax of column kn (values t, already updated) over the unpivoted rows,
+  // run by the warp that owns the column; publishes the pivot and multipliers.
+  // The maximum of the key's high word decides unless two lanes share it.
+  auto publish = [&](const R (&t)[RPL], unsigned used, int kn) {
+    unsigned long long bk = 0ull;
+    unsigned brow = 0xffffffffu;
+    R bv = R(0);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n && !((used >> r) & 1u)) {
+        const unsigned long long kk = pivot_key(t[r]);
+        if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; bv = t[r]; }
+      }
+    }
+    const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+    const unsigned m1 = __reduce_max_sync(FULL, hi);
+    const unsigned tie = __ballot_sync(FULL, hi == m1 && brow != 0xffffffffu);
+    int p1;
+    R piv;
+    if (__popc(tie) == 1) {
+      const int wl = __ffs(tie) - 1;
+      p1 = __shfl_sync(FULL, (int)brow, wl);
+      piv = __shfl_sync(FULL, bv, wl);
+    } else {
+      const unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
+      p1 = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
+      piv = __shfl_sync(FULL, pick(t, p1 >> 5), p1 & 31);
+    }
+    if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
+    const R rp = rcp_rn(piv);
+    R* cb = colb + (kn & 1) * NPR;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int i = lane + 32 * r;
+      cb[i] = (i < n && i != p1) ? t[r] * rp : R(0);
+    }
+    pb[kn & 1] = p1;   // every lane stores the same values
+    pivs[kn] = p1;
+    rps[p1] = rp;
+  };
+
+  R a[RPL][CPW];
   for (int j = 0; j < nz; ++j) {
-    const double* D = Din + (int64_t)j * n * ld;
-    const R* Dp = out + (int64_t)(j > 0 ? j - 1 : 0) * n * ld;   // Inv_{j-1}
-    for (int i = threadIdx.x; i < NP; i += blockDim.x) qinv[i] = -1;
-    // ---- load D_j and apply the Hadamard Schur update from Inv_{j-1} (solver.py:47)
-#pragma unroll
-    for (int r = 0; r < RPW; ++r) {
-      int i = warp * RPW + r;
-#pragma unroll
-      for (int c = 0; c < CPL; ++c) {
-        int col = lane + 32 * c;
-        double v = 0.0;
-        if (i < n && col < n) {
-          v = D[(int64_t)i * ld + col];
-          if (j > 0) {
-            double cb = subn[(int64_t)(j - 1) * n + i] * supn[(int64_t)(j - 1) * n + col];
-            v = v - cb * (double)Dp[(int64_t)i * ld + col];
-          }
+    if (DPF) {
+      const bool ok = mbar_wait(bar, (uint32_t)(j & 1), WAIT_LIMIT);
+      if (__syncthreads_or(!ok)) {
+        // give up: wait (bounded) for the copy still in flight, report, return
+        if (threadIdx.x == 0) {
+          mbar_wait(bar, (uint32_t)(j & 1), WAIT_LIMIT);
+          atomicOr(status, VB_STATUS_WATCHDOG);
         }
-        a[r][c] = (R)v;
+        return;
       }
     }
-    unsigned usedw = 0;     // warp 0: rows lane + 32*r already pivoted
-    // ================================================================ LU
-    for (int pb = 0; pb < npan; ++pb) {
-      const int k0 = pb * PW;
-      const int kw = min(PW, n - k0);
-      R* Pn = (pb & 1) ? Pn1 : Pn0;
-      // (a) owners of the panel columns stage them
+    // the next layer's rhs and sub_d rows, for the forward sweep at the end of the layer
+    double rn = 0.0, sn = 0.0;
+    const bool ride = rhs && j + 1 < nz && (int)threadIdx.x < n;
+    if (ride) {
+      rn = rhs[(int64_t)(j + 1) * n + threadIdx.x];
+      sn = subn[(int64_t)j * n + threadIdx.x];
+    }
+    // ---- D_j and the Hadamard Schur update from Inv_{j-1} (solver.py:47),
+    //      loaded transposed: tile element (i, m) = A'_j[m][i]
+    {
+      const double* D = DPF ? Db : Din + (int64_t)j * blk;
+      double su[RPL], sb[CPW];
 #pragma unroll
-      for (int c = 0; c < CPL; ++c) {
-        int col = lane + 32 * c;
-        if (col >= k0 && col < k0 + PW) {
-#pragma unroll
-          for (int r = 0; r < RPW; ++r) Pn[(warp * RPW + r) * PLD + (col - k0)] = a[r][c];
-        }
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        su[r] = (j > 0 && i < n) ? supn[(int64_t)(j - 1) * n + i] : 0.0;
       }
-      __syncthreads();
-      // (b) warp 0: unblocked LU of the panel (in shared memory) over the
-      //     unpivoted rows, then L_KK^{-1} of its unit lower triangle
-      if (warp == 0) {
-        // warp 0's own tile waits in Mb..V (free until the multipliers and
-        // pivot rows are staged) so the panel has the registers
 #pragma unroll
-        for (int r = 0; r < RPW; ++r)
-#pragma unroll
-          for (int c = 0; c < CPL; ++c) Mb[(r * CPL + c) * 32 + lane] = a[r][c];
-        panel_lu<PRL, PW, PLD, R>(Pn, n, k0, kw, usedw, st_local, pivs, qinv, lane);
-#pragma unroll
-        for (int r = 0; r < RPW; ++r)
-#pragma unroll
-          for (int c = 0; c < CPL; ++c) a[r][c] = Mb[(r * CPL + c) * 32 + lane];
-        __syncwarp();
-        // L_KK^{-1} (unit lower): lane s builds column s from the pivot rows' multipliers
-        if (lane < PW) {
-          const int sc = lane;
-          R li[PW];
-#pragma unroll
-          for (int t = 0; t < PW; ++t) {
-            R x = (t == sc) ? R(1) : R(0);
-            if (t > sc && t < kw) {
-              const R* lrow = Pn + pivs[k0 + t] * PLD;
-#pragma unroll
-              for (int m = 0; m < t; ++m)
-                if (m >= sc) x = fma(-lrow[m], li[m], x);
-            }
-            li[t] = x;
-          }
-#pragma unroll
-          for (int t = 0; t < PW; ++t) Linv[t * PW + sc] = li[t];
-        }
+      for (int c = 0; c < CPW; ++c) {
+        const int m = warp * CPW + c;
+        sb[c] = (j > 0 && m < n) ? subn[(int64_t)(j - 1) * n + m] : 0.0;
       }
-      __syncthreads();
-      // (b') every warp: update multipliers of its own rows. Unpivoted rows
-      //     M = -L[i,K] L_KK^{-1}; pivot row p_t: M = L_KK^{-1}[t,:] - e_t (so
-      //     W + M V = U[t,:]); rows pivoted earlier: 0.
-      for (int e = lane; e < RPW * PW; e += 32) {
-        const int r = e / PW, u = e - r * PW;
-        const int i = warp * RPW + r;
-        const int q = i < n ? qinv[i] : -2;
-        R x = R(0);
-        if (i < n && q < 0) {
-          const R* row = Pn + i * PLD;
 #pragma unroll
-          for (int s2 = 0; s2 < PW; ++s2)
-            if (s2 >= u && s2 < kw) x = fma(-row[s2], Linv[s2 * PW + u], x);
-        } else if (q >= k0 && q < k0 + kw) {
-          const int t = q - k0;
-          x = (u <= t) ? Linv[t * PW + u] - (u == t ? R(1) : R(0)) : R(0);
-        }
-        Mb[i * PLD + u] = x;
-      }
-      // (c) owners of the new pivot rows stage them: V[t] = A[p_t, :]
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) {
-        int i = warp * RPW + r;
-        int q = qinv[i];
-        if (q >= k0 && q < k0 + kw) {
-#pragma unroll
-          for (int c = 0; c < CPL; ++c) V[(q - k0) * NP + lane + 32 * c] = a[r][c];
-        }
-      }
-      __syncthreads();
-      // (d) rank-kw update A[i, C] += M[i, K] V[K, C] (C = columns right of the
-      //     panel): unpivoted rows get the Schur update, pivot rows become
-      //     U[K, C] = L_KK^{-1} V; rows pivoted in earlier panels are final.
-      //     The pivot rows of this lane's columns are read from shared memory
-      //     once per panel (all column slots when registers allow, else one
-      //     slot at a time).
-      constexpr int VC = (MB == 1 && (RPW + PW) * CPL <= 48) ? CPL : 1;   // column slots held at once
-#pragma unroll
-      for (int c0s = 0; c0s < CPL; c0s += VC) {
-        if (32 * (c0s + VC) - 1 < k0) continue;   // these column slots are left of the panel
-        R vv[PW][VC];
-#pragma unroll
-        for (int t = 0; t < PW; ++t)
-#pragma unroll
-          for (int cv = 0; cv < VC; ++cv) vv[t][cv] = t < kw ? V[t * NP + lane + 32 * (c0s + cv)] : R(0);
-#pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-          const int i = warp * RPW + r;
-          if (i >= n) break;
-          const int q = qinv[i];
-          if (q >= 0 && q < k0) continue;
-          R mi[PW];
-#pragma unroll
-          for (int t = 0; t < PW; ++t) mi[t] = Mb[i * PLD + t];
-#pragma unroll
-          for (int cv = 0; cv < VC; ++cv) {
-            const int c = c0s + cv;
-            if (32 * c + 31 < k0) continue;
-            const int col = lane + 32 * c;
-            if (col >= k0 && col < k0 + PW) {
-              a[r][c] = Pn[i * PLD + (col - k0)];
-            } else if (col >= k0 + PW) {
-              R acc = a[r][c];
-#pragma unroll
-              for (int t = 0; t < PW; ++t) acc = fma(mi[t], vv[t][cv], acc);
-              a[r][c] = acc;
+        for (int c = 0; c < CPW; ++c) {
+          const int m = warp * CPW + c;
+          double v = 0.0;
+          if (i < n && m < n) {
+            v = D[(int64_t)m * ld + i];
+            if (j > 0) {
+              const double cb = sb[c] * su[r];
+              v = v - cb * (double)Ib[m * ld + i];
             }
           }
+          a[r][c] = (R)v;
         }
       }
     }
-    // ---- factors to shared memory in pivot order (LAPACK layout), 1/U_kk
-    __syncthreads();
+    __syncthreads();   // Db and Ib consumed
+    if (DPF && threadIdx.x == 0 && j + 1 < nz) {
+      fence_proxy_async();
+      mbar_expect_tx(bar, dbytes);
+      bulk_g2s(Db, Din + (int64_t)(j + 1) * blk, dbytes, bar);
+    }
+    unsigned used = 0;   // rows lane + 32 r already pivoted
+    int q[RPL];          // step whose pivot row is lane + 32 r
 #pragma unroll
-    for (int r = 0; r < RPW; ++r) {
-      int i = warp * RPW + r;
-      if (i < n) {
-        int qi = qinv[i];
+    for (int r = 0; r < RPL; ++r) q[r] = 0;
+    if (warp == 0) {
+      R t[RPL];
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) S[qi * SLD + lane + 32 * c] = a[r][c];
-      }
+      for (int r = 0; r < RPL; ++r) t[r] = a[r][0];
+      publish(t, 0u, 0);
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) rdiag[k] = R(1) / S[k * SLD + k];
-    __syncthreads();
-    // ================================================================ inverse by column blocks
-    // X = U^{-1} L^{-1} P (lu_solve(LU, I)), columns split over warps: warp w
-    // solves L U x = P e_col for col = w*RPW + cc, CB columns at a time,
-    // column-oriented as LAPACK's getrs / dtrsm: forward with the unit lower
-    // factor from the pivot step of col downwards, then backward with U.
-    // Lane l holds rows l + 32 t; no block barrier (the factors in S are read
-    // only). Each finished chunk goes straight to global memory (natural row
-    // order) and into the partial products Inv_j * rhs_j.
-    R* O = out + (int64_t)j * n * ld;
-    // per-warp double buffer through which the owner lane of step k hands x_k
-    // to the warp (after the rhs partial products in Pn0..Pn1)
-    R* xb = Pn0 + NW * NP + warp * 2 * CB;
-    R pu[PRL];
-#pragma unroll
-    for (int t = 0; t < PRL; ++t) pu[t] = R(0);
+    // ================================================================ elimination
 #pragma unroll 1
-    for (int h = 0; h < NCH; ++h) {
-      const int c0 = warp * RPW + h * CB;
-      const int cbw = min(min(CB, RPW - h * CB), n - c0);
-      if (cbw <= 0) break;
-      R x[PRL][CB];
-      int kmin = n;
+    for (int w0 = 0; w0 < NW; ++w0) {
+      if (w0 * CPW >= n) break;
 #pragma unroll
-      for (int cc = 0; cc < CB; ++cc) {
-        const int q = cc < cbw ? qinv[c0 + cc] : n;
-        kmin = min(kmin, q);
+      for (int c = 0; c < CPW; ++c) {
+        const int k = w0 * CPW + c;
+        if (k < n) {
+          const int p = pb[k & 1];
+          const int ps = p >> 5, po = p & 31;
+          R m[RPL];
 #pragma unroll
-        for (int t = 0; t < PRL; ++t) x[t][cc] = (lane + 32 * t == q) ? R(1) : R(0);
-      }
-      // forward: steps k of segment sg = k / 32 are owned by slot sg (compile time)
+          for (int r = 0; r < RPL; ++r) m[r] = colb[(k & 1) * NPR + lane + 32 * r];
 #pragma unroll
-      for (int sg = 0; sg < PRL; ++sg) {
-        const int ke = min(n - 1, 32 * sg + 32);
-        for (int k = max(kmin, 32 * sg); k < ke; ++k) {
-          const int owner = k & 31;
-          R2* slot = reinterpret_cast<R2*>(xb + (k & 1) * CB);
-          if (lane == owner) {
-#pragma unroll
-            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = R2{x[sg][cc], x[sg][cc + 1]};
-          }
-          __syncwarp();
-          R xk[CB];
-#pragma unroll
-          for (int cc = 0; cc < CB; cc += 2) {
-            const R2 v = slot[cc / 2];
-            xk[cc] = v.x;
-            xk[cc + 1] = v.y;
-          }
-#pragma unroll
-          for (int t = sg; t < PRL; ++t) {
-            const int i = lane + 32 * t;
-            if (i > k && i < n) {
-              const R l = S[i * SLD + k];
-#pragma unroll
-              for (int cc = 0; cc < CB; ++cc) x[t][cc] = fma(-l, xk[cc], x[t][cc]);
+          for (int r = 0; r < RPL; ++r)
+            if (r == ps && lane == po) {
+              used |= 1u << r;
+              q[r] = k;
             }
+          // this warp's part of the pivot row, from its owner lane
+          R prow[CPW];
+#pragma unroll
+          for (int c2 = 0; c2 < CPW; ++c2) {
+            R col[RPL];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) col[r] = a[r][c2];
+            prow[c2] = __shfl_sync(FULL, pick(col, ps), po);
           }
+          const int cl = (c + 1) % CPW;                     // column k+1: slot and owner warp
+          const int wl = (c + 1 < CPW) ? w0 : w0 + 1;
+          if (k + 1 < n && warp == wl) {
+            R t[RPL];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[cl], a[r][cl]);
+            publish(t, used, k + 1);
+          }
+#pragma unroll
+          for (int r = 0; r < RPL; ++r)
+#pragma unroll
+            for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+          if (warp == w0) {
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) a[r][c] = (lane + 32 * r == p) ? R(1) : -m[r];
+          }
+          __syncthreads();
         }
       }
-      // backward with U, scaling by 1/U_kk as each x_k completes
+    }
+    if (ride) {
+      rsb[threadIdx.x] = rn;
+      rsb[NPR + threadIdx.x] = sn;
+    }
+    // ---- scale rows by 1/piv, scatter A'^{-1}[p_m][q(i)] = T[i][m] into Ib
 #pragma unroll
-      for (int sg = PRL - 1; sg >= 0; --sg) {
-        for (int k = min(n - 1, 32 * sg + 31); k >= 32 * sg; --k) {
-          const int owner = k & 31;
-          R2* slot = reinterpret_cast<R2*>(xb + (k & 1) * CB);
-          if (lane == owner) {
-            const R rd = rdiag[k];
+    for (int r = 0; r < RPL; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n) {
+        const R s = rps[i];
 #pragma unroll
-            for (int cc = 0; cc < CB; ++cc) x[sg][cc] = x[sg][cc] * rd;
-#pragma unroll
-            for (int cc = 0; cc < CB; cc += 2) slot[cc / 2] = R2{x[sg][cc], x[sg][cc + 1]};
-          }
-          __syncwarp();
-          R xk[CB];
-#pragma unroll
-          for (int cc = 0; cc < CB; cc += 2) {
-            const R2 v = slot[cc / 2];
-            xk[cc] = v.x;
-            xk[cc + 1] = v.y;
-          }
-#pragma unroll
-          for (int t = 0; t <= sg; ++t) {
-            const int i = lane + 32 * t;
-            if (i < k) {
-              const R u = S[i * SLD + k];
-#pragma unroll
-              for (int cc = 0; cc < CB; ++cc) x[t][cc] = fma(-u, xk[cc], x[t][cc]);
-            }
-          }
-        }
-      }
-      __syncwarp();   // every lane has read the last hand-over before the next chunk writes one
-#pragma unroll
-      for (int t = 0; t < PRL; ++t) {
-        const int i = lane + 32 * t;
-        if (i < n) {
-#pragma unroll
-          for (int cc = 0; cc < CB; ++cc) {
-            if (cc < cbw) {
-              const R v = x[t][cc];
-              if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
-              O[(int64_t)i * ld + c0 + cc] = v;
-              pu[t] = fma(v, vec[c0 + cc], pu[t]);
-            }
+        for (int c = 0; c < CPW; ++c) {
+          const int m = warp * CPW + c;
+          if (m < n) {
+            const R v = a[r][c] * s;
+            if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
+            Ib[pivs[m] * ld + q[r]] = v;
           }
         }
       }
     }
-    R* part = Pn0;   // [NW][NP] partial products of the forward sweep (Pn0..Pn1)
-    if (rhs) {
-#pragma unroll
-      for (int t = 0; t < PRL; ++t) {
-        const int i = lane + 32 * t;
-        if (i < n) part[warp * NP + i] = pu[t];
-      }
+    __syncthreads();
+    // ---- Inv_j to global memory (natural order, padding column 0)
+    {
+      R2* O = reinterpret_cast<R2*>(out + (int64_t)j * blk);
+      const R2* S2 = reinterpret_cast<const R2*>(Ib);
+      for (int e = threadIdx.x; e < blk / 2; e += blockDim.x) O[e] = S2[e];
     }
-    __syncthreads();   // Inv_j complete in global memory; partial products staged
     // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
     if (rhs && j + 1 < nz) {
-      const int nwu = min(NW, (n + RPW - 1) / RPW);
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double u = part[i];
-        for (int w = 1; w < nwu; ++w) u += (double)part[w * NP + i];
-        const double v = rhs[(int64_t)(j + 1) * n + i] - subn[(int64_t)j * n + i] * u;
-        rhs[(int64_t)(j + 1) * n + i] = v;
-        vec[i] = (R)v;
+      const double* vc = vecs + (j & 1) * NPR;
+      double* vn = vecs + ((j + 1) & 1) * NPR;
+      for (int i = warp; i < n; i += NW) {
+        double s = 0.0;
+        for (int m = lane; m < n; m += 32) s = fma((double)Ib[i * ld + m], vc[m], s);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
+        if (lane == 0) {
+          const double v = rsb[i] - rsb[NPR + i] * s;
+          rhs[(int64_t)(j + 1) * n + i] = v;
+          vn[i] = v;
+        }
       }
     }
-    __syncthreads();
   }
   if (st_local) atomicOr(status, st_local);
 }
@@ -472,18 +348,18 @@ __device__ void factor_atmosphere(int nz, int n, int ld, const double* Din, R* o
 // out == nullptr: the inverses replace the blocks in the workspace (FP64
 // path); otherwise they go to out (layer-major, ni x ld per layer) and the
 // FP64 blocks stay. only != nullptr: atmospheres with only[b] == 0 are skipped.
-template <int NP, int NW, int PW, int MB, typename R>
+template <int RPL, int CPW, int NW, int MB, bool DPF, typename R>
 __global__ void __launch_bounds__(NW * 32, MB)
-factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __restrict__ only,
-              int32_t* __restrict__ status, int with_rhs) {
+gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __restrict__ only,
+                 int32_t* __restrict__ status, int with_rhs) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
   if (only && only[b] == 0) return;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
   R* o = out ? out + g.z0 * B.ni * B.ld : reinterpret_cast<R*>(w.inv);
-  factor_atmosphere<NP, NW, PW, MB, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
-                                       status + b, smem_raw);
+  gj_factor_atmosphere<RPL, CPW, NW, DPF, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn,
+                                             with_rhs ? w.rmod : nullptr, status + b, smem_raw);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -658,17 +534,6 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, c
   return cudaGetLastError();
 }
 
-template <int NP, int NW, int PW, int MB = 1, typename R = double>
-static cudaError_t launch_factor_t(const Batch& B, double* ws, int32_t* status, int with_rhs,
-                                   cudaStream_t st, R* out = nullptr, const int32_t* only = nullptr) {
-  size_t sm = LUK<NP, NW, PW, R>::smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(factor_kernel<NP, NW, PW, MB, R>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  factor_kernel<NP, NW, PW, MB, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs);
-  return cudaGetLastError();
-}
-
 // SM count of the current device (the factor's layout depends on how many
 // atmospheres share an SM).
 static int sm_count() {
@@ -679,19 +544,32 @@ static int sm_count() {
   return n;
 }
 
+template <int RPL, int CPW, int NW, int MB, bool DPF, typename R = double>
+static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
+                               R* out = nullptr, const int32_t* only = nullptr) {
+  size_t sm = GJK<RPL, CPW, NW, R>::smem_bytes(B.ni, B.ld, DPF);
+  cudaError_t e = cudaFuncSetAttribute(gj_factor_kernel<RPL, CPW, NW, MB, DPF, R>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs);
+  return cudaGetLastError();
+}
+
+// Tile shapes by block size: rows over 32 lanes x RPL, columns over NW warps
+// x CPW; up to 72 species two atmospheres share an SM (the next diagonal
+// block is prefetched into shared memory in every shape whose two buffers fit).
+template <typename R>
+static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
+                             R* out, const int32_t* only) {
+  if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R>(B, ws, status, with_rhs, st, out, only);
+  if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R>(B, ws, status, with_rhs, st, out, only);
+  if (B.ni <= 72) return launch_gj_t<3, 9, 8, 2, true, R>(B, ws, status, with_rhs, st, out, only);
+  if (B.ni <= 96) return launch_gj_t<3, 8, 12, 1, true, R>(B, ws, status, with_rhs, st, out, only);
+  return launch_gj_t<4, 8, 16, 1, false, R>(B, ws, status, with_rhs, st, out, only);
+}
+
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st) {
-  if (B.ni <= 32) return launch_factor_t<32, 8, 8>(B, ws, status, with_rhs, st);
-  if (B.ni <= 64) return launch_factor_t<64, 16, 8>(B, ws, status, with_rhs, st);
-  if (B.ni <= 96) {
-    // Up to one atmosphere per SM: 12 warps per CTA give the shortest chain per
-    // layer. Beyond that, two 8-warp CTAs share an SM so that one atmosphere's
-    // pivot chain fills the other's idle issue slots (measured on B200 for
-    // ni=69, nz=120: 12.9 ms vs 16.0 ms at 1 atmosphere, 26.2 ms vs 19.7 ms
-    // at 296).
-    if (B.count <= sm_count()) return launch_factor_t<96, 12, 8, 1>(B, ws, status, with_rhs, st);
-    return launch_factor_t<96, 8, 8, 2>(B, ws, status, with_rhs, st);
-  }
-  return launch_factor_t<128, 16, 8>(B, ws, status, with_rhs, st);
+  return launch_gj<double>(B, ws, status, with_rhs, st, nullptr, nullptr);
 }
 
 // Factors into a separate inverse region (the workspace keeps the FP64
@@ -700,13 +578,7 @@ cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_
 template <typename R>
 cudaError_t launch_factor_into(const Batch& B, double* ws, R* out, const int32_t* only, int32_t* status,
                                cudaStream_t st) {
-  if (B.ni <= 32) return launch_factor_t<32, 8, 8, 1, R>(B, ws, status, 0, st, out, only);
-  if (B.ni <= 64) return launch_factor_t<64, 16, 8, 1, R>(B, ws, status, 0, st, out, only);
-  if (B.ni <= 96) {
-    if (B.count <= sm_count()) return launch_factor_t<96, 12, 8, 1, R>(B, ws, status, 0, st, out, only);
-    return launch_factor_t<96, 8, 8, 2, R>(B, ws, status, 0, st, out, only);
-  }
-  return launch_factor_t<128, 16, 8, 1, R>(B, ws, status, 0, st, out, only);
+  return launch_gj<R>(B, ws, status, 0, st, out, only);
 }
 template cudaError_t launch_factor_into<float>(const Batch&, double*, float*, const int32_t*, int32_t*, cudaStream_t);
 template cudaError_t launch_factor_into<double>(const Batch&, double*, double*, const int32_t*, int32_t*,

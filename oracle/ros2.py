@@ -67,8 +67,8 @@ def chem_rhs(y, M, k, net):
     p_idx = net.product_idx.reshape(-1)
     r_st = net.reactant_stoich.reshape(-1)
     p_st = net.product_stoich.reshape(-1)
-    loss = np.zeros((ni + 1, nz))
-    prod = np.zeros((ni + 1, nz))
+    loss = np.zeros((ni + 1, nz), dtype=rate.dtype)            # complex for complex-step derivatives
+    prod = np.zeros((ni + 1, nz), dtype=rate.dtype)
     np.add.at(loss, r_idx, (r_st[None, :] * rate_rep).T)       # chem.py:113-118
     np.add.at(prod, p_idx, (p_st[None, :] * rate_rep).T)       # chem.py:119-124
     return (prod[:ni] - loss[:ni]).T
