@@ -27,6 +27,10 @@ __device__ __forceinline__ unsigned long long pivot_key(float v) {
   return (a >= 0.0f) ? ((unsigned long long)__float_as_uint(a) << 32) : 0ull;
 }
 
+// High word of |v| (sign cleared): orders |v| up to ties of the low word.
+__device__ __forceinline__ unsigned hi_key(double v) { return (unsigned)__double2hiint(v) & 0x7fffffffu; }
+__device__ __forceinline__ unsigned hi_key(float v) { return __float_as_uint(v) & 0x7fffffffu; }
+
 // Correctly rounded reciprocal (the value of 1 / x).
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 __device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
@@ -43,6 +47,7 @@ template <int RPL, int CPW, int NW, typename R>
 struct GJK {
   static constexpr int NPR = 32 * RPL;          // row capacity (lane l holds rows l + 32 r)
   static constexpr int NPC = CPW * NW;          // column capacity (warp w holds columns w*CPW + c)
+  static constexpr int CPWP = (CPW + 1) & ~1;   // stride of a warp's pivot-row slot (pairs)
   __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
   static size_t smem_bytes(int n, int ld, bool dpf) {
     const size_t blk = (size_t)n * ld;
@@ -51,6 +56,7 @@ struct GJK {
            + al(2 * NPR * sizeof(R))                  // colb: multipliers of the next step (2 parities)
            + al(NPR * sizeof(R))                      // rps: 1 / pivot of each row
            + al(2 * NPR * sizeof(double))             // rsb: the next layer's rhs and sub_d rows
+           + al(NW * CPWP * sizeof(R))                // prs: pivot-row hand-over, one slot per warp
            + al(2 * NPR * sizeof(double))             // vecs: right-hand side ping-pong
            + al(NPC * sizeof(int))                    // pivs: pivot row of each step
            + al(2 * sizeof(int))                      // pb: pivot row of the next step (2 parities)
@@ -88,7 +94,7 @@ struct GJK {
 //    64-bit |v| key, ties to the lowest row, as LAPACK's idamax), inverts the
 //    pivot and publishes p_{k+1} with the scaled multipliers; the other warps
 //    update meanwhile. A warp takes its part of the pivot row from the owner
-//    lane by shuffles (no block barrier).
+//    lane through a per-warp shared slot (no block barrier).
 //  * Layer j's Schur update reads Inv_{j-1} from Ib (shared), D_j from Db
 //    (bulk-prefetched during layer j-1) when DPF, else from global memory.
 template <int RPL, int CPW, int NW, bool DPF, typename R>
@@ -98,7 +104,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
                                                      int32_t* status, char* smem_raw) {
   using G = GJK<RPL, CPW, NW, R>;
   using R2 = typename Pair<R>::T;
-  constexpr int NPR = G::NPR;
+  constexpr int NPR = G::NPR, CPWP = G::CPWP;
   // value of slot s (warp-uniform) of a per-lane row array
   auto pick = [](const R* v, int s) {
     R x = v[0];
@@ -120,6 +126,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   R* colb = reinterpret_cast<R*>(take(2 * NPR * sizeof(R)));
   R* rps = reinterpret_cast<R*>(take(NPR * sizeof(R)));
   double* rsb = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
+  R* prs = reinterpret_cast<R*>(take(NW * G::CPWP * sizeof(R)));
   double* vecs = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
   int* pivs = reinterpret_cast<int*>(take(G::NPC * sizeof(int)));
   int* pb = reinterpret_cast<int*>(take(2 * sizeof(int)));
@@ -139,31 +146,50 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
 
   // argmax of column kn (values t, already updated) over the unpivoted rows,
   // run by the warp that owns the column; publishes the pivot and multipliers.
-  // The maximum of the key's high word decides unless two lanes share it.
+  // Fast path: a unique maximum of the high word of |t| (valid rows keyed +1,
+  // NaN as 0) decides. Otherwise the full 64-bit key, ties to the lowest row.
   auto publish = [&](const R (&t)[RPL], unsigned used, int kn) {
-    unsigned long long bk = 0ull;
-    unsigned brow = 0xffffffffu;
-    R bv = R(0);
+    unsigned h[RPL];
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
-      if (i < n && !((used >> r) & 1u)) {
-        const unsigned long long kk = pivot_key(t[r]);
-        if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; bv = t[r]; }
-      }
+      const bool ok = i < n && !((used >> r) & 1u) && !isnan(t[r]);
+      h[r] = ok ? hi_key(t[r]) + 1u : 0u;
     }
-    const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-    const unsigned m1 = __reduce_max_sync(FULL, hi);
-    const unsigned tie = __ballot_sync(FULL, hi == m1 && brow != 0xffffffffu);
+    unsigned hm = h[0];
+#pragma unroll
+    for (int r = 1; r < RPL; ++r) hm = max(hm, h[r]);
+    const unsigned m1 = __reduce_max_sync(FULL, hm);
+    int cnt = 0, mys = 0;
+#pragma unroll
+    for (int r = RPL - 1; r >= 0; --r)
+      if (h[r] == m1) {
+        ++cnt;
+        mys = r;
+      }
+    const unsigned b1 = __ballot_sync(FULL, cnt > 0);
+    const unsigned b2 = __ballot_sync(FULL, cnt > 1);
     int p1;
     R piv;
-    if (__popc(tie) == 1) {
-      const int wl = __ffs(tie) - 1;
-      p1 = __shfl_sync(FULL, (int)brow, wl);
-      piv = __shfl_sync(FULL, bv, wl);
+    if (__popc(b1) == 1 && b2 == 0u) {
+      const int wl = __ffs(b1) - 1;
+      p1 = __shfl_sync(FULL, lane + 32 * mys, wl);
+      piv = __shfl_sync(FULL, pick(t, mys), wl);
     } else {
-      const unsigned m2 = __reduce_max_sync(FULL, hi == m1 ? lo : 0u);
-      p1 = (int)__reduce_min_sync(FULL, (hi == m1 && lo == m2) ? brow : 0xffffffffu);
+      unsigned long long bk = 0ull;
+      unsigned brow = 0xffffffffu;
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < n && !((used >> r) & 1u)) {
+          const unsigned long long kk = pivot_key(t[r]);
+          if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
+        }
+      }
+      const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+      const unsigned n1 = __reduce_max_sync(FULL, hi);
+      const unsigned n2 = __reduce_max_sync(FULL, hi == n1 ? lo : 0u);
+      p1 = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
       piv = __shfl_sync(FULL, pick(t, p1 >> 5), p1 & 31);
     }
     if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
@@ -268,14 +294,23 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
               used |= 1u << r;
               q[r] = k;
             }
-          // this warp's part of the pivot row, from its owner lane
-          R prow[CPW];
+          // this warp's part of the pivot row, from its owner lane (pair
+          // stores predicated on the slot: no selects)
+          R* ph = prs + warp * CPWP;
 #pragma unroll
-          for (int c2 = 0; c2 < CPW; ++c2) {
-            R col[RPL];
+          for (int r = 0; r < RPL; ++r)
+            if (r == ps && lane == po) {
 #pragma unroll
-            for (int r = 0; r < RPL; ++r) col[r] = a[r][c2];
-            prow[c2] = __shfl_sync(FULL, pick(col, ps), po);
+              for (int c2 = 0; c2 < CPWP; c2 += 2)
+                reinterpret_cast<R2*>(ph)[c2 / 2] = R2{a[r][c2], c2 + 1 < CPW ? a[r][c2 + 1] : R(0)};
+            }
+          __syncwarp();
+          R prow[CPWP];
+#pragma unroll
+          for (int c2 = 0; c2 < CPWP; c2 += 2) {
+            const R2 v = reinterpret_cast<const R2*>(ph)[c2 / 2];
+            prow[c2] = v.x;
+            prow[c2 + 1] = v.y;
           }
           const int cl = (c + 1) % CPW;                     // column k+1: slot and owner warp
           const int wl = (c + 1 < CPW) ? w0 : w0 + 1;
@@ -284,11 +319,16 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
 #pragma unroll
             for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[cl], a[r][cl]);
             publish(t, used, k + 1);
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+#pragma unroll
+              for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+          } else {
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+#pragma unroll
+              for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
           }
-#pragma unroll
-          for (int r = 0; r < RPL; ++r)
-#pragma unroll
-            for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
           if (warp == w0) {
 #pragma unroll
             for (int r = 0; r < RPL; ++r) a[r][c] = (lane + 32 * r == p) ? R(1) : -m[r];
