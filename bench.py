@@ -720,10 +720,8 @@ def main():
     # algorithmic bytes of the factor: read each D_j, write each inverse (ni^2 doubles each)
     fac_bytes = B * nz * 2.0 * ni * ni * 8
     # DRAM read + write bytes of one factor launch measured by ncu, per atmosphere,
-    # scaled to the batch: 8-warp layout (two atmospheres per SM) on 160 atmospheres
-    # (776.3 MB + 700.8 MB), 12-warp layout on 32 atmospheres (154.9 MB + 96.9 MB)
-    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
-    fac_traffic = ((776.26e6 + 700.78e6) / 160 if B > n_sm else (154.86e6 + 96.91e6) / 32) * B
+    # scaled to the batch: 160 atmospheres, 773.8 MB read + 693.9 MB written
+    fac_traffic = (773.76e6 + 693.90e6) / 160 * B
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

@@ -459,7 +459,7 @@ int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const d
   double* ws = (double*)workspace;
   VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
   VB_CHECK(vb::launch_stage1(net->dev, B, y, k, nullptr, atm, flags, nullptr, ws, st, v), "adjoint blocks");
-  VB_CHECK(vb::launch_factor(B, ws, status, 0, st), "factor");
+  VB_CHECK(vb::launch_factor(B, ws, status, 0, st, true), "factor");
   vb::SweepArgs a{};
   a.transposed = 1;
   a.status = status;

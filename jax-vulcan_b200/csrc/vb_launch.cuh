@@ -39,7 +39,11 @@ cudaError_t launch_chem(const NetDev&, int batch, int nz, const double* y, const
                         double* dydt, double* jac, cudaStream_t);
 cudaError_t launch_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int flags,
                              double* diff, double* diag_d, double* sup_d, double* sub_d, cudaStream_t);
-cudaError_t launch_factor(const Batch&, double* ws, int32_t* status, int with_rhs, cudaStream_t);
+// Inverts every layer's Schur-updated block. for_transposed_solves: the
+// inverses will be applied transposed (the adjoint's sweeps), so the
+// elimination bounds |X A' - I| instead of |A' X - I|.
+cudaError_t launch_factor(const Batch&, double* ws, int32_t* status, int with_rhs, cudaStream_t,
+                          bool for_transposed_solves = false);
 cudaError_t launch_sweep(const Batch&, double* ws, const SweepArgs&, cudaStream_t);
 cudaError_t launch_pack_blocks(const Batch&, const double* diag, const double* sup_d, const double* sub_d,
                                double* ws, cudaStream_t);

@@ -72,23 +72,26 @@ struct GJK {
 // The reference inverts each block by lu_factor then lu_solve(LU, I)
 // (solver.py:46-48). Here the inverse comes from one serial chain of ni
 // Gauss-Jordan steps instead of three (factor, forward and back
-// substitution). The elimination runs on the transposed block A'^T with
-// partial pivoting (so on A' it pivots within a row): the inverse of A'^T
-// then has a small left residual, i.e. X = A'^{-1} has a small right residual
-// |A' X - I| as the reference's lu_solve(LU, I) columns do, which is what the
-// later solves x = X b need (Gauss-Jordan on A' itself only bounds |X A' - I|;
-// on the stiff config-0 draw that left the block solve's normwise backward
-// error at 4e-12 instead of 7e-15).
+// substitution). Gauss-Jordan bounds the left residual |X B - I| of the
+// inverse X of the matrix B it eliminates on. With tr set the elimination
+// runs on the transposed block B = A'^T (partial pivoting within a row of
+// A'), so X = A'^{-1} has a small right residual |A' X - I| as the
+// reference's lu_solve(LU, I) columns do: what solves x = X b need (the Ros2
+// step; on the stiff config-0 draw eliminating on A' itself left the block
+// solve's normwise backward error at 4e-12 instead of 7e-15). Without tr it
+// runs on B = A' (partial pivoting within a column, as lu_factor), for
+// callers that solve with X^T (the transposed sweeps of the adjoint), which
+// need |X A' - I| small.
 //  * Tile in registers: lane l holds rows l + 32 r (r < RPL), warp w columns
-//    w*CPW + c (c < CPW) of A'^T. No row exchanges: row p_k is the pivot row
+//    w*CPW + c (c < CPW) of B. No row exchanges: row p_k is the pivot row
 //    of step k. Pivot rows are not normalised during the elimination (row i
 //    carries the factor piv_i of its own step), so every element update is
 //    one FMA
 //        S[i][:] -= m_i S[p][:],   m_i = S[i][k] / piv_k  (m_p = 0),
 //    column k becomes -m_i (row p: 1), and each row is scaled by 1/piv_i at
-//    the end. The stored result T satisfies (A'^T)^{-1}[q(i)][p_m] = T[i][m]
-//    (q(i): the step whose pivot row is i), so A'^{-1}[p_m][q(i)] = T[i][m],
-//    applied by the scatter into Ib.
+//    the end. The stored result T satisfies B^{-1}[q(i)][p_m] = T[i][m]
+//    (q(i): the step whose pivot row is i), applied (transposed back when
+//    tr) by the scatter into Ib.
 //  * One block barrier per step. During step k the owner warp of column
 //    k+1 updates that column first, takes its argmax (three redux.sync on the
 //    64-bit |v| key, ties to the lowest row, as LAPACK's idamax), inverts the
@@ -101,7 +104,7 @@ template <int RPL, int CPW, int NW, bool DPF, typename R>
 __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
                                                      const double* __restrict__ supn,
                                                      const double* __restrict__ subn, double* rhs,
-                                                     int32_t* status, char* smem_raw) {
+                                                     bool tr, int32_t* status, char* smem_raw) {
   using G = GJK<RPL, CPW, NW, R>;
   using R2 = typename Pair<R>::T;
   constexpr int NPR = G::NPR, CPWP = G::CPWP;
@@ -225,21 +228,22 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
       rn = rhs[(int64_t)(j + 1) * n + threadIdx.x];
       sn = subn[(int64_t)j * n + threadIdx.x];
     }
-    // ---- D_j and the Hadamard Schur update from Inv_{j-1} (solver.py:47),
-    //      loaded transposed: tile element (i, m) = A'_j[m][i]
+    // ---- D_j and the Hadamard Schur update from Inv_{j-1} (solver.py:47):
+    //      tile element (i, m) = B[i][m], A'_j[m][i] when tr, else A'_j[i][m]
     {
       const double* D = DPF ? Db : Din + (int64_t)j * blk;
-      double su[RPL], sb[CPW];
+      double sr[RPL], sc[CPW];   // the sub_d / sup_d factor of tile row i and column m
 #pragma unroll
       for (int r = 0; r < RPL; ++r) {
         const int i = lane + 32 * r;
-        su[r] = (j > 0 && i < n) ? supn[(int64_t)(j - 1) * n + i] : 0.0;
+        sr[r] = (j > 0 && i < n) ? (tr ? supn : subn)[(int64_t)(j - 1) * n + i] : 0.0;
       }
 #pragma unroll
       for (int c = 0; c < CPW; ++c) {
         const int m = warp * CPW + c;
-        sb[c] = (j > 0 && m < n) ? subn[(int64_t)(j - 1) * n + m] : 0.0;
+        sc[c] = (j > 0 && m < n) ? (tr ? subn : supn)[(int64_t)(j - 1) * n + m] : 0.0;
       }
+      const int si = tr ? 1 : ld, sm = tr ? ld : 1;   // element strides of tile rows / columns
 #pragma unroll
       for (int r = 0; r < RPL; ++r) {
         const int i = lane + 32 * r;
@@ -248,10 +252,11 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
           const int m = warp * CPW + c;
           double v = 0.0;
           if (i < n && m < n) {
-            v = D[(int64_t)m * ld + i];
+            const int e = i * si + m * sm;
+            v = D[e];
             if (j > 0) {
-              const double cb = sb[c] * su[r];
-              v = v - cb * (double)Ib[m * ld + i];
+              const double cb = tr ? sc[c] * sr[r] : sr[r] * sc[c];
+              v = v - cb * (double)Ib[e];
             }
           }
           a[r][c] = (R)v;
@@ -341,7 +346,8 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
       rsb[threadIdx.x] = rn;
       rsb[NPR + threadIdx.x] = sn;
     }
-    // ---- scale rows by 1/piv, scatter A'^{-1}[p_m][q(i)] = T[i][m] into Ib
+    // ---- scale rows by 1/piv, scatter B^{-1}[q(i)][p_m] = T[i][m] into Ib
+    //      (A'^{-1}[p_m][q(i)] when tr)
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
@@ -353,7 +359,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
           if (m < n) {
             const R v = a[r][c] * s;
             if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
-            Ib[pivs[m] * ld + q[r]] = v;
+            Ib[tr ? pivs[m] * ld + q[r] : q[r] * ld + pivs[m]] = v;
           }
         }
       }
@@ -391,7 +397,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
 template <int RPL, int CPW, int NW, int MB, bool DPF, typename R>
 __global__ void __launch_bounds__(NW * 32, MB)
 gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __restrict__ only,
-                 int32_t* __restrict__ status, int with_rhs) {
+                 int32_t* __restrict__ status, int with_rhs, int tr) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
   if (only && only[b] == 0) return;
@@ -399,7 +405,7 @@ gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __rest
   WsView w = ws_view(ws, g, B.ni, B.ld);
   R* o = out ? out + g.z0 * B.ni * B.ld : reinterpret_cast<R*>(w.inv);
   gj_factor_atmosphere<RPL, CPW, NW, DPF, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn,
-                                             with_rhs ? w.rmod : nullptr, status + b, smem_raw);
+                                             with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -585,13 +591,13 @@ static int sm_count() {
 }
 
 template <int RPL, int CPW, int NW, int MB, bool DPF, typename R = double>
-static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
+static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
                                R* out = nullptr, const int32_t* only = nullptr) {
   size_t sm = GJK<RPL, CPW, NW, R>::smem_bytes(B.ni, B.ld, DPF);
   cudaError_t e = cudaFuncSetAttribute(gj_factor_kernel<RPL, CPW, NW, MB, DPF, R>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs);
+  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs, tr);
   return cudaGetLastError();
 }
 
@@ -599,17 +605,18 @@ static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int 
 // x CPW; up to 72 species two atmospheres share an SM (the next diagonal
 // block is prefetched into shared memory in every shape whose two buffers fit).
 template <typename R>
-static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
+static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
                              R* out, const int32_t* only) {
-  if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R>(B, ws, status, with_rhs, st, out, only);
-  if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R>(B, ws, status, with_rhs, st, out, only);
-  if (B.ni <= 72) return launch_gj_t<3, 9, 8, 2, true, R>(B, ws, status, with_rhs, st, out, only);
-  if (B.ni <= 96) return launch_gj_t<3, 8, 12, 1, true, R>(B, ws, status, with_rhs, st, out, only);
-  return launch_gj_t<4, 8, 16, 1, false, R>(B, ws, status, with_rhs, st, out, only);
+  if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 72) return launch_gj_t<3, 9, 8, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 96) return launch_gj_t<3, 8, 12, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+  return launch_gj_t<4, 8, 16, 1, false, R>(B, ws, status, with_rhs, tr, st, out, only);
 }
 
-cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st) {
-  return launch_gj<double>(B, ws, status, with_rhs, st, nullptr, nullptr);
+cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
+                          bool for_transposed_solves) {
+  return launch_gj<double>(B, ws, status, with_rhs, for_transposed_solves ? 0 : 1, st, nullptr, nullptr);
 }
 
 // Factors into a separate inverse region (the workspace keeps the FP64
@@ -618,7 +625,7 @@ cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_
 template <typename R>
 cudaError_t launch_factor_into(const Batch& B, double* ws, R* out, const int32_t* only, int32_t* status,
                                cudaStream_t st) {
-  return launch_gj<R>(B, ws, status, 0, st, out, only);
+  return launch_gj<R>(B, ws, status, 0, 1, st, out, only);
 }
 template cudaError_t launch_factor_into<float>(const Batch&, double*, float*, const int32_t*, int32_t*, cudaStream_t);
 template cudaError_t launch_factor_into<double>(const Batch&, double*, double*, const int32_t*, int32_t*,
