@@ -107,6 +107,18 @@ __device__ inline void rates_t(const NetDev& net, const double* yrow, const doub
 // (chem.py:92-99); with jac, also drate[r][s] (chem.py:156-182).
 __device__ inline void layer_rates(const NetDev& net, const double* yrow, const double* kcol,
                                    int64_t kstride, double M, double* rate, double* drate, bool jac) {
+  if (!jac) {   // the right-hand-side kernels run at full occupancy: fewer loads in flight per thread
+    switch (net.T) {
+      case 1: rates_t<1, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      case 2: rates_t<2, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      case 3: rates_t<3, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      case 4: rates_t<4, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      case 5: rates_t<5, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      case 6: rates_t<6, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      case 7: rates_t<7, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+      default: rates_t<8, 2>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
+    }
+  }
   switch (net.T) {
     case 1: rates_t<1, 6>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
     case 2: rates_t<2, 6>(net, yrow, kcol, kstride, M, rate, drate, jac); return;
@@ -243,7 +255,10 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
 
 // Stage-1 assembly: rmod[j] = rhs(y), inv[j] = c0*I - J - diag(diag_d),
 // supn[j] = -sup_d, subn[j-1] = -sub_d, with fix_mask (jax_step.py:263-298).
-__global__ void __launch_bounds__(LAYER_THREADS, 3)
+// Latency-bound gathers: four CTAs per SM (the shared-memory limit with the
+// drate buffer) beat three without spills (measured on B200, ni=69, nr=1400:
+// 4.79 vs 4.89 ms at 296 atmospheres; two per SM: 6.32 ms).
+__global__ void __launch_bounds__(LAYER_THREADS, 4)
 stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
               const double* __restrict__ dt, const double* __restrict__ atm, int flags,
               const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, const double* __restrict__ adj_v) {
@@ -322,8 +337,12 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
 }
 
 // Stage-2 right-hand side: rmod[j] = rhs(yk2) - 2/(r dt) k1[j] with
-// yk2 = y + k1/r (jax_step.py:303-310).
-__global__ void __launch_bounds__(LAYER_THREADS, 3)
+// yk2 = y + k1/r (jax_step.py:303-310). No drate buffer, so eight CTAs fit an
+// SM; occupancy, not per-thread ILP, hides the gathers' latency (measured on
+// B200, ni=69, nr=1400, 296 atmospheres: 3 / 4 / 5 / 6 CTAs per SM 2.22 /
+// 1.87 / 1.70 / 1.57 ms; 8 with rate constants loaded 2 deep instead of 6:
+// 1.53 ms, despite the spills at 32 registers).
+__global__ void __launch_bounds__(LAYER_THREADS, 8)
 stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
               const double* __restrict__ dt, const double* __restrict__ atm, int flags,
               const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, double* __restrict__ resid) {
