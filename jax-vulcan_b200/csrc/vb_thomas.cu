@@ -417,16 +417,30 @@ __host__ __device__ inline size_t sweep_smem_bytes(int ni, int stages) {
 }
 
 // out = Inv v (or Inv^T v) for one n x n block held in shared memory.
+// Inv v: four lanes per row (two interleaved partial sums each, then two
+// shuffle levels), eight rows per warp per pass; the pass loop is
+// warp-uniform so every lane reaches the shuffles.
 __device__ inline void block_matvec_s(const double* __restrict__ Inv, int n, int ld, bool trans,
                                       const double* v, double* out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (!trans) {
-    for (int i = warp; i < n; i += nw) {
-      double s = 0.0;
-      for (int m = lane; m < n; m += 32) s = fma(Inv[i * ld + m], v[m], s);
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-      if (lane == 0) out[i] = s;
+    const int sub = lane & 3;
+    for (int i0 = warp * 8; i0 < n; i0 += nw * 8) {
+      const int i = i0 + (lane >> 2);
+      double s0 = 0.0, s1 = 0.0;
+      if (i < n) {
+        const double* row = Inv + i * ld;
+        int m = sub;
+        for (; m + 4 < n; m += 8) {
+          s0 = fma(row[m], v[m], s0);
+          s1 = fma(row[m + 4], v[m + 4], s1);
+        }
+        if (m < n) s0 = fma(row[m], v[m], s0);
+      }
+      double s = s0 + s1;
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      if (sub == 0 && i < n) out[i] = s;
     }
   } else {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -474,20 +488,40 @@ sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages) {
   }
   double* out = A.user ? A.user + g.z0 * n : w.k1;
   const double r = ros2_r();
-  if (fwd) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] = vecs[i];
-  }
+  const int tid = threadIdx.x;
+  const bool own = tid < n;   // thread i owns element i of every vector (ni <= 128 < SWEEP_THREADS)
+  if (fwd && own) v[tid] = vecs[tid];
+  // Operands of a layer that do not depend on the running vector, loaded one
+  // layer ahead so their latency hides behind the block copy and the product
+  // (none of them is written by this kernel before it is read).
+  double p_vec = 0.0, p_cpl = 0.0, p_y = 0.0, p_k1 = 0.0;
+  auto prefetch = [&](int s2) {
+    if (!own || s2 >= count) return;
+    const int j = block_of(s2);
+    if (fwd) {
+      p_vec = vecs[(int64_t)(j + 1) * n + tid];
+      p_cpl = lo[(int64_t)j * n + tid];
+    } else {
+      p_vec = vecs[(int64_t)j * n + tid];
+      p_cpl = j < nz - 1 ? up[(int64_t)j * n + tid] : 0.0;
+      if (A.mode == SWEEP_BACK_FINAL) {
+        p_y = A.y[g.z0 * n + (int64_t)j * n + tid];
+        p_k1 = w.k1[(int64_t)j * n + tid];
+      }
+    }
+  };
+  prefetch(0);
   int issued = min(stages, count);
   for (int s2 = 0; s2 < count; ++s2) {
     const int st = s2 % stages;
     const uint32_t parity = (uint32_t)((s2 / stages) & 1);
     const int j = block_of(s2);
-    if (!fwd) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double x = vecs[(int64_t)j * n + i];
-        if (j < nz - 1) x = x - up[(int64_t)j * n + i] * u[i];
-        v[i] = x;
-      }
+    const double c_vec = p_vec, c_cpl = p_cpl, c_y = p_y, c_k1 = p_k1;
+    prefetch(s2 + 1);
+    if (!fwd && own) {
+      double x = c_vec;
+      if (j < nz - 1) x = x - c_cpl * u[tid];
+      v[tid] = x;
     }
     const bool ok = mbar_wait(&bars[st], parity, WAIT_LIMIT);
     if (__syncthreads_or(!ok)) {
@@ -507,25 +541,21 @@ sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages) {
       bulk_g2s(ring + (size_t)st * blk, w.inv + (int64_t)block_of(s2 + stages) * blk, blk_bytes, &bars[st]);
       ++issued;
     }
-    if (fwd) {
-      // rhs'[j+1] = rhs[j+1] - sub_d[j] o (Inv_j rhs'[j])
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double x = vecs[(int64_t)(j + 1) * n + i] - lo[(int64_t)j * n + i] * u[i];
-        vecs[(int64_t)(j + 1) * n + i] = x;
-        v[i] = x;
-      }
-    } else {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double kj = u[i];
+    if (own) {
+      if (fwd) {
+        // rhs'[j+1] = rhs[j+1] - sub_d[j] o (Inv_j rhs'[j])
+        const double x = c_vec - c_cpl * u[tid];
+        vecs[(int64_t)(j + 1) * n + tid] = x;
+        v[tid] = x;
+      } else {
+        const double kj = u[tid];
         if (A.mode == SWEEP_BACK) {
-          out[(int64_t)j * n + i] = kj;
+          out[(int64_t)j * n + tid] = kj;
         } else {
           // sol = y + 3/(2r) k1 + 1/(2r) k2 ; delta = |sol - yk2| (jax_step.py:313-314)
-          int64_t e = g.z0 * n + (int64_t)j * n + i;
-          double yv = A.y[e];
-          double k1v = w.k1[(int64_t)j * n + i];
-          double s = yv + (3.0 / (2.0 * r)) * k1v + (1.0 / (2.0 * r)) * kj;
-          double yk2 = yv + k1v / r;
+          const int64_t e = g.z0 * n + (int64_t)j * n + tid;
+          const double s = c_y + (3.0 / (2.0 * r)) * c_k1 + (1.0 / (2.0 * r)) * kj;
+          const double yk2 = c_y + c_k1 / r;
           A.sol[e] = s;
           A.delta[e] = fabs(s - yk2);
           if (!isfinite(s)) atomicOr(A.status + b, VB_STATUS_NONFINITE);
