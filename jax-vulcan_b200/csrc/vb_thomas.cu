@@ -375,12 +375,23 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
     if (rhs && j + 1 < nz) {
       const double* vc = vecs + (j & 1) * NPR;
       double* vn = vecs + ((j + 1) & 1) * NPR;
-      for (int i = warp; i < n; i += NW) {
-        double s = 0.0;
-        for (int m = lane; m < n; m += 32) s = fma((double)Ib[i * ld + m], vc[m], s);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
-        if (lane == 0) {
+      // four lanes per row, eight rows per warp per pass (warp-uniform passes)
+      const int sub = lane & 3;
+      for (int i0 = warp * 8; i0 < n; i0 += NW * 8) {
+        const int i = i0 + (lane >> 2);
+        double s0 = 0.0, s1 = 0.0;
+        if (i < n) {
+          int m = sub;
+          for (; m + 4 < n; m += 8) {
+            s0 = fma((double)Ib[i * ld + m], vc[m], s0);
+            s1 = fma((double)Ib[i * ld + m + 4], vc[m + 4], s1);
+          }
+          if (m < n) s0 = fma((double)Ib[i * ld + m], vc[m], s0);
+        }
+        double s = s0 + s1;
+        s += __shfl_xor_sync(FULL, s, 1);
+        s += __shfl_xor_sync(FULL, s, 2);
+        if (sub == 0 && i < n) {
           const double v = rsb[i] - rsb[NPR + i] * s;
           rhs[(int64_t)(j + 1) * n + i] = v;
           vn[i] = v;
