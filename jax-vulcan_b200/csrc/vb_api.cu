@@ -161,8 +161,9 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   if (coefs.empty()) coefs.push_back(0.0);
   // destinations in decreasing term count (ties: increasing index); threads
   // take them in rank bands (thread t: ranks t, t + LAYER_THREADS, ...) so the
-  // lanes of a warp sum lists of similar length. Word: d | row << 16 | col << 24.
-  std::vector<uint32_t> order((size_t)ni * ni);
+  // lanes of a warp sum lists of similar length. Descriptor of rank q: first
+  // term, then count | row << 16 | col << 24 (one load per destination).
+  std::vector<uint32_t> order(2 * (size_t)ni * ni);
   {
     std::vector<int32_t> perm((size_t)ni * ni);
     for (size_t d = 0; d < perm.size(); ++d) perm[d] = (int32_t)d;
@@ -170,7 +171,10 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
                      [&](int32_t x, int32_t y) { return jp[x + 1] - jp[x] > jp[y + 1] - jp[y]; });
     for (size_t q = 0; q < perm.size(); ++q) {
       const uint32_t d = (uint32_t)perm[q];
-      order[q] = d | ((d / (uint32_t)ni) << 16) | ((d % (uint32_t)ni) << 24);
+      const uint32_t cnt = (uint32_t)(jp[d + 1] - jp[d]);
+      if (cnt > 0xffffu) return fail(VB_ERR_ARG, "a Jacobian entry has more than 65535 terms");
+      order[2 * q] = (uint32_t)jp[d];
+      order[2 * q + 1] = cnt | ((d / (uint32_t)ni) << 16) | ((d % (uint32_t)ni) << 24);
     }
   }
   std::vector<int32_t> ri(R * T), pi(R * T);
@@ -212,7 +216,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   d.jac_w = (const uint32_t*)(b + parts[10].off);
   d.coef_tab = (const double*)(b + parts[11].off);
   d.n_coef = (int)coefs.size();
-  d.jac_order = (const uint32_t*)(b + parts[12].off);
+  d.jac_desc = (const uint2*)(b + parts[12].off);
   net->base = base;
   net->bytes = total;
   *out = net;

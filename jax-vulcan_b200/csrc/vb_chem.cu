@@ -157,22 +157,25 @@ __device__ inline void load_coefs(const NetDev& net, double* coef) {
 
 // Dense Jacobian of one layer (chem.py:183-208), each entry summed in the
 // reference's scatter order. Threads take the destinations in rank bands of
-// decreasing term count (jac_order), so the lanes of a warp run loops of
+// decreasing term count (jac_desc), so the lanes of a warp run loops of
 // similar length.
 template <typename Store>
 __device__ inline void layer_jacobian_each(const NetDev& net, const double* coef, const double* drate, Store store) {
   const int nd = net.ni * net.ni;
-  for (int q = threadIdx.x; q < nd; q += blockDim.x) {
-    const uint32_t o = net.jac_order[q];
-    const int d = (int)(o & 0xffffu);
-    const int e1 = net.jac_ptr[d + 1];
+  const int stride = blockDim.x;
+  int q = threadIdx.x;
+  uint2 dn = q < nd ? net.jac_desc[q] : make_uint2(0u, 0u);
+  for (; q < nd; q += stride) {
+    const uint2 dc = dn;
+    if (q + stride < nd) dn = net.jac_desc[q + stride];   // the next destination's descriptor, one ahead
+    const int e0 = (int)dc.x, e1 = e0 + (int)(dc.y & 0xffffu);
     double J = 0.0;
 #pragma unroll 4
-    for (int e = net.jac_ptr[d]; e < e1; ++e) {
+    for (int e = e0; e < e1; ++e) {
       const uint32_t x = net.jac_w[e];
       J = J + coef[x >> 16] * drate[x & 0xffffu];
     }
-    store((int)((o >> 16) & 0xffu), (int)(o >> 24), J);
+    store((int)((dc.y >> 16) & 0xffu), (int)(dc.y >> 24), J);
   }
 }
 

@@ -32,8 +32,9 @@ struct NetDev {
   const uint32_t* jac_w;
   const double* coef_tab;        // [n_coef]
   int n_coef;
-  // Destinations in decreasing term count: d | row << 16 | col << 24.
-  const uint32_t* jac_order;     // [ni*ni]
+  // Destinations in decreasing term count: {first term in jac_w,
+  // count | row << 16 | col << 24}.
+  const uint2* jac_desc;         // [ni*ni]
 };
 
 constexpr int LAYER_THREADS = 256;
