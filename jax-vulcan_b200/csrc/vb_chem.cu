@@ -159,11 +159,14 @@ __device__ inline void load_coefs(const NetDev& net, double* coef) {
 // reference's scatter order. Threads take the destinations in rank bands of
 // decreasing term count (jac_desc), so the lanes of a warp run loops of
 // similar length.
+// busy: the first threads are also summing species lists in the same phase;
+// the rank bands are rotated so those threads take the lightest ranks of each band.
 template <typename Store>
-__device__ inline void layer_jacobian_each(const NetDev& net, const double* coef, const double* drate, Store store) {
+__device__ inline void layer_jacobian_each(const NetDev& net, const double* coef, const double* drate, Store store,
+                                           int busy = 0) {
   const int nd = net.ni * net.ni;
   const int stride = blockDim.x;
-  int q = threadIdx.x;
+  int q = ((int)threadIdx.x - busy + stride) % stride;
   uint2 dn = q < nd ? net.jac_desc[q] : make_uint2(0u, 0u);
   for (; q < nd; q += stride) {
     const uint2 dc = dn;
@@ -282,13 +285,14 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   __shared__ double coefs[MAX_COEF];
   load_coefs(net, coefs);   // visible after the barriers in load_rows
   load_rows(yb, nullptr, a.gas, nz, ni, j, r, false, L);
-  layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
   __shared__ double supb[VB_MAX_NI], subb[VB_MAX_NI];
+  layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);   // needs only the state rows
+  layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
   __syncthreads();
-  species_sums(net, coefs, L.rate, L.part);
-  layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);
-  __syncthreads();
-  // the Jacobian gather writes each block entry in its final form
+  // One phase for the species sums and the Jacobian gather: the first 2*ni
+  // threads sum a species list, then join the gather on the light end of
+  // each rank band. The gather writes each block entry in its final form.
+  if (!adj) species_sums(net, coefs, L.rate, L.part);
   double* blk = w.inv + (int64_t)j * ni * B.ld;
   const int ld = B.ld;
   const double bot = (j == 0 && (flags & VB_USE_BOTFLUX)) ? 1.0 : 0.0;
@@ -320,7 +324,8 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
     }
     if (fm && fm[row]) v = (row == col) ? c0 : 0.0;
     blk[(int64_t)row * ld + col] = v;
-  });
+  }, min(2 * ni, (int)blockDim.x));
+  __syncthreads();   // the species sums
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
     bool fixed = fm && fm[i];
@@ -366,10 +371,10 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   __shared__ double coefs[MAX_COEF];
   load_coefs(net, coefs);   // visible after the barriers in load_rows
   load_rows(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
+  layer_diffusion(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
   __syncthreads();
   species_sums(net, coefs, L.rate, L.part);
-  layer_diffusion(a, nz, ni, j, flags, L, nullptr, nullptr, false);
   __syncthreads();
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
