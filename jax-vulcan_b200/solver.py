@@ -82,8 +82,9 @@ class MixedFactors(NamedTuple):
 
 
 def factor_block_thomas_mixed(diag, sup_d, sub_d, stream=None) -> MixedFactors:
-    """Mixed-precision factorisation: FP32 LU and inverses of the eliminated
-    diagonal blocks, the FP64 blocks kept for the refinement residual."""
+    """Mixed-precision factorisation: FP32 inverses of the eliminated diagonal
+    blocks (Gauss-Jordan, as the FP64 factor), the FP64 blocks kept for the
+    refinement residual."""
     d = as_device(diag)
     single = d.dim() == 3
     if single:
