@@ -720,8 +720,8 @@ def main():
     # algorithmic bytes of the factor: read each D_j, write each inverse (ni^2 doubles each)
     fac_bytes = B * nz * 2.0 * ni * ni * 8
     # DRAM read + write bytes of one factor launch measured by ncu, per atmosphere,
-    # scaled to the batch: 160 atmospheres, 773.8 MB read + 693.9 MB written
-    fac_traffic = (773.76e6 + 693.90e6) / 160 * B
+    # scaled to the batch: 160 atmospheres, 775.3 MB read + 697.2 MB written
+    fac_traffic = (775.31e6 + 697.17e6) / 160 * B
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
