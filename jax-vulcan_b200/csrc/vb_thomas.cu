@@ -644,19 +644,20 @@ static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int 
 
 // Tile shapes by block size: rows over 32 lanes x RPL, columns over NW warps
 // x CPW (the next diagonal block is prefetched into shared memory in every
-// shape whose two buffers fit). Up to 72 species: with more atmospheres than
-// SMs two 12-warp CTAs (6 columns per warp) share an SM; otherwise one
-// 16-warp CTA of 5 columns per warp shortens each step's update. Measured on
-// B200, ni=69, nz=120: one atmosphere 5.52 ms per Ros2 step (8 warps: 5.92),
-// 148 atmospheres 4.77 ms per factor (8 warps: 5.30), 296 atmospheres 6.15 ms
-// (two CTAs of 8 warps x 9 columns: 6.29; of 10 x 7: 6.15; of 14 x 5: 7.09).
+// shape whose two buffers fit). Up to 72 species: 12 warps of 6 columns, two
+// CTAs per SM when the batch has more atmospheres than SMs (register cap 85),
+// else one (no register cap). Measured on B200, ni=69, nz=120: 148
+// atmospheres 4.11 ms per factor (16 warps x 5: 4.77; 8 x 9: 5.30; 32 x 3:
+// 6.43), one atmosphere 4.84 ms per Ros2 step (16 x 5: 5.50; 8 x 9: 5.92),
+// 296 atmospheres 6.15 ms (two CTAs of 8 x 9: 6.29; 10 x 7: 6.15; 14 x 5:
+// 7.09; 16 x 5: 9.14).
 template <typename R>
 static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
                              R* out, const int32_t* only) {
   if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 72) {
-    if (B.count <= sm_count()) return launch_gj_t<3, 5, 16, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+    if (B.count <= sm_count()) return launch_gj_t<3, 6, 12, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
     return launch_gj_t<3, 6, 12, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   }
   if (B.ni <= 96) return launch_gj_t<3, 8, 12, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
