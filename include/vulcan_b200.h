@@ -89,6 +89,31 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff,
                  double* sol, double* delta, int32_t* status,
                  void* workspace, size_t workspace_bytes, void* stream);
 
+/* Stage vectors of the last vb_ros2_step run on `workspace` (the reference's
+ * k1 and k2 of jax_step.py:300-311, which jax_ros2_step keeps internal):
+ * k1, k2 [B][nz][ni] (or packed by zoff), either may be NULL. For checking a
+ * step's two block solves by their backward errors; same batch arguments as
+ * the step. */
+int vb_ros2_stages(const VbNet* net, int batch, int nz, const int64_t* zoff, const void* workspace,
+                   double* k1, double* k2, void* stream);
+
+/* Failure-detection testing: every bulk copy of the factor and sweep kernels
+ * is awaited with a bounded poll loop; a wait that runs out sets
+ * VB_STATUS_WATCHDOG for its atmosphere, drains the copies still in flight
+ * (with the full limit) and returns early. vb_set_wait_limit sets the poll
+ * limit of that first wait for later launches from this process (0: give up
+ * at once); polls < 0 restores the default (2^22). No counterpart in the
+ * reference (its solver has no waits). */
+int vb_set_wait_limit(long long polls);
+
+/* FP64 block-factor kernel of the step, the block solver and the adjoint, for
+ * later launches from this process: 0 (default) = blocked Gauss-Jordan, one
+ * warp per 8-column panel, the panel's pivot steps inside the warp and the
+ * rank-8 trailing updates on the FP64 tensor cores (mma.sync m8n8k4); 1 =
+ * scalar Gauss-Jordan, one block barrier per pivot step. Both replace the
+ * reference's lu_factor + lu_solve(LU, I) pair (solver.py:46-48). */
+int vb_set_factor_kernel(int variant);
+
 /* Chemistry (reference chem.py:83-131 chem_rhs and chem.py:144-214
  * chem_jac_analytical, vmapped over layers and a uniform batch):
  * y [B][nz][ni], M [B][nz], k [B][nr+1][nz] -> dydt [B][nz][ni], jac [B][nz][ni][ni]. */
@@ -176,6 +201,10 @@ typedef struct VbLoopParams {
   int32_t flags;                 /* VB_LOOP_* */
   int32_t adapt_rtol_dec_period, adapt_rtol_inc_period;
   int32_t reserved;
+  /* species whose delta the error norm drops in every layer (bit i % 32 of
+   * word i / 32): the reference's condense_zero_mask, condense_sp + non_gas_sp
+   * when use_condense is on (outer_loop.py:244, :1380-1386); all zero otherwise */
+  uint32_t cond_zero_bits[4];
   double loss_eps, pos_cut, nega_cut, mtol, atol;
   double dt_var_min, dt_var_max, dt_min, dt_max;
   double rtol_min, rtol_max, adapt_rtol_dec, adapt_rtol_inc, adapt_rtol_loss_mul, adapt_rtol_inc_loss_thresh;
@@ -451,7 +480,11 @@ int vb_fp64_probe(double* out, int blocks, int threads, int iters, void* stream)
  * All calls on a device share the array and it keeps the last call's
  * contents: calls that overlap on the GPU (streams without an ordering
  * between them) race. Nothing in the array needs to start at zero (every
- * value is written before it is read); status[B] is cleared by each call. */
+ * value is written before it is read); status[B] is cleared by each call.
+ * The looked-up address is cached per device for the life of the process: a
+ * device reset (cudaDeviceReset, or the primary context destroyed and
+ * recreated) makes it stale, so this entry point must not be called again in
+ * a process after its device was reset. */
 #define VB_STATIC_SCRATCH_BYTES ((size_t)64 << 20)
 int vb_ros2_step_static(const VbNet* net, int batch, int nz,
                         const double* y, const double* k, const double* dt,

@@ -206,18 +206,26 @@ vjp_atm_kernel(Batch B, const double* __restrict__ y, const double* __restrict__
   g_atm[g.atm + field_off[f] + q] = -gsum;
 }
 
-__global__ void gather_k1_kernel(Batch B, double* __restrict__ ws, double* __restrict__ out) {
+// Copy the workspace's first-stage rows (k1: the adjoint's lambda, or the
+// Ros2 step's k1) and, with k2 != nullptr, the Ros2 step's second-stage rows
+// (kept in the aux rows by the final back sweep) into [layers][ni] arrays.
+__global__ void gather_stages_kernel(Batch B, const double* __restrict__ ws, double* __restrict__ k1,
+                                     double* __restrict__ k2) {
   const int b = blockIdx.y, j = blockIdx.x;
   Geo g = geo_of(B, b);
   if (j >= g.nz) return;
-  const double* src = ws_view(ws, g, B.ni, B.ld).k1 + (int64_t)j * B.ni;
-  for (int i = threadIdx.x; i < B.ni; i += blockDim.x) out[g.z0 * B.ni + (int64_t)j * B.ni + i] = src[i];
+  WsView w = ws_view(const_cast<double*>(ws), g, B.ni, B.ld);
+  const int64_t src = (int64_t)j * B.ni, dst = g.z0 * B.ni + (int64_t)j * B.ni;
+  for (int i = threadIdx.x; i < B.ni; i += blockDim.x) {
+    if (k1) k1[dst + i] = w.k1[src + i];
+    if (k2) k2[dst + i] = w.aux[src + i];
+  }
 }
 
-cudaError_t launch_gather_k1(const Batch& B, double* ws, double* out, cudaStream_t st) {
-  if (!out) return cudaSuccess;
+cudaError_t launch_gather_stages(const Batch& B, const double* ws, double* k1, double* k2, cudaStream_t st) {
+  if (!k1 && !k2) return cudaSuccess;
   dim3 grid(B.nz, B.count);
-  gather_k1_kernel<<<grid, 128, 0, st>>>(B, ws, out);
+  gather_stages_kernel<<<grid, 128, 0, st>>>(B, ws, k1, k2);
   return cudaGetLastError();
 }
 

@@ -296,6 +296,26 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const
   return VB_OK;
 }
 
+int vb_ros2_stages(const VbNet* net, int batch, int nz, const int64_t* zoff, const void* workspace, double* k1,
+                   double* k2, void* stream) {
+  if (!net || !workspace) return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  vb::Batch B = make_batch(net, batch, nz, zoff);
+  VB_CHECK(vb::launch_gather_stages(B, (const double*)workspace, k1, k2, (cudaStream_t)stream), "stages");
+  return VB_OK;
+}
+
+int vb_set_wait_limit(long long polls) {
+  vb::set_wait_limit(polls);
+  return VB_OK;
+}
+
+int vb_set_factor_kernel(int variant) {
+  if (variant < 0 || variant > 1) return fail(VB_ERR_ARG, "factor kernel variant must be 0 or 1");
+  vb::set_factor_variant(variant);
+  return VB_OK;
+}
+
 int vb_chem_rhs(const VbNet* net, int batch, int nz, const double* y, const double* M, const double* k,
                 double* dydt, void* stream) {
   if (!net || !y || !M || !k || !dydt) return fail(VB_ERR_ARG, "null argument");
@@ -472,7 +492,7 @@ int vb_adjoint(const VbNet* net, int batch, int nz, const int64_t* zoff, const d
   a.mode = 1;
   VB_CHECK(vb::launch_sweep(B, ws, a, st), "transposed back sweep");
   // lambda is in the workspace's k1 rows
-  VB_CHECK(vb::launch_gather_k1(B, ws, lambda, st), "lambda");
+  VB_CHECK(vb::launch_gather_stages(B, ws, lambda, nullptr, st), "lambda");
   VB_CHECK(vb::launch_vjp(net->dev, B, y, k, atm, flags, ws, g_k, g_M, g_Kzz, g_top, g_bot, g_vdep, st), "vjp");
   return VB_OK;
 }

@@ -121,6 +121,7 @@ loop_body_kernel(Batch B, VbLoopParams p, const uint8_t* __restrict__ gas, const
         double m = (Eb.ymix[e] < p.mtol) ? 0.0 : d;
         if (c < p.atol) m = 0.0;
         if (bot0 && j == 0) m = 0.0;
+        if ((p.cond_zero_bits[i >> 5] >> (i & 31)) & 1u) m = 0.0;
         const double ratio = (c > 0.0) ? m / fmax(fabs(c), 1e-300) : 0.0;
         dmax = jmax(dmax, ratio);
         notnonneg |= !(c >= 0.0);

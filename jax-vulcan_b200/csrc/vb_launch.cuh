@@ -34,7 +34,15 @@ cudaError_t launch_vjp_atm(const Batch& B, const double* y, const double* atm, i
 cudaError_t launch_vjp(const NetDev&, const Batch&, const double* y, const double* k, const double* atm, int flags,
                        double* ws, double* g_k, double* g_M, double* g_Kzz, double* g_top, double* g_bot,
                        double* g_vdep, cudaStream_t);
-cudaError_t launch_gather_k1(const Batch&, double* ws, double* out, cudaStream_t);
+// Stage rows of the workspace: k1 (or the adjoint's lambda) and, with k2 set,
+// the Ros2 step's k2, into [layers][ni] arrays (either may be nullptr).
+cudaError_t launch_gather_stages(const Batch&, const double* ws, double* k1, double* k2, cudaStream_t);
+// Poll limit of the bounded waits of the factor and sweep kernels (a wait that
+// runs out sets VB_STATUS_WATCHDOG); polls < 0 restores the default.
+void set_wait_limit(long long polls);
+// FP64 factor kernel: 0 = blocked Gauss-Jordan with FP64 tensor-core trailing
+// updates, 1 = scalar Gauss-Jordan.
+void set_factor_variant(int v);
 cudaError_t launch_chem(const NetDev&, int batch, int nz, const double* y, const double* M, const double* k,
                         double* dydt, double* jac, cudaStream_t);
 cudaError_t launch_diffusion(int batch, int nz, int ni, const double* y, const double* atm, int flags,

@@ -104,7 +104,7 @@ template <int RPL, int CPW, int NW, bool DPF, typename R>
 __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
                                                      const double* __restrict__ supn,
                                                      const double* __restrict__ subn, double* rhs,
-                                                     bool tr, int32_t* status, char* smem_raw) {
+                                                     bool tr, int32_t* status, char* smem_raw, long long wlim) {
   using G = GJK<RPL, CPW, NW, R>;
   using R2 = typename Pair<R>::T;
   constexpr int NPR = G::NPR, CPWP = G::CPWP;
@@ -211,7 +211,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   R a[RPL][CPW];
   for (int j = 0; j < nz; ++j) {
     if (DPF) {
-      const bool ok = mbar_wait(bar, (uint32_t)(j & 1), WAIT_LIMIT);
+      const bool ok = mbar_wait(bar, (uint32_t)(j & 1), wlim);
       if (__syncthreads_or(!ok)) {
         // give up: wait (bounded) for the copy still in flight, report, return
         if (threadIdx.x == 0) {
@@ -408,7 +408,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
 template <int RPL, int CPW, int NW, int MB, bool DPF, typename R>
 __global__ void __launch_bounds__(NW * 32, MB)
 gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __restrict__ only,
-                 int32_t* __restrict__ status, int with_rhs, int tr) {
+                 int32_t* __restrict__ status, int with_rhs, int tr, long long wlim) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
   if (only && only[b] == 0) return;
@@ -416,7 +416,396 @@ gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __rest
   WsView w = ws_view(ws, g, B.ni, B.ld);
   R* o = out ? out + g.z0 * B.ni * B.ld : reinterpret_cast<R*>(w.inv);
   gj_factor_atmosphere<RPL, CPW, NW, DPF, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn,
-                                             with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw);
+                                             with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw, wlim);
+}
+
+// ---------------------------------------------------------------- blocked Gauss-Jordan factor (FP64 tensor cores)
+// The same inverse as gj_factor_atmosphere (implicit partial pivoting,
+// unnormalised pivot rows, result scattered to natural order), eliminated in
+// panels of 8 columns, one warp per panel:
+//  * Tile in registers in the FP64 mma accumulator layout: warp w holds
+//    columns 8w..8w+7 of B (B = A'^T when tr), lane (g = lane/4, t = lane%4)
+//    rows 8a+g (a < NW) and columns 8w+2t, 8w+2t+1 - an 8N x 8 column of
+//    m8n8 accumulator tiles.
+//  * Panel q (columns 8q..8q+7): warp q runs its up to 8 pivot steps alone,
+//    with warp-level communication only (argmax by redux.sync, pivot row and
+//    column by shuffles), recording the multipliers m^(s)_i = S[i][k] / piv
+//    of each step s (the m8n8k4 A-operand layout) and the pivot rows p_s.
+//  * Every other warp then applies the panel's 8 steps to its columns C at
+//    once, as the right-looking blocked update (blocked LU's form)
+//        U = L11^{-1} S[P, C]        (L11[s2][s] = m^(s)_{p_s2}, s < s2:
+//                                     the pivot rows as they stood when they
+//                                     pivoted; forward substitution)
+//        S[:, C] -= M U              (M[i][s] = m^(s)_i: rank-8 update,
+//                                     2 NW mma.sync.m8n8k4.f64 per warp)
+//    which equals the 8 single-pivot updates in exact arithmetic. The warp
+//    that owns the next panel applies it to its own columns first and
+//    starts that panel's pivot steps while the others update: one block
+//    barrier per panel instead of one per pivot.
+template <int NW>
+struct BGJ {
+  static constexpr int N = 8 * NW;   // padded rows and columns
+  static constexpr int PBS = 12;     // column stride of a warp's pivot-row block (doubles)
+  __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
+  static size_t smem_bytes(int n, int ld, bool dpf) {
+    const size_t blk = (size_t)n * ld;
+    return al(blk * sizeof(double))                   // Ib: the inverse of the layer (natural order)
+           + (dpf ? al(blk * sizeof(double)) : 0)     // Db: the next diagonal block, prefetched
+           + al(2 * NW * 2 * 32 * sizeof(double))     // Mf: multipliers of a panel, A fragments (2 parities)
+           + al(NW * 8 * PBS * sizeof(double))        // Pb: per-warp pivot-row blocks
+           + al(N * sizeof(double))                   // rps: 1 / pivot of each row
+           + al(2 * N * sizeof(double))               // rsb: the next layer's rhs and sub_d rows
+           + al(2 * N * sizeof(double))               // vecs: right-hand side ping-pong
+           + al(N * sizeof(int))                      // pivs: pivot row of each step
+           + al(N * sizeof(int))                      // pslot: step at which each row pivoted (-1: not yet)
+           + al(2 * 8 * sizeof(int))                  // ppan: pivot rows of a panel (2 parities; -1: none)
+           + 16;                                      // mbarrier of the prefetch
+  }
+};
+
+// D += A B for one m8n8k4 FP64 tile (A: 8x4 row, B: 4x8 col; per lane a0 =
+// A[g][t], b0 = B[t][g], d = D[g][2t], D[g][2t+1]).
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+template <int NW, bool DPF>
+__device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, const double* Din, double* out,
+                                                      const double* __restrict__ supn,
+                                                      const double* __restrict__ subn, double* rhs, bool tr,
+                                                      int32_t* status, char* smem_raw, long long wlim) {
+  using G = BGJ<NW>;
+  constexpr int N = G::N, PBS = G::PBS;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const unsigned FULL = 0xffffffffu;
+  const int blk = n * ld;
+  const int np = (n + 7) >> 3;   // panels holding columns of the block
+  char* sp = smem_raw;
+  auto take = [&](size_t bytes) {
+    char* q = sp;
+    sp += G::al(bytes);
+    return q;
+  };
+  double* Ib = reinterpret_cast<double*>(take((size_t)blk * sizeof(double)));
+  double* Db = DPF ? reinterpret_cast<double*>(take((size_t)blk * sizeof(double))) : nullptr;
+  double* Mf = reinterpret_cast<double*>(take(2 * NW * 2 * 32 * sizeof(double)));
+  double* Pb = reinterpret_cast<double*>(take(NW * 8 * PBS * sizeof(double)));
+  double* rps = reinterpret_cast<double*>(take(N * sizeof(double)));
+  double* rsb = reinterpret_cast<double*>(take(2 * N * sizeof(double)));
+  double* vecs = reinterpret_cast<double*>(take(2 * N * sizeof(double)));
+  int* pivs = reinterpret_cast<int*>(take(N * sizeof(int)));
+  int* pslot = reinterpret_cast<int*>(take(N * sizeof(int)));
+  int* ppan = reinterpret_cast<int*>(take(2 * 8 * sizeof(int)));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(take(16));
+  const uint32_t dbytes = (uint32_t)(blk * sizeof(double));
+  int st_local = 0;
+
+  for (int e = threadIdx.x; e < blk; e += blockDim.x) Ib[e] = 0.0;   // the padding column stays 0
+  if (rhs)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) vecs[i] = rhs[i];
+  if (DPF && threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (DPF && threadIdx.x == 0) {
+    mbar_expect_tx(bar, dbytes);
+    bulk_g2s(Db, Din, dbytes, bar);
+  }
+  // multiplier m^(s)_r of the panel in buffer `buf` (A-fragment order)
+  auto mval = [&](int buf, int r, int s) {
+    return Mf[((buf * NW + (r >> 3)) * 2 + (s >> 2)) * 32 + (r & 7) * 4 + (s & 3)];
+  };
+  double acc[NW][2] = {};
+  // value of row-slot a (warp-uniform or per-lane) of accumulator column e
+  auto pick = [&](int a, int e) {
+    double x = acc[0][e];
+#pragma unroll
+    for (int a2 = 1; a2 < NW; ++a2) x = (a == a2) ? acc[a2][e] : x;
+    return x;
+  };
+
+  // Apply panel q's eliminations to this warp's columns (warp != q).
+  auto apply_panel = [&](int q) {
+    const int buf = q & 1;
+    double* pb = Pb + warp * 8 * PBS;   // pb[c * PBS + s]: pivot row p_s, column c of this warp
+#pragma unroll
+    for (int a = 0; a < NW; ++a) {
+      const int r = 8 * a + g;
+      if (r < n) {
+        const int sl = pslot[r];
+        if (sl >= 0 && (sl >> 3) == q) {
+          const int s = sl & 7;
+          pb[(2 * t) * PBS + s] = acc[a][0];
+          pb[(2 * t + 1) * PBS + s] = acc[a][1];
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < 8) {
+      // forward substitution U = L11^{-1} S[P, c] for column c = lane; stored negated
+      const int* pp = ppan + buf * 8;
+      double u[8];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) u[s] = pp[s] >= 0 ? pb[lane * PBS + s] : 0.0;
+#pragma unroll
+      for (int s2 = 1; s2 < 8; ++s2) {
+        const int r2 = pp[s2];
+        if (r2 >= 0) {
+#pragma unroll
+          for (int s = 0; s < s2; ++s) u[s2] = fma(-mval(buf, r2, s), u[s], u[s2]);
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 8; ++s) pb[lane * PBS + s] = -u[s];
+    }
+    __syncwarp();
+    const double b0 = pb[g * PBS + t], b1 = pb[g * PBS + 4 + t];
+    const double* mf = Mf + (size_t)buf * NW * 2 * 32;
+#pragma unroll
+    for (int a = 0; a < NW; ++a) {
+      dmma_m8n8k4(acc[a][0], acc[a][1], mf[(a * 2 + 0) * 32 + lane], b0);
+      dmma_m8n8k4(acc[a][0], acc[a][1], mf[(a * 2 + 1) * 32 + lane], b1);
+    }
+  };
+
+  // Pivot steps of panel q in warp q (columns 8q + 2t + e of this warp).
+  auto factor_panel = [&](int q) {
+    const int buf = q & 1, k0 = 8 * q;
+    const int cnt = min(8, n - k0);
+    double* mf = Mf + (size_t)buf * NW * 2 * 32;
+    unsigned used = 0;   // row slots a of this lane already pivoted (or padding)
+#pragma unroll
+    for (int a = 0; a < NW; ++a)
+      if (8 * a + g >= n || pslot[8 * a + g] >= 0) used |= 1u << a;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      if (s < cnt) {
+        const int te = s >> 1, ee = s & 1;
+        const bool own = t == te;
+        // ---- argmax of column s over the unpivoted rows (ties to the lowest row)
+        unsigned h[NW];
+#pragma unroll
+        for (int a = 0; a < NW; ++a) {
+          const double v = acc[a][ee];
+          const bool ok = own && 8 * a + g < n && !((used >> a) & 1u) && !isnan(v);
+          h[a] = ok ? hi_key(v) + 1u : 0u;
+        }
+        unsigned hm = h[0];
+#pragma unroll
+        for (int a = 1; a < NW; ++a) hm = max(hm, h[a]);
+        const unsigned m1 = __reduce_max_sync(FULL, hm);
+        int c1 = 0, mys = 0;
+#pragma unroll
+        for (int a = NW - 1; a >= 0; --a)
+          if (h[a] == m1) {
+            ++c1;
+            mys = a;
+          }
+        if (!own) c1 = 0;
+        const unsigned b1 = __ballot_sync(FULL, c1 > 0);
+        const unsigned b2 = __ballot_sync(FULL, c1 > 1);
+        int p;
+        double piv;
+        if (m1 > 0u && __popc(b1) == 1 && b2 == 0u) {
+          const int wl = __ffs(b1) - 1;
+          p = __shfl_sync(FULL, 8 * mys + g, wl);
+          piv = __shfl_sync(FULL, pick(mys, ee), wl);
+        } else {
+          unsigned long long bk = 0ull;
+          unsigned brow = 0xffffffffu;
+#pragma unroll
+          for (int a = 0; a < NW; ++a) {
+            const int r = 8 * a + g;
+            if (own && r < n && !((used >> a) & 1u)) {
+              const unsigned long long kk = pivot_key(acc[a][ee]);
+              if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)r; }
+            }
+          }
+          const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+          const unsigned n1 = __reduce_max_sync(FULL, hi);
+          const unsigned n2 = __reduce_max_sync(FULL, hi == n1 ? lo : 0u);
+          p = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
+          piv = __shfl_sync(FULL, pick(p >> 3, ee), ((p & 7) << 2) | te);
+        }
+        if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
+        const int ap = p >> 3, gp = p & 7;
+        // column s to every lane of the quad, and this lane's part of row p
+        double m[NW];
+#pragma unroll
+        for (int a = 0; a < NW; ++a) m[a] = __shfl_sync(FULL, acc[a][ee], (g << 2) | te);
+        const double pr0 = __shfl_sync(FULL, pick(ap, 0), (gp << 2) | t);
+        const double pr1 = __shfl_sync(FULL, pick(ap, 1), (gp << 2) | t);
+        const double rp = rcp_rn(piv);
+#pragma unroll
+        for (int a = 0; a < NW; ++a) m[a] = (8 * a + g != p) ? m[a] * rp : 0.0;
+#pragma unroll
+        for (int a = 0; a < NW; ++a) {
+          acc[a][0] = fma(-m[a], pr0, acc[a][0]);
+          acc[a][1] = fma(-m[a], pr1, acc[a][1]);
+        }
+#pragma unroll
+        for (int a = 0; a < NW; ++a) {
+          if (own) acc[a][ee] = (8 * a + g == p) ? 1.0 : -m[a];
+          if (t == (s & 3)) mf[(a * 2 + (s >> 2)) * 32 + lane] = m[a];
+        }
+        if (g == gp) used |= 1u << ap;
+        if (lane == 0) {
+          pivs[k0 + s] = p;
+          rps[p] = rp;
+          pslot[p] = k0 + s;
+          ppan[buf * 8 + s] = p;
+        }
+      } else {
+        // no step s: its multiplier column is zero
+#pragma unroll
+        for (int a = 0; a < NW; ++a)
+          if (t == (s & 3)) mf[(a * 2 + (s >> 2)) * 32 + lane] = 0.0;
+        if (lane == 0) ppan[buf * 8 + s] = -1;
+      }
+    }
+  };
+
+  for (int j = 0; j < nz; ++j) {
+    if (DPF) {
+      const bool ok = mbar_wait(bar, (uint32_t)(j & 1), wlim);
+      if (__syncthreads_or(!ok)) {
+        // give up: wait (bounded) for the copy still in flight, report, return
+        if (threadIdx.x == 0) {
+          mbar_wait(bar, (uint32_t)(j & 1), WAIT_LIMIT);
+          atomicOr(status, VB_STATUS_WATCHDOG);
+        }
+        return;
+      }
+    }
+    double rn = 0.0, sn = 0.0;
+    const bool ride = rhs && j + 1 < nz && (int)threadIdx.x < n;
+    if (ride) {
+      rn = rhs[(int64_t)(j + 1) * n + threadIdx.x];
+      sn = subn[(int64_t)j * n + threadIdx.x];
+    }
+    // ---- D_j and the Hadamard Schur update from Inv_{j-1} (solver.py:47):
+    //      tile element (i, m) = B[i][m], A'_j[m][i] when tr, else A'_j[i][m]
+    {
+      const double* D = DPF ? Db : Din + (int64_t)j * blk;
+      double sc[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int mcol = 8 * warp + 2 * t + e;
+        sc[e] = (j > 0 && mcol < n) ? (tr ? subn : supn)[(int64_t)(j - 1) * n + mcol] : 0.0;
+      }
+      const int si = tr ? 1 : ld, sm = tr ? ld : 1;
+#pragma unroll
+      for (int a = 0; a < NW; ++a) {
+        const int i = 8 * a + g;
+        const double sr = (j > 0 && i < n) ? (tr ? supn : subn)[(int64_t)(j - 1) * n + i] : 0.0;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int mcol = 8 * warp + 2 * t + e;
+          double v = 0.0;
+          if (i < n && mcol < n) {
+            const int el = i * si + mcol * sm;
+            v = D[el];
+            if (j > 0) {
+              const double cb = tr ? sc[e] * sr : sr * sc[e];
+              v = v - cb * Ib[el];
+            }
+          }
+          acc[a][e] = v;
+        }
+      }
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) pslot[i] = -1;
+    __syncthreads();   // Db and Ib consumed, pslot cleared
+    if (DPF && threadIdx.x == 0 && j + 1 < nz) {
+      fence_proxy_async();
+      mbar_expect_tx(bar, dbytes);
+      bulk_g2s(Db, Din + (int64_t)(j + 1) * blk, dbytes, bar);
+    }
+    // ================================================================ elimination by panels
+#pragma unroll 1
+    for (int q = 0; q < np; ++q) {
+      if (warp == q) {
+        if (q > 0) apply_panel(q - 1);
+        factor_panel(q);
+      } else if (q > 0 && warp < np && warp != q - 1) {
+        apply_panel(q - 1);
+      }
+      __syncthreads();
+    }
+    if (warp < np && warp != np - 1) apply_panel(np - 1);
+    if (ride) {
+      rsb[threadIdx.x] = rn;
+      rsb[N + threadIdx.x] = sn;
+    }
+    // ---- scale rows by 1/piv, scatter B^{-1}[q(i)][p_m] = T[i][m] into Ib
+    //      (A'^{-1}[p_m][q(i)] when tr)
+#pragma unroll
+    for (int a = 0; a < NW; ++a) {
+      const int i = 8 * a + g;
+      if (i < n) {
+        const double s = rps[i];
+        const int qi = pslot[i];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int mcol = 8 * warp + 2 * t + e;
+          if (mcol < n) {
+            const double v = acc[a][e] * s;
+            if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
+            Ib[tr ? pivs[mcol] * ld + qi : qi * ld + pivs[mcol]] = v;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // ---- Inv_j to global memory (natural order, padding column 0)
+    {
+      double2* O = reinterpret_cast<double2*>(out + (int64_t)j * blk);
+      const double2* S2 = reinterpret_cast<const double2*>(Ib);
+      for (int e = threadIdx.x; e < blk / 2; e += blockDim.x) O[e] = S2[e];
+    }
+    // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
+    if (rhs && j + 1 < nz) {
+      const double* vc = vecs + (j & 1) * N;
+      double* vn = vecs + ((j + 1) & 1) * N;
+      const int sub = lane & 3;
+      for (int i0 = warp * 8; i0 < n; i0 += NW * 8) {
+        const int i = i0 + (lane >> 2);
+        double s0 = 0.0, s1 = 0.0;
+        if (i < n) {
+          int m2 = sub;
+          for (; m2 + 4 < n; m2 += 8) {
+            s0 = fma(Ib[i * ld + m2], vc[m2], s0);
+            s1 = fma(Ib[i * ld + m2 + 4], vc[m2 + 4], s1);
+          }
+          if (m2 < n) s0 = fma(Ib[i * ld + m2], vc[m2], s0);
+        }
+        double s = s0 + s1;
+        s += __shfl_xor_sync(FULL, s, 1);
+        s += __shfl_xor_sync(FULL, s, 2);
+        if (sub == 0 && i < n) {
+          const double v = rsb[i] - rsb[N + i] * s;
+          rhs[(int64_t)(j + 1) * n + i] = v;
+          vn[i] = v;
+        }
+      }
+    }
+  }
+  if (st_local) atomicOr(status, st_local);
+}
+
+template <int NW, int MB, bool DPF>
+__global__ void __launch_bounds__(NW * 32, MB)
+bgj_factor_kernel(Batch B, double* __restrict__ ws, double* out, const int32_t* __restrict__ only,
+                  int32_t* __restrict__ status, int with_rhs, int tr, long long wlim) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const int b = blockIdx.x;
+  if (only && only[b] == 0) return;
+  Geo g = geo_of(B, b);
+  WsView w = ws_view(ws, g, B.ni, B.ld);
+  double* o = out ? out + g.z0 * B.ni * B.ld : w.inv;
+  bgj_factor_atmosphere<NW, DPF>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
+                                 tr != 0, status + b, smem_raw, wlim);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -467,7 +856,7 @@ __device__ inline void block_matvec_s(const double* __restrict__ Inv, int n, int
 // with the Ros2 combination (jax_step.py:313-314). The inverse blocks stream
 // through a ring of `stages` shared-memory buffers filled by bulk copies.
 __global__ void __launch_bounds__(SWEEP_THREADS)
-sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages) {
+sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages, long long wlim) {
   extern __shared__ __align__(128) char smem_raw[];
   const int b = blockIdx.x;
   Geo g = geo_of(B, b);
@@ -534,7 +923,7 @@ sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages) {
       if (j < nz - 1) x = x - c_cpl * u[tid];
       v[tid] = x;
     }
-    const bool ok = mbar_wait(&bars[st], parity, WAIT_LIMIT);
+    const bool ok = mbar_wait(&bars[st], parity, wlim);
     if (__syncthreads_or(!ok)) {
       // give up: wait (bounded) for the copies still in flight, report, return
       if (threadIdx.x == 0) {
@@ -567,6 +956,7 @@ sweep_kernel(Batch B, double* __restrict__ ws, SweepArgs A, int stages) {
           const int64_t e = g.z0 * n + (int64_t)j * n + tid;
           const double s = c_y + (3.0 / (2.0 * r)) * c_k1 + (1.0 / (2.0 * r)) * kj;
           const double yk2 = c_y + c_k1 / r;
+          w.aux[(int64_t)j * n + tid] = kj;   // k2, kept for vb_ros2_stages
           A.sol[e] = s;
           A.delta[e] = fabs(s - yk2);
           if (!isfinite(s)) atomicOr(A.status + b, VB_STATUS_NONFINITE);
@@ -616,6 +1006,12 @@ __global__ void fp64_probe_kernel(double* out, int iters) {
 }
 
 // ---------------------------------------------------------------- launchers
+// Poll limit of the first bounded wait of each bulk copy; a wait that gives up
+// drains the copies still in flight with the full WAIT_LIMIT before the CTA
+// returns, so a lowered limit never leaves a copy writing to a finished CTA.
+static long long g_wait_limit = WAIT_LIMIT;
+void set_wait_limit(long long polls) { g_wait_limit = polls < 0 ? WAIT_LIMIT : polls; }
+
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t st) {
   fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, iters);
   return cudaGetLastError();
@@ -638,9 +1034,42 @@ static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int 
   cudaError_t e = cudaFuncSetAttribute(gj_factor_kernel<RPL, CPW, NW, MB, DPF, R>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs, tr);
+  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs, tr,
+                                                                                 g_wait_limit);
   return cudaGetLastError();
 }
+
+template <int NW, int MB, bool DPF>
+static cudaError_t launch_bgj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
+                                double* out, const int32_t* only) {
+  size_t sm = BGJ<NW>::smem_bytes(B.ni, B.ld, DPF);
+  cudaError_t e = cudaFuncSetAttribute(bgj_factor_kernel<NW, MB, DPF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm);
+  if (e != cudaSuccess) return e;
+  bgj_factor_kernel<NW, MB, DPF><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs, tr, g_wait_limit);
+  return cudaGetLastError();
+}
+
+// Blocked factor shapes: one warp per 8-column panel (NW = ceil(ni / 8)
+// rounded up to the instantiated sizes), the next diagonal block prefetched
+// into shared memory where two copies fit.
+static cudaError_t launch_bgj(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
+                              double* out, const int32_t* only) {
+  if (B.ni <= 32) return launch_bgj_t<4, 4, true>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 64) return launch_bgj_t<8, 2, true>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 72) {
+    if (B.count <= sm_count()) return launch_bgj_t<9, 1, true>(B, ws, status, with_rhs, tr, st, out, only);
+    return launch_bgj_t<9, 2, true>(B, ws, status, with_rhs, tr, st, out, only);
+  }
+  if (B.ni <= 96) return launch_bgj_t<12, 1, true>(B, ws, status, with_rhs, tr, st, out, only);
+  return launch_bgj_t<16, 1, false>(B, ws, status, with_rhs, tr, st, out, only);
+}
+
+// FP64 factor kernel: 0 = blocked Gauss-Jordan with the trailing updates on
+// the FP64 tensor cores (default), 1 = scalar Gauss-Jordan (one block barrier
+// per pivot step).
+static int g_factor_variant = 0;
+void set_factor_variant(int v) { g_factor_variant = v; }
 
 // Tile shapes by block size: rows over 32 lanes x RPL, columns over NW warps
 // x CPW (the next diagonal block is prefetched into shared memory in every
@@ -669,7 +1098,9 @@ static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int wi
 
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
                           bool for_transposed_solves) {
-  return launch_gj<double>(B, ws, status, with_rhs, for_transposed_solves ? 0 : 1, st, nullptr, nullptr);
+  const int tr = for_transposed_solves ? 0 : 1;
+  if (g_factor_variant == 0) return launch_bgj(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
+  return launch_gj<double>(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
 }
 
 // Factors into a separate inverse region (the workspace keeps the FP64
@@ -681,8 +1112,12 @@ cudaError_t launch_factor_into(const Batch& B, double* ws, R* out, const int32_t
   return launch_gj<R>(B, ws, status, 0, 1, st, out, only);
 }
 template cudaError_t launch_factor_into<float>(const Batch&, double*, float*, const int32_t*, int32_t*, cudaStream_t);
-template cudaError_t launch_factor_into<double>(const Batch&, double*, double*, const int32_t*, int32_t*,
-                                                cudaStream_t);
+template <>
+cudaError_t launch_factor_into<double>(const Batch& B, double* ws, double* out, const int32_t* only, int32_t* status,
+                                       cudaStream_t st) {
+  if (g_factor_variant == 0) return launch_bgj(B, ws, status, 0, 1, st, out, only);
+  return launch_gj<double>(B, ws, status, 0, 1, st, out, only);
+}
 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {
   int stages = SWEEP_MAX_STAGES;
@@ -693,7 +1128,7 @@ cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStr
   size_t sm = sweep_smem_bytes(B.ni, stages);
   cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  sweep_kernel<<<B.count, SWEEP_THREADS, sm, st>>>(B, ws, A, stages);
+  sweep_kernel<<<B.count, SWEEP_THREADS, sm, st>>>(B, ws, A, stages, g_wait_limit);
   return cudaGetLastError();
 }
 

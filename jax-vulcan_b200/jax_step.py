@@ -134,6 +134,25 @@ class Ros2Step:
             _lib.ptr(self.ws), self.ws_bytes, _lib.stream_handle(stream)), "vb_ros2_step")
         return sol, delta, self.status
 
+    def stages(self, stream=None):
+        """(k1, k2) of the last call, ``[B, nz, ni]``: the two block solves of
+        the step (reference `jax_step.py:300-311`), read back from the
+        workspace (``vb_ros2_stages``)."""
+        B, nz, ni = self.batch, self.nz, self.net.ni
+        k1 = torch.empty((B, nz, ni), dtype=torch.float64, device="cuda")
+        k2 = torch.empty_like(k1)
+        _lib.check(_lib.lib().vb_ros2_stages(self.net.handle, B, nz, None, _lib.ptr(self.ws), _lib.ptr(k1),
+                                             _lib.ptr(k2), _lib.stream_handle(stream)), "vb_ros2_stages")
+        return k1, k2
+
+
+def set_wait_limit(polls: int | None) -> None:
+    """Poll limit of the first bounded wait on each bulk copy in the factor
+    and sweep kernels (``vb_set_wait_limit``); ``None`` restores the default.
+    For failure-detection tests: a wait that runs out gives the atmosphere
+    ``VB_STATUS_WATCHDOG`` and the kernel returns early."""
+    _lib.check(_lib.lib().vb_set_wait_limit(-1 if polls is None else int(polls)), "vb_set_wait_limit")
+
 
 class RaggedRos2Step:
     """Ros2 step for atmospheres of one network with different layer counts

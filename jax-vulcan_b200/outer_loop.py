@@ -33,7 +33,7 @@ VB_LOOP_ADAPT_RTOL = 4
 class VbLoopParams(C.Structure):
     _fields_ = [("n_atoms", C.c_int32), ("batch_max_retries", C.c_int32), ("flags", C.c_int32),
                 ("adapt_rtol_dec_period", C.c_int32), ("adapt_rtol_inc_period", C.c_int32),
-                ("reserved", C.c_int32)] + [(n, C.c_double) for n in (
+                ("reserved", C.c_int32), ("cond_zero_bits", C.c_uint32 * 4)] + [(n, C.c_double) for n in (
                     "loss_eps", "pos_cut", "nega_cut", "mtol", "atol", "dt_var_min", "dt_var_max", "dt_min",
                     "dt_max", "rtol_min", "rtol_max", "adapt_rtol_dec", "adapt_rtol_inc", "adapt_rtol_loss_mul",
                     "adapt_rtol_inc_loss_thresh")]
@@ -127,6 +127,10 @@ class LoopStatics:
     adapt_rtol_inc_loss_thresh: float = 1e-3
     zero_bot_row: bool = False
     hydro_partial: bool = False
+    # species indices dropped from the error norm (the reference's
+    # condense_zero_mask: condense_sp + non_gas_sp when use_condense is on,
+    # `outer_loop.py:244`, `:1380-1386`)
+    cond_zero: tuple = ()
 
     def params(self, n_atoms: int) -> VbLoopParams:
         if not 1 <= n_atoms <= VB_LOOP_MAX_ATOMS:
@@ -138,6 +142,11 @@ class LoopStatics:
                    | (VB_LOOP_ZERO_BOT_ROW if self.zero_bot_row else 0)
                    | (VB_LOOP_ADAPT_RTOL if self.use_adapt_rtol else 0))
         p.adapt_rtol_dec_period = int(self.adapt_rtol_dec_period)
+        for i in self.cond_zero:
+            i = int(i)
+            if not 0 <= i < 128:
+                raise ValueError("cond_zero species index out of [0, 128)")
+            p.cond_zero_bits[i >> 5] |= 1 << (i & 31)
         p.adapt_rtol_inc_period = int(self.adapt_rtol_inc_period)
         for n in ("loss_eps", "pos_cut", "nega_cut", "mtol", "atol", "dt_var_min", "dt_var_max", "dt_min",
                   "dt_max", "rtol_min", "rtol_max", "adapt_rtol_dec", "adapt_rtol_inc", "adapt_rtol_loss_mul",
@@ -190,11 +199,18 @@ class LoopState:
     _FIELDS = ("y", "y_prev", "ymix", "dt", "atom_loss", "atom_loss_prev", "scalars", "conv", "ring_y", "ring_t",
                "photo_due")
 
-    def save(self, path, **extra):
+    def save(self, path, stream=None, **extra):
         """Checkpoint of the carry (and of any device tensors the run owns,
         given by name: k, the packed atmosphere, the photo carry, dz) to one
         ``.npz``; ``load`` restores it bit for bit, so a run continues as if
-        it had not stopped."""
+        it had not stopped. The attempts may have been queued on another
+        stream than torch's current one: ``stream`` (default: the whole
+        device) is synchronised before the copies, so the checkpoint never
+        holds a half-updated carry."""
+        if stream is not None:
+            stream.synchronize()
+        else:
+            torch.cuda.synchronize()
         arrays = {}
         for f in self._FIELDS:
             t = getattr(self, f, None)

@@ -74,7 +74,7 @@ def mix_from_y(y, gas=None):
 
 
 def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partial=False,
-                zero_bot_row=False, fix_mask=None, fix_y=None, conden=None):
+                zero_bot_row=False, fix_mask=None, fix_y=None, conden=None, cond_zero=None):
     """State after one attempt of the reference loop body given the step's
     (sol, delta_arr): fixed species (`outer_loop.py:733-739`), clip, atom loss,
     error norm (`:741-743`), accept / force-accept (`:745-756`), reject
@@ -89,14 +89,16 @@ def body_update(s, sol, delta_arr, M, compo, atom_ini, p, gas=None, hydro_partia
     use_adapt_rtol, rtol_min, rtol_max, adapt_rtol_dec_period,
     adapt_rtol_inc_period, adapt_rtol_dec, adapt_rtol_inc, adapt_rtol_loss_mul,
     adapt_rtol_inc_loss_thresh. ``gas``: gas-species mask when non-gas species
-    are present (the ysum of clip and mix), else None.
+    are present (the ysum of clip and mix), else None. ``cond_zero``: species
+    mask [ni] whose delta the error norm drops (`:244`), or None.
     """
     if fix_mask is not None:
         sol = np.where(fix_mask, fix_y, sol)
         delta_arr = np.where(fix_mask, 0.0, delta_arr)
     sol_clip, ymix_new, small_inc, nega_inc = clip(sol, s["ymix"], p["mtol"], p["pos_cut"], p["nega_cut"], gas)
     al_new = atom_loss(sol_clip, compo, atom_ini)
-    delta = aggregate_delta(sol_clip, delta_arr, s["ymix"], p["mtol"], p["atol"], zero_bot_row)
+    cz = None if cond_zero is None else np.broadcast_to(np.asarray(cond_zero, bool)[None, :], sol_clip.shape)
+    delta = aggregate_delta(sol_clip, delta_arr, s["ymix"], p["mtol"], p["atol"], zero_bot_row, cz)
     rtol = s["rtol"]
     loss_diff = np.max(np.abs(al_new - s["atom_loss_prev"]))
     accept = bool(np.all(sol_clip >= 0) & (loss_diff < p["loss_eps"]) & (delta <= rtol))

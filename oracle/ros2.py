@@ -448,3 +448,65 @@ def chem_jac_abs(y, M, k, net):
     J = np.zeros(((ni + 1) * (ni + 1), nz))
     np.add.at(J, keys, contrib.reshape(nz, -1).T)
     return J.T.reshape(nz, ni + 1, ni + 1)[:, :ni, :ni]
+
+
+# ----------------------------------------------------------------------------
+# checks of a step computed elsewhere (by its two block solves)
+# ----------------------------------------------------------------------------
+def stage_rhs(y, k, atm, net, fix_mask=None, grav=None):
+    """f(y) = chem_rhs + diffusion with boundary fluxes, the right-hand side
+    of either Ros2 stage before the k1 term (jax_step.py:275-282, :304-309)."""
+    if grav is None:
+        grav = compute_diff_grav(atm)
+    A_e, B_e, C_e, A_m, B_m, C_m, _ = build_diff_coeffs(y, atm, grav)
+    f = chem_rhs(y, atm["M"], k, net) + apply_diffusion(y, A_e, B_e, C_e, A_m, B_m, C_m, atm)
+    if fix_mask is not None:
+        f = np.where(np.asarray(fix_mask, bool), 0.0, f)
+    return f
+
+
+def block_apply(diag, sup_n, sub_n, x):
+    """M x for the block-tridiagonal system of solver.py:33-112 (dense
+    diagonal blocks, diagonal off-diagonal blocks as the solver receives them)."""
+    out = np.einsum("zij,zj->zi", diag, x)
+    out[:-1] += sup_n * x[1:]
+    out[1:] += sub_n * x[:-1]
+    return out
+
+
+def backward_error(diag, sup_n, sub_n, x, rhs):
+    """Normwise backward error ||M x - rhs||_inf / (||M||_inf ||x||_inf + ||rhs||_inf)
+    of a computed solution x of the block system."""
+    res = block_apply(diag, sup_n, sub_n, x) - rhs
+    normM = np.abs(diag).sum(axis=2)
+    normM[:-1] += np.abs(sup_n)
+    normM[1:] += np.abs(sub_n)
+    den = normM.max() * np.abs(x).max() + np.abs(rhs).max()
+    return float(np.abs(res).max() / den) if den > 0 else float(np.abs(res).max())
+
+
+def stage_backward_errors(y, k, dt, atm, net, k1, k2, fix_mask=None):
+    """Backward errors of the two block solves of a Ros2 step whose stage
+    vectors k1, k2 were computed elsewhere: LHS k1 = f(y) and
+    LHS k2 = f(y + k1/r) - 2/(r dt) k1 (jax_step.py:300-311), with the LHS and
+    right-hand sides built here in FP64. Returns (bwd1, bwd2)."""
+    diag, sup_n, sub_n, rhs1, grav = lhs_blocks(y, k, dt, atm, net, fix_mask)
+    yk2 = y + k1 / R_ROS2
+    rhs2 = stage_rhs(yk2, k, atm, net, fix_mask, grav) - (2.0 / (R_ROS2 * dt)) * k1
+    return (backward_error(diag, sup_n, sub_n, k1, rhs1), backward_error(diag, sup_n, sub_n, k2, rhs2))
+
+
+def schur_block_conditions(diag, sup_n, sub_n):
+    """inf-norm condition number of every Schur-updated diagonal block A'_j of
+    the factor recursion (solver.py:44-48)."""
+    nz, ni, _ = diag.shape
+    eye = np.eye(ni)
+    conds = np.empty(nz)
+    A = diag[0]
+    for j in range(nz):
+        if j > 0:
+            A = diag[j] - (sub_n[j - 1][:, None] * sup_n[j - 1][None, :]) * inv
+        lu = sla.lu_factor(A, check_finite=False)
+        inv = sla.lu_solve(lu, eye, check_finite=False)
+        conds[j] = np.abs(A).sum(axis=1).max() * np.abs(inv).sum(axis=1).max()
+    return conds

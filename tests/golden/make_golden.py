@@ -2,7 +2,9 @@
 
 Run in the build container (the reference sources are not on the GPU box):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
+
+(or with the checkout's path in $VULCAN_REFERENCE).
 
 JAX is not installed, so the unmodified reference modules (`network.py`,
 `chem.py`, `solver.py`, `jax_step.py`, `photo.py`, `integrate.py`,
@@ -580,7 +582,9 @@ def refresh_fixture(mods):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("VULCAN_REFERENCE"),
+                    required="VULCAN_REFERENCE" not in os.environ,
+                    help="the reference checkout (default: $VULCAN_REFERENCE)")
     ap.add_argument("--only", default="", help="comma-separated fixture names (default: all)")
     args = ap.parse_args()
     mods, shim = load_reference(args.reference)

@@ -1,0 +1,93 @@
+"""Correctness of the step on the exact inputs the benchmark times.
+
+The default benchmark batch is 296 config-0-shaped atmospheres (two per SM on
+a B200) from ``bench.make_batch``: ni=69, 700+700 reactions, nz=120,
+dt=1e-6 and the specified stiff draw (k log-uniform in [1e-40, 1e-8], mixing
+ratios down to 1e-20). On that draw a single step is ill-conditioned (Schur
+block condition numbers up to ~1e30 and beyond), so elementwise agreement with
+the oracle is not defined; the step is judged by its two block solves:
+
+* every atmosphere: status word 0, sol and delta finite;
+* sampled atmospheres: the normwise backward error
+  ``||M k - rhs||_inf / (||M||_inf ||k||_inf + ||rhs||_inf)`` of both stage
+  solves (k1 with rhs f(y); k2 with rhs f(y + k1/r) - 2/(r dt) k1,
+  reference `jax_step.py:300-311`), with M and the right-hand sides built by
+  the oracle in FP64, must stay below 1e-12;
+* the per-species relative error of sol against the oracle is reported next
+  to the largest Schur block condition number.
+
+The well-conditioned variant of the same batch (order-scaled rate constants,
+``bench.make_batch(..., mild=True)``) must match the oracle elementwise within
+the step bound ``1e-10 * max(|sol_ref|, 1e-30)``.
+"""
+import numpy as np
+import pytest
+import torch
+
+import bench
+from conftest import load_pkg
+from oracle import ros2 as orc
+
+pytestmark = pytest.mark.gpu
+
+chem = load_pkg("chem")
+jstep = load_pkg("jax_step")
+
+BWD_TOL = 1e-12
+STEP_TOL = 1e-10
+
+
+def _run(B, mild):
+    net, cases, Y, K, DT, A = bench.make_batch(B, 0, mild=mild)
+    dn = chem.to_device(net.tables)
+    step = jstep.Ros2Step(dn, jstep.atm_from_dict(A))
+    y = torch.as_tensor(Y, device="cuda")
+    k = torch.as_tensor(K, device="cuda")
+    dt = torch.as_tensor(DT, device="cuda")
+    sol, delta, status = step(y, k, dt)
+    k1, k2 = step.stages()
+    torch.cuda.synchronize()
+    return net, cases, sol.cpu().numpy(), delta.cpu().numpy(), status.cpu().numpy(), k1.cpu().numpy(), \
+        k2.cpu().numpy()
+
+
+def _samples(B):
+    return sorted({0, 1, B // 2 - 1, B // 2, B - 1})
+
+
+@pytest.fixture(scope="module")
+def batch_size():
+    return 2 * torch.cuda.get_device_properties(0).multi_processor_count
+
+
+def test_stiff_bench_batch_status_and_stage_backward_errors(batch_size):
+    B = batch_size
+    net, cases, sol, delta, status, k1, k2 = _run(B, mild=False)
+    assert (status == 0).all(), np.flatnonzero(status)
+    assert np.isfinite(sol).all() and np.isfinite(delta).all()
+    for b in _samples(B):
+        c = cases[b]
+        bwd1, bwd2 = orc.stage_backward_errors(c.y, c.k, c.dt, c.atm, net.tables, k1[b], k2[b])
+        sref, dref, parts = orc.ros2_step(c.y, c.k, c.dt, c.atm, net.tables, return_parts=True)
+        kappa = orc.schur_block_conditions(parts["diag"], parts["sup_neg"], parts["sub_neg"]).max()
+        rel = np.abs(sol[b] - sref) / np.maximum(np.abs(sref), 1e-30)
+        per_species = rel.max(axis=0)
+        print(f"atmosphere {b}: backward errors k1 {bwd1:.2e} k2 {bwd2:.2e}; max Schur block cond "
+              f"{kappa:.2e}; sol rel err vs oracle max {per_species.max():.2e}, median over species "
+              f"{np.median(per_species):.2e}, species within 1e-10: {(per_species <= 1e-10).sum()}/{rel.shape[1]}")
+        assert bwd1 < BWD_TOL, (b, bwd1)
+        assert bwd2 < BWD_TOL, (b, bwd2)
+
+
+def test_well_conditioned_bench_batch_matches_oracle(batch_size):
+    B = batch_size
+    net, cases, sol, delta, status, k1, k2 = _run(B, mild=True)
+    assert (status == 0).all(), np.flatnonzero(status)
+    for b in _samples(B):
+        c = cases[b]
+        sref, dref = orc.ros2_step(c.y, c.k, c.dt, c.atm, net.tables)
+        e_sol = np.max(np.abs(sol[b] - sref) / np.maximum(np.abs(sref), 1e-30))
+        e_del = np.max(np.abs(delta[b] - dref) / np.maximum(np.abs(sref), 1e-30))
+        assert e_sol <= STEP_TOL and e_del <= STEP_TOL, (b, e_sol, e_del)
+        bwd1, bwd2 = orc.stage_backward_errors(c.y, c.k, c.dt, c.atm, net.tables, k1[b], k2[b])
+        assert bwd1 < BWD_TOL and bwd2 < BWD_TOL, (b, bwd1, bwd2)

@@ -18,6 +18,7 @@ import torch
 
 from conftest import BODY_FIELDS, body_kwargs, golden_body, load_pkg
 from oracle import contract as oc
+from oracle import ros2 as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -279,3 +280,40 @@ def test_loop_condensation_matches_oracle_chain():
     kd = k[0].cpu().numpy()
     for r in (row, row + 1):
         assert np.max(np.abs(kd[r] - k_o[r]) / np.maximum(np.abs(k_o[r]), 1e-300)) <= 1e-9, r
+
+
+def test_condensation_mask_drops_species_from_the_error_norm():
+    """The reference's condense_zero_mask (`outer_loop.py:244`, `:1380-1386`):
+    with use_condense on, delta of the condense_sp + non_gas_sp columns is
+    left out of the error norm. A delta field that is small everywhere except
+    one species (above rtol there) makes the attempt a reject without the
+    mask and an accept with that species masked, on the GPU as in the oracle."""
+    net, atm, compo, atom_ini, k, params, cases = golden_body()
+    c = cases["accept"]
+    p, kw = body_kwargs(c, params)
+    inp = c["inp"]
+    sol, delta = orc.ros2_step(inp["y"], k, inp["dt"], atm, net)
+    sol = np.abs(sol) + 1.0          # every entry counts in the norm (sol > atol, positive)
+    ymix_ok = np.asarray(inp["ymix"]) >= p["mtol"]
+    col = int(np.argmax(ymix_ok.all(axis=0)))
+    delta = 1e-6 * np.abs(sol)
+    delta[:, col] = 10.0 * inp["rtol"] * np.abs(sol[:, col])
+    dn = chem.to_device(net)
+    blob = jstep.pack_atm(jstep.atm_from_dict(atm))
+    for masked in (False, True):
+        st = statics_of(p, kw)
+        if masked:
+            st.cond_zero = (col,)
+        state = state_of([inp])
+        loop.loop_body(state, torch.as_tensor(sol[None], device="cuda"), torch.as_tensor(delta[None], device="cuda"),
+                       blob, compo, atom_ini, st, gas_mask=kw["gas"])
+        got = state.snapshot()
+        cz = np.zeros(sol.shape[1], bool)
+        if masked:
+            cz[col] = True
+        ref = oc.body_update(dict(inp), sol, delta, atm["M"], compo, atom_ini, dict(p), gas=kw["gas"],
+                             hydro_partial=kw["hydro_partial"], zero_bot_row=kw["zero_bot_row"],
+                             cond_zero=cz if masked else None)
+        assert int(got["accept_count"][0]) == int(ref["accept_count"]), masked
+        assert int(got["accept_count"][0]) == int(inp["accept_count"]) + (1 if masked else 0), masked
+        check_state(got, 0, ref, f"cond_zero={masked}")

@@ -220,3 +220,39 @@ def test_status_flags():
     f = solver.factor_block_thomas_diag_offdiag(diag, su, sb)
     st = int(f.status.cpu()[0])
     assert st & 1, st
+
+
+@pytest.mark.parametrize("ni,n_fwd", [(48, 400), (120, 900)])
+def test_ros2_step_factor_shapes_mid_and_large(ni, n_fwd):
+    """The factor's tile shapes for 33-64 species and for 97-128 species
+    (the latter without the bulk prefetch of the next block), through the
+    Ros2 step, well-conditioned draw."""
+    net = syn.make_network(47, ni, n_fwd)
+    case = syn.make_case(seed=48, net=net, nz=30, mild=True, k_range=(-40.0, 4.0), moldiff=True)
+    sol_ref, delta_ref = orc.ros2_step(case.y, case.k, case.dt, case.atm, net.tables)
+    dn = chem.to_device(net.tables)
+    sol, delta = jstep.jax_ros2_step(case.y, case.k, case.dt, atm_of(case.atm), dn)
+    check_step(sol.cpu(), delta.cpu(), sol_ref, delta_ref)
+
+
+@pytest.mark.parametrize("ni", [48, 120])
+def test_block_solves_fp64_and_mixed_mid_and_large(ni):
+    """FP64 factor + solve and the mixed-precision (FP32 factor, FP64
+    refinement) solve at the same two tile shapes, against the oracle's
+    block Thomas at 1e-10."""
+    rng = np.random.default_rng(ni)
+    nz, B = 12, 3
+    diag = rng.standard_normal((B, nz, ni, ni))
+    diag = diag + (5.0 + np.abs(diag).sum(axis=3))[..., None] * np.eye(ni)
+    su = 0.1 * rng.standard_normal((B, nz - 1, ni))
+    sb = 0.1 * rng.standard_normal((B, nz - 1, ni))
+    rhs = rng.standard_normal((B, nz, ni))
+    x64 = solver.block_thomas_diag_offdiag(diag, su, sb, rhs).cpu().numpy()
+    f = solver.factor_block_thomas_mixed(diag, su, sb)
+    xm, passes = solver.solve_block_thomas_mixed(f, rhs, max_refine=3, tol=1e-14)
+    xm = xm.cpu().numpy()
+    assert int(f.status.cpu().max()) == 0
+    for b in range(B):
+        ref = orc.block_thomas(diag[b], su[b], sb[b], rhs[b])
+        assert rel_err(x64[b], ref, 1e-12) <= 1e-10
+        assert rel_err(xm[b], ref, 1e-12) <= 1e-10

@@ -60,3 +60,47 @@ def test_vul_round_trip(tmp_path):
         assert p["count"] == snap["accept_count"][b] and p["delta_count"] == snap["delta_count"][b]
         assert p["end_case"] == int(conv["done"][b]) and p["switch_final_photo_frq"] == bool(conv["is_final_photo_frq"][b])
         assert p["where_varies_most"].shape == snap["y"][b].shape
+
+
+def _reference_dir():
+    """The reference checkout: $VULCAN_REFERENCE, else a `reference` directory
+    beside this repository (None when neither exists)."""
+    import os
+    from conftest import ROOT
+    for cand in (os.environ.get("VULCAN_REFERENCE"), os.path.join(os.path.dirname(ROOT), "reference")):
+        if cand and os.path.exists(os.path.join(cand, "tests", "compare_vul.py")):
+            return cand
+    return None
+
+
+def test_vul_read_by_reference_comparison_tool(tmp_path, capsys):
+    """The reference's own reader and comparison tool (`tests/compare_vul.py`:
+    load_vul, the static invariants, time alignment, atom-loss table and
+    per-species log10 ymix metrics) run on files from write_vul: a file
+    against itself passes with bit-exact invariants, and two atmospheres of
+    the same network and initial state are compared species by species."""
+    import importlib.util
+    import pytest
+    ref = _reference_dir()
+    if ref is None:
+        pytest.skip("reference checkout not available")
+    spec = importlib.util.spec_from_file_location("ref_compare_vul", f"{ref}/tests/compare_vul.py")
+    cv = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cv)
+    snap, conv, k, compo, atm = fake_carry()
+    y_ini = snap["y"][0] * 0.9
+    y_ini_b = np.stack([y_ini, y_ini])
+    species = ["A", "B", "C", "D"]
+    snap["t"][1] = snap["t"][0] * 1.01
+    paths = [lio.write_vul(tmp_path / f"atm{b}.vul", species, k, snap, b=b, y_ini=y_ini_b, compo=compo,
+                           atom_order=["H", "O"], atom_ini=np.einsum("bzi,ia->ba", y_ini_b, compo), conv=conv,
+                           atm=atm) for b in range(2)]
+    d = cv.load_vul(paths[0])
+    ok, msgs = cv._check_static_invariants(d["variable"], d["variable"])
+    assert ok and any("bit-exact" in m for m in msgs), msgs
+    assert cv.main([str(paths[0]), str(paths[0])]) == 0
+    out = capsys.readouterr().out
+    assert "species list: identical (4 species)" in out and "y_ini       : bit-exact" in out
+    rc = cv.main([str(paths[0]), str(paths[1]), "--floor", "1e-3"])
+    out = capsys.readouterr().out
+    assert rc in (0, 1) and "Per-species" in out and "H" in out, out
