@@ -89,11 +89,36 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff,
                  double* sol, double* delta, int32_t* status,
                  void* workspace, size_t workspace_bytes, void* stream);
 
+/* Mixed-precision Ros2 step: the same inputs, outputs and FP64 interface as
+ * vb_ros2_step, with the demotion inside. The LHS blocks are assembled in
+ * FP64 (kept for the residual); each Schur-updated block is row-equilibrated
+ * (exact powers of two) and inverted in FP32 by the blocked Gauss-Jordan
+ * factor with its rank-8 trailing updates on the TF32 tensor cores (each
+ * operand split into a TF32 head and tail, three products); each stage solve
+ * LHS k = rhs (jax_step.py:300-311) starts from the FP32 factors and is
+ * refined in FP64 on the full block-tridiagonal system (r = rhs - LHS k from
+ * the FP64 blocks, k += M~^{-1} r) until max|correction| <= tol * max|k|, at
+ * most max_refine passes; atmospheres whose refinement stalls (or whose FP32
+ * factor meets a zero pivot or a non-finite value) are refactored in FP64
+ * and solved directly, with VB_STATUS_REFINE_STALL. sol and delta are formed
+ * in FP64 from the refined stages. passes [B] (nullable): solve and
+ * refinement passes run per atmosphere over both stages. ni <= 96. The
+ * workspace holds the FP64 step workspace, the FP32 inverses and row scales,
+ * and per-atmosphere state (vb_ros2_mixed_workspace_bytes; a ragged batch
+ * sizes it with zoff_host = NULL and nz = its maximum layer count). */
+size_t vb_ros2_mixed_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host);
+int vb_ros2_step_mixed(const VbNet* net, int batch, int nz, const int64_t* zoff,
+                       const double* y, const double* k, const double* dt,
+                       const double* atm, int32_t atm_flags, const uint8_t* fix_mask,
+                       int max_refine, double tol, double* sol, double* delta, int32_t* status,
+                       int32_t* passes, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Stage vectors of the last vb_ros2_step run on `workspace` (the reference's
  * k1 and k2 of jax_step.py:300-311, which jax_ros2_step keeps internal):
  * k1, k2 [B][nz][ni] (or packed by zoff), either may be NULL. For checking a
  * step's two block solves by their backward errors; same batch arguments as
- * the step. */
+ * the step. Also valid after vb_ros2_step_mixed (its workspace starts with
+ * the same layout). */
 int vb_ros2_stages(const VbNet* net, int batch, int nz, const int64_t* zoff, const void* workspace,
                    double* k1, double* k2, void* stream);
 

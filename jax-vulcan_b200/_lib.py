@@ -35,6 +35,9 @@ SIGNATURES = {
     "vb_ros2_workspace_bytes": (_sz, [_i, _i, _i, _p]),
     "vb_ros2_step": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _p, _sz, _p]),
     "vb_ros2_stages": (_i, [_p, _i, _i, _p, _p, _p, _p, _p]),
+    "vb_ros2_mixed_workspace_bytes": (_sz, [_i, _i, _i, _p]),
+    "vb_ros2_step_mixed": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _i32, _p, _i, C.c_double, _p, _p, _p, _p, _p, _sz,
+                                _p]),
     "vb_set_wait_limit": (_i, [C.c_longlong]),
     "vb_set_factor_kernel": (_i, [_i]),
     "vb_chem_rhs": (_i, [_p, _i, _i, _p, _p, _p, _p, _p]),

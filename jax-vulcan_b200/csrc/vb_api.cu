@@ -296,6 +296,90 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const
   return VB_OK;
 }
 
+// ---- mixed-precision step: workspace = FP64 step workspace, mixed region,
+// per-atmosphere mode / todo / FP32 status / pass counters (256-byte aligned)
+namespace {
+struct MixedStepLayout {
+  size_t mx, mode, todo, st32, npass, total;
+};
+MixedStepLayout mixed_step_layout(int batch, int nz, int ni) {
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const int64_t layers = (int64_t)batch * nz;
+  MixedStepLayout m;
+  m.mx = al(vb_ros2_workspace_bytes(batch, nz, ni, nullptr));
+  m.mode = m.mx + al((size_t)layers * vb::mx_bytes_per_layer(ni));
+  m.todo = m.mode + al((size_t)batch * 4);
+  m.st32 = m.todo + al((size_t)batch * 4);
+  m.npass = m.st32 + al((size_t)batch * 4);
+  m.total = m.npass + al((size_t)batch * 4);
+  return m;
+}
+}  // namespace
+
+size_t vb_ros2_mixed_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host) {
+  if (batch < 1 || ni < 1) return 0;
+  const int64_t layers = zoff_host ? zoff_host[batch] : (int64_t)batch * nz;
+  const int nzs = (int)((layers + batch - 1) / batch);   // a ragged batch is sized by its layer total
+  return mixed_step_layout(batch, zoff_host ? (nz > nzs ? nz : nzs) : nz, ni).total;
+}
+
+int vb_ros2_step_mixed(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
+                       const double* dt, const double* atm, int32_t flags, const uint8_t* fix_mask, int max_refine,
+                       double tol, double* sol, double* delta, int32_t* status, int32_t* passes, void* workspace,
+                       size_t ws_bytes, void* stream) {
+  if (!net || !y || !k || !dt || !atm || !sol || !delta || !status || !workspace)
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  if (net->dev.ni > 96) return fail(VB_ERR_ARG, "the mixed-precision step supports ni <= 96");
+  if (max_refine < 0 || max_refine > 8) return fail(VB_ERR_ARG, "max_refine must be in [0, 8]");
+  if (!(tol > 0.0)) return fail(VB_ERR_ARG, "tol must be positive");
+  const MixedStepLayout L = mixed_step_layout(batch, nz, net->dev.ni);
+  if (ws_bytes < L.total)
+    return fail(VB_ERR_ARG, "workspace too small (vb_ros2_mixed_workspace_bytes with zoff_host = NULL and nz = "
+                            "the maximum layer count)");
+  cudaStream_t st = (cudaStream_t)stream;
+  vb::Batch B = make_batch(net, batch, nz, zoff);
+  char* base = (char*)workspace;
+  double* ws = (double*)base;
+  void* mxr = base + L.mx;
+  int32_t* mode = (int32_t*)(base + L.mode);
+  int32_t* todo = (int32_t*)(base + L.todo);
+  int32_t* st32 = (int32_t*)(base + L.st32);
+  int32_t* np = (int32_t*)(base + L.npass);
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  VB_CHECK(cudaMemsetAsync(st32, 0, sizeof(int32_t) * batch, st), "fp32 status reset");
+  VB_CHECK(cudaMemsetAsync(np, 0, sizeof(int32_t) * batch, st), "passes reset");
+  {
+    ProfScope p(0, st);
+    VB_CHECK(vb::launch_stage1(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage1");
+  }
+  {
+    ProfScope p(1, st);
+    VB_CHECK(vb::launch_factor32(B, ws, mxr, st32, st), "fp32 factor");
+    VB_CHECK(vb::launch_mx_mode(batch, 0, mode, todo, st32, status, st), "modes");
+    VB_CHECK(vb::launch_factor_only(B, ws, todo, status, st), "fp64 factor (fp32 failures)");
+  }
+  for (int stage = 0; stage < 2; ++stage) {
+    if (stage == 1) {
+      ProfScope p(3, st);
+      VB_CHECK(vb::launch_stage2(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage2");
+    }
+    ProfScope p(stage == 0 ? 2 : 4, st);
+    VB_CHECK(vb::launch_mx_pass(B, ws, mxr, stage, true, mode, nullptr, np, tol, status, st), "solve");
+    for (int it = 0; it < max_refine; ++it)
+      VB_CHECK(vb::launch_mx_pass(B, ws, mxr, stage, false, mode, nullptr, np, tol, status, st), "refinement");
+    VB_CHECK(vb::launch_mx_mode(batch, 1, mode, todo, st32, status, st), "stall");
+    VB_CHECK(vb::launch_factor_only(B, ws, todo, status, st), "fp64 factor (stalled)");
+    VB_CHECK(vb::launch_mx_pass(B, ws, mxr, stage, true, mode, todo, np, tol, status, st), "fp64 solve");
+  }
+  {
+    ProfScope p(5, st);
+    VB_CHECK(vb::launch_mx_finish(B, ws, y, sol, delta, status, st), "sol and delta");
+  }
+  if (passes) VB_CHECK(cudaMemcpyAsync(passes, np, sizeof(int32_t) * batch, cudaMemcpyDeviceToDevice, st), "passes");
+  return VB_OK;
+}
+
 int vb_ros2_stages(const VbNet* net, int batch, int nz, const int64_t* zoff, const void* workspace, double* k1,
                    double* k2, void* stream) {
   if (!net || !workspace) return fail(VB_ERR_ARG, "null argument");

@@ -124,6 +124,29 @@ __device__ __forceinline__ WsView ws_view(double* ws, const Geo& g, int ni, int 
 
 __host__ __device__ inline int round_even(int n) { return (n + 1) & ~1; }
 
+// ---- mixed-precision region of the Ros2 step (after the FP64 workspace):
+// per atmosphere, [nz][ni][ldf] FP32 inverses of the row-equilibrated
+// eliminated blocks (ldf = ni rounded up to 4, so each block is a multiple of
+// 16 bytes), then [nz][ni] row scales r (A'^{-1} = X diag(r)), then [nz][ni]
+// scratch (the forward-eliminated residual of a refinement pass).
+__host__ __device__ inline int round4(int n) { return (n + 3) & ~3; }
+__host__ __device__ inline int64_t mx_bytes_per_layer(int ni) {
+  return (int64_t)ni * round4(ni) * 4 + 16 * (int64_t)ni;
+}
+struct MxView {
+  float* X;      // [nz][ni][ldf]
+  double* rs;    // [nz][ni]
+  double* tmp;   // [nz][ni]
+};
+__host__ __device__ inline MxView mx_view(void* mx, int64_t z0, int nz, int ni) {
+  char* base = static_cast<char*>(mx) + z0 * mx_bytes_per_layer(ni);
+  MxView v;
+  v.X = reinterpret_cast<float*>(base);
+  v.rs = reinterpret_cast<double*>(base + (int64_t)nz * ni * round4(ni) * 4);
+  v.tmp = v.rs + (int64_t)nz * ni;
+  return v;
+}
+
 // ---------------------------------------------------------------- bulk copies
 // Global -> shared bulk copies (cp.async.bulk, no multicast) completed on an
 // mbarrier. Every wait is bounded: a wait that gives up reports false and the

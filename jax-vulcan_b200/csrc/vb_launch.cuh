@@ -40,6 +40,7 @@ cudaError_t launch_gather_stages(const Batch&, const double* ws, double* k1, dou
 // Poll limit of the bounded waits of the factor and sweep kernels (a wait that
 // runs out sets VB_STATUS_WATCHDOG); polls < 0 restores the default.
 void set_wait_limit(long long polls);
+long long wait_limit();
 // FP64 factor kernel: 0 = blocked Gauss-Jordan with FP64 tensor-core trailing
 // updates, 1 = scalar Gauss-Jordan.
 void set_factor_variant(int v);
@@ -81,6 +82,21 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, c
 template <typename R>
 cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,
                           int32_t* passes, double tol, int first, const int32_t* only, cudaStream_t st);
+// Mixed-precision Ros2 step (vb_mixed.cu): one solve pass (first: x = M~^{-1} b;
+// else one FP64-residual refinement pass) over rmod -> k1 (xsel 0) / aux (1).
+cudaError_t launch_mx_pass(const Batch& B, double* ws, void* mxr, int xsel, bool first, int32_t* mode,
+                           const int32_t* only, int32_t* passes, double tol, int32_t* status, cudaStream_t st);
+// op 0: modes after the FP32 factor; op 1: stalled refinements to FP64 (todo)
+cudaError_t launch_mx_mode(int batch, int op, int32_t* mode, int32_t* todo, int32_t* status32, int32_t* status,
+                           cudaStream_t st);
+cudaError_t launch_mx_finish(const Batch& B, const double* ws, const double* y, double* sol, double* delta,
+                             int32_t* status, cudaStream_t st);
+// FP32 factor of the mixed step: row-equilibrated blocks, blocked Gauss-Jordan
+// with 3xTF32 tensor-core trailing updates; inverses and row scales into the
+// mixed region, the FP64 blocks stay in the workspace.
+cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st);
+// FP64 factor of the atmospheres with only[b] != 0, in place over their blocks.
+cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, int32_t* status, cudaStream_t st);
 cudaError_t launch_refine_finalize(int batch, const int32_t* state, int32_t* fallback, int32_t* status,
                                    cudaStream_t st);
 template <typename R>

@@ -419,47 +419,59 @@ gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __rest
                                              with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw, wlim);
 }
 
-// ---------------------------------------------------------------- blocked Gauss-Jordan factor (FP64 tensor cores)
+// ---------------------------------------------------------------- blocked Gauss-Jordan factor (tensor cores)
 // The same inverse as gj_factor_atmosphere (implicit partial pivoting,
 // unnormalised pivot rows, result scattered to natural order), eliminated in
 // panels of 8 columns, one warp per panel:
-//  * Tile in registers in the FP64 mma accumulator layout: warp w holds
-//    columns 8w..8w+7 of B (B = A'^T when tr), lane (g = lane/4, t = lane%4)
-//    rows 8a+g (a < NW) and columns 8w+2t, 8w+2t+1 - an 8N x 8 column of
-//    m8n8 accumulator tiles.
+//  * Tile in registers in the mma accumulator layout: warp w holds columns
+//    8w..8w+7 of B (B = A'^T when tr), lane (g = lane/4, t = lane%4) rows
+//    8a+g (a < MR) and columns 8w+2t, 8w+2t+1: FP64 m8n8 accumulator tiles,
+//    or (FP32) pairs of row groups forming m16n8 tiles.
 //  * Panel q (columns 8q..8q+7): warp q runs its up to 8 pivot steps alone,
 //    with warp-level communication only (argmax by redux.sync, pivot row and
 //    column by shuffles), recording the multipliers m^(s)_i = S[i][k] / piv
-//    of each step s (the m8n8k4 A-operand layout) and the pivot rows p_s.
+//    of each step s (the mma A-operand layout) and the pivot rows p_s.
 //  * Every other warp then applies the panel's 8 steps to its columns C at
 //    once, as the right-looking blocked update (blocked LU's form)
 //        U = L11^{-1} S[P, C]        (L11[s2][s] = m^(s)_{p_s2}, s < s2:
 //                                     the pivot rows as they stood when they
 //                                     pivoted; forward substitution)
-//        S[:, C] -= M U              (M[i][s] = m^(s)_i: rank-8 update,
-//                                     2 NW mma.sync.m8n8k4.f64 per warp)
+//        S[:, C] -= M U              (M[i][s] = m^(s)_i: a rank-8 update,
+//                                     mma.sync m8n8k4 FP64, or m16n8k8 TF32
+//                                     with each operand split into a TF32
+//                                     head and tail and three products
+//                                     (head*head + head*tail + tail*head)
+//                                     accumulated in FP32)
 //    which equals the 8 single-pivot updates in exact arithmetic. The warp
 //    that owns the next panel applies it to its own columns first and
 //    starts that panel's pivot steps while the others update: one block
 //    barrier per panel instead of one per pivot.
-template <int NW>
+//  * EQ (FP32, tr): before the elimination every row of A'_j is scaled by a
+//    power of two bringing its largest magnitude to [1, 2) (row
+//    equilibration, exact); the stored inverse is X = (R A'_j)^{-1} with the
+//    scales r, so A'_j^{-1} = X diag(r).
+template <int NW, int MR, typename R>
 struct BGJ {
-  static constexpr int N = 8 * NW;   // padded rows and columns
-  static constexpr int PBS = 12;     // column stride of a warp's pivot-row block (doubles)
+  static constexpr int N = 8 * NW;   // padded columns (and rows of the FP64 tile)
+  static constexpr int NR = 8 * MR;  // padded rows
+  static constexpr int PBS = 12;     // column stride of a warp's pivot-row block
+  static constexpr int MF = 2 * MR * 2 * 32;   // multiplier fragments of a panel (2 parities)
+  static constexpr bool F32 = sizeof(R) == 4;
   __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
-  static size_t smem_bytes(int n, int ld, bool dpf) {
-    const size_t blk = (size_t)n * ld;
-    return al(blk * sizeof(double))                   // Ib: the inverse of the layer (natural order)
-           + (dpf ? al(blk * sizeof(double)) : 0)     // Db: the next diagonal block, prefetched
-           + al(2 * NW * 2 * 32 * sizeof(double))     // Mf: multipliers of a panel, A fragments (2 parities)
-           + al(NW * 8 * PBS * sizeof(double))        // Pb: per-warp pivot-row blocks
-           + al(N * sizeof(double))                   // rps: 1 / pivot of each row
-           + al(2 * N * sizeof(double))               // rsb: the next layer's rhs and sub_d rows
-           + al(2 * N * sizeof(double))               // vecs: right-hand side ping-pong
-           + al(N * sizeof(int))                      // pivs: pivot row of each step
-           + al(N * sizeof(int))                      // pslot: step at which each row pivoted (-1: not yet)
-           + al(2 * 8 * sizeof(int))                  // ppan: pivot rows of a panel (2 parities; -1: none)
-           + 16;                                      // mbarrier of the prefetch
+  static size_t smem_bytes(int n, int ld, int li, bool dpf) {
+    return al((size_t)n * li * sizeof(R))                      // Ib: the inverse of the layer (natural order)
+           + (dpf ? al((size_t)n * ld * sizeof(double)) : 0)   // Db: the next diagonal block, prefetched
+           + al(MF * sizeof(R))                                // Mf: multipliers, A fragments
+           + (F32 ? 2 * al(MF * sizeof(uint32_t)) : 0)         // TF32 head and tail of Mf
+           + al(NW * 8 * PBS * sizeof(R))                      // Pb: per-warp pivot-row blocks
+           + al(NR * sizeof(R))                                // rps: 1 / pivot of each row
+           + al(2 * NR * sizeof(double))                       // rsb: the next layer's rhs and sub_d rows
+           + al(2 * NR * sizeof(double))                       // vecs: right-hand side ping-pong
+           + al(2 * N * sizeof(double))                        // rsc: row scales of this and the previous layer
+           + al(N * sizeof(int))                               // pivs: pivot row of each step
+           + al(NR * sizeof(int))                              // pslot: step at which each row pivoted (-1: not yet)
+           + al(2 * 8 * sizeof(int))                           // ppan: pivot rows of a panel (2 parities; -1: none)
+           + 16;                                               // mbarrier of the prefetch
   }
 };
 
@@ -471,17 +483,49 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
       : "d"(a), "d"(b));
 }
 
-template <int NW, bool DPF>
-__device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, const double* Din, double* out,
-                                                      const double* __restrict__ supn,
+// D += A B for one m16n8k8 TF32 tile (FP32 accumulation; per lane a = A[g][t],
+// A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g]; d = D[g][2t],
+// D[g][2t+1], D[g+8][2t], D[g+8][2t+1]).
+__device__ __forceinline__ void mma_tf32(float& d0, float& d1, float& d2, float& d3, uint32_t a0, uint32_t a1,
+                                         uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d0), "+f"(d1), "+f"(d2), "+f"(d3)
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// TF32 head of x (round to nearest, ties away) and the TF32 head of the rest.
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+
+// Power of two s with s * m in [1, 2) for a finite m > 0 (1 otherwise).
+__device__ __forceinline__ double pow2_scale(double m) {
+  if (!(m > 0.0) || !isfinite(m)) return 1.0;
+  int e;
+  frexp(m, &e);               // m = f 2^e, f in [0.5, 1)
+  return ldexp(1.0, 1 - e);   // s m = 2 f in [1, 2)
+}
+
+template <int NW, int MR, bool DPF, bool EQ, typename R>
+__device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, int li, const double* Din, R* out,
+                                                      double* rs_out, const double* __restrict__ supn,
                                                       const double* __restrict__ subn, double* rhs, bool tr,
                                                       int32_t* status, char* smem_raw, long long wlim) {
-  using G = BGJ<NW>;
-  constexpr int N = G::N, PBS = G::PBS;
+  using G = BGJ<NW, MR, R>;
+  constexpr int N = G::N, NR = G::NR, PBS = G::PBS, MF = G::MF;
+  constexpr bool F32 = G::F32;
+  static_assert(!F32 || (MR % 2) == 0, "the FP32 tile pairs row groups into m16 tiles");
+  static_assert(MR >= NW, "rows cover the columns");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const unsigned FULL = 0xffffffffu;
-  const int blk = n * ld;
+  const int dblk = n * ld, iblk = n * li;
   const int np = (n + 7) >> 3;   // panels holding columns of the block
   char* sp = smem_raw;
   auto take = [&](size_t bytes) {
@@ -489,21 +533,24 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
     sp += G::al(bytes);
     return q;
   };
-  double* Ib = reinterpret_cast<double*>(take((size_t)blk * sizeof(double)));
-  double* Db = DPF ? reinterpret_cast<double*>(take((size_t)blk * sizeof(double))) : nullptr;
-  double* Mf = reinterpret_cast<double*>(take(2 * NW * 2 * 32 * sizeof(double)));
-  double* Pb = reinterpret_cast<double*>(take(NW * 8 * PBS * sizeof(double)));
-  double* rps = reinterpret_cast<double*>(take(N * sizeof(double)));
-  double* rsb = reinterpret_cast<double*>(take(2 * N * sizeof(double)));
-  double* vecs = reinterpret_cast<double*>(take(2 * N * sizeof(double)));
+  R* Ib = reinterpret_cast<R*>(take((size_t)iblk * sizeof(R)));
+  double* Db = DPF ? reinterpret_cast<double*>(take((size_t)dblk * sizeof(double))) : nullptr;
+  R* Mf = reinterpret_cast<R*>(take(MF * sizeof(R)));
+  uint32_t* Mh = F32 ? reinterpret_cast<uint32_t*>(take(MF * sizeof(uint32_t))) : nullptr;
+  uint32_t* Ml = F32 ? reinterpret_cast<uint32_t*>(take(MF * sizeof(uint32_t))) : nullptr;
+  R* Pb = reinterpret_cast<R*>(take(NW * 8 * PBS * sizeof(R)));
+  R* rps = reinterpret_cast<R*>(take(NR * sizeof(R)));
+  double* rsb = reinterpret_cast<double*>(take(2 * NR * sizeof(double)));
+  double* vecs = reinterpret_cast<double*>(take(2 * NR * sizeof(double)));
+  double* rsc = reinterpret_cast<double*>(take(2 * N * sizeof(double)));
   int* pivs = reinterpret_cast<int*>(take(N * sizeof(int)));
-  int* pslot = reinterpret_cast<int*>(take(N * sizeof(int)));
+  int* pslot = reinterpret_cast<int*>(take(NR * sizeof(int)));
   int* ppan = reinterpret_cast<int*>(take(2 * 8 * sizeof(int)));
   uint64_t* bar = reinterpret_cast<uint64_t*>(take(16));
-  const uint32_t dbytes = (uint32_t)(blk * sizeof(double));
+  const uint32_t dbytes = (uint32_t)(dblk * sizeof(double));
   int st_local = 0;
 
-  for (int e = threadIdx.x; e < blk; e += blockDim.x) Ib[e] = 0.0;   // the padding column stays 0
+  for (int e = threadIdx.x; e < iblk; e += blockDim.x) Ib[e] = R(0);   // padding columns stay 0
   if (rhs)
     for (int i = threadIdx.x; i < n; i += blockDim.x) vecs[i] = rhs[i];
   if (DPF && threadIdx.x == 0) mbar_init(bar, 1);
@@ -514,23 +561,23 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
   }
   // multiplier m^(s)_r of the panel in buffer `buf` (A-fragment order)
   auto mval = [&](int buf, int r, int s) {
-    return Mf[((buf * NW + (r >> 3)) * 2 + (s >> 2)) * 32 + (r & 7) * 4 + (s & 3)];
+    return Mf[((buf * MR + (r >> 3)) * 2 + (s >> 2)) * 32 + (r & 7) * 4 + (s & 3)];
   };
-  double acc[NW][2] = {};
+  R acc[MR][2] = {};
   // value of row-slot a (warp-uniform or per-lane) of accumulator column e
   auto pick = [&](int a, int e) {
-    double x = acc[0][e];
+    R x = acc[0][e];
 #pragma unroll
-    for (int a2 = 1; a2 < NW; ++a2) x = (a == a2) ? acc[a2][e] : x;
+    for (int a2 = 1; a2 < MR; ++a2) x = (a == a2) ? acc[a2][e] : x;
     return x;
   };
 
   // Apply panel q's eliminations to this warp's columns (warp != q).
   auto apply_panel = [&](int q) {
     const int buf = q & 1;
-    double* pb = Pb + warp * 8 * PBS;   // pb[c * PBS + s]: pivot row p_s, column c of this warp
+    R* pb = Pb + warp * 8 * PBS;   // pb[c * PBS + s]: pivot row p_s, column c of this warp
 #pragma unroll
-    for (int a = 0; a < NW; ++a) {
+    for (int a = 0; a < MR; ++a) {
       const int r = 8 * a + g;
       if (r < n) {
         const int sl = pslot[r];
@@ -545,9 +592,9 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
     if (lane < 8) {
       // forward substitution U = L11^{-1} S[P, c] for column c = lane; stored negated
       const int* pp = ppan + buf * 8;
-      double u[8];
+      R u[8];
 #pragma unroll
-      for (int s = 0; s < 8; ++s) u[s] = pp[s] >= 0 ? pb[lane * PBS + s] : 0.0;
+      for (int s = 0; s < 8; ++s) u[s] = pp[s] >= 0 ? pb[lane * PBS + s] : R(0);
 #pragma unroll
       for (int s2 = 1; s2 < 8; ++s2) {
         const int r2 = pp[s2];
@@ -560,12 +607,31 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
       for (int s = 0; s < 8; ++s) pb[lane * PBS + s] = -u[s];
     }
     __syncwarp();
-    const double b0 = pb[g * PBS + t], b1 = pb[g * PBS + 4 + t];
-    const double* mf = Mf + (size_t)buf * NW * 2 * 32;
+    const R b0 = pb[g * PBS + t], b1 = pb[g * PBS + 4 + t];
+    if constexpr (!F32) {
+      const R* mf = Mf + (size_t)buf * MR * 2 * 32;
 #pragma unroll
-    for (int a = 0; a < NW; ++a) {
-      dmma_m8n8k4(acc[a][0], acc[a][1], mf[(a * 2 + 0) * 32 + lane], b0);
-      dmma_m8n8k4(acc[a][0], acc[a][1], mf[(a * 2 + 1) * 32 + lane], b1);
+      for (int a = 0; a < MR; ++a) {
+        dmma_m8n8k4(acc[a][0], acc[a][1], mf[(a * 2 + 0) * 32 + lane], b0);
+        dmma_m8n8k4(acc[a][0], acc[a][1], mf[(a * 2 + 1) * 32 + lane], b1);
+      }
+    } else {
+      uint32_t bh0, bl0, bh1, bl1;
+      tf32_split(b0, bh0, bl0);
+      tf32_split(b1, bh1, bl1);
+      const uint32_t* mh = Mh + (size_t)buf * MR * 2 * 32;
+      const uint32_t* ml = Ml + (size_t)buf * MR * 2 * 32;
+#pragma unroll
+      for (int T = 0; T < MR / 2; ++T) {
+        const int a0 = 2 * T, a1 = 2 * T + 1;
+        const uint32_t h0 = mh[(a0 * 2 + 0) * 32 + lane], h1 = mh[(a1 * 2 + 0) * 32 + lane];
+        const uint32_t h2 = mh[(a0 * 2 + 1) * 32 + lane], h3 = mh[(a1 * 2 + 1) * 32 + lane];
+        const uint32_t l0 = ml[(a0 * 2 + 0) * 32 + lane], l1 = ml[(a1 * 2 + 0) * 32 + lane];
+        const uint32_t l2 = ml[(a0 * 2 + 1) * 32 + lane], l3 = ml[(a1 * 2 + 1) * 32 + lane];
+        mma_tf32(acc[a0][0], acc[a0][1], acc[a1][0], acc[a1][1], l0, l1, l2, l3, bh0, bh1);   // tail * head
+        mma_tf32(acc[a0][0], acc[a0][1], acc[a1][0], acc[a1][1], h0, h1, h2, h3, bl0, bl1);   // head * tail
+        mma_tf32(acc[a0][0], acc[a0][1], acc[a1][0], acc[a1][1], h0, h1, h2, h3, bh0, bh1);   // head * head
+      }
     }
   };
 
@@ -573,10 +639,10 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
   auto factor_panel = [&](int q) {
     const int buf = q & 1, k0 = 8 * q;
     const int cnt = min(8, n - k0);
-    double* mf = Mf + (size_t)buf * NW * 2 * 32;
+    R* mf = Mf + (size_t)buf * MR * 2 * 32;
     unsigned used = 0;   // row slots a of this lane already pivoted (or padding)
 #pragma unroll
-    for (int a = 0; a < NW; ++a)
+    for (int a = 0; a < MR; ++a)
       if (8 * a + g >= n || pslot[8 * a + g] >= 0) used |= 1u << a;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
@@ -584,20 +650,20 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
         const int te = s >> 1, ee = s & 1;
         const bool own = t == te;
         // ---- argmax of column s over the unpivoted rows (ties to the lowest row)
-        unsigned h[NW];
+        unsigned h[MR];
 #pragma unroll
-        for (int a = 0; a < NW; ++a) {
-          const double v = acc[a][ee];
+        for (int a = 0; a < MR; ++a) {
+          const R v = acc[a][ee];
           const bool ok = own && 8 * a + g < n && !((used >> a) & 1u) && !isnan(v);
           h[a] = ok ? hi_key(v) + 1u : 0u;
         }
         unsigned hm = h[0];
 #pragma unroll
-        for (int a = 1; a < NW; ++a) hm = max(hm, h[a]);
+        for (int a = 1; a < MR; ++a) hm = max(hm, h[a]);
         const unsigned m1 = __reduce_max_sync(FULL, hm);
         int c1 = 0, mys = 0;
 #pragma unroll
-        for (int a = NW - 1; a >= 0; --a)
+        for (int a = MR - 1; a >= 0; --a)
           if (h[a] == m1) {
             ++c1;
             mys = a;
@@ -606,7 +672,7 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
         const unsigned b1 = __ballot_sync(FULL, c1 > 0);
         const unsigned b2 = __ballot_sync(FULL, c1 > 1);
         int p;
-        double piv;
+        R piv;
         if (m1 > 0u && __popc(b1) == 1 && b2 == 0u) {
           const int wl = __ffs(b1) - 1;
           p = __shfl_sync(FULL, 8 * mys + g, wl);
@@ -615,7 +681,7 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
           unsigned long long bk = 0ull;
           unsigned brow = 0xffffffffu;
 #pragma unroll
-          for (int a = 0; a < NW; ++a) {
+          for (int a = 0; a < MR; ++a) {
             const int r = 8 * a + g;
             if (own && r < n && !((used >> a) & 1u)) {
               const unsigned long long kk = pivot_key(acc[a][ee]);
@@ -628,26 +694,30 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
           p = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
           piv = __shfl_sync(FULL, pick(p >> 3, ee), ((p & 7) << 2) | te);
         }
-        if (piv == 0.0) st_local |= VB_STATUS_ZERO_PIVOT;
+        if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
         const int ap = p >> 3, gp = p & 7;
         // column s to every lane of the quad, and this lane's part of row p
-        double m[NW];
+        R m[MR];
 #pragma unroll
-        for (int a = 0; a < NW; ++a) m[a] = __shfl_sync(FULL, acc[a][ee], (g << 2) | te);
-        const double pr0 = __shfl_sync(FULL, pick(ap, 0), (gp << 2) | t);
-        const double pr1 = __shfl_sync(FULL, pick(ap, 1), (gp << 2) | t);
-        const double rp = rcp_rn(piv);
+        for (int a = 0; a < MR; ++a) m[a] = __shfl_sync(FULL, acc[a][ee], (g << 2) | te);
+        const R pr0 = __shfl_sync(FULL, pick(ap, 0), (gp << 2) | t);
+        const R pr1 = __shfl_sync(FULL, pick(ap, 1), (gp << 2) | t);
+        const R rp = rcp_rn(piv);
 #pragma unroll
-        for (int a = 0; a < NW; ++a) m[a] = (8 * a + g != p) ? m[a] * rp : 0.0;
+        for (int a = 0; a < MR; ++a) m[a] = (8 * a + g != p) ? m[a] * rp : R(0);
 #pragma unroll
-        for (int a = 0; a < NW; ++a) {
+        for (int a = 0; a < MR; ++a) {
           acc[a][0] = fma(-m[a], pr0, acc[a][0]);
           acc[a][1] = fma(-m[a], pr1, acc[a][1]);
         }
 #pragma unroll
-        for (int a = 0; a < NW; ++a) {
-          if (own) acc[a][ee] = (8 * a + g == p) ? 1.0 : -m[a];
-          if (t == (s & 3)) mf[(a * 2 + (s >> 2)) * 32 + lane] = m[a];
+        for (int a = 0; a < MR; ++a) {
+          if (own) acc[a][ee] = (8 * a + g == p) ? R(1) : -m[a];
+          if (t == (s & 3)) {
+            const int fi = (a * 2 + (s >> 2)) * 32 + lane;
+            mf[fi] = m[a];
+            if constexpr (F32) tf32_split(m[a], Mh[buf * MR * 2 * 32 + fi], Ml[buf * MR * 2 * 32 + fi]);
+          }
         }
         if (g == gp) used |= 1u << ap;
         if (lane == 0) {
@@ -659,8 +729,15 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
       } else {
         // no step s: its multiplier column is zero
 #pragma unroll
-        for (int a = 0; a < NW; ++a)
-          if (t == (s & 3)) mf[(a * 2 + (s >> 2)) * 32 + lane] = 0.0;
+        for (int a = 0; a < MR; ++a)
+          if (t == (s & 3)) {
+            const int fi = (a * 2 + (s >> 2)) * 32 + lane;
+            mf[fi] = R(0);
+            if constexpr (F32) {
+              Mh[buf * MR * 2 * 32 + fi] = 0u;
+              Ml[buf * MR * 2 * 32 + fi] = 0u;
+            }
+          }
         if (lane == 0) ppan[buf * 8 + s] = -1;
       }
     }
@@ -686,41 +763,72 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
     }
     // ---- D_j and the Hadamard Schur update from Inv_{j-1} (solver.py:47):
     //      tile element (i, m) = B[i][m], A'_j[m][i] when tr, else A'_j[i][m]
+    //      (EQ: Inv_{j-1} = X_{j-1} diag(r_{j-1}), and row m of A'_j is scaled)
     {
-      const double* D = DPF ? Db : Din + (int64_t)j * blk;
+      const double* D = DPF ? Db : Din + (int64_t)j * dblk;
+      const double* rprev = rsc + ((j + 1) & 1) * N;
       double sc[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int mcol = 8 * warp + 2 * t + e;
         sc[e] = (j > 0 && mcol < n) ? (tr ? subn : supn)[(int64_t)(j - 1) * n + mcol] : 0.0;
       }
-      const int si = tr ? 1 : ld, sm = tr ? ld : 1;
+      const int si = tr ? 1 : ld, sm = tr ? ld : 1;     // element strides of D (tile rows / columns)
+      const int ii = tr ? 1 : li, im = tr ? li : 1;     // and of Ib
+      double v[MR][2];
+      double cmax[2] = {0.0, 0.0};
 #pragma unroll
-      for (int a = 0; a < NW; ++a) {
+      for (int a = 0; a < MR; ++a) {
         const int i = 8 * a + g;
         const double sr = (j > 0 && i < n) ? (tr ? supn : subn)[(int64_t)(j - 1) * n + i] : 0.0;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int mcol = 8 * warp + 2 * t + e;
-          double v = 0.0;
+          double x = 0.0;
           if (i < n && mcol < n) {
-            const int el = i * si + mcol * sm;
-            v = D[el];
+            x = D[i * si + mcol * sm];
             if (j > 0) {
               const double cb = tr ? sc[e] * sr : sr * sc[e];
-              v = v - cb * Ib[el];
+              double inv = (double)Ib[i * ii + mcol * im];
+              if (EQ) inv = inv * rprev[i];
+              x = x - cb * inv;
             }
           }
-          acc[a][e] = v;
+          v[a][e] = x;
+          if (EQ) cmax[e] = fmax(cmax[e], fabs(x));
         }
       }
+      if (EQ) {
+        // largest magnitude of each tile column (row m of A'_j) over the 8 lanes sharing t
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+#pragma unroll
+          for (int off = 4; off < 32; off <<= 1) cmax[e] = fmax(cmax[e], __shfl_xor_sync(FULL, cmax[e], off));
+        double* rcur = rsc + (j & 1) * N;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const double s = pow2_scale(cmax[e]);
+          const int mcol = 8 * warp + 2 * t + e;
+          if (g == 0 && mcol < n) {
+            rcur[mcol] = s;
+            rs_out[(int64_t)j * n + mcol] = s;
+          }
+#pragma unroll
+          for (int a = 0; a < MR; ++a) v[a][e] *= s;
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < MR; ++a) {
+        acc[a][0] = (R)v[a][0];
+        acc[a][1] = (R)v[a][1];
+      }
     }
-    for (int i = threadIdx.x; i < N; i += blockDim.x) pslot[i] = -1;
+    for (int i = threadIdx.x; i < NR; i += blockDim.x) pslot[i] = -1;
     __syncthreads();   // Db and Ib consumed, pslot cleared
     if (DPF && threadIdx.x == 0 && j + 1 < nz) {
       fence_proxy_async();
       mbar_expect_tx(bar, dbytes);
-      bulk_g2s(Db, Din + (int64_t)(j + 1) * blk, dbytes, bar);
+      bulk_g2s(Db, Din + (int64_t)(j + 1) * dblk, dbytes, bar);
     }
     // ================================================================ elimination by panels
 #pragma unroll 1
@@ -736,38 +844,39 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
     if (warp < np && warp != np - 1) apply_panel(np - 1);
     if (ride) {
       rsb[threadIdx.x] = rn;
-      rsb[N + threadIdx.x] = sn;
+      rsb[NR + threadIdx.x] = sn;
     }
     // ---- scale rows by 1/piv, scatter B^{-1}[q(i)][p_m] = T[i][m] into Ib
     //      (A'^{-1}[p_m][q(i)] when tr)
 #pragma unroll
-    for (int a = 0; a < NW; ++a) {
+    for (int a = 0; a < MR; ++a) {
       const int i = 8 * a + g;
       if (i < n) {
-        const double s = rps[i];
+        const R s = rps[i];
         const int qi = pslot[i];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int mcol = 8 * warp + 2 * t + e;
           if (mcol < n) {
-            const double v = acc[a][e] * s;
+            const R v = acc[a][e] * s;
             if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
-            Ib[tr ? pivs[mcol] * ld + qi : qi * ld + pivs[mcol]] = v;
+            Ib[tr ? pivs[mcol] * li + qi : qi * li + pivs[mcol]] = v;
           }
         }
       }
     }
     __syncthreads();
-    // ---- Inv_j to global memory (natural order, padding column 0)
+    // ---- Inv_j to global memory (natural order, padding columns 0)
     {
-      double2* O = reinterpret_cast<double2*>(out + (int64_t)j * blk);
-      const double2* S2 = reinterpret_cast<const double2*>(Ib);
-      for (int e = threadIdx.x; e < blk / 2; e += blockDim.x) O[e] = S2[e];
+      using V = typename Pair<R>::T;
+      V* O = reinterpret_cast<V*>(out + (int64_t)j * iblk);
+      const V* S2 = reinterpret_cast<const V*>(Ib);
+      for (int e = threadIdx.x; e < iblk / 2; e += blockDim.x) O[e] = S2[e];
     }
     // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
     if (rhs && j + 1 < nz) {
-      const double* vc = vecs + (j & 1) * N;
-      double* vn = vecs + ((j + 1) & 1) * N;
+      const double* vc = vecs + (j & 1) * NR;
+      double* vn = vecs + ((j + 1) & 1) * NR;
       const int sub = lane & 3;
       for (int i0 = warp * 8; i0 < n; i0 += NW * 8) {
         const int i = i0 + (lane >> 2);
@@ -775,16 +884,16 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
         if (i < n) {
           int m2 = sub;
           for (; m2 + 4 < n; m2 += 8) {
-            s0 = fma(Ib[i * ld + m2], vc[m2], s0);
-            s1 = fma(Ib[i * ld + m2 + 4], vc[m2 + 4], s1);
+            s0 = fma((double)Ib[i * li + m2], vc[m2], s0);
+            s1 = fma((double)Ib[i * li + m2 + 4], vc[m2 + 4], s1);
           }
-          if (m2 < n) s0 = fma(Ib[i * ld + m2], vc[m2], s0);
+          if (m2 < n) s0 = fma((double)Ib[i * li + m2], vc[m2], s0);
         }
         double s = s0 + s1;
         s += __shfl_xor_sync(FULL, s, 1);
         s += __shfl_xor_sync(FULL, s, 2);
         if (sub == 0 && i < n) {
-          const double v = rsb[i] - rsb[N + i] * s;
+          const double v = rsb[i] - rsb[NR + i] * s;
           rhs[(int64_t)(j + 1) * n + i] = v;
           vn[i] = v;
         }
@@ -794,6 +903,9 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, con
   if (st_local) atomicOr(status, st_local);
 }
 
+// FP64: out == nullptr: the inverses replace the blocks in the workspace,
+// otherwise they go to out (layer-major, ni x ld per layer). only != nullptr:
+// atmospheres with only[b] == 0 are skipped.
 template <int NW, int MB, bool DPF>
 __global__ void __launch_bounds__(NW * 32, MB)
 bgj_factor_kernel(Batch B, double* __restrict__ ws, double* out, const int32_t* __restrict__ only,
@@ -804,8 +916,24 @@ bgj_factor_kernel(Batch B, double* __restrict__ ws, double* out, const int32_t* 
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
   double* o = out ? out + g.z0 * B.ni * B.ld : w.inv;
-  bgj_factor_atmosphere<NW, DPF>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn, with_rhs ? w.rmod : nullptr,
-                                 tr != 0, status + b, smem_raw, wlim);
+  bgj_factor_atmosphere<NW, NW, DPF, false, double>(g.nz, B.ni, B.ld, B.ld, w.inv, o, nullptr, w.supn, w.subn,
+                                                     with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw,
+                                                     wlim);
+}
+
+// FP32 factor of the mixed-precision step (row-equilibrated, transposed
+// orientation): FP32 inverses and row scales into the mixed region.
+template <int NW, int MR, int MB, bool DPF>
+__global__ void __launch_bounds__(NW * 32, MB)
+bgj32_factor_kernel(Batch B, double* __restrict__ ws, void* __restrict__ mxr, int32_t* __restrict__ status,
+                    long long wlim) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const int b = blockIdx.x;
+  Geo g = geo_of(B, b);
+  WsView w = ws_view(ws, g, B.ni, B.ld);
+  MxView m = mx_view(mxr, g.z0, g.nz, B.ni);
+  bgj_factor_atmosphere<NW, MR, DPF, true, float>(g.nz, B.ni, B.ld, round4(B.ni), w.inv, m.X, m.rs, w.supn, w.subn,
+                                                   nullptr, true, status + b, smem_raw, wlim);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -1011,6 +1139,7 @@ __global__ void fp64_probe_kernel(double* out, int iters) {
 // returns, so a lowered limit never leaves a copy writing to a finished CTA.
 static long long g_wait_limit = WAIT_LIMIT;
 void set_wait_limit(long long polls) { g_wait_limit = polls < 0 ? WAIT_LIMIT : polls; }
+long long wait_limit() { return g_wait_limit; }
 
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t st) {
   fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, iters);
@@ -1042,7 +1171,7 @@ static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int 
 template <int NW, int MB, bool DPF>
 static cudaError_t launch_bgj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
                                 double* out, const int32_t* only) {
-  size_t sm = BGJ<NW>::smem_bytes(B.ni, B.ld, DPF);
+  size_t sm = BGJ<NW, NW, double>::smem_bytes(B.ni, B.ld, B.ld, DPF);
   cudaError_t e = cudaFuncSetAttribute(bgj_factor_kernel<NW, MB, DPF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sm);
   if (e != cudaSuccess) return e;
@@ -1063,6 +1192,31 @@ static cudaError_t launch_bgj(const Batch& B, double* ws, int32_t* status, int w
   }
   if (B.ni <= 96) return launch_bgj_t<12, 1, true>(B, ws, status, with_rhs, tr, st, out, only);
   return launch_bgj_t<16, 1, false>(B, ws, status, with_rhs, tr, st, out, only);
+}
+
+template <int NW, int MR, int MB, bool DPF>
+static cudaError_t launch_bgj32_t(const Batch& B, double* ws, void* mxr, int32_t* status, cudaStream_t st) {
+  size_t sm = BGJ<NW, MR, float>::smem_bytes(B.ni, B.ld, round4(B.ni), DPF);
+  cudaError_t e = cudaFuncSetAttribute(bgj32_factor_kernel<NW, MR, MB, DPF>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  bgj32_factor_kernel<NW, MR, MB, DPF><<<B.count, NW * 32, sm, st>>>(B, ws, mxr, status, g_wait_limit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st) {
+  if (B.ni <= 32) return launch_bgj32_t<4, 4, 4, true>(B, ws, mxr, status32, st);
+  if (B.ni <= 64) return launch_bgj32_t<8, 8, 2, true>(B, ws, mxr, status32, st);
+  if (B.ni <= 72) {
+    if (B.count <= sm_count()) return launch_bgj32_t<9, 10, 1, true>(B, ws, mxr, status32, st);
+    return launch_bgj32_t<9, 10, 2, true>(B, ws, mxr, status32, st);
+  }
+  if (B.ni <= 96) return launch_bgj32_t<12, 12, 1, true>(B, ws, mxr, status32, st);
+  return launch_bgj32_t<16, 16, 1, false>(B, ws, mxr, status32, st);
+}
+
+cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, int32_t* status, cudaStream_t st) {
+  return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
 }
 
 // FP64 factor kernel: 0 = blocked Gauss-Jordan with the trailing updates on

@@ -98,8 +98,16 @@ class Ros2Step:
     so repeated calls allocate nothing.
     """
 
-    def __init__(self, net: NetworkArrays, atm: AtmStatic, batch: int | None = None):
+    def __init__(self, net: NetworkArrays, atm: AtmStatic, batch: int | None = None, mixed: bool = False,
+                 max_refine: int = 3, tol: float = 1e-12):
+        """``mixed=True``: the mixed-precision step (``vb_ros2_step_mixed``:
+        FP32 row-equilibrated factor on the TF32 tensor cores, FP64 refinement
+        of both stages, at most ``max_refine`` passes to ``tol``, FP64
+        fallback); ``self.passes`` then holds the passes run per atmosphere."""
         self.net = net
+        self.mixed = bool(mixed)
+        self.max_refine = int(max_refine)
+        self.tol = float(tol)
         self.blob = pack_atm(atm)
         self.flags = atm_flags(atm)
         self.batch = self.blob.shape[0] if batch is None else int(batch)
@@ -110,9 +118,11 @@ class Ros2Step:
         ni = net.ni
         self.nz = (self.blob.shape[1] - 6 * ni) // (8 + 3 * ni)
         L = _lib.lib()
-        self.ws_bytes = int(L.vb_ros2_workspace_bytes(self.batch, self.nz, ni, None))
+        size = L.vb_ros2_mixed_workspace_bytes if self.mixed else L.vb_ros2_workspace_bytes
+        self.ws_bytes = int(size(self.batch, self.nz, ni, None))
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
         self.status = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
+        self.passes = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
 
     def __call__(self, y, k, dt, fix_mask=None, out=None, stream=None):
         """Returns (sol, delta, status) as device tensors of the batch shape."""
@@ -128,10 +138,17 @@ class Ros2Step:
             delta = torch.empty_like(y)
         else:
             sol, delta = out
-        _lib.check(_lib.lib().vb_ros2_step(
-            self.net.handle, B, nz, None, _lib.ptr(y), _lib.ptr(k), _lib.ptr(dt), _lib.ptr(self.blob),
-            self.flags, _lib.ptr(fm), _lib.ptr(sol), _lib.ptr(delta), _lib.ptr(self.status),
-            _lib.ptr(self.ws), self.ws_bytes, _lib.stream_handle(stream)), "vb_ros2_step")
+        if self.mixed:
+            _lib.check(_lib.lib().vb_ros2_step_mixed(
+                self.net.handle, B, nz, None, _lib.ptr(y), _lib.ptr(k), _lib.ptr(dt), _lib.ptr(self.blob),
+                self.flags, _lib.ptr(fm), self.max_refine, self.tol, _lib.ptr(sol), _lib.ptr(delta),
+                _lib.ptr(self.status), _lib.ptr(self.passes), _lib.ptr(self.ws), self.ws_bytes,
+                _lib.stream_handle(stream)), "vb_ros2_step_mixed")
+        else:
+            _lib.check(_lib.lib().vb_ros2_step(
+                self.net.handle, B, nz, None, _lib.ptr(y), _lib.ptr(k), _lib.ptr(dt), _lib.ptr(self.blob),
+                self.flags, _lib.ptr(fm), _lib.ptr(sol), _lib.ptr(delta), _lib.ptr(self.status),
+                _lib.ptr(self.ws), self.ws_bytes, _lib.stream_handle(stream)), "vb_ros2_step")
         return sol, delta, self.status
 
     def stages(self, stream=None):
