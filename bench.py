@@ -270,7 +270,9 @@ def run_config2(args, torch):
     nets, cases = syn.config2_batch(seed=2, batch=args.batch or 256)
     dev = {id(n): chem.to_device(n.tables) for n in nets.values()}
     items = [(dev[id(c.net)], jstep.atm_from_dict(c.atm), c.y, c.k, c.dt) for c in cases]
-    batch = jstep.MultiNetworkBatch(items)
+    # launch shapes per network group chosen by the autotuner on this GPU (timed
+    # candidates: factor kernel, factor CTAs per SM, sweep ring depth)
+    batch = jstep.MultiNetworkBatch(items, tuning="tune")
     batch.capture()
     for _ in range(args.warmup):
         batch.step()
@@ -309,6 +311,8 @@ def run_config2(args, torch):
                        "groups": len(batch.groups), "l2": "inputs larger than L2, no flush"},
             "sequential_single_instance": {"value": n / (seq_ms * 1e-3), "unit": UNIT, "ms_per_pass": seq_ms},
             "speedup_vs_sequential": seq_ms / ms, "gpu_launches": 6 * len(batch.groups) * args.steps,
+            "tuning": {k: {"tuning": v["tuning"], "ms": v["ms"], "candidates_ms": v["candidates"]}
+                       for k, v in batch.tuned.items()},
             "clocks": clk}
 
 
@@ -802,6 +806,37 @@ def main():
     wcheck = oracle_check(net, wcases, solw, deltaw, stepw.status, *stepw.stages(), samples=(0, B - 1)) \
         if rank == 0 else None
 
+    # the mixed-precision step (FP32 row-equilibrated factor on the TF32
+    # tensor cores, FP64 refinement, FP64 fallback) on both draws, same batch
+    def mixed_run(stepm, yy, kk, dd, cs):
+        sm_, dm_ = torch.empty_like(yy), torch.empty_like(yy)
+        for _ in range(args.warmup):
+            stepm(yy, kk, dd, out=(sm_, dm_))
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            stepm(yy, kk, dd, out=(sm_, dm_))
+        e1.record()
+        torch.cuda.synchronize()
+        mms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, world, "cuda")
+        st_m = stepm.status.cpu().numpy()
+        out = {"value": job_value(world, B, mms), "unit": UNIT, "ms_per_step": mms,
+               "fallback_fraction": float(((st_m & 4) != 0).mean()),
+               "passes_max": int(stepm.passes.max().item()), "passes_mean": float(stepm.passes.float().mean())}
+        if rank == 0:
+            chk = oracle_check(net, cs, sm_, dm_, stepm.status, *stepm.stages(), samples=(0, B - 1))
+            out.update(status_ok_or_fallback=bool(((st_m & ~4) == 0).all()) and chk["finite"],
+                       max_rel_err_vs_oracle=chk["max_rel_err_vs_oracle"],
+                       stage_backward_error_max=chk["stage_backward_error_max"],
+                       per_species_max_rel_err_vs_oracle=chk["per_species_max_rel_err_vs_oracle"])
+        return out
+
+    stepm = jstep.Ros2Step(dn, atm, mixed=True)
+    mixed_stiff = mixed_run(stepm, y, k, dt, cases)
+    stepmw = jstep.Ros2Step(dn, jstep.atm_from_dict(Aw), mixed=True)
+    mixed_wc = mixed_run(stepmw, yw, kw, dtw, wcases)
+    del stepm, stepmw
+
     peak64 = fp64_peak_tflops(L, torch, sh)
     ni, nz = net.tables.ni, Y.shape[1]
     # Gauss-Jordan inverse of every layer block: ni^3 FMAs = 2*ni^3 flops counted
@@ -867,6 +902,14 @@ def main():
                                             "(Schur block condition numbers far beyond 1/eps), so sol is judged "
                                             "by the backward errors of its two block solves; elementwise errors "
                                             "are reported, not bounded"),
+            "mixed_precision": {"well_conditioned": mixed_wc, "stiff": mixed_stiff,
+                                "vs_single_instance_fp64_well_conditioned":
+                                    mixed_wc["value"] * single_ms * 1e-3,
+                                "note": "vb_ros2_step_mixed: FP64 assembly, row-equilibrated FP32 blocked "
+                                        "Gauss-Jordan factor with TF32 tensor-core trailing updates (head/tail "
+                                        "split, three products), FP64-residual refinement of both stages "
+                                        "(<= 3 passes, tol 1e-12), FP64 refactor fallback; errors against the "
+                                        "oracle on atmospheres 0 and B-1"},
             "well_conditioned": {"value": job_value(world, B, wc_ms), "unit": UNIT, "ms_per_step": wc_ms,
                                  "data": "same shapes, order-scaled rate constants (pseudo-first-order rates "
                                          "log-uniform in [1e-40, 1e4] s^-1)",

@@ -75,6 +75,21 @@ int vb_net_create(int ni, int nr, int max_terms,
                   const double* reactant_stoich, const double* product_stoich,
                   const uint8_t* is_three_body, VbNet** out);
 int vb_net_destroy(VbNet* net);
+/* Launch shapes of the steps run with a network (no counterpart in the
+ * reference, whose XLA compiler picks its own): set by the project's
+ * autotuner (jax-vulcan_b200/autotune.py), which times the candidates on the
+ * device per network and batch; 0 in a field = the automatic choice.
+ *   factor_kernel: 1 blocked Gauss-Jordan on the tensor cores, 2 scalar
+ *                  Gauss-Jordan (0: the process default, vb_set_factor_kernel)
+ *   factor_ctas:   CTAs per SM of the factor, 1 or 2 (honoured for 65-72
+ *                  species, the shape with both variants compiled)
+ *   sweep_stages:  depth of the sweeps' bulk-copy ring, 1..3 (lowered when
+ *                  the ring does not fit in shared memory) */
+typedef struct VbTuning {
+  int32_t factor_kernel, factor_ctas, sweep_stages, reserved;
+} VbTuning;
+int vb_net_set_tuning(VbNet* net, const VbTuning* tuning);
+int vb_net_get_tuning(const VbNet* net, VbTuning* tuning);
 /* Device bytes held by a network. */
 size_t vb_net_device_bytes(const VbNet* net);
 

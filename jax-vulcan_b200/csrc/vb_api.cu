@@ -18,6 +18,7 @@ struct VbNet {
   vb::NetDev dev;
   void* base;
   size_t bytes;
+  VbTuning tune;
 };
 
 static thread_local std::string g_err;
@@ -200,6 +201,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
     if (e != cudaSuccess) { cudaFree(base); return cuda_fail(e, "cudaMemcpy"); }
   }
   VbNet* net = new VbNet;
+  net->tune = VbTuning{0, 0, 0, 0};
   char* b = (char*)base;
   vb::NetDev& d = net->dev;
   d.ni = ni; d.nr = nr; d.T = T;
@@ -233,6 +235,21 @@ int vb_net_destroy(VbNet* net) {
 
 size_t vb_net_device_bytes(const VbNet* net) { return net ? net->bytes : 0; }
 
+int vb_net_set_tuning(VbNet* net, const VbTuning* t) {
+  if (!net || !t) return fail(VB_ERR_ARG, "null argument");
+  if (t->factor_kernel < 0 || t->factor_kernel > 2 || t->factor_ctas < 0 || t->factor_ctas > 2 ||
+      t->sweep_stages < 0 || t->sweep_stages > 3)
+    return fail(VB_ERR_ARG, "tuning out of range (factor_kernel 0..2, factor_ctas 0..2, sweep_stages 0..3)");
+  net->tune = *t;
+  return VB_OK;
+}
+
+int vb_net_get_tuning(const VbNet* net, VbTuning* t) {
+  if (!net || !t) return fail(VB_ERR_ARG, "null argument");
+  *t = net->tune;
+  return VB_OK;
+}
+
 size_t vb_ros2_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host) {
   int64_t layers = zoff_host ? zoff_host[batch] : (int64_t)batch * nz;
   return (size_t)layers * vb::ws_per_layer(ni, vb::round_even(ni)) * sizeof(double);
@@ -246,6 +263,9 @@ static vb::Batch make_batch(const VbNet* net, int batch, int nz, const int64_t* 
   B.nr = net->dev.nr;
   B.ld = vb::round_even(B.ni);
   B.zoff = zoff;
+  B.factor_kernel = net->tune.factor_kernel;
+  B.factor_ctas = net->tune.factor_ctas;
+  B.sweep_stages = net->tune.sweep_stages;
   return B;
 }
 

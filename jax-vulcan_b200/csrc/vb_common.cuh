@@ -69,6 +69,10 @@ struct Batch {
   int nr;             // reaction slots (k has nr+1 rows)
   int ld;             // row stride of stored inverse blocks (ni rounded up to even)
   const int64_t* zoff;  // [count+1] prefix sums of layers, or nullptr (uniform)
+  // launch shapes chosen by the network's tuning (VbTuning; 0 = automatic)
+  int factor_kernel = 0;   // 1 blocked tensor-core, 2 scalar Gauss-Jordan
+  int factor_ctas = 0;     // CTAs per SM of the factor (1 or 2, where both fit)
+  int sweep_stages = 0;    // bulk-copy ring depth of the sweeps (1..3)
 };
 
 struct Geo {

@@ -1156,6 +1156,13 @@ static int sm_count() {
   return n;
 }
 
+// One factor CTA per SM (the wider tile) or two: the tuning's choice, else
+// one when the batch has at most one atmosphere per SM.
+static bool one_cta_per_sm(const Batch& B) {
+  if (B.factor_ctas) return B.factor_ctas == 1;
+  return B.count <= sm_count();
+}
+
 template <int RPL, int CPW, int NW, int MB, bool DPF, typename R = double>
 static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
                                R* out = nullptr, const int32_t* only = nullptr) {
@@ -1187,7 +1194,7 @@ static cudaError_t launch_bgj(const Batch& B, double* ws, int32_t* status, int w
   if (B.ni <= 32) return launch_bgj_t<4, 4, true>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 64) return launch_bgj_t<8, 2, true>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 72) {
-    if (B.count <= sm_count()) return launch_bgj_t<9, 1, true>(B, ws, status, with_rhs, tr, st, out, only);
+    if (one_cta_per_sm(B)) return launch_bgj_t<9, 1, true>(B, ws, status, with_rhs, tr, st, out, only);
     return launch_bgj_t<9, 2, true>(B, ws, status, with_rhs, tr, st, out, only);
   }
   if (B.ni <= 96) return launch_bgj_t<12, 1, true>(B, ws, status, with_rhs, tr, st, out, only);
@@ -1208,7 +1215,7 @@ cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* stat
   if (B.ni <= 32) return launch_bgj32_t<4, 4, 4, true>(B, ws, mxr, status32, st);
   if (B.ni <= 64) return launch_bgj32_t<8, 8, 2, true>(B, ws, mxr, status32, st);
   if (B.ni <= 72) {
-    if (B.count <= sm_count()) return launch_bgj32_t<9, 10, 1, true>(B, ws, mxr, status32, st);
+    if (one_cta_per_sm(B)) return launch_bgj32_t<9, 10, 1, true>(B, ws, mxr, status32, st);
     return launch_bgj32_t<9, 10, 2, true>(B, ws, mxr, status32, st);
   }
   if (B.ni <= 96) return launch_bgj32_t<12, 12, 1, true>(B, ws, mxr, status32, st);
@@ -1240,7 +1247,7 @@ static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int wi
   if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 72) {
-    if (B.count <= sm_count()) return launch_gj_t<3, 6, 12, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+    if (one_cta_per_sm(B)) return launch_gj_t<3, 6, 12, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
     return launch_gj_t<3, 6, 12, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   }
   // up to 96 species: 16 warps of 6 columns (the uneven 256-atmosphere batch,
@@ -1253,7 +1260,8 @@ static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int wi
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
                           bool for_transposed_solves) {
   const int tr = for_transposed_solves ? 0 : 1;
-  if (g_factor_variant == 0) return launch_bgj(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
+  const bool blocked = B.factor_kernel ? B.factor_kernel == 1 : g_factor_variant == 0;
+  if (blocked) return launch_bgj(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
   return launch_gj<double>(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
 }
 
@@ -1274,10 +1282,10 @@ cudaError_t launch_factor_into<double>(const Batch& B, double* ws, double* out, 
 }
 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {
-  int stages = SWEEP_MAX_STAGES;
+  int stages = B.sweep_stages ? B.sweep_stages : SWEEP_MAX_STAGES;
   while (stages > 1 && sweep_smem_bytes(B.ni, stages) > 220 * 1024) --stages;
   // more atmospheres than SMs: a shallower ring lets two CTAs share an SM (one wave)
-  if (B.count > sm_count())
+  if (!B.sweep_stages && B.count > sm_count())
     while (stages > 2 && 2 * sweep_smem_bytes(B.ni, stages) > 224 * 1024) --stages;
   size_t sm = sweep_smem_bytes(B.ni, stages);
   cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

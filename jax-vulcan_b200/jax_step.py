@@ -243,10 +243,13 @@ class MultiNetworkBatch:
     records the whole batch step as one CUDA graph for replay.
 
     ``cases``: sequence of ``(net, atm, y, k, dt)`` with ``y [nz, ni]``,
-    ``k [nr+1, nz]``; results come back in the order given.
+    ``k [nr+1, nz]``; results come back in the order given. ``tuning``:
+    launch shapes per group from the autotuner (``autotune.py``): a cache
+    dict, the path of a cache file, or "tune" to time the candidates now
+    (``self.tuned`` records what was applied).
     """
 
-    def __init__(self, cases):
+    def __init__(self, cases, tuning=None):
         cases = list(cases)
         groups = {}
         for idx, (net, atm, y, k, dt) in enumerate(cases):
@@ -262,6 +265,17 @@ class MultiNetworkBatch:
                                     stream=torch.cuda.Stream()))
         self.batch = len(cases)
         self.graph = None
+        self.tuned = {}
+        if tuning is not None:
+            from . import autotune
+            if isinstance(tuning, str) and tuning == "tune":
+                self.tuned = autotune.tune_batch(self)
+            else:
+                cache = autotune.load_cache(tuning) if isinstance(tuning, str) else dict(tuning)
+                autotune.apply_cache(self, cache)
+                self.tuned = {k: v for k, v in cache.items()
+                              if k in {autotune.group_key(g["step"].net, g["step"].batch, g["step"].layers)
+                                       for g in self.groups}}
 
     def _launch(self):
         main = torch.cuda.current_stream()

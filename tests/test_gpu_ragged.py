@@ -149,3 +149,37 @@ def test_loop_body_and_convergence_on_a_ragged_batch():
         assert cv_all[b].tobytes() == st1.conv_host()[0].tobytes(), b
         rs = slice(int(z[b]) * cs, int(z[b + 1]) * cs)
         assert torch.equal(ring_y[rs].reshape(cs, -1, ni), st1.ring_y[0]) and torch.equal(ring_t[b], st1.ring_t[0]), b
+
+
+def test_autotuned_multi_network_batch():
+    """The autotuner times every candidate shape per network group on the
+    device, applies the fastest (read back through vb_net_get_tuning) and the
+    tuned batch still matches the oracle; a cache round trip re-applies it."""
+    at = load_pkg("autotune")
+    nets = [syn.make_network(54, 30, 185), syn.make_network(55, 69, 700)]
+    dns = [chem.to_device(n.tables) for n in nets]
+    cases, items = [], []
+    for b in range(6):
+        g = b % 2
+        c = syn.make_case(seed=(540 + b,), net=nets[g], nz=10 + b, mild=True, k_range=(-40.0, 4.0))
+        cases.append((c, 1e-6, g))
+        items.append((dns[g], jstep.atm_from_dict(c.atm), c.y, c.k, 1e-6))
+    batch = jstep.MultiNetworkBatch(items, tuning="tune")
+    assert len(batch.tuned) == 2
+    for g in batch.groups:
+        key = at.group_key(g["step"].net, g["step"].batch, g["step"].layers)
+        assert at.get_tuning(g["step"].net) == batch.tuned[key]["tuning"]
+        assert len(batch.tuned[key]["candidates"]) == len(list(at.candidates(g["step"].net.ni)))
+    batch.step()
+    torch.cuda.synchronize()
+    for (c, dt, g), (s, d, st) in zip(cases, batch.results()):
+        sref, dref = orc.ros2_step(c.y, c.k, dt, c.atm, c.net.tables)
+        check_step(s.cpu(), d.cpu(), sref, dref)
+        assert int(st) == 0
+    for n in dns:
+        at.set_tuning(n, {})
+    again = jstep.MultiNetworkBatch(items, tuning=dict(batch.tuned))
+    assert len(again.tuned) == 2
+    for g in again.groups:
+        key = at.group_key(g["step"].net, g["step"].batch, g["step"].layers)
+        assert at.get_tuning(g["step"].net) == batch.tuned[key]["tuning"]
