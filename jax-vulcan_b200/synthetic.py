@@ -561,3 +561,49 @@ def make_nasa9(seed, ni):
         c[:, j, 8] = rng.uniform(-1e4, 1e4, ni)
         c[:, j, 9] = rng.uniform(-10.0, 20.0, ni)
     return c
+
+
+def make_balanced_rates(seed, net: SyntheticNetwork, nz, n, lo=-12.0, hi=4.0, M=None):
+    """Rate constants in detailed balance with a seeded equilibrium: a network
+    whose adaptive integration settles.
+
+    The forward constants (odd rows) are order-scaled log-uniform draws
+    (pseudo-first-order rates in ``[10**lo, 10**hi]`` at the densest layer,
+    as `make_rates` with ``n_ref``); each reverse constant (the next row, the
+    same reaction with the sides swapped) is set so that the pair's rates
+    are equal at ``y* = ymix* n`` in every layer, for one seeded composition
+    ``ymix*`` (log-uniform in [1e-8, 1], normalised) shared by all layers:
+        k_rev = k_fwd prod_reactants y*^nu (M) / prod_products y*^nu (M).
+    ``y*`` is then a steady state of the chemistry (every pair balanced, as
+    Gibbs-consistent reverse rates make a thermodynamic equilibrium) and of
+    eddy diffusion (uniform mixing ratios carry no flux), and a fixed point
+    of the hydrostatic rebalance (its layer sums are n). Photolysis rows stay
+    zero (the photo branch writes them). Returns (k [nr+1, nz], ymix* [ni]).
+    """
+    t = net.tables
+    ni, nr = t.ni, t.nr
+    n = np.asarray(n, dtype=np.float64)
+    M = n if M is None else np.asarray(M, dtype=np.float64)
+    rng = _rng(seed, 13)
+    ymix = 10.0 ** rng.uniform(-8.0, 0.0, ni)
+    ymix /= ymix.sum()
+    ystar = ymix[None, :] * n[:, None]                        # [nz, ni]
+    k = make_rates(seed, net, nz, lo, hi, n_ref=float(n.max()))
+    ypad = np.concatenate([ystar, np.ones((nz, 1))], axis=1)   # padding index ni -> 1
+
+    def side(r, idx, st):
+        f = np.ones(nz)
+        for s in range(idx.shape[1]):
+            if st[r, s] > 0:
+                f = f * ypad[:, idx[r, s]] ** st[r, s]
+        if t.is_three_body[r]:
+            f = f * M
+        return f
+
+    for r in range(1, nr, 2):
+        if t.is_photo[r] or t.is_photo[r + 1]:
+            continue
+        assert sorted(t.reactant_idx[r + 1][t.reactant_stoich[r + 1] > 0].tolist()) == \
+            sorted(t.product_idx[r][t.product_stoich[r] > 0].tolist()), "row r+1 must reverse row r"
+        k[r + 1] = k[r] * side(r, t.reactant_idx, t.reactant_stoich) / side(r + 1, t.reactant_idx, t.reactant_stoich)
+    return k, ymix

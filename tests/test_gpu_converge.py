@@ -301,3 +301,67 @@ def test_checkpoint_resume_is_bit_exact(tmp_path):
     for f in carry_fields:
         assert torch.equal(getattr(ra.photo_carry, f), getattr(rb.photo_carry, f)), f
     assert int(sa.scalars_host()["accept_count"][0]) >= 8
+
+
+def test_relaxing_network_runs_to_the_reference_stop_like_the_oracle():
+    """A network that settles (30 species, 185+185 reactions, nz=40): the
+    reverse constants are in detailed balance with a seeded equilibrium
+    composition (``synthetic.make_balanced_rates``), the start is that
+    composition with each mixing ratio scaled by up to 2x. The device loop
+    (step, body, convergence) and the oracle chain (the reference body and
+    cond_fn restated) both run with the reference's default stopping rule
+    (vulcan_cfg: yconv_cri 0.01, yconv_min 0.1, slope_cri 1e-4, count_min
+    120, trun_min 1e2) until their own loop condition stops them. They must
+    stop at the same attempt with the same counters, the same final mixing
+    ratios (1e-6 relative where ymix > 1e-20) and atom losses (1e-8)."""
+    from oracle import contract as oc
+    syn = load_pkg("synthetic")
+    net = syn.make_network(60, 30, 185)
+    nz = 40
+    atm, ex = syn.make_atmosphere(60, net, nz=nz)
+    k, ymix_eq = syn.make_balanced_rates(60, net, nz, ex["n"], M=atm["M"])
+    rng = np.random.default_rng(1)
+    ymix0 = ymix_eq * 10.0 ** rng.uniform(-0.3, 0.3, ymix_eq.shape)
+    ymix0 = ymix0 / ymix0.sum()
+    y0 = ymix0[None] * ex["n"][:, None]
+    compo = net.compo
+    atom_ini = np.einsum("zi,ia->a", y0, compo)
+    al0 = np.zeros(compo.shape[1])
+    body = dict(loss_eps=0.1, pos_cut=0.0, nega_cut=-1.0, mtol=1e-22, atol=0.1, dt_var_min=0.5, dt_var_max=2.0,
+                dt_min=1e-14, dt_max=1e17, batch_max_retries=8, rtol_min=0.02, rtol_max=1.0,
+                adapt_rtol_dec_period=5, adapt_rtol_inc_period=10, adapt_rtol_dec=0.5, adapt_rtol_inc=1.5,
+                adapt_rtol_loss_mul=10.0, adapt_rtol_inc_loss_thresh=1e-3)
+    cs = loop.ConvStatics()
+    p = dict(body, use_adapt_rtol=False, **{f: getattr(cs, f) for f in (
+        "conv_step", "count_min", "count_max", "conv_stall_window", "st_factor", "mtol_conv", "yconv_cri",
+        "yconv_min", "slope_cri", "flux_cri", "trun_min", "runtime", "use_photo", "final_update_photo_frq",
+        "photo_switch_longdy", "photo_switch_longdydt")})
+    sm = float(loop.slope_min_of(atm["Kzz"], ex["Hp"])[0])
+    # oracle chain to its own stop
+    s = dict(y=y0, y_prev=y0, ymix=ymix0, dt=1e-10, t=0.0, delta=0.0, accept_count=0, retry_count=0,
+             atom_loss=al0, atom_loss_prev=al0, nega_count=0, loss_count=0, delta_count=0, small_y=0.0, nega_y=0.0,
+             rtol=0.2, loss_criteria=1e-3, longdy=1.0, longdydt=1.0, longdy_seen_min=np.inf,
+             count_since_new_min=0)
+    ring_y, ring_t = np.zeros((cs.conv_step, nz, net.tables.ni)), np.zeros(cs.conv_step)
+    n_oracle = 0
+    while n_oracle < 2000:
+        s = oc.attempt(s, k, atm, net.tables, compo, atom_ini, p)
+        s.update(oc.conv_update(s, ring_y, ring_t, atm["M"], p, do_accept=s["_accept"] or s["_force"]))
+        n_oracle += 1
+        if not oc.loop_continues(s, p, sm):
+            break
+    assert n_oracle < 2000 and s["longdy"] < cs.yconv_min, (n_oracle, s["longdy"])
+    # the device loop to its own stop
+    runner = loop.AdaptiveRunner(chem.to_device(net.tables), jstep.atm_from_dict(atm), loop.LoopStatics(**body), compo,
+                                 atom_ini, conv=cs, slope_min=sm)
+    state = loop.LoopState(y0[None], ymix0[None], 1e-10, al0[None], rtol=0.2)
+    n_dev = runner.run_to_convergence(state, k[None], max_attempts=2000, check_every=1)
+    sc, cv = state.scalars_host()[0], state.conv_host()[0]
+    assert cv["done"] == 1 and n_dev == n_oracle, (n_dev, n_oracle)
+    for f in ("accept_count", "retry_count", "delta_count", "loss_count"):
+        assert int(sc[f]) == int(s[f]), f
+    ym = state.ymix.cpu().numpy()[0]
+    mask = s["ymix"] > 1e-20
+    assert np.max(np.abs(ym - s["ymix"])[mask] / s["ymix"][mask]) <= 1e-6
+    assert np.max(np.abs(state.atom_loss.cpu().numpy()[0] - s["atom_loss"])) <= 1e-8
+    assert rel(sc["t"], s["t"]) <= 1e-6
