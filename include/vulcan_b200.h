@@ -84,9 +84,15 @@ int vb_net_destroy(VbNet* net);
  *   factor_ctas:   CTAs per SM of the factor, 1 or 2 (honoured for 65-72
  *                  species, the shape with both variants compiled)
  *   sweep_stages:  depth of the sweeps' bulk-copy ring, 1..3 (lowered when
- *                  the ring does not fit in shared memory) */
+ *                  the ring does not fit in shared memory)
+ *   streams:       2 = vb_ros2_step runs the two halves of a uniform batch
+ *                  on the caller's stream and a second stream of the
+ *                  library's (created on first use, one per device; forked
+ *                  and joined with events, so the call stays stream-ordered
+ *                  on the caller's stream), so one half's assembly overlaps
+ *                  the other half's factor; 0 or 1 = one stream */
 typedef struct VbTuning {
-  int32_t factor_kernel, factor_ctas, sweep_stages, reserved;
+  int32_t factor_kernel, factor_ctas, sweep_stages, streams;
 } VbTuning;
 int vb_net_set_tuning(VbNet* net, const VbTuning* tuning);
 int vb_net_get_tuning(const VbNet* net, VbTuning* tuning);
@@ -147,9 +153,10 @@ int vb_ros2_stages(const VbNet* net, int batch, int nz, const int64_t* zoff, con
 int vb_set_wait_limit(long long polls);
 
 /* FP64 block-factor kernel of the step, the block solver and the adjoint, for
- * later launches from this process: 0 (default) = blocked Gauss-Jordan, one
- * warp per 8-column panel, the panel's pivot steps inside the warp and the
- * rank-8 trailing updates on the FP64 tensor cores (mma.sync m8n8k4); 1 =
+ * later launches from this process (a network's VbTuning.factor_kernel
+ * overrides it for that network): 0 = blocked Gauss-Jordan, one warp per
+ * 8-column panel, the panel's pivot steps inside the warp and the rank-8
+ * trailing updates on the FP64 tensor cores (mma.sync m8n8k4); 1 (default) =
  * scalar Gauss-Jordan, one block barrier per pivot step. Both replace the
  * reference's lu_factor + lu_solve(LU, I) pair (solver.py:46-48). */
 int vb_set_factor_kernel(int variant);

@@ -25,15 +25,15 @@ from . import _lib
 
 class VbTuning(C.Structure):
     _fields_ = [("factor_kernel", C.c_int32), ("factor_ctas", C.c_int32), ("sweep_stages", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("streams", C.c_int32)]
 
 
-FIELDS = ("factor_kernel", "factor_ctas", "sweep_stages")
+FIELDS = ("factor_kernel", "factor_ctas", "sweep_stages", "streams")
 
 
 def set_tuning(net, tuning: dict) -> None:
     """Apply a tuning (dict with the FIELDS; missing fields automatic) to a network."""
-    t = VbTuning(*(int(tuning.get(f, 0)) for f in FIELDS), 0)
+    t = VbTuning(*(int(tuning.get(f, 0)) for f in FIELDS))
     _lib.check(_lib.lib().vb_net_set_tuning(net.handle, C.addressof(t)), "vb_net_set_tuning")
 
 
@@ -43,11 +43,13 @@ def get_tuning(net) -> dict:
     return {f: int(getattr(t, f)) for f in FIELDS}
 
 
-def candidates(ni: int):
-    """Candidate tunings of a network with ni species."""
+def candidates(ni: int, split: bool = False):
+    """Candidate tunings of a network with ni species; ``split``: also the
+    two-stream step (uniform batches only)."""
     ctas = (1, 2) if 64 < ni <= 72 else (0,)
-    for fk, fc, ss in itertools.product((1, 2), ctas, (2, 3)):
-        yield {"factor_kernel": fk, "factor_ctas": fc, "sweep_stages": ss}
+    streams = (1, 2) if split else (1,)
+    for fk, fc, ss, sn in itertools.product((1, 2), ctas, (2, 3), streams):
+        yield {"factor_kernel": fk, "factor_ctas": fc, "sweep_stages": ss, "streams": sn}
 
 
 def group_key(net, batch: int, layers: int) -> str:
@@ -69,13 +71,14 @@ def time_call(fn, reps: int = 5, warm: int = 2) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def tune_group(group: dict, reps: int = 5) -> tuple[dict, dict]:
-    """Best tuning of one group of a MultiNetworkBatch (dict with step, y, k,
-    dt, sol, delta) -> (tuning, {candidate label: ms})."""
+def tune_group(group: dict, reps: int = 5, split: bool = False) -> tuple[dict, dict]:
+    """Best tuning of one group (dict with step, y, k, dt, sol, delta: a
+    MultiNetworkBatch group or a uniform Ros2Step batch) -> (tuning,
+    {candidate label: ms})."""
     step = group["step"]
     net = step.net
     timings, best, best_ms = {}, None, float("inf")
-    for cand in candidates(net.ni):
+    for cand in candidates(net.ni, split):
         set_tuning(net, cand)
         ms = time_call(lambda: step(group["y"], group["k"], group["dt"], out=(group["sol"], group["delta"])), reps)
         timings[json.dumps(cand, sort_keys=True)] = ms

@@ -201,7 +201,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
     if (e != cudaSuccess) { cudaFree(base); return cuda_fail(e, "cudaMemcpy"); }
   }
   VbNet* net = new VbNet;
-  net->tune = VbTuning{0, 0, 0, 0};
+  net->tune = VbTuning{0, 0, 0, 1};
   char* b = (char*)base;
   vb::NetDev& d = net->dev;
   d.ni = ni; d.nr = nr; d.T = T;
@@ -238,8 +238,9 @@ size_t vb_net_device_bytes(const VbNet* net) { return net ? net->bytes : 0; }
 int vb_net_set_tuning(VbNet* net, const VbTuning* t) {
   if (!net || !t) return fail(VB_ERR_ARG, "null argument");
   if (t->factor_kernel < 0 || t->factor_kernel > 2 || t->factor_ctas < 0 || t->factor_ctas > 2 ||
-      t->sweep_stages < 0 || t->sweep_stages > 3)
-    return fail(VB_ERR_ARG, "tuning out of range (factor_kernel 0..2, factor_ctas 0..2, sweep_stages 0..3)");
+      t->sweep_stages < 0 || t->sweep_stages > 3 || t->streams < 0 || t->streams > 2)
+    return fail(VB_ERR_ARG, "tuning out of range (factor_kernel 0..2, factor_ctas 0..2, sweep_stages 0..3, "
+                            "streams 0..2)");
   net->tune = *t;
   return VB_OK;
 }
@@ -269,18 +270,10 @@ static vb::Batch make_batch(const VbNet* net, int batch, int nz, const int64_t* 
   return B;
 }
 
-int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
-                 const double* dt, const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol,
-                 double* delta, int32_t* status, void* workspace, size_t ws_bytes, void* stream) {
-  if (!net || !y || !k || !dt || !atm || !sol || !delta || !status || !workspace)
-    return fail(VB_ERR_ARG, "null argument");
-  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
-  if (!zoff && ws_bytes < vb_ros2_workspace_bytes(batch, nz, net->dev.ni, nullptr))
-    return fail(VB_ERR_ARG, "workspace too small");
-  cudaStream_t st = (cudaStream_t)stream;
-  vb::Batch B = make_batch(net, batch, nz, zoff);
-  double* ws = (double*)workspace;
-  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+// The launch sequence of one Ros2 step (jax_step.py:249-315) on one stream.
+static int ros2_sequence(const VbNet* net, const vb::Batch& B, const double* y, const double* k, const double* dt,
+                         const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol, double* delta,
+                         int32_t* status, double* ws, cudaStream_t st) {
   {
     ProfScope p(0, st);
     VB_CHECK(vb::launch_stage1(net->dev, B, y, k, dt, atm, flags, fix_mask, ws, st), "stage1");
@@ -313,6 +306,67 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const
     ProfScope p(5, st);
     VB_CHECK(vb::launch_sweep(B, ws, a, st), "back sweep 2");
   }
+  return VB_OK;
+}
+
+// Second stream and fork / join events of the two-stream step, one set per
+// device, created on first use.
+namespace {
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_side_mu;
+SideStream g_side[kScratchDevices];
+}  // namespace
+
+static int side_stream(SideStream** out) {
+  int dev = 0;
+  VB_CHECK(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kScratchDevices) return fail(VB_ERR_ARG, "device ordinal beyond the stream table");
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  SideStream& s = g_side[dev];
+  if (!s.s) {
+    VB_CHECK(cudaStreamCreateWithFlags(&s.s, cudaStreamNonBlocking), "cudaStreamCreate");
+    VB_CHECK(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming), "cudaEventCreate");
+    VB_CHECK(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  *out = &s;
+  return VB_OK;
+}
+
+int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const double* y, const double* k,
+                 const double* dt, const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol,
+                 double* delta, int32_t* status, void* workspace, size_t ws_bytes, void* stream) {
+  if (!net || !y || !k || !dt || !atm || !sol || !delta || !status || !workspace)
+    return fail(VB_ERR_ARG, "null argument");
+  if (batch < 1 || nz < 2) return fail(VB_ERR_ARG, "batch >= 1 and nz >= 2 required");
+  if (!zoff && ws_bytes < vb_ros2_workspace_bytes(batch, nz, net->dev.ni, nullptr))
+    return fail(VB_ERR_ARG, "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  double* ws = (double*)workspace;
+  VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
+  if (net->tune.streams != 2 || zoff || batch < 2)
+    return ros2_sequence(net, make_batch(net, batch, nz, zoff), y, k, dt, atm, flags, fix_mask, sol, delta, status,
+                         ws, st);
+  // two halves of a uniform batch, one per stream: the assembly of one half
+  // overlaps the factor of the other (they bind different units of the SM)
+  SideStream* side = nullptr;
+  if (int rc = side_stream(&side)) return rc;
+  const int h = batch / 2, ni = net->dev.ni, nr = net->dev.nr;
+  const int64_t e = (int64_t)h * nz * ni;
+  VB_CHECK(cudaEventRecord(side->fork, st), "fork");
+  VB_CHECK(cudaStreamWaitEvent(side->s, side->fork, 0), "fork wait");
+  if (int rc = ros2_sequence(net, make_batch(net, h, nz, nullptr), y, k, dt, atm, flags, fix_mask, sol, delta, status,
+                             ws, st))
+    return rc;
+  if (int rc = ros2_sequence(net, make_batch(net, batch - h, nz, nullptr), y + e, k + (int64_t)h * (nr + 1) * nz,
+                             dt + h, atm + (int64_t)h * VB_ATM_DOUBLES(nz, ni), flags, fix_mask ? fix_mask + e : nullptr,
+                             sol + e, delta + e, status + h,
+                             ws + (int64_t)h * nz * vb::ws_per_layer(ni, vb::round_even(ni)), side->s))
+    return rc;
+  VB_CHECK(cudaEventRecord(side->join, side->s), "join");
+  VB_CHECK(cudaStreamWaitEvent(st, side->join, 0), "join wait");
   return VB_OK;
 }
 
