@@ -690,6 +690,11 @@ def main():
     def one():
         step(y, k, dt, out=(sol, delta))
 
+    # launch shapes chosen by the project's autotuner on this GPU (factor kernel,
+    # factor CTAs per SM, sweep ring depth, one or two streams), timed before
+    # the measured region
+    at = pkg("autotune")
+    tuned, tune_ms = at.tune_group(dict(step=step, y=y, k=k, dt=dt, sol=sol, delta=delta), reps=3, split=True)
     for _ in range(args.warmup):
         one()
     torch.cuda.synchronize()
@@ -710,7 +715,9 @@ def main():
         dist.barrier()
     value = job_value(world, B, ms)
 
-    # per-kernel device times over a separate profiled pass (events on the launch stream)
+    # per-kernel device times over a separate profiled pass (events on the launch
+    # stream; kernels serialised on one stream so each launch is attributed)
+    at.set_tuning(dn, dict(tuned, streams=1))
     L.vb_profile(1)
     for _ in range(args.steps):
         one()
@@ -723,8 +730,8 @@ def main():
 
     # the two FP64 factor kernels on the same batch (per-launch event split)
     variants = {}
-    for vid, vname in ((1, "scalar_gauss_jordan"), (0, "blocked_dmma")):
-        L.vb_set_factor_kernel(vid)
+    for vid, vname in ((2, "scalar_gauss_jordan"), (1, "blocked_dmma")):
+        at.set_tuning(dn, dict(tuned, streams=1, factor_kernel=vid))
         for _ in range(args.warmup):
             one()
         torch.cuda.synchronize()
@@ -737,7 +744,7 @@ def main():
         L.vb_profile(0)
         variants[vname] = {"factor_ms": float(vms[1] / max(vcnt[1], 1)),
                            "step_ms_sum_of_kernels": float(sum(vms[i] / max(vcnt[i], 1) for i in range(6)))}
-    L.vb_set_factor_kernel(1)
+    at.set_tuning(dn, tuned)
     names = _lib.PROFILE_SITES
     per_kernel = {n: {"ms_per_launch": float(site_ms[0][i] / max(site_ms[1][i], 1)),
                       "launches": int(site_ms[1][i])} for i, n in enumerate(names)}
@@ -853,11 +860,13 @@ def main():
                        per_species_max_rel_err_vs_oracle=chk["per_species_max_rel_err_vs_oracle"])
         return out
 
+    at.set_tuning(dn, {})
     stepm = jstep.Ros2Step(dn, atm, mixed=True)
     mixed_stiff = mixed_run(stepm, y, k, dt, cases)
     stepmw = jstep.Ros2Step(dn, jstep.atm_from_dict(Aw), mixed=True)
     mixed_wc = mixed_run(stepmw, yw, kw, dtw, wcases)
     del stepm, stepmw
+    at.set_tuning(dn, tuned)
 
     peak64 = fp64_peak_tflops(L, torch, sh)
     ni, nz = net.tables.ni, Y.shape[1]
@@ -890,6 +899,7 @@ def main():
                                    f"(ni={ni}, nr={net.tables.nr}, nz={nz}, dt=1e-6)",
                        "batch_per_gpu": B, "ni": ni, "nr": int(net.tables.nr), "nz": int(nz),
                        "precision": "fp64", "parallelism": f"replicas x{world}",
+                       "tuning": tuned, "tuning_candidates_ms": tune_ms,
                        "l2": f"inputs larger than L2 (rates {K.nbytes / 1e6:.0f} MB + solver workspace "
                              f"{step.ws_bytes / 1e6:.0f} MB per GPU), no flush"},
             "e2e": {"value": job_value(world, B, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -898,7 +908,7 @@ def main():
                             "on two copy streams with double-buffered device arrays (step i's inputs go up and "
                             "step i-1's results come down while the steps compute); rates and atmosphere stay "
                             "resident (as in the reference runner's device carry)"},
-            "gpu_launches": 6 * args.steps,
+            "gpu_launches": (12 if tuned.get("streams") == 2 else 6) * args.steps,
             "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan inverse with partial pivoting of "
                                                     "each layer block, serial in z, one CTA per atmosphere)",
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",

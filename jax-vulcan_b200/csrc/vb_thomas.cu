@@ -35,6 +35,14 @@ __device__ __forceinline__ unsigned hi_key(float v) { return __float_as_uint(v) 
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 __device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
 
+// Power of two s with s * m in [1, 2) for a finite m > 0 (1 otherwise).
+__device__ __forceinline__ double pow2_scale(double m) {
+  if (!(m > 0.0) || !isfinite(m)) return 1.0;
+  int e;
+  frexp(m, &e);               // m = f 2^e, f in [0.5, 1)
+  return ldexp(1.0, 1 - e);   // s m = 2 f in [1, 2)
+}
+
 // Two values of the factor's element type handed over in one shared-memory access.
 template <typename R> struct Pair;
 template <> struct Pair<double> { using T = double2; };
@@ -49,10 +57,11 @@ struct GJK {
   static constexpr int NPC = CPW * NW;          // column capacity (warp w holds columns w*CPW + c)
   static constexpr int CPWP = (CPW + 1) & ~1;   // stride of a warp's pivot-row slot (pairs)
   __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
-  static size_t smem_bytes(int n, int ld, bool dpf) {
-    const size_t blk = (size_t)n * ld;
-    return al(blk * sizeof(R))                        // Ib: the inverse of the layer (natural order)
+  static size_t smem_bytes(int n, int ld, bool dpf, int li = 0) {
+    const size_t blk = (size_t)n * ld, iblk = (size_t)n * (li ? li : ld);
+    return al(iblk * sizeof(R))                       // Ib: the inverse of the layer (natural order, stride li)
            + (dpf ? al(blk * sizeof(double)) : 0)     // Db: the next diagonal block, prefetched
+           + al(2 * NPC * sizeof(double))             // rsc: row scales of this and the previous layer (EQ)
            + al(2 * NPR * sizeof(R))                  // colb: multipliers of the next step (2 parities)
            + al(NPR * sizeof(R))                      // rps: 1 / pivot of each row
            + al(2 * NPR * sizeof(double))             // rsb: the next layer's rhs and sub_d rows
@@ -100,14 +109,21 @@ struct GJK {
 //    lane through a per-warp shared slot (no block barrier).
 //  * Layer j's Schur update reads Inv_{j-1} from Ib (shared), D_j from Db
 //    (bulk-prefetched during layer j-1) when DPF, else from global memory.
-template <int RPL, int CPW, int NW, bool DPF, typename R>
+//  * EQ (transposed orientation): every row of A'_j is scaled by a power of
+//    two bringing its largest magnitude to [1, 2) before the elimination
+//    (row equilibration, exact); the stored inverse is X = (R A'_j)^{-1},
+//    the scales go to rs_out, and A'_j^{-1} = X diag(r).
+//  * li: row stride of Ib and of the stored inverses (ld when 0).
+template <int RPL, int CPW, int NW, bool DPF, typename R, bool EQ = false>
 __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
                                                      const double* __restrict__ supn,
                                                      const double* __restrict__ subn, double* rhs,
-                                                     bool tr, int32_t* status, char* smem_raw, long long wlim) {
+                                                     bool tr, int32_t* status, char* smem_raw, long long wlim,
+                                                     int li = 0, double* rs_out = nullptr) {
   using G = GJK<RPL, CPW, NW, R>;
   using R2 = typename Pair<R>::T;
-  constexpr int NPR = G::NPR, CPWP = G::CPWP;
+  constexpr int NPR = G::NPR, CPWP = G::CPWP, NPC = G::NPC;
+  if (li == 0) li = ld;
   // value of slot s (warp-uniform) of a per-lane row array
   auto pick = [](const R* v, int s) {
     R x = v[0];
@@ -117,15 +133,16 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned FULL = 0xffffffffu;
-  const int blk = n * ld;
+  const int blk = n * ld, iblk = n * li;
   char* sp = smem_raw;
   auto take = [&](size_t bytes) {
     char* q = sp;
     sp += G::al(bytes);
     return q;
   };
-  R* Ib = reinterpret_cast<R*>(take((size_t)blk * sizeof(R)));
+  R* Ib = reinterpret_cast<R*>(take((size_t)iblk * sizeof(R)));
   double* Db = DPF ? reinterpret_cast<double*>(take((size_t)blk * sizeof(double))) : nullptr;
+  double* rsc = reinterpret_cast<double*>(take(2 * NPC * sizeof(double)));
   R* colb = reinterpret_cast<R*>(take(2 * NPR * sizeof(R)));
   R* rps = reinterpret_cast<R*>(take(NPR * sizeof(R)));
   double* rsb = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
@@ -137,7 +154,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   const uint32_t dbytes = (uint32_t)(blk * sizeof(double));
   int st_local = 0;
 
-  for (int e = threadIdx.x; e < blk; e += blockDim.x) Ib[e] = R(0);   // the padding column stays 0
+  for (int e = threadIdx.x; e < iblk; e += blockDim.x) Ib[e] = R(0);   // the padding columns stay 0
   if (rhs)
     for (int i = threadIdx.x; i < n; i += blockDim.x) vecs[i] = rhs[i];
   if (DPF && threadIdx.x == 0) mbar_init(bar, 1);
@@ -243,25 +260,53 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
         const int m = warp * CPW + c;
         sc[c] = (j > 0 && m < n) ? (tr ? subn : supn)[(int64_t)(j - 1) * n + m] : 0.0;
       }
-      const int si = tr ? 1 : ld, sm = tr ? ld : 1;   // element strides of tile rows / columns
+      const int si = tr ? 1 : ld, sm = tr ? ld : 1;   // element strides of tile rows / columns in D
+      const int ii = tr ? 1 : li, im = tr ? li : 1;   // and in Ib
+      const double* rprev = rsc + ((j + 1) & 1) * NPC;
+      double v[RPL][CPW];
 #pragma unroll
       for (int r = 0; r < RPL; ++r) {
         const int i = lane + 32 * r;
 #pragma unroll
         for (int c = 0; c < CPW; ++c) {
           const int m = warp * CPW + c;
-          double v = 0.0;
+          double x = 0.0;
           if (i < n && m < n) {
-            const int e = i * si + m * sm;
-            v = D[e];
+            x = D[i * si + m * sm];
             if (j > 0) {
               const double cb = tr ? sc[c] * sr[r] : sr[r] * sc[c];
-              v = v - cb * (double)Ib[e];
+              double inv = (double)Ib[i * ii + m * im];
+              if (EQ) inv = inv * rprev[i];
+              x = x - cb * inv;
             }
           }
-          a[r][c] = (R)v;
+          v[r][c] = x;
         }
       }
+      if (EQ) {
+        // largest magnitude of each tile column (row m of A'_j): the column lives in this warp
+        double* rcur = rsc + (j & 1) * NPC;
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) {
+          double cm = 0.0;
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) cm = fmax(cm, fabs(v[r][c]));
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) cm = fmax(cm, __shfl_xor_sync(FULL, cm, off));
+          const double s = pow2_scale(cm);
+          const int m = warp * CPW + c;
+          if (lane == 0 && m < n) {
+            rcur[m] = s;
+            rs_out[(int64_t)j * n + m] = s;
+          }
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) v[r][c] *= s;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RPL; ++r)
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) a[r][c] = (R)v[r][c];
     }
     __syncthreads();   // Db and Ib consumed
     if (DPF && threadIdx.x == 0 && j + 1 < nz) {
@@ -359,17 +404,17 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
           if (m < n) {
             const R v = a[r][c] * s;
             if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
-            Ib[tr ? pivs[m] * ld + q[r] : q[r] * ld + pivs[m]] = v;
+            Ib[tr ? pivs[m] * li + q[r] : q[r] * li + pivs[m]] = v;
           }
         }
       }
     }
     __syncthreads();
-    // ---- Inv_j to global memory (natural order, padding column 0)
+    // ---- Inv_j to global memory (natural order, padding columns 0)
     {
-      R2* O = reinterpret_cast<R2*>(out + (int64_t)j * blk);
+      R2* O = reinterpret_cast<R2*>(out + (int64_t)j * iblk);
       const R2* S2 = reinterpret_cast<const R2*>(Ib);
-      for (int e = threadIdx.x; e < blk / 2; e += blockDim.x) O[e] = S2[e];
+      for (int e = threadIdx.x; e < iblk / 2; e += blockDim.x) O[e] = S2[e];
     }
     // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
     if (rhs && j + 1 < nz) {
@@ -383,10 +428,10 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
         if (i < n) {
           int m = sub;
           for (; m + 4 < n; m += 8) {
-            s0 = fma((double)Ib[i * ld + m], vc[m], s0);
-            s1 = fma((double)Ib[i * ld + m + 4], vc[m + 4], s1);
+            s0 = fma((double)Ib[i * li + m], vc[m], s0);
+            s1 = fma((double)Ib[i * li + m + 4], vc[m + 4], s1);
           }
-          if (m < n) s0 = fma((double)Ib[i * ld + m], vc[m], s0);
+          if (m < n) s0 = fma((double)Ib[i * li + m], vc[m], s0);
         }
         double s = s0 + s1;
         s += __shfl_xor_sync(FULL, s, 1);
@@ -417,6 +462,22 @@ gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __rest
   R* o = out ? out + g.z0 * B.ni * B.ld : reinterpret_cast<R*>(w.inv);
   gj_factor_atmosphere<RPL, CPW, NW, DPF, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn,
                                              with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw, wlim);
+}
+
+// FP32 factor of the mixed-precision step by the scalar Gauss-Jordan kernel
+// (row-equilibrated, transposed orientation): FP32 inverses and row scales
+// into the mixed region, the FP64 blocks stay in the workspace.
+template <int RPL, int CPW, int NW, int MB, bool DPF>
+__global__ void __launch_bounds__(NW * 32, MB)
+gj32_factor_kernel(Batch B, double* __restrict__ ws, void* __restrict__ mxr, int32_t* __restrict__ status,
+                   long long wlim) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const int b = blockIdx.x;
+  Geo g = geo_of(B, b);
+  WsView w = ws_view(ws, g, B.ni, B.ld);
+  MxView m = mx_view(mxr, g.z0, g.nz, B.ni);
+  gj_factor_atmosphere<RPL, CPW, NW, DPF, float, true>(g.nz, B.ni, B.ld, w.inv, m.X, w.supn, w.subn, nullptr, true,
+                                                       status + b, smem_raw, wlim, round4(B.ni), m.rs);
 }
 
 // ---------------------------------------------------------------- blocked Gauss-Jordan factor (tensor cores)
@@ -502,14 +563,6 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
 __device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
   hi = tf32_rna(x);
   lo = tf32_rna(x - __uint_as_float(hi));
-}
-
-// Power of two s with s * m in [1, 2) for a finite m > 0 (1 otherwise).
-__device__ __forceinline__ double pow2_scale(double m) {
-  if (!(m > 0.0) || !isfinite(m)) return 1.0;
-  int e;
-  frexp(m, &e);               // m = f 2^e, f in [0.5, 1)
-  return ldexp(1.0, 1 - e);   // s m = 2 f in [1, 2)
 }
 
 template <int NW, int MR, bool DPF, bool EQ, typename R>
@@ -1175,6 +1228,14 @@ static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int 
   return cudaGetLastError();
 }
 
+// FP64 factor kernel: 0 = blocked Gauss-Jordan with the trailing updates on
+// the FP64 tensor cores, 1 = scalar Gauss-Jordan (one block barrier per pivot
+// step; the default: faster on B200, 6.2 against 11.2 ms at 296 config-0
+// atmospheres, since a panel's pivot steps run serially in one warp).
+static int g_factor_variant = 1;
+static int g_factor32_variant = 1;
+void set_factor_variant(int v) { g_factor_variant = g_factor32_variant = v; }
+
 template <int NW, int MB, bool DPF>
 static cudaError_t launch_bgj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
                                 double* out, const int32_t* only) {
@@ -1211,7 +1272,27 @@ static cudaError_t launch_bgj32_t(const Batch& B, double* ws, void* mxr, int32_t
   return cudaGetLastError();
 }
 
+template <int RPL, int CPW, int NW, int MB, bool DPF>
+static cudaError_t launch_gj32_t(const Batch& B, double* ws, void* mxr, int32_t* status, cudaStream_t st) {
+  size_t sm = GJK<RPL, CPW, NW, float>::smem_bytes(B.ni, B.ld, DPF, round4(B.ni));
+  cudaError_t e = cudaFuncSetAttribute(gj32_factor_kernel<RPL, CPW, NW, MB, DPF>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  gj32_factor_kernel<RPL, CPW, NW, MB, DPF><<<B.count, NW * 32, sm, st>>>(B, ws, mxr, status, g_wait_limit);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st) {
+  const bool blocked = B.factor_kernel ? B.factor_kernel == 1 : g_factor32_variant == 0;
+  if (!blocked) {
+    if (B.ni <= 32) return launch_gj32_t<1, 4, 8, 4, true>(B, ws, mxr, status32, st);
+    if (B.ni <= 64) return launch_gj32_t<2, 8, 8, 2, true>(B, ws, mxr, status32, st);
+    if (B.ni <= 72) {
+      if (one_cta_per_sm(B)) return launch_gj32_t<3, 6, 12, 1, true>(B, ws, mxr, status32, st);
+      return launch_gj32_t<3, 6, 12, 2, true>(B, ws, mxr, status32, st);
+    }
+    return launch_gj32_t<3, 6, 16, 1, true>(B, ws, mxr, status32, st);
+  }
   if (B.ni <= 32) return launch_bgj32_t<4, 4, 4, true>(B, ws, mxr, status32, st);
   if (B.ni <= 64) return launch_bgj32_t<8, 8, 2, true>(B, ws, mxr, status32, st);
   if (B.ni <= 72) {
@@ -1226,12 +1307,6 @@ cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, 
   return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
 }
 
-// FP64 factor kernel: 0 = blocked Gauss-Jordan with the trailing updates on
-// the FP64 tensor cores, 1 = scalar Gauss-Jordan (one block barrier per pivot
-// step; the default: faster on B200, 6.2 against 11.2 ms at 296 config-0
-// atmospheres, since a panel's pivot steps run serially in one warp).
-static int g_factor_variant = 1;
-void set_factor_variant(int v) { g_factor_variant = v; }
 
 // Tile shapes by block size: rows over 32 lanes x RPL, columns over NW warps
 // x CPW (the next diagonal block is prefetched into shared memory in every

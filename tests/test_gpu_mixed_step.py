@@ -49,8 +49,18 @@ def _run(net, cases, Y, K, DT, A, **kw):
             k2.cpu().numpy(), step.passes.cpu().numpy().copy())
 
 
+_lib = load_pkg("_lib")
+
+
+@pytest.fixture(params=[1, 0], ids=["scalar_gj", "blocked_tf32"])
+def factor_kernel(request):
+    _lib.check(_lib.lib().vb_set_factor_kernel(request.param), "vb_set_factor_kernel")
+    yield request.param
+    _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
+
+
 @pytest.mark.parametrize("ni,n_fwd,nz", [(30, 185, 40), (69, 700, 120), (89, 1000, 60)])
-def test_mixed_step_well_conditioned_within_1e6(ni, n_fwd, nz):
+def test_mixed_step_well_conditioned_within_1e6(factor_kernel, ni, n_fwd, nz):
     elements = ("C", "H", "O", "N", "S") if ni == 89 else ("C", "H", "O", "N")
     net = syn.make_network(80 + ni, ni, n_fwd, elements)
     cases, Y, K, DT, A = _batch(net, (1, 2, 3), nz, True, moldiff=True)
