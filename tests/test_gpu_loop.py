@@ -317,3 +317,37 @@ def test_condensation_mask_drops_species_from_the_error_norm():
         assert int(got["accept_count"][0]) == int(ref["accept_count"]), masked
         assert int(got["accept_count"][0]) == int(inp["accept_count"]) + (1 if masked else 0), masked
         check_state(got, 0, ref, f"cond_zero={masked}")
+
+
+def test_runstate_round_trip_continues_bit_for_bit():
+    """The device carry as the reference RunState runner slots (StepInputs,
+    ParamInputs, AtomInputs: `state.py:106-141`) and back: after some attempts
+    (at an accepted attempt, so no retry is pending), the rebuilt carry runs
+    the next attempts exactly as the original does."""
+    rsm = load_pkg("runstate")
+    case = syn.make_case(seed=44, ni=12, n_fwd=30, nz=10, mild=True, k_range=(-40.0, 4.0), moldiff=True)
+    tables, compo, y0, atm = case.net.tables, case.net.compo, case.y, case.atm
+    atom_ini = np.einsum("zi,ia->a", y0, compo) * (1 + 1e-7)
+    al0 = (np.einsum("zi,ia->a", y0, compo) - atom_ini) / atom_ini
+    p = oc_params()
+    conv = loop.ConvStatics(conv_step=4, count_min=10 ** 6)
+    runner = loop.AdaptiveRunner(chem.to_device(tables), jstep.atm_from_dict(atm), loop.LoopStatics(**p), compo,
+                                 atom_ini, conv=conv)
+    state = loop.LoopState(y0[None], (y0 / y0.sum(axis=1, keepdims=True))[None], 1e-8, al0[None], rtol=0.2,
+                           y_prev=y0[None])
+    k = torch.as_tensor(case.k[None], device="cuda").contiguous()
+    for _ in range(6):
+        runner.attempt(state, k)
+    while int(state.scalars_host()["retry_count"][0]) != 0:
+        runner.attempt(state, k)
+    slots = rsm.runstate_slots(state, 0, compo, ["C", "H", "O", "N"], atom_ini)
+    assert set(slots["step"]) == set(rsm.STEP_FIELDS) and set(slots["params"]) == set(rsm.PARAM_FIELDS)
+    assert set(slots["atoms"]) == set(rsm.ATOM_FIELDS)
+    assert slots["params"]["count"] == int(state.scalars_host()["accept_count"][0])
+    again = rsm.state_from_runstate([slots], rtol=0.2, conv_step=4)
+    for _ in range(3):
+        runner.attempt(state, k)
+        runner.attempt(again, k)
+    a, b = state.snapshot(), again.snapshot()
+    for f in ("y", "y_prev", "ymix", "dt", "t", "atom_loss", "accept_count", "delta_count"):
+        assert np.array_equal(a[f], b[f]), f
