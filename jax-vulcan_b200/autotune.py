@@ -25,15 +25,15 @@ from . import _lib
 
 class VbTuning(C.Structure):
     _fields_ = [("factor_kernel", C.c_int32), ("factor_ctas", C.c_int32), ("sweep_stages", C.c_int32),
-                ("streams", C.c_int32)]
+                ("streams", C.c_int32), ("stage1_layers", C.c_int32), ("reserved", C.c_int32)]
 
 
-FIELDS = ("factor_kernel", "factor_ctas", "sweep_stages", "streams")
+FIELDS = ("factor_kernel", "factor_ctas", "sweep_stages", "streams", "stage1_layers")
 
 
 def set_tuning(net, tuning: dict) -> None:
     """Apply a tuning (dict with the FIELDS; missing fields automatic) to a network."""
-    t = VbTuning(*(int(tuning.get(f, 0)) for f in FIELDS))
+    t = VbTuning(*(int(tuning.get(f, 0)) for f in FIELDS), 0)
     _lib.check(_lib.lib().vb_net_set_tuning(net.handle, C.addressof(t)), "vb_net_set_tuning")
 
 
@@ -48,8 +48,8 @@ def candidates(ni: int, split: bool = False):
     two-stream step (uniform batches only)."""
     ctas = (1, 2) if 64 < ni <= 72 else (0,)
     streams = (1, 2) if split else (1,)
-    for fk, fc, ss, sn in itertools.product((1, 2), ctas, (2, 3), streams):
-        yield {"factor_kernel": fk, "factor_ctas": fc, "sweep_stages": ss, "streams": sn}
+    for fk, fc, ss, sn, s1 in itertools.product((1, 2), ctas, (2, 3), streams, (1, 2)):
+        yield {"factor_kernel": fk, "factor_ctas": fc, "sweep_stages": ss, "streams": sn, "stage1_layers": s1}
 
 
 def group_key(net, batch: int, layers: int) -> str:

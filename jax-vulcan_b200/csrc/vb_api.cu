@@ -201,7 +201,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
     if (e != cudaSuccess) { cudaFree(base); return cuda_fail(e, "cudaMemcpy"); }
   }
   VbNet* net = new VbNet;
-  net->tune = VbTuning{0, 0, 0, 1};
+  net->tune = VbTuning{0, 0, 0, 1, 0, 0};
   char* b = (char*)base;
   vb::NetDev& d = net->dev;
   d.ni = ni; d.nr = nr; d.T = T;
@@ -238,9 +238,10 @@ size_t vb_net_device_bytes(const VbNet* net) { return net ? net->bytes : 0; }
 int vb_net_set_tuning(VbNet* net, const VbTuning* t) {
   if (!net || !t) return fail(VB_ERR_ARG, "null argument");
   if (t->factor_kernel < 0 || t->factor_kernel > 2 || t->factor_ctas < 0 || t->factor_ctas > 2 ||
-      t->sweep_stages < 0 || t->sweep_stages > 3 || t->streams < 0 || t->streams > 2)
+      t->sweep_stages < 0 || t->sweep_stages > 3 || t->streams < 0 || t->streams > 2 || t->stage1_layers < 0 ||
+      t->stage1_layers > 2)
     return fail(VB_ERR_ARG, "tuning out of range (factor_kernel 0..2, factor_ctas 0..2, sweep_stages 0..3, "
-                            "streams 0..2)");
+                            "streams 0..2, stage1_layers 0..2)");
   net->tune = *t;
   return VB_OK;
 }
@@ -267,6 +268,7 @@ static vb::Batch make_batch(const VbNet* net, int batch, int nz, const int64_t* 
   B.factor_kernel = net->tune.factor_kernel;
   B.factor_ctas = net->tune.factor_ctas;
   B.sweep_stages = net->tune.sweep_stages;
+  B.stage1_layers = net->tune.stage1_layers;
   return B;
 }
 

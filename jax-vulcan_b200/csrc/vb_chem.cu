@@ -344,6 +344,221 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   }
 }
 
+// ---------------------------------------------------------------- stage 1, two layers per CTA
+// The same assembly as stage1_kernel for layers j0 = 2 blockIdx.x and j0 + 1
+// of one atmosphere: every gather word, rate-constant sector and network
+// table entry is loaded once for both layers, and each sum runs as two
+// independent chains (each in the reference's order, so every value is
+// bit-identical to the one-layer kernel's).
+constexpr int PAIR_THREADS = 512;
+
+struct PairSmem {
+  double* y4;      // [4][ni+1]: layers j0-1 .. j0+2 (padding slot 1.0)
+  double* rate;    // [2][nr+1]
+  double* drate;   // [2][(nr+1)*T]
+  double* diff;    // [2][ni]
+  double* diagd;   // [2][ni]
+  double* part;    // [2][2*ni]
+  double* scal;    // [8]: ysums of the four rows
+  double* supb;    // [2][ni]
+  double* subb;    // [2][ni]
+};
+
+__host__ __device__ inline size_t pair_smem_bytes(int ni, int nr, int T) {
+  const size_t d = 4 * (size_t)(ni + 1) + 2 * (size_t)(nr + 1) + 2 * (size_t)(nr + 1) * T + 10 * (size_t)ni + 8 +
+                   4 * (size_t)ni;
+  return d * sizeof(double);
+}
+
+__device__ inline PairSmem carve_pair(double* s, int ni, int nr, int T) {
+  PairSmem P;
+  P.y4 = s; s += 4 * (ni + 1);
+  P.rate = s; s += 2 * (nr + 1);
+  P.drate = s; s += 2 * (nr + 1) * T;
+  P.diff = s; s += 2 * ni;
+  P.diagd = s; s += 2 * ni;
+  P.part = s; s += 4 * ni;
+  P.scal = s; s += 8;
+  P.supb = s; s += 2 * ni;
+  P.subb = s;
+  return P;
+}
+
+// Rates and drates of both layers (rate_slot's expression order per layer).
+template <int TT, int RU>
+__device__ inline void rates_pair_t(const NetDev& net, const double* y0, const double* y1, const double* kcol,
+                                    int64_t kstride, bool two, double M0, double M1, double* rate, double* drate) {
+  const int R = net.nr + 1;
+  for (int r0 = threadIdx.x; r0 < R; r0 += RU * blockDim.x) {
+    double kv[RU][2];
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int r = r0 + u * blockDim.x;
+      kv[u][0] = r < R ? __ldcg(kcol + (int64_t)r * kstride) : 0.0;
+      kv[u][1] = (two && r < R) ? __ldcg(kcol + (int64_t)r * kstride + 1) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int r = r0 + u * blockDim.x;
+      if (r < R) {
+        rate_slot<TT>(net, r, y0, kv[u][0], M0, rate, drate, true);
+        if (two) rate_slot<TT>(net, r, y1, kv[u][1], M1, rate + R, drate + (int64_t)R * TT, true);
+      }
+    }
+  }
+}
+
+__device__ inline void rates_pair(const NetDev& net, const double* y0, const double* y1, const double* kcol,
+                                  int64_t kstride, bool two, double M0, double M1, double* rate, double* drate) {
+  switch (net.T) {
+    case 1: rates_pair_t<1, 3>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    case 2: rates_pair_t<2, 3>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    case 3: rates_pair_t<3, 3>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    case 4: rates_pair_t<4, 3>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    case 5: rates_pair_t<5, 2>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    case 6: rates_pair_t<6, 2>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    case 7: rates_pair_t<7, 2>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+    default: rates_pair_t<8, 2>(net, y0, y1, kcol, kstride, two, M0, M1, rate, drate); return;
+  }
+}
+
+// Loss and production sums of both layers (species_sums' order per layer).
+__device__ inline void species_sums_pair(const NetDev& net, const double* coef, const double* rate, double* part) {
+  const int R = net.nr + 1;
+  for (int t = threadIdx.x; t < 2 * net.ni; t += blockDim.x) {
+    const int i = t >> 1;
+    const int32_t* ptr = (t & 1) ? net.prod_ptr : net.loss_ptr;
+    const uint32_t* w = (t & 1) ? net.prod_w : net.loss_w;
+    double a0 = 0.0, a1 = 0.0;
+    const int e1 = ptr[i + 1];
+#pragma unroll 4
+    for (int e = ptr[i]; e < e1; ++e) {
+      const uint32_t x = w[e];
+      const double c = coef[x >> 16];
+      const int s = x & 0xffffu;
+      a0 = a0 + c * rate[s];
+      a1 = a1 + c * rate[R + s];
+    }
+    part[t] = a0;
+    part[2 * net.ni + t] = a1;
+  }
+}
+
+// Dense Jacobians of both layers (layer_jacobian_each's order and rank bands).
+template <typename Store>
+__device__ inline void jacobian_pair(const NetDev& net, const double* coef, const double* drate, Store store,
+                                     int busy) {
+  const int nd = net.ni * net.ni;
+  const int64_t D = (int64_t)(net.nr + 1) * net.T;
+  const int stride = blockDim.x;
+  int q = ((int)threadIdx.x - busy + stride) % stride;
+  uint2 dn = q < nd ? net.jac_desc[q] : make_uint2(0u, 0u);
+  for (; q < nd; q += stride) {
+    const uint2 dc = dn;
+    if (q + stride < nd) dn = net.jac_desc[q + stride];
+    const int e0 = (int)dc.x, e1 = e0 + (int)(dc.y & 0xffffu);
+    double J0 = 0.0, J1 = 0.0;
+#pragma unroll 4
+    for (int e = e0; e < e1; ++e) {
+      const uint32_t x = net.jac_w[e];
+      const double c = coef[x >> 16];
+      const int s = x & 0xffffu;
+      J0 = J0 + c * drate[s];
+      J1 = J1 + c * drate[D + s];
+    }
+    store((int)((dc.y >> 16) & 0xffu), (int)(dc.y >> 24), J0, J1);
+  }
+}
+
+__global__ void __launch_bounds__(PAIR_THREADS, 2)
+stage1_pair_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
+                   const double* __restrict__ dt, const double* __restrict__ atm, int flags,
+                   const uint8_t* __restrict__ fix_mask, double* __restrict__ ws) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.y, j0 = 2 * blockIdx.x;
+  Geo g = geo_of(B, b);
+  if (j0 >= g.nz) return;
+  const int ni = B.ni, nz = g.nz, ld = B.ld;
+  const bool two = j0 + 1 < nz;
+  PairSmem P = carve_pair(smem, ni, B.nr, net.T);
+  AtmRef a = atm_ref(atm + g.atm, nz, ni);
+  WsView w = ws_view(ws, g, ni, ld);
+  const double* yb = y + g.z0 * ni;
+  const double r = ros2_r();
+  const double c0 = 1.0 / (r * dt[b]);
+  __shared__ double coefs[MAX_COEF];
+  load_coefs(net, coefs);
+  // rows j0-1 .. j0+2 and their gas sums
+  for (int t = threadIdx.x; t < 4 * (ni + 1); t += blockDim.x) {
+    const int wr = t / (ni + 1), i = t % (ni + 1), jj = j0 - 1 + wr;
+    double v = 1.0;
+    if (i < ni) v = (jj >= 0 && jj < nz) ? yb[(int64_t)jj * ni + i] : 0.0;
+    P.y4[t] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int wr = threadIdx.x, jj = j0 - 1 + wr;
+    P.scal[wr] = (jj >= 0 && jj < nz) ? pairwise_sum_masked(P.y4 + wr * (ni + 1), a.gas, ni) : 0.0;
+  }
+  __syncthreads();
+  // diffusion of each layer (layer_diffusion on a one-layer view of the rows)
+  for (int l = 0; l < 2; ++l) {
+    if (l == 1 && !two) break;
+    LayerSmem L;
+    L.y3 = P.y4 + l * (ni + 1);
+    L.scal = P.scal + l;
+    L.diff = P.diff + l * ni;
+    L.diagd = P.diagd + l * ni;
+    layer_diffusion(a, nz, ni, j0 + l, flags, L, P.supb + l * ni, P.subb + l * ni, true);
+  }
+  rates_pair(net, P.y4 + (ni + 1), P.y4 + 2 * (ni + 1), k + g.z0 * (B.nr + 1) + j0, nz, two, a.M[j0],
+             two ? a.M[j0 + 1] : 0.0, P.rate, P.drate);
+  __syncthreads();
+  species_sums_pair(net, coefs, P.rate, P.part);
+  double* blk0 = w.inv + (int64_t)j0 * ni * ld;
+  double* blk1 = blk0 + (int64_t)ni * ld;
+  const uint8_t* fm0 = fix_mask ? fix_mask + g.z0 * ni + (int64_t)j0 * ni : nullptr;
+  const uint8_t* fm1 = fm0 ? fm0 + ni : nullptr;
+  const double bot = (j0 == 0 && (flags & VB_USE_BOTFLUX)) ? 1.0 : 0.0;
+  jacobian_pair(net, coefs, P.drate, [&](int row, int col, double J0, double J1) {
+    double v = (row == col ? c0 : 0.0) - J0;
+    if (row == col) {
+      double dd = P.diagd[row];
+      if (j0 == 0) dd = dd + (bot != 0.0 ? -a.vdep[row] / a.dzi[0] : 0.0);
+      v = v + (-dd);
+    }
+    if (fm0 && fm0[row]) v = (row == col) ? c0 : 0.0;
+    blk0[(int64_t)row * ld + col] = v;
+    if (two) {
+      double v1 = (row == col ? c0 : 0.0) - J1;
+      if (row == col) v1 = v1 + (-P.diagd[ni + row]);
+      if (fm1 && fm1[row]) v1 = (row == col) ? c0 : 0.0;
+      blk1[(int64_t)row * ld + col] = v1;
+    }
+  }, min(2 * ni, (int)blockDim.x));
+  __syncthreads();   // the species sums
+  for (int t = threadIdx.x; t < 2 * ni; t += blockDim.x) {
+    const int l = t / ni, i = t - l * ni, j = j0 + l;
+    if (l == 1 && !two) break;
+    const double* part = P.part + l * 2 * ni;
+    const uint8_t* fm = l ? fm1 : fm0;
+    double v = (part[2 * i + 1] - part[2 * i]) + P.diff[l * ni + i];
+    const bool fixed = fm && fm[i];
+    if (fixed) v = 0.0;
+    w.rmod[(int64_t)j * ni + i] = v;
+    if (j < nz - 1) {
+      double s2 = -P.supb[l * ni + i];
+      if (fixed) s2 = 0.0;
+      w.supn[(int64_t)j * ni + i] = s2;
+    }
+    if (j > 0) {
+      double s2 = -P.subb[l * ni + i];
+      if (fixed) s2 = 0.0;
+      w.subn[(int64_t)(j - 1) * ni + i] = s2;
+    }
+  }
+}
+
 // Stage-2 right-hand side: rmod[j] = rhs(yk2) - 2/(r dt) k1[j] with
 // yk2 = y + k1/r (jax_step.py:303-310). No drate buffer, so eight CTAs fit an
 // SM; occupancy, not per-thread ILP, hides the gathers' latency (measured on
@@ -444,9 +659,21 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
 }
 
 // ---------------------------------------------------------------- launchers
+// Stage-1 kernel of the Ros2 step (VbTuning.stage1_layers, default two layers per CTA).
+static constexpr int kStage1DefaultLayers = 2;
+
 cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, const double* k,
                           const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
                           cudaStream_t st, const double* adj_v) {
+  const int layers = B.stage1_layers ? B.stage1_layers : kStage1DefaultLayers;
+  if (!adj_v && layers == 2) {
+    size_t sm = pair_smem_bytes(B.ni, B.nr, net.T);
+    cudaError_t e = cudaFuncSetAttribute(stage1_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid((B.nz + 1) / 2, B.count);
+    stage1_pair_kernel<<<grid, PAIR_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
+    return cudaGetLastError();
+  }
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, true);
   cudaFuncSetAttribute(stage1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(B.nz, B.count);

@@ -73,6 +73,7 @@ struct Batch {
   int factor_kernel = 0;   // 1 blocked tensor-core, 2 scalar Gauss-Jordan
   int factor_ctas = 0;     // CTAs per SM of the factor (1 or 2, where both fit)
   int sweep_stages = 0;    // bulk-copy ring depth of the sweeps (1..3)
+  int stage1_layers = 0;   // layers per stage-1 CTA (1 or 2)
 };
 
 struct Geo {

@@ -256,3 +256,37 @@ def test_block_solves_fp64_and_mixed_mid_and_large(ni):
         ref = orc.block_thomas(diag[b], su[b], sb[b], rhs[b])
         assert rel_err(x64[b], ref, 1e-12) <= 1e-10
         assert rel_err(xm[b], ref, 1e-12) <= 1e-10
+
+
+@pytest.mark.parametrize("nz,kw", [(121, dict(moldiff=True, fluxes=True)), (24, dict(advection=True, fluxes=True)),
+                                   (7, dict())])
+def test_stage1_two_layers_per_cta_bit_identical(nz, kw):
+    """The stage-1 assembly with two layers per CTA (VbTuning.stage1_layers =
+    2) shares gather words between the layers but keeps each sum's order:
+    the step is bit-identical to the one-layer kernel's (odd layer counts,
+    bottom fluxes, a fix mask, a ragged batch included)."""
+    at = load_pkg("autotune")
+    net = syn.make_network(61, 30, 185)
+    dn = chem.to_device(net.tables)
+    cases = [syn.make_case(seed=(610 + b,), net=net, nz=nz, mild=True, k_range=(-40.0, 4.0), **kw) for b in range(3)]
+    Y = np.stack([c.y for c in cases])
+    K = np.stack([c.k for c in cases])
+    A = {kk: (np.stack([c.atm[kk] for c in cases]) if not isinstance(cases[0].atm[kk], bool)
+              else cases[0].atm[kk]) for kk in cases[0].atm}
+    fm = np.random.default_rng(nz).random(Y.shape) < 0.03
+    out = []
+    for layers in (1, 2):
+        at.set_tuning(dn, {"stage1_layers": layers})
+        step = jstep.Ros2Step(dn, atm_of(A))
+        s, d, st = step(Y, K, np.array([1e-6, 1e-4, 1e-8]), fix_mask=fm)
+        out.append((s.clone(), d.clone(), st.clone()))
+        rag = jstep.RaggedRos2Step(dn, [jstep.atm_from_dict(c.atm) for c in cases])
+        y, k = rag.pack([c.y for c in cases], [c.k for c in cases])
+        rs, rd, _ = rag(y, k, torch.as_tensor([1e-6, 1e-4, 1e-8], device="cuda"))
+        out.append((rs.clone(), rd.clone(), None))
+    at.set_tuning(dn, {})
+    assert torch.equal(out[0][0], out[2][0]) and torch.equal(out[0][1], out[2][1])
+    assert torch.equal(out[0][2], out[2][2]) and int(out[0][2].abs().sum()) == 0
+    assert torch.equal(out[1][0], out[3][0]) and torch.equal(out[1][1], out[3][1])
+    sref, dref = orc.ros2_step(cases[0].y, cases[0].k, 1e-6, cases[0].atm, net.tables, fix_mask=fm[0])
+    check_step(out[2][0][0].cpu(), out[2][1][0].cpu(), sref, dref)
