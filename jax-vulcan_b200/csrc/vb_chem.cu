@@ -470,6 +470,118 @@ __device__ inline void jacobian_pair(const NetDev& net, const double* coef, cons
   }
 }
 
+// Rates of both layers without drates (the stage-2 right-hand side).
+template <int TT>
+__device__ inline void rates_pair_rhs_t(const NetDev& net, const double* y0, const double* y1, const double* kcol,
+                                        int64_t kstride, bool two, double M0, double M1, double* rate) {
+  const int R = net.nr + 1;
+  constexpr int RU = 2;
+  for (int r0 = threadIdx.x; r0 < R; r0 += RU * blockDim.x) {
+    double kv[RU][2];
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int r = r0 + u * blockDim.x;
+      kv[u][0] = r < R ? __ldcg(kcol + (int64_t)r * kstride) : 0.0;
+      kv[u][1] = (two && r < R) ? __ldcg(kcol + (int64_t)r * kstride + 1) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int r = r0 + u * blockDim.x;
+      if (r < R) {
+        rate_slot<TT>(net, r, y0, kv[u][0], M0, rate, nullptr, false);
+        if (two) rate_slot<TT>(net, r, y1, kv[u][1], M1, rate + R, nullptr, false);
+      }
+    }
+  }
+}
+
+// Stage-2 right-hand side for layers j0 = 2 blockIdx.x and j0 + 1 (the rates
+// and species sums of stage2_kernel, gather words shared by the pair; every
+// value bit-identical to the one-layer kernel's).
+__host__ __device__ inline size_t pair2_smem_bytes(int ni, int nr) {
+  return (4 * (size_t)(ni + 1) + 2 * (size_t)(nr + 1) + 8 * (size_t)ni + 8) * sizeof(double);
+}
+
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
+stage2_pair_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
+                   const double* __restrict__ dt, const double* __restrict__ atm, int flags,
+                   const uint8_t* __restrict__ fix_mask, double* __restrict__ ws) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.y, j0 = 2 * blockIdx.x;
+  Geo g = geo_of(B, b);
+  if (j0 >= g.nz) return;
+  const int ni = B.ni, nz = g.nz, R = B.nr + 1;
+  const bool two = j0 + 1 < nz;
+  double* y4 = smem;
+  double* rate = y4 + 4 * (ni + 1);
+  double* diff = rate + 2 * R;
+  double* part = diff + 2 * ni;
+  double* scal = part + 4 * ni;
+  AtmRef a = atm_ref(atm + g.atm, nz, ni);
+  WsView w = ws_view(ws, g, ni, B.ld);
+  const double* yb = y + g.z0 * ni;
+  const double r = ros2_r();
+  const double dtb = dt[b];
+  __shared__ double coefs[MAX_COEF];
+  load_coefs(net, coefs);
+  // rows j0-1 .. j0+2 of yk2 = y + k1/r (load_rows' expression) and their gas sums
+  for (int t = threadIdx.x; t < 4 * (ni + 1); t += blockDim.x) {
+    const int wr = t / (ni + 1), i = t % (ni + 1), jj = j0 - 1 + wr;
+    double v = 1.0;
+    if (i < ni) {
+      if (jj >= 0 && jj < nz) {
+        v = yb[(int64_t)jj * ni + i];
+        v = v + w.k1[(int64_t)jj * ni + i] / r;
+      } else {
+        v = 0.0;
+      }
+    }
+    y4[t] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int wr = threadIdx.x, jj = j0 - 1 + wr;
+    scal[wr] = (jj >= 0 && jj < nz) ? pairwise_sum_masked(y4 + wr * (ni + 1), a.gas, ni) : 0.0;
+  }
+  __syncthreads();
+  for (int l = 0; l < 2; ++l) {
+    if (l == 1 && !two) break;
+    LayerSmem L;
+    L.y3 = y4 + l * (ni + 1);
+    L.scal = scal + l;
+    L.diff = diff + l * ni;
+    L.diagd = nullptr;
+    layer_diffusion(a, nz, ni, j0 + l, flags, L, nullptr, nullptr, false);
+  }
+  {
+    const double* kcol = k + g.z0 * R + j0;
+    const double M0 = a.M[j0], M1 = two ? a.M[j0 + 1] : 0.0;
+    switch (net.T) {
+      case 1: rates_pair_rhs_t<1>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      case 2: rates_pair_rhs_t<2>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      case 3: rates_pair_rhs_t<3>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      case 4: rates_pair_rhs_t<4>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      case 5: rates_pair_rhs_t<5>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      case 6: rates_pair_rhs_t<6>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      case 7: rates_pair_rhs_t<7>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+      default: rates_pair_rhs_t<8>(net, y4 + (ni + 1), y4 + 2 * (ni + 1), kcol, nz, two, M0, M1, rate); break;
+    }
+  }
+  __syncthreads();
+  species_sums_pair(net, coefs, rate, part);
+  __syncthreads();
+  for (int t = threadIdx.x; t < 2 * ni; t += blockDim.x) {
+    const int l = t / ni, i = t - l * ni, j = j0 + l;
+    if (l == 1 && !two) break;
+    const double* pt = part + l * 2 * ni;
+    double v = (pt[2 * i + 1] - pt[2 * i]) + diff[l * ni + i];
+    const uint8_t* fm = fix_mask ? fix_mask + g.z0 * ni + (int64_t)j * ni : nullptr;
+    if (fm && fm[i]) v = 0.0;
+    const double k1v = w.k1[(int64_t)j * ni + i];
+    w.rmod[(int64_t)j * ni + i] = v - (2.0 / (r * dtb)) * k1v;
+  }
+}
+
 __global__ void __launch_bounds__(PAIR_THREADS, 2)
 stage1_pair_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
                    const double* __restrict__ dt, const double* __restrict__ atm, int flags,
@@ -684,6 +796,15 @@ cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, co
 cudaError_t launch_stage2(const NetDev& net, const Batch& B, const double* y, const double* k,
                           const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
                           cudaStream_t st, double* resid) {
+  const int layers = B.stage1_layers ? B.stage1_layers : kStage1DefaultLayers;
+  if (!resid && layers == 2) {
+    size_t sm = pair2_smem_bytes(B.ni, B.nr);
+    cudaError_t e = cudaFuncSetAttribute(stage2_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid((B.nz + 1) / 2, B.count);
+    stage2_pair_kernel<<<grid, PAIR_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
+    return cudaGetLastError();
+  }
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, false);
   cudaFuncSetAttribute(stage2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(B.nz, B.count);
