@@ -640,6 +640,9 @@ def main():
                     help="atmospheres per GPU (default: two per SM, 296 on a B200)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--minimal", choices=["fp64", "mixed"], default=None,
+                    help="profiling runs: only the warm-up and the timed steps of the config-0 batch with the "
+                         "default launch shapes (plain FP64 or mixed step), one short JSON line")
     ap.add_argument("--workload", default="config0", choices=["config0", "config1", "config2", "config3",
                                                              "config4", "photo"],
                     help="config0: the headline batch (default); config1: the adaptive loop with "
@@ -689,6 +692,24 @@ def main():
 
     def one():
         step(y, k, dt, out=(sol, delta))
+
+    if args.minimal:
+        if args.minimal == "mixed":
+            step = jstep.Ros2Step(dn, atm, mixed=True)
+        for _ in range(args.warmup):
+            one()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            one()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                              "minimal": args.minimal, "batch": B, "status_ok": bool((step.status == 0).all())}))
+        return
 
     # launch shapes chosen by the project's autotuner on this GPU (factor kernel,
     # factor CTAs per SM, sweep ring depth, one or two streams), timed before
