@@ -1303,9 +1303,6 @@ cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* stat
   return launch_bgj32_t<16, 16, 1, false>(B, ws, mxr, status32, st);
 }
 
-cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, int32_t* status, cudaStream_t st) {
-  return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
-}
 
 
 // Tile shapes by block size: rows over 32 lanes x RPL, columns over NW warps
@@ -1331,6 +1328,12 @@ static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int wi
   // with 12 warps of 8)
   if (B.ni <= 96) return launch_gj_t<3, 6, 16, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
   return launch_gj_t<4, 8, 16, 1, false, R>(B, ws, status, with_rhs, tr, st, out, only);
+}
+
+cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, int32_t* status, cudaStream_t st) {
+  const bool blocked = B.factor_kernel ? B.factor_kernel == 1 : g_factor_variant == 0;
+  if (blocked) return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
+  return launch_gj<double>(B, ws, status, 0, 1, st, nullptr, only);
 }
 
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
