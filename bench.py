@@ -823,7 +823,9 @@ def main():
     h2d = y_h.numel() * 8 + dt_h.numel() * 8
     d2h = 2 * y_h.numel() * 8
 
-    # plain single-instance FP64 step (one atmosphere)
+    # plain single-instance FP64 step (one atmosphere; automatic launch shapes for
+    # a batch of one, not the batch's tuning)
+    at.set_tuning(dn, {})
     step1 = jstep.Ros2Step(dn, jstep.atm_from_dict(cases[0].atm))
     y1, k1, dt1 = y[:1].contiguous(), k[:1].contiguous(), dt[:1].contiguous()
     s1, d1 = torch.empty_like(y1), torch.empty_like(y1)
@@ -837,6 +839,7 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     single_ms = e0.elapsed_time(e1) / n1
+    at.set_tuning(dn, tuned)
 
     # the same batch size on the well-conditioned draw (order-scaled rate
     # constants), where the step agrees with the oracle elementwise
