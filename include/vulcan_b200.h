@@ -91,9 +91,9 @@ int vb_net_destroy(VbNet* net);
  *                  and joined with events, so the call stays stream-ordered
  *                  on the caller's stream), so one half's assembly overlaps
  *                  the other half's factor; 0 or 1 = one stream
- *   stage1_layers: layers per CTA of the stage-1 assembly, 1 or 2 (two share
- *                  every gather-table word and rate-constant sector; 0 =
- *                  the process default, 2) */
+ *   stage1_layers: layers per CTA of the stage-1 and stage-2 assembly, 1 or
+ *                  2 (two share every gather-table word and rate-constant
+ *                  sector; 0 = the default, 1) */
 typedef struct VbTuning {
   int32_t factor_kernel, factor_ctas, sweep_stages, streams, stage1_layers, reserved;
 } VbTuning;

@@ -771,8 +771,11 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
 }
 
 // ---------------------------------------------------------------- launchers
-// Stage-1 kernel of the Ros2 step (VbTuning.stage1_layers, default two layers per CTA).
-static constexpr int kStage1DefaultLayers = 2;
+// Stage-1 / stage-2 kernels of the Ros2 step (VbTuning.stage1_layers): one
+// layer per CTA by default (measured on B200 at 296 config-0 atmospheres, the
+// two-layer kernels make the step 13.08 ms against 12.81: the gather latency
+// is hidden better by more resident CTAs than by two chains per thread).
+static constexpr int kStage1DefaultLayers = 1;
 
 cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, const double* k,
                           const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,

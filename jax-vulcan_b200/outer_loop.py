@@ -162,13 +162,22 @@ class LoopState:
     def __init__(self, y, ymix, dt, atom_loss, atom_loss_prev=None, y_prev=None, t=0.0, rtol=0.2,
                  loss_criteria=1e-3, counters=None, small_y=0.0, nega_y=0.0):
         self.y = as_device(y).contiguous().clone()
+        if self.y.dim() != 3:
+            raise ValueError("y must be [B, nz, ni]")
         B = self.y.shape[0]
         self.y_prev = self.y if y_prev is None else as_device(y_prev).contiguous().clone()
         self.ymix = as_device(ymix).contiguous().clone()
+        # the kernels write [B, nz, ni] arrays through these pointers: a buffer
+        # of another shape would be written past its end
+        for name, t in (("y_prev", self.y_prev), ("ymix", self.ymix)):
+            if tuple(t.shape) != tuple(self.y.shape):
+                raise ValueError(f"{name} must have the shape of y {tuple(self.y.shape)}, got {tuple(t.shape)}")
         self.dt = as_device(np.broadcast_to(np.asarray(dt, np.float64), (B,)).copy())
         self.atom_loss = as_device(atom_loss).reshape(B, -1).contiguous().clone()
         self.atom_loss_prev = (self.atom_loss.clone() if atom_loss_prev is None
                                else as_device(atom_loss_prev).reshape(B, -1).contiguous().clone())
+        if self.atom_loss_prev.shape != self.atom_loss.shape:
+            raise ValueError("atom_loss_prev must have the shape of atom_loss")
         rec = np.zeros(B, SCALARS_DTYPE)
         rec["t"], rec["rtol"], rec["loss_criteria"] = t, rtol, loss_criteria
         rec["small_y"], rec["nega_y"] = small_y, nega_y

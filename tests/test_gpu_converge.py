@@ -338,10 +338,10 @@ def test_relaxing_network_runs_to_the_reference_stop_like_the_oracle():
         "photo_switch_longdy", "photo_switch_longdydt")})
     sm = float(loop.slope_min_of(atm["Kzz"], ex["Hp"])[0])
     # oracle chain to its own stop
-    s = dict(y=y0, y_prev=y0, ymix=ymix0, dt=1e-10, t=0.0, delta=0.0, accept_count=0, retry_count=0,
-             atom_loss=al0, atom_loss_prev=al0, nega_count=0, loss_count=0, delta_count=0, small_y=0.0, nega_y=0.0,
-             rtol=0.2, loss_criteria=1e-3, longdy=1.0, longdydt=1.0, longdy_seen_min=np.inf,
-             count_since_new_min=0)
+    s = dict(y=y0, y_prev=y0, ymix=np.broadcast_to(ymix0, y0.shape).copy(), dt=1e-10, t=0.0, delta=0.0,
+             accept_count=0, retry_count=0, atom_loss=al0, atom_loss_prev=al0, nega_count=0, loss_count=0,
+             delta_count=0, small_y=0.0, nega_y=0.0, rtol=0.2, loss_criteria=1e-3, longdy=1.0, longdydt=1.0,
+             longdy_seen_min=np.inf, count_since_new_min=0)
     ring_y, ring_t = np.zeros((cs.conv_step, nz, net.tables.ni)), np.zeros(cs.conv_step)
     n_oracle = 0
     while n_oracle < 2000:
@@ -354,7 +354,7 @@ def test_relaxing_network_runs_to_the_reference_stop_like_the_oracle():
     # the device loop to its own stop
     runner = loop.AdaptiveRunner(chem.to_device(net.tables), jstep.atm_from_dict(atm), loop.LoopStatics(**body), compo,
                                  atom_ini, conv=cs, slope_min=sm)
-    state = loop.LoopState(y0[None], ymix0[None], 1e-10, al0[None], rtol=0.2)
+    state = loop.LoopState(y0[None], np.broadcast_to(ymix0, y0.shape)[None], 1e-10, al0[None], rtol=0.2)
     n_dev = runner.run_to_convergence(state, k[None], max_attempts=2000, check_every=1)
     sc, cv = state.scalars_host()[0], state.conv_host()[0]
     assert cv["done"] == 1 and n_dev == n_oracle, (n_dev, n_oracle)
