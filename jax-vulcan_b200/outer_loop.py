@@ -169,9 +169,9 @@ class LoopState:
         self.ymix = as_device(ymix).contiguous().clone()
         # the kernels write [B, nz, ni] arrays through these pointers: a buffer
         # of another shape would be written past its end
-        for name, t in (("y_prev", self.y_prev), ("ymix", self.ymix)):
-            if tuple(t.shape) != tuple(self.y.shape):
-                raise ValueError(f"{name} must have the shape of y {tuple(self.y.shape)}, got {tuple(t.shape)}")
+        for name, arr in (("y_prev", self.y_prev), ("ymix", self.ymix)):
+            if tuple(arr.shape) != tuple(self.y.shape):
+                raise ValueError(f"{name} must have the shape of y {tuple(self.y.shape)}, got {tuple(arr.shape)}")
         self.dt = as_device(np.broadcast_to(np.asarray(dt, np.float64), (B,)).copy())
         self.atom_loss = as_device(atom_loss).reshape(B, -1).contiguous().clone()
         self.atom_loss_prev = (self.atom_loss.clone() if atom_loss_prev is None
