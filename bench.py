@@ -408,9 +408,15 @@ def run_config1(args, torch):
         atms, extras = zip(*[syn.make_atmosphere((b,), net, nz=nz) for b in range(B)])
         A = {kk: (v if isinstance(v, bool) else np.stack([a[kk] for a in atms])) for kk, v in atms[0].items()}
         ph = syn.make_photo(0, net, atms[0]["Tco"], bins, din12)       # Tco is the same profile for every seed
-        K = np.stack([syn.make_balanced_rates((b,), net, nz, e["n"], -12.0, 4.0, M=a["M"])[0]
-                      for b, (a, e) in enumerate(zip(atms, extras))])
-        y0 = np.stack([e["y"] for e in extras])
+        KY = [syn.make_balanced_rates((b,), net, nz, e["n"], -12.0, 4.0, M=a["M"]) for b, (a, e) in
+              enumerate(zip(atms, extras))]
+        K = np.stack([kk for kk, _ in KY])
+        # start near each network's equilibrium composition (each mixing ratio
+        # scaled by up to 2x), as a run restarted from a nearby state
+        rng = np.random.default_rng(17)
+        ymix0 = [ym * 10.0 ** rng.uniform(-0.3, 0.3, ym.shape) for _, ym in KY]
+        ymix0 = [ym / ym.sum() for ym in ymix0]
+        y0 = np.stack([ym[None, :] * e["n"][:, None] for ym, e in zip(ymix0, extras)])
         atom_ini = np.einsum("bzi,ia->ba", y0, net.compo)
         sm = np.concatenate([loop.slope_min_of(a["Kzz"], e["Hp"]) for a, e in zip(atms, extras)])
         refresh = ar.AtmRefreshStatic(pico=np.stack([e["pico"] for e in extras]), mol_mass=net.ms,
@@ -419,7 +425,7 @@ def run_config1(args, torch):
                                      batch=B, conv=loop.ConvStatics(use_photo=True), slope_min=sm,
                                      photo=photo.PhotoDevice(ph, nz), dz=np.stack([e["dz"] for e in extras]),
                                      flux_atol=1.0, refresh=refresh, update_frq=100)
-        state = loop.LoopState(y0, np.stack([e["ymix"] for e in extras]), 1e-10, np.zeros_like(atom_ini), rtol=0.2)
+        state = loop.LoopState(y0, y0 / y0.sum(axis=2, keepdims=True), 1e-10, np.zeros_like(atom_ini), rtol=0.2)
         runner.start(state)
         return runner, state, torch.as_tensor(K, device="cuda").contiguous()
 
