@@ -80,7 +80,8 @@ int vb_net_destroy(VbNet* net);
  * autotuner (jax-vulcan_b200/autotune.py), which times the candidates on the
  * device per network and batch; 0 in a field = the automatic choice.
  *   factor_kernel: 1 blocked Gauss-Jordan on the tensor cores, 2 scalar
- *                  Gauss-Jordan (0: the process default, vb_set_factor_kernel)
+ *                  Gauss-Jordan, 3 scalar Gauss-Jordan pipelined per column
+ *                  panel (0: the process default, vb_set_factor_kernel)
  *   factor_ctas:   CTAs per SM of the factor, 1 or 2 (honoured for 65-72
  *                  species, the shape with both variants compiled)
  *   sweep_stages:  depth of the sweeps' bulk-copy ring, 1..3 (lowered when
@@ -154,13 +155,24 @@ int vb_ros2_stages(const VbNet* net, int batch, int nz, const int64_t* zoff, con
  * at once); polls < 0 restores the default (2^22). No counterpart in the
  * reference (its solver has no waits). */
 int vb_set_wait_limit(long long polls);
+/* Poll limit of every wait between the warps of the pipelined factor
+ * (vb_set_factor_kernel(2), VbTuning.factor_kernel 3) for later launches from
+ * this process: a warp that gives up stops every other warp's wait, the
+ * atmosphere gets VB_STATUS_WATCHDOG and its factor returns after draining
+ * the prefetch in flight; polls < 0 restores the default (2^22). A test hook
+ * with no counterpart in the reference. */
+int vb_set_pipeline_wait_limit(long long polls);
 
 /* FP64 block-factor kernel of the step, the block solver and the adjoint, for
  * later launches from this process (a network's VbTuning.factor_kernel
  * overrides it for that network): 0 = blocked Gauss-Jordan, one warp per
  * 8-column panel, the panel's pivot steps inside the warp and the rank-8
  * trailing updates on the FP64 tensor cores (mma.sync m8n8k4); 1 (default) =
- * scalar Gauss-Jordan, one block barrier per pivot step. Both replace the
+ * scalar Gauss-Jordan, one block barrier per pivot step; 2 = the same scalar
+ * elimination pipelined: the warp owning a column panel runs its pivot steps
+ * back to back and publishes each (pivot row, multipliers) through a
+ * shared-memory ring signalled by mbarriers, the other warps apply the steps
+ * as they arrive (bounded waits; no block barrier per step). All replace the
  * reference's lu_factor + lu_solve(LU, I) pair (solver.py:46-48). */
 int vb_set_factor_kernel(int variant);
 

@@ -41,6 +41,7 @@ SIGNATURES = {
     "vb_ros2_step_mixed": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _i32, _p, _i, C.c_double, _p, _p, _p, _p, _p, _sz,
                                 _p]),
     "vb_set_wait_limit": (_i, [C.c_longlong]),
+    "vb_set_pipeline_wait_limit": (_i, [C.c_longlong]),
     "vb_set_factor_kernel": (_i, [_i]),
     "vb_chem_rhs": (_i, [_p, _i, _i, _p, _p, _p, _p, _p]),
     "vb_chem_jac": (_i, [_p, _i, _i, _p, _p, _p, _p, _p]),

@@ -48,7 +48,7 @@ def candidates(ni: int, split: bool = False):
     two-stream step (uniform batches only)."""
     ctas = (1, 2) if 64 < ni <= 72 else (0,)
     streams = (1, 2) if split else (1,)
-    for fk, fc, ss, sn, s1 in itertools.product((1, 2), ctas, (2, 3), streams, (1, 2)):
+    for fk, fc, ss, sn, s1 in itertools.product((1, 2, 3), ctas, (2, 3), streams, (1, 2)):
         yield {"factor_kernel": fk, "factor_ctas": fc, "sweep_stages": ss, "streams": sn, "stage1_layers": s1}
 
 

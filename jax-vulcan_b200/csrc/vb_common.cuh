@@ -190,6 +190,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
 }
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
+// mbarriers as intra-CTA producer/consumer signals (no async copies): an
+// arrival (release) per producing thread, a bounded wait (acquire) that also
+// gives up as soon as another warp has raised *abort.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, long long limit,
+                                                   const volatile int* abort) {
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort) return false;
+  }
+  return false;
+}
+
 // Ros2 constants (reference jax_step.py:257-258).
 __device__ __forceinline__ double ros2_r() { return 1.0 + 1.0 / sqrt(2.0); }
 

@@ -40,6 +40,7 @@ cudaError_t launch_gather_stages(const Batch&, const double* ws, double* k1, dou
 // Poll limit of the bounded waits of the factor and sweep kernels (a wait that
 // runs out sets VB_STATUS_WATCHDOG); polls < 0 restores the default.
 void set_wait_limit(long long polls);
+void set_pipe_wait_limit(long long polls);
 long long wait_limit();
 // FP64 factor kernel: 0 = blocked Gauss-Jordan with FP64 tensor-core trailing
 // updates, 1 = scalar Gauss-Jordan.

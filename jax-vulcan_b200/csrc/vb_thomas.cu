@@ -57,19 +57,25 @@ struct GJK {
   static constexpr int NPC = CPW * NW;          // column capacity (warp w holds columns w*CPW + c)
   static constexpr int CPWP = (CPW + 1) & ~1;   // stride of a warp's pivot-row slot (pairs)
   __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
-  static size_t smem_bytes(int n, int ld, bool dpf, int li = 0) {
+  static size_t smem_bytes(int n, int ld, bool dpf, int li = 0, bool pipe = false) {
     const size_t blk = (size_t)n * ld, iblk = (size_t)n * (li ? li : ld);
     return al(iblk * sizeof(R))                       // Ib: the inverse of the layer (natural order, stride li)
            + (dpf ? al(blk * sizeof(double)) : 0)     // Db: the next diagonal block, prefetched
            + al(2 * NPC * sizeof(double))             // rsc: row scales of this and the previous layer (EQ)
            + al(2 * NPR * sizeof(R))                  // colb: multipliers of the next step (2 parities)
            + al(NPR * sizeof(R))                      // rps: 1 / pivot of each row
-           + al(2 * NPR * sizeof(double))             // rsb: the next layer's rhs and sub_d rows
-           + al(NW * CPWP * sizeof(R))                // prs: pivot-row hand-over, one slot per warp
+           + al(4 * NPR * sizeof(double))             // rsb: the next layer's rhs and sub_d rows (2 parities)
+           + al((pipe ? 2 : 1) * NW * CPWP * sizeof(R))  // prs: pivot-row hand-over, a slot per warp (x2: parity)
            + al(2 * NPR * sizeof(double))             // vecs: right-hand side ping-pong
            + al(NPC * sizeof(int))                    // pivs: pivot row of each step
+           + al(NPR * sizeof(int))                    // qs: step of each pivot row
            + al(2 * sizeof(int))                      // pb: pivot row of the next step (2 parities)
-           + 16;                                      // mbarrier of the prefetch
+           + 16                                       // mbarrier of the prefetch
+           + (pipe ? al(2 * CPW * NPR * sizeof(R))    // colr: multiplier ring, one slot per column of two panels
+                         + al(2 * CPW * sizeof(int))  // pring: pivot row of each ring slot
+                         + al((2 * CPW + 2) * 8)      // mbarriers: a slot's publication (2 CPW), a panel consumed (2)
+                         + 16                         // abort flag
+                   : 0);
   }
 };
 
@@ -114,12 +120,13 @@ struct GJK {
 //    (row equilibration, exact); the stored inverse is X = (R A'_j)^{-1},
 //    the scales go to rs_out, and A'_j^{-1} = X diag(r).
 //  * li: row stride of Ib and of the stored inverses (ld when 0).
-template <int RPL, int CPW, int NW, bool DPF, typename R, bool EQ = false>
+template <int RPL, int CPW, int NW, bool DPF, typename R, bool EQ = false, bool PIPE = false>
 __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, const double* Din, R* out,
                                                      const double* __restrict__ supn,
                                                      const double* __restrict__ subn, double* rhs,
                                                      bool tr, int32_t* status, char* smem_raw, long long wlim,
-                                                     int li = 0, double* rs_out = nullptr) {
+                                                     int li = 0, double* rs_out = nullptr,
+                                                     long long plim = WAIT_LIMIT) {
   using G = GJK<RPL, CPW, NW, R>;
   using R2 = typename Pair<R>::T;
   constexpr int NPR = G::NPR, CPWP = G::CPWP, NPC = G::NPC;
@@ -145,19 +152,38 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   double* rsc = reinterpret_cast<double*>(take(2 * NPC * sizeof(double)));
   R* colb = reinterpret_cast<R*>(take(2 * NPR * sizeof(R)));
   R* rps = reinterpret_cast<R*>(take(NPR * sizeof(R)));
-  double* rsb = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
-  R* prs = reinterpret_cast<R*>(take(NW * G::CPWP * sizeof(R)));
+  double* rsb = reinterpret_cast<double*>(take(4 * NPR * sizeof(double)));
+  R* prs = reinterpret_cast<R*>(take((PIPE ? 2 : 1) * NW * G::CPWP * sizeof(R)));
   double* vecs = reinterpret_cast<double*>(take(2 * NPR * sizeof(double)));
   int* pivs = reinterpret_cast<int*>(take(G::NPC * sizeof(int)));
+  int* qs = reinterpret_cast<int*>(take(NPR * sizeof(int)));
   int* pb = reinterpret_cast<int*>(take(2 * sizeof(int)));
   uint64_t* bar = reinterpret_cast<uint64_t*>(take(16));
+  R* colr = PIPE ? reinterpret_cast<R*>(take(2 * CPW * NPR * sizeof(R))) : nullptr;
+  int* pring = PIPE ? reinterpret_cast<int*>(take(2 * CPW * sizeof(int))) : nullptr;
+  uint64_t* fbar = PIPE ? reinterpret_cast<uint64_t*>(take((2 * CPW + 2) * 8)) : nullptr;
+  uint64_t* ebar = PIPE ? fbar + 2 * CPW : nullptr;
+  volatile int* abortp = PIPE ? reinterpret_cast<volatile int*>(take(16)) : nullptr;
   const uint32_t dbytes = (uint32_t)(blk * sizeof(double));
   int st_local = 0;
+  // pipeline signals: fbar[s] completes when the owner warp of ring slot s
+  // has published it (32 arrivals), ebar[x] when every warp has applied a
+  // panel of parity x (32 NW arrivals)
+  auto pipe_init = [&]() {
+#pragma unroll 1
+    for (int s2 = 0; s2 < 2 * CPW; ++s2) mbar_init(fbar + s2, 32);
+    mbar_init(ebar, 32 * NW);
+    mbar_init(ebar + 1, 32 * NW);
+  };
 
   for (int e = threadIdx.x; e < iblk; e += blockDim.x) Ib[e] = R(0);   // the padding columns stay 0
   if (rhs)
     for (int i = threadIdx.x; i < n; i += blockDim.x) vecs[i] = rhs[i];
   if (DPF && threadIdx.x == 0) mbar_init(bar, 1);
+  if (PIPE && threadIdx.x == 0) {
+    pipe_init();
+    *abortp = 0;
+  }
   __syncthreads();
   if (DPF && threadIdx.x == 0) {
     mbar_expect_tx(bar, dbytes);
@@ -168,7 +194,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   // run by the warp that owns the column; publishes the pivot and multipliers.
   // Fast path: a unique maximum of the high word of |t| (valid rows keyed +1,
   // NaN as 0) decides. Otherwise the full 64-bit key, ties to the lowest row.
-  auto publish = [&](const R (&t)[RPL], unsigned used, int kn) {
+  auto publish = [&](const R (&t)[RPL], unsigned used, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
     unsigned h[RPL];
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
@@ -214,18 +240,154 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
     }
     if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
     const R rp = rcp_rn(piv);
-    R* cb = colb + (kn & 1) * NPR;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
-      cb[i] = (i < n && i != p1) ? t[r] * rp : R(0);
+      mo[r] = (i < n && i != p1) ? t[r] * rp : R(0);
+      cb[i] = mo[r];
     }
-    pb[kn & 1] = p1;   // every lane stores the same values
+    *pbp = p1;   // every lane stores the same values
     pivs[kn] = p1;
+    qs[p1] = kn;
     rps[p1] = rp;
+    return p1;
   };
 
   R a[RPL][CPW];
+
+  // PIPE: the same elimination without a block barrier per step. The warp
+  // that owns column k publishes step k (pivot row, multipliers) into ring
+  // slot (panel parity, column in panel) and signals fbar of the slot; the
+  // owner of a panel runs its steps back to back from registers while the
+  // other warps apply the published steps as they arrive. Before a panel
+  // reuses the slots of the panel two before it, its owner waits until every
+  // warp has applied that panel (ebar). Panel numbers and barrier phases
+  // restart every layer (a partial last panel publishes fewer slots). Every
+  // wait is bounded; a warp that gives up raises *abortp, which ends every
+  // other wait, and the layer's caller reports VB_STATUS_WATCHDOG.
+  auto eliminate_pipelined = [&](unsigned& used) {
+    bool dead = false;
+    auto fail = [&](bool ok) {
+      if (__any_sync(FULL, !ok)) {
+        dead = true;
+        *abortp = 1;
+      }
+    };
+    // multipliers and pivot row of the step this warp published last: the
+    // owner of a panel runs its steps from these registers
+    R mk[RPL];
+    int pk = 0;
+    if (warp == 0) {
+      R t[RPL];
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) t[r] = a[r][0];
+      pk = publish(t, 0u, 0, colr, pring, mk);
+      mbar_arrive(fbar);
+    }
+#pragma unroll 1
+    for (int w0 = 0; w0 < NW; ++w0) {
+      if (w0 * CPW >= n || dead) break;
+#pragma unroll
+      for (int c = 0; c < CPW; ++c) {
+        const int k = w0 * CPW + c;
+        if (k < n && !dead) {
+          if (warp == w0) {
+            // ---- owner of column k: the step from registers, this warp's
+            //      part of the pivot row by shuffles from the owner lane
+            const int p = pk, ps = p >> 5, po = p & 31;
+            R m[RPL];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+              m[r] = mk[r];
+              if (r == ps && lane == po) used |= 1u << r;
+            }
+            R prow[CPW];
+#pragma unroll
+            for (int c2 = 0; c2 < CPW; ++c2) {
+              R v = a[0][c2];
+#pragma unroll
+              for (int r = 1; r < RPL; ++r) v = (ps == r) ? a[r][c2] : v;
+              prow[c2] = __shfl_sync(FULL, v, po);
+            }
+            if (c + 1 < CPW && k + 1 < n) {   // column k+1 is this warp's too: publish step k+1
+              R t[RPL];
+#pragma unroll
+              for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[c + 1], a[r][c + 1]);
+#pragma unroll
+              for (int r = 0; r < RPL; ++r)
+#pragma unroll
+                for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+              const int sn = (w0 & 1) * CPW + c + 1;
+              pk = publish(t, used, k + 1, colr + sn * NPR, pring + sn, mk);
+              mbar_arrive(fbar + sn);
+            } else {
+#pragma unroll
+              for (int r = 0; r < RPL; ++r)
+#pragma unroll
+                for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+            }
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) a[r][c] = (lane + 32 * r == p) ? R(1) : -m[r];
+          } else {
+            // ---- every other warp: wait for the slot, then the step from
+            //      shared memory (pivot row through a per-warp hand-over slot,
+            //      two by step parity: one __syncwarp per step)
+            const int sl = (w0 & 1) * CPW + c;
+            fail(mbar_wait_or_abort(fbar + sl, (uint32_t)((w0 >> 1) & 1), plim, abortp));
+            if (!dead) {
+              const int p = pring[sl], ps = p >> 5, po = p & 31;
+              R m[RPL];
+#pragma unroll
+              for (int r = 0; r < RPL; ++r) {
+                m[r] = colr[sl * NPR + lane + 32 * r];
+                if (r == ps && lane == po) used |= 1u << r;
+              }
+              R* ph = prs + ((k & 1) * NW + warp) * CPWP;
+#pragma unroll
+              for (int r = 0; r < RPL; ++r)
+                if (r == ps && lane == po) {
+#pragma unroll
+                  for (int c2 = 0; c2 < CPWP; c2 += 2)
+                    reinterpret_cast<R2*>(ph)[c2 / 2] = R2{a[r][c2], c2 + 1 < CPW ? a[r][c2 + 1] : R(0)};
+                }
+              __syncwarp();
+              R prow[CPWP];
+#pragma unroll
+              for (int c2 = 0; c2 < CPWP; c2 += 2) {
+                const R2 v = reinterpret_cast<const R2*>(ph)[c2 / 2];
+                prow[c2] = v.x;
+                prow[c2 + 1] = v.y;
+              }
+              if (c + 1 == CPW && k + 1 < n && warp == w0 + 1) {
+                // column k+1 opens this warp's panel: publish step k+1, into
+                // the slots of the panel two before, once every warp has applied it
+                R t[RPL];
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[0], a[r][0]);
+#pragma unroll
+                for (int r = 0; r < RPL; ++r)
+#pragma unroll
+                  for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+                const int pn = w0 + 1, sn = (pn & 1) * CPW;
+                if (pn >= 2) fail(mbar_wait_or_abort(ebar + (pn & 1), (uint32_t)(((pn - 2) >> 1) & 1), plim, abortp));
+                if (!dead) {
+                  pk = publish(t, used, k + 1, colr + sn * NPR, pring + sn, mk);
+                  mbar_arrive(fbar + sn);
+                }
+              } else {
+#pragma unroll
+                for (int r = 0; r < RPL; ++r)
+#pragma unroll
+                  for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+              }
+            }
+          }
+          if (!dead && (c + 1 == CPW || k + 1 == n)) mbar_arrive(ebar + (w0 & 1));   // panel w0 applied
+        }
+      }
+    }
+  };
+
   for (int j = 0; j < nz; ++j) {
     if (DPF) {
       const bool ok = mbar_wait(bar, (uint32_t)(j & 1), wlim);
@@ -308,6 +470,11 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
 #pragma unroll
         for (int c = 0; c < CPW; ++c) a[r][c] = (R)v[r][c];
     }
+    double* rsj = rsb + (j & 1) * 2 * NPR;   // read by this layer's forward sweep
+    if (ride) {
+      rsj[threadIdx.x] = rn;
+      rsj[NPR + threadIdx.x] = sn;
+    }
     __syncthreads();   // Db and Ib consumed
     if (DPF && threadIdx.x == 0 && j + 1 < nz) {
       fence_proxy_async();
@@ -315,14 +482,29 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
       bulk_g2s(Db, Din + (int64_t)(j + 1) * blk, dbytes, bar);
     }
     unsigned used = 0;   // rows lane + 32 r already pivoted
-    int q[RPL];          // step whose pivot row is lane + 32 r
-#pragma unroll
-    for (int r = 0; r < RPL; ++r) q[r] = 0;
+    if constexpr (PIPE) {
+      eliminate_pipelined(used);
+      __syncthreads();
+      if (*abortp) {
+        // a wait gave up: drain the prefetch in flight, report, return
+        if (threadIdx.x == 0) {
+          if (DPF && j + 1 < nz) mbar_wait(bar, (uint32_t)((j + 1) & 1), WAIT_LIMIT);
+          atomicOr(status, VB_STATUS_WATCHDOG);
+        }
+        return;
+      }
+      if (threadIdx.x == 0) {   // every signal of this layer has completed: restart the phases
+#pragma unroll 1
+        for (int s2 = 0; s2 < 2 * CPW + 2; ++s2) mbar_inval(fbar + s2);
+        pipe_init();
+      }
+    } else {
+    R mo[RPL];
     if (warp == 0) {
       R t[RPL];
 #pragma unroll
       for (int r = 0; r < RPL; ++r) t[r] = a[r][0];
-      publish(t, 0u, 0);
+      publish(t, 0u, 0, colb, pb, mo);
     }
     __syncthreads();
     // ================================================================ elimination
@@ -340,10 +522,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
           for (int r = 0; r < RPL; ++r) m[r] = colb[(k & 1) * NPR + lane + 32 * r];
 #pragma unroll
           for (int r = 0; r < RPL; ++r)
-            if (r == ps && lane == po) {
-              used |= 1u << r;
-              q[r] = k;
-            }
+            if (r == ps && lane == po) used |= 1u << r;
           // this warp's part of the pivot row, from its owner lane (pair
           // stores predicated on the slot: no selects)
           R* ph = prs + warp * CPWP;
@@ -368,7 +547,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
             R t[RPL];
 #pragma unroll
             for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[cl], a[r][cl]);
-            publish(t, used, k + 1);
+            publish(t, used, k + 1, colb + ((k + 1) & 1) * NPR, pb + ((k + 1) & 1), mo);
 #pragma unroll
             for (int r = 0; r < RPL; ++r)
 #pragma unroll
@@ -387,24 +566,22 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
         }
       }
     }
-    if (ride) {
-      rsb[threadIdx.x] = rn;
-      rsb[NPR + threadIdx.x] = sn;
     }
     // ---- scale rows by 1/piv, scatter B^{-1}[q(i)][p_m] = T[i][m] into Ib
-    //      (A'^{-1}[p_m][q(i)] when tr)
+    //      (A'^{-1}[p_m][q(i)] when tr; q(i) = qs[i], the step pivoting on row i)
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
       if (i < n) {
         const R s = rps[i];
+        const int qi = qs[i];
 #pragma unroll
         for (int c = 0; c < CPW; ++c) {
           const int m = warp * CPW + c;
           if (m < n) {
             const R v = a[r][c] * s;
             if (!isfinite(v)) st_local |= VB_STATUS_NONFINITE;
-            Ib[tr ? pivs[m] * li + q[r] : q[r] * li + pivs[m]] = v;
+            Ib[tr ? pivs[m] * li + qi : qi * li + pivs[m]] = v;
           }
         }
       }
@@ -437,7 +614,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
         s += __shfl_xor_sync(FULL, s, 1);
         s += __shfl_xor_sync(FULL, s, 2);
         if (sub == 0 && i < n) {
-          const double v = rsb[i] - rsb[NPR + i] * s;
+          const double v = rsj[i] - rsj[NPR + i] * s;
           rhs[(int64_t)(j + 1) * n + i] = v;
           vn[i] = v;
         }
@@ -450,34 +627,36 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
 // out == nullptr: the inverses replace the blocks in the workspace (FP64
 // path); otherwise they go to out (layer-major, ni x ld per layer) and the
 // FP64 blocks stay. only != nullptr: atmospheres with only[b] == 0 are skipped.
-template <int RPL, int CPW, int NW, int MB, bool DPF, typename R>
+template <int RPL, int CPW, int NW, int MB, bool DPF, typename R, bool PIPE = false>
 __global__ void __launch_bounds__(NW * 32, MB)
 gj_factor_kernel(Batch B, double* __restrict__ ws, R* out, const int32_t* __restrict__ only,
-                 int32_t* __restrict__ status, int with_rhs, int tr, long long wlim) {
+                 int32_t* __restrict__ status, int with_rhs, int tr, long long wlim, long long plim) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
   if (only && only[b] == 0) return;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
   R* o = out ? out + g.z0 * B.ni * B.ld : reinterpret_cast<R*>(w.inv);
-  gj_factor_atmosphere<RPL, CPW, NW, DPF, R>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn,
-                                             with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw, wlim);
+  gj_factor_atmosphere<RPL, CPW, NW, DPF, R, false, PIPE>(g.nz, B.ni, B.ld, w.inv, o, w.supn, w.subn,
+                                                          with_rhs ? w.rmod : nullptr, tr != 0, status + b, smem_raw,
+                                                          wlim, 0, nullptr, plim);
 }
 
 // FP32 factor of the mixed-precision step by the scalar Gauss-Jordan kernel
 // (row-equilibrated, transposed orientation): FP32 inverses and row scales
 // into the mixed region, the FP64 blocks stay in the workspace.
-template <int RPL, int CPW, int NW, int MB, bool DPF>
+template <int RPL, int CPW, int NW, int MB, bool DPF, bool PIPE = false>
 __global__ void __launch_bounds__(NW * 32, MB)
 gj32_factor_kernel(Batch B, double* __restrict__ ws, void* __restrict__ mxr, int32_t* __restrict__ status,
-                   long long wlim) {
+                   long long wlim, long long plim) {
   extern __shared__ __align__(16) char smem_raw[];
   const int b = blockIdx.x;
   Geo g = geo_of(B, b);
   WsView w = ws_view(ws, g, B.ni, B.ld);
   MxView m = mx_view(mxr, g.z0, g.nz, B.ni);
-  gj_factor_atmosphere<RPL, CPW, NW, DPF, float, true>(g.nz, B.ni, B.ld, w.inv, m.X, w.supn, w.subn, nullptr, true,
-                                                       status + b, smem_raw, wlim, round4(B.ni), m.rs);
+  gj_factor_atmosphere<RPL, CPW, NW, DPF, float, true, PIPE>(g.nz, B.ni, B.ld, w.inv, m.X, w.supn, w.subn, nullptr,
+                                                             true, status + b, smem_raw, wlim, round4(B.ni), m.rs,
+                                                             plim);
 }
 
 // ---------------------------------------------------------------- blocked Gauss-Jordan factor (tensor cores)
@@ -1193,6 +1372,10 @@ __global__ void fp64_probe_kernel(double* out, int iters) {
 static long long g_wait_limit = WAIT_LIMIT;
 void set_wait_limit(long long polls) { g_wait_limit = polls < 0 ? WAIT_LIMIT : polls; }
 long long wait_limit() { return g_wait_limit; }
+// Poll limit of the pipelined factor's step signals (every wait of the
+// pipeline; giving up ends the atmosphere's factor with VB_STATUS_WATCHDOG).
+static long long g_pipe_wait_limit = WAIT_LIMIT;
+void set_pipe_wait_limit(long long polls) { g_pipe_wait_limit = polls < 0 ? WAIT_LIMIT : polls; }
 
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t st) {
   fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, iters);
@@ -1216,25 +1399,27 @@ static bool one_cta_per_sm(const Batch& B) {
   return B.count <= sm_count();
 }
 
-template <int RPL, int CPW, int NW, int MB, bool DPF, typename R = double>
+template <int RPL, int CPW, int NW, int MB, bool DPF, typename R, bool PIPE>
 static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
-                               R* out = nullptr, const int32_t* only = nullptr) {
-  size_t sm = GJK<RPL, CPW, NW, R>::smem_bytes(B.ni, B.ld, DPF);
-  cudaError_t e = cudaFuncSetAttribute(gj_factor_kernel<RPL, CPW, NW, MB, DPF, R>,
+                               R* out, const int32_t* only) {
+  size_t sm = GJK<RPL, CPW, NW, R>::smem_bytes(B.ni, B.ld, DPF, 0, PIPE);
+  cudaError_t e = cudaFuncSetAttribute(gj_factor_kernel<RPL, CPW, NW, MB, DPF, R, PIPE>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs, tr,
-                                                                                 g_wait_limit);
+  gj_factor_kernel<RPL, CPW, NW, MB, DPF, R, PIPE><<<B.count, NW * 32, sm, st>>>(B, ws, out, only, status, with_rhs,
+                                                                                       tr, g_wait_limit,
+                                                                                       g_pipe_wait_limit);
   return cudaGetLastError();
 }
 
-// FP64 factor kernel: 0 = blocked Gauss-Jordan with the trailing updates on
-// the FP64 tensor cores, 1 = scalar Gauss-Jordan (one block barrier per pivot
-// step; the default: faster on B200, 6.2 against 11.2 ms at 296 config-0
-// atmospheres, since a panel's pivot steps run serially in one warp).
+// Factor kernel of the process: 0 = blocked Gauss-Jordan with the trailing
+// updates on the FP64 tensor cores, 1 = scalar Gauss-Jordan with one block
+// barrier per pivot step, 2 = scalar Gauss-Jordan pipelined per column panel
+// (no block barrier per step). A network's tuning (factor_kernel 1..3 =
+// variant 0..2) overrides it.
 static int g_factor_variant = 1;
-static int g_factor32_variant = 1;
-void set_factor_variant(int v) { g_factor_variant = g_factor32_variant = v; }
+void set_factor_variant(int v) { g_factor_variant = v; }
+static int factor_choice(const Batch& B) { return B.factor_kernel ? B.factor_kernel - 1 : g_factor_variant; }
 
 template <int NW, int MB, bool DPF>
 static cudaError_t launch_bgj_t(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
@@ -1272,27 +1457,32 @@ static cudaError_t launch_bgj32_t(const Batch& B, double* ws, void* mxr, int32_t
   return cudaGetLastError();
 }
 
-template <int RPL, int CPW, int NW, int MB, bool DPF>
+template <int RPL, int CPW, int NW, int MB, bool DPF, bool PIPE>
 static cudaError_t launch_gj32_t(const Batch& B, double* ws, void* mxr, int32_t* status, cudaStream_t st) {
-  size_t sm = GJK<RPL, CPW, NW, float>::smem_bytes(B.ni, B.ld, DPF, round4(B.ni));
-  cudaError_t e = cudaFuncSetAttribute(gj32_factor_kernel<RPL, CPW, NW, MB, DPF>,
+  size_t sm = GJK<RPL, CPW, NW, float>::smem_bytes(B.ni, B.ld, DPF, round4(B.ni), PIPE);
+  cudaError_t e = cudaFuncSetAttribute(gj32_factor_kernel<RPL, CPW, NW, MB, DPF, PIPE>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  gj32_factor_kernel<RPL, CPW, NW, MB, DPF><<<B.count, NW * 32, sm, st>>>(B, ws, mxr, status, g_wait_limit);
+  gj32_factor_kernel<RPL, CPW, NW, MB, DPF, PIPE><<<B.count, NW * 32, sm, st>>>(B, ws, mxr, status, g_wait_limit,
+                                                                                      g_pipe_wait_limit);
   return cudaGetLastError();
 }
 
-cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st) {
-  const bool blocked = B.factor_kernel ? B.factor_kernel == 1 : g_factor32_variant == 0;
-  if (!blocked) {
-    if (B.ni <= 32) return launch_gj32_t<1, 4, 8, 4, true>(B, ws, mxr, status32, st);
-    if (B.ni <= 64) return launch_gj32_t<2, 8, 8, 2, true>(B, ws, mxr, status32, st);
-    if (B.ni <= 72) {
-      if (one_cta_per_sm(B)) return launch_gj32_t<3, 6, 12, 1, true>(B, ws, mxr, status32, st);
-      return launch_gj32_t<3, 6, 12, 2, true>(B, ws, mxr, status32, st);
-    }
-    return launch_gj32_t<3, 6, 16, 1, true>(B, ws, mxr, status32, st);
+template <bool PIPE>
+static cudaError_t launch_gj32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st) {
+  if (B.ni <= 32) return launch_gj32_t<1, 4, 8, 4, true, PIPE>(B, ws, mxr, status32, st);
+  if (B.ni <= 64) return launch_gj32_t<2, 8, 8, 2, true, PIPE>(B, ws, mxr, status32, st);
+  if (B.ni <= 72) {
+    if (one_cta_per_sm(B)) return launch_gj32_t<3, 6, 12, 1, true, PIPE>(B, ws, mxr, status32, st);
+    return launch_gj32_t<3, 6, 12, 2, true, PIPE>(B, ws, mxr, status32, st);
   }
+  return launch_gj32_t<3, 6, 16, 1, true, PIPE>(B, ws, mxr, status32, st);
+}
+
+cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st) {
+  const int v = factor_choice(B);
+  if (v == 1) return launch_gj32<false>(B, ws, mxr, status32, st);
+  if (v == 2) return launch_gj32<true>(B, ws, mxr, status32, st);
   if (B.ni <= 32) return launch_bgj32_t<4, 4, 4, true>(B, ws, mxr, status32, st);
   if (B.ni <= 64) return launch_bgj32_t<8, 8, 2, true>(B, ws, mxr, status32, st);
   if (B.ni <= 72) {
@@ -1314,34 +1504,41 @@ cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* stat
 // 6.43), one atmosphere 4.84 ms per Ros2 step (16 x 5: 5.50; 8 x 9: 5.92),
 // 296 atmospheres 6.15 ms (two CTAs of 8 x 9: 6.29; 10 x 7: 6.15; 14 x 5:
 // 7.09; 16 x 5: 9.14).
-template <typename R>
-static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
-                             R* out, const int32_t* only) {
-  if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R>(B, ws, status, with_rhs, tr, st, out, only);
-  if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+template <typename R, bool PIPE>
+static cudaError_t launch_gj_p(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
+                               R* out, const int32_t* only) {
+  if (B.ni <= 32) return launch_gj_t<1, 4, 8, 4, true, R, PIPE>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 64) return launch_gj_t<2, 8, 8, 2, true, R, PIPE>(B, ws, status, with_rhs, tr, st, out, only);
   if (B.ni <= 72) {
-    if (one_cta_per_sm(B)) return launch_gj_t<3, 6, 12, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
-    return launch_gj_t<3, 6, 12, 2, true, R>(B, ws, status, with_rhs, tr, st, out, only);
+    if (one_cta_per_sm(B))
+      return launch_gj_t<3, 6, 12, 1, true, R, PIPE>(B, ws, status, with_rhs, tr, st, out, only);
+    return launch_gj_t<3, 6, 12, 2, true, R, PIPE>(B, ws, status, with_rhs, tr, st, out, only);
   }
   // up to 96 species: 16 warps of 6 columns (the uneven 256-atmosphere batch,
   // whose ni=89 atmospheres set its floor: 16.49 ms per step against 16.99
   // with 12 warps of 8)
-  if (B.ni <= 96) return launch_gj_t<3, 6, 16, 1, true, R>(B, ws, status, with_rhs, tr, st, out, only);
-  return launch_gj_t<4, 8, 16, 1, false, R>(B, ws, status, with_rhs, tr, st, out, only);
+  if (B.ni <= 96) return launch_gj_t<3, 6, 16, 1, true, R, PIPE>(B, ws, status, with_rhs, tr, st, out, only);
+  return launch_gj_t<4, 8, 16, 1, false, R, PIPE>(B, ws, status, with_rhs, tr, st, out, only);
+}
+template <typename R>
+static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr, cudaStream_t st,
+                             R* out, const int32_t* only, bool pipe = false) {
+  if (pipe) return launch_gj_p<R, true>(B, ws, status, with_rhs, tr, st, out, only);
+  return launch_gj_p<R, false>(B, ws, status, with_rhs, tr, st, out, only);
 }
 
 cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, int32_t* status, cudaStream_t st) {
-  const bool blocked = B.factor_kernel ? B.factor_kernel == 1 : g_factor_variant == 0;
-  if (blocked) return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
-  return launch_gj<double>(B, ws, status, 0, 1, st, nullptr, only);
+  const int v = factor_choice(B);
+  if (v == 0) return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
+  return launch_gj<double>(B, ws, status, 0, 1, st, nullptr, only, v == 2);
 }
 
 cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_rhs, cudaStream_t st,
                           bool for_transposed_solves) {
   const int tr = for_transposed_solves ? 0 : 1;
-  const bool blocked = B.factor_kernel ? B.factor_kernel == 1 : g_factor_variant == 0;
-  if (blocked) return launch_bgj(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
-  return launch_gj<double>(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
+  const int v = factor_choice(B);
+  if (v == 0) return launch_bgj(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
+  return launch_gj<double>(B, ws, status, with_rhs, tr, st, nullptr, nullptr, v == 2);
 }
 
 // Factors into a separate inverse region (the workspace keeps the FP64
@@ -1356,8 +1553,9 @@ template cudaError_t launch_factor_into<float>(const Batch&, double*, float*, co
 template <>
 cudaError_t launch_factor_into<double>(const Batch& B, double* ws, double* out, const int32_t* only, int32_t* status,
                                        cudaStream_t st) {
-  if (g_factor_variant == 0) return launch_bgj(B, ws, status, 0, 1, st, out, only);
-  return launch_gj<double>(B, ws, status, 0, 1, st, out, only);
+  const int v = factor_choice(B);
+  if (v == 0) return launch_bgj(B, ws, status, 0, 1, st, out, only);
+  return launch_gj<double>(B, ws, status, 0, 1, st, out, only, v == 2);
 }
 
 cudaError_t launch_sweep(const Batch& B, double* ws, const SweepArgs& A, cudaStream_t st) {

@@ -171,6 +171,15 @@ def set_wait_limit(polls: int | None) -> None:
     _lib.check(_lib.lib().vb_set_wait_limit(-1 if polls is None else int(polls)), "vb_set_wait_limit")
 
 
+def set_pipeline_wait_limit(polls: int | None) -> None:
+    """Poll limit of the waits between the warps of the pipelined factor
+    (``vb_set_pipeline_wait_limit``); ``None`` restores the default. For
+    failure-detection tests: a wait that runs out ends every wait of the
+    atmosphere's factor and gives it ``VB_STATUS_WATCHDOG``."""
+    _lib.check(_lib.lib().vb_set_pipeline_wait_limit(-1 if polls is None else int(polls)),
+               "vb_set_pipeline_wait_limit")
+
+
 class RaggedRos2Step:
     """Ros2 step for atmospheres of one network with different layer counts
     (the ``zoff`` path of ``vb_ros2_step``).

@@ -10,12 +10,12 @@ at = load_pkg("autotune")
 
 def test_candidates_cover_the_compiled_variants():
     c69 = list(at.candidates(69))
-    assert len(c69) == 16 and len(list(at.candidates(69, split=True))) == 32
+    assert len(c69) == 24 and len(list(at.candidates(69, split=True))) == 48
     assert {c["factor_ctas"] for c in c69} == {1, 2}
-    assert {c["factor_kernel"] for c in c69} == {1, 2}
+    assert {c["factor_kernel"] for c in c69} == {1, 2, 3}
     assert {c["sweep_stages"] for c in c69} == {2, 3}
     c30 = list(at.candidates(30))
-    assert len(c30) == 8 and all(c["factor_ctas"] == 0 for c in c30)
+    assert len(c30) == 12 and all(c["factor_ctas"] == 0 for c in c30)
 
 
 def test_cache_round_trip(tmp_path):

@@ -1,6 +1,9 @@
-"""Both FP64 block-factor kernels (``vb_set_factor_kernel``): 0 = blocked
+"""The FP64 block-factor kernels (``vb_set_factor_kernel``): 0 = blocked
 Gauss-Jordan with the rank-8 trailing updates on the FP64 tensor cores, 1 =
-scalar Gauss-Jordan (default). Each is checked on the Ros2 step against the
+scalar Gauss-Jordan (default), 2 = the scalar elimination pipelined per column
+panel (mbarrier-signalled steps, no block barrier per step; the same
+arithmetic as 1, so its results equal 1's bit for bit). Each is checked on the
+Ros2 step against the
 oracle (well-conditioned draws, the step bound 1e-10 relative), on the
 reference's block-Thomas systems (1e-10), on the transposed solve the adjoint
 uses, and on the stiff config-0 draw by the normwise backward error of both
@@ -25,7 +28,7 @@ solver = load_pkg("solver")
 syn = load_pkg("synthetic")
 
 
-@pytest.fixture(params=[0, 1], ids=["blocked_dmma", "scalar_gj"])
+@pytest.fixture(params=[0, 1, 2], ids=["blocked_dmma", "scalar_gj", "pipelined_gj"])
 def variant(request):
     _lib.check(_lib.lib().vb_set_factor_kernel(request.param), "vb_set_factor_kernel")
     yield request.param
@@ -93,3 +96,31 @@ def test_stiff_draw_stage_backward_errors(variant):
     for b, c in enumerate(cases):
         bwd = orc.stage_backward_errors(c.y, c.k, c.dt, c.atm, net.tables, k1[b], k2[b])
         assert max(bwd) < 1e-11, (b, bwd)
+
+
+@pytest.mark.parametrize("ni,n_fwd", [(12, 30), (30, 185), (69, 700), (89, 1000)])
+def test_pipelined_equals_scalar_bit_for_bit(ni, n_fwd):
+    """The pipelined elimination performs the scalar kernel's operations in
+    the same order on the same values (only the hand-over between warps
+    differs), on a ragged batch (layer counts 2..20; partial last panels and
+    warps without columns at ni=12 and 30) of one network."""
+    elements = ("C", "H", "O", "N", "S") if ni == 89 else ("C", "H", "O", "N")
+    net = syn.make_network(90 + ni, ni, n_fwd, elements)
+    dn = chem.to_device(net.tables)
+    nzs = [12, 20, 7, 3, 2, 15]
+    cases = [syn.make_case(seed=(600 + b,), net=net, nz=nz, mild=True, k_range=(-40.0, 4.0), moldiff=True)
+             for b, nz in enumerate(nzs)]
+    dts = torch.as_tensor(np.array([1e-6, 1e-4, 1e-8, 1e-5, 1e-3, 1e-7]), device="cuda")
+    step = jstep.RaggedRos2Step(dn, [jstep.atm_from_dict(c.atm) for c in cases])
+    y, k = step.pack([c.y for c in cases], [c.k for c in cases])
+    out = {}
+    try:
+        for v in (1, 2):
+            _lib.check(_lib.lib().vb_set_factor_kernel(v), "vb_set_factor_kernel")
+            sol, delta, status = step(y, k, dts)
+            torch.cuda.synchronize()
+            out[v] = (sol.clone(), delta.clone(), status.clone())
+    finally:
+        _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
+    assert int(out[2][2].abs().sum()) == 0
+    assert torch.equal(out[1][0], out[2][0]) and torch.equal(out[1][1], out[2][1])

@@ -9,6 +9,10 @@ told to give up at once; nothing faults, traps or hangs a GPU.
   factor and sweep kernels gives up, each atmosphere gets VB_STATUS_WATCHDOG
   and the kernels return after draining their copies; with the default limit
   restored the next step is correct again.
+* ``vb_set_pipeline_wait_limit(0)`` with the pipelined factor: the first wait
+  of a warp for a step another warp publishes gives up, that warp stops every
+  other warp's wait, each atmosphere gets VB_STATUS_WATCHDOG; with the limit
+  restored the next step equals the first bit for bit.
 """
 import numpy as np
 import pytest
@@ -73,5 +77,24 @@ def test_wait_limit_gives_watchdog_status_and_recovers():
         jstep.set_wait_limit(None)
     assert (st & WATCHDOG).all(), st
     sol, delta, st2 = _step(step, Y, K, DT)
+    assert (st2 == 0).all(), st2
+    assert np.array_equal(sol, sol0) and np.array_equal(delta, delta0)
+
+
+def test_pipeline_wait_limit_gives_watchdog_status_and_recovers():
+    dn, step, Y, K, DT = _batch()
+    try:
+        _lib.check(_lib.lib().vb_set_factor_kernel(2), "vb_set_factor_kernel")
+        sol0, delta0, st0 = _step(step, Y, K, DT)
+        assert (st0 == 0).all()
+        try:
+            jstep.set_pipeline_wait_limit(0)
+            _, _, st = _step(step, Y, K, DT)
+        finally:
+            jstep.set_pipeline_wait_limit(None)
+        assert (st & WATCHDOG).all(), st
+        sol, delta, st2 = _step(step, Y, K, DT)
+    finally:
+        _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
     assert (st2 == 0).all(), st2
     assert np.array_equal(sol, sol0) and np.array_equal(delta, delta0)

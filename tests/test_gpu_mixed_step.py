@@ -55,7 +55,7 @@ def _run(net, cases, Y, K, DT, A, **kw):
 _lib = load_pkg("_lib")
 
 
-@pytest.fixture(params=[1, 0], ids=["scalar_gj", "blocked_tf32"])
+@pytest.fixture(params=[1, 0, 2], ids=["scalar_gj", "blocked_tf32", "pipelined_gj"])
 def factor_kernel(request):
     _lib.check(_lib.lib().vb_set_factor_kernel(request.param), "vb_set_factor_kernel")
     yield request.param
