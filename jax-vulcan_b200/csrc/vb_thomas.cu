@@ -194,7 +194,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   // run by the warp that owns the column; publishes the pivot and multipliers.
   // Fast path: a unique maximum of the high word of |t| (valid rows keyed +1,
   // NaN as 0) decides. Otherwise the full 64-bit key, ties to the lowest row.
-  auto publish = [&](const R (&t)[RPL], unsigned used, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
+  auto pivot_of = [&](const R (&t)[RPL], unsigned used, R& piv) {
     unsigned h[RPL];
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
@@ -216,7 +216,6 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
     const unsigned b1 = __ballot_sync(FULL, cnt > 0);
     const unsigned b2 = __ballot_sync(FULL, cnt > 1);
     int p1;
-    R piv;
     if (__popc(b1) == 1 && b2 == 0u) {
       const int wl = __ffs(b1) - 1;
       p1 = __shfl_sync(FULL, lane + 32 * mys, wl);
@@ -238,6 +237,11 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
       p1 = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
       piv = __shfl_sync(FULL, pick(t, p1 >> 5), p1 & 31);
     }
+    return p1;
+  };
+  // multipliers t / piv of step kn into cb (0 on the pivot row), its pivot
+  // row into *pbp, pivs[kn], qs[p1] and 1 / piv into rps[p1]
+  auto store_step = [&](const R (&t)[RPL], int p1, R piv, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
     if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
     const R rp = rcp_rn(piv);
 #pragma unroll
@@ -250,6 +254,11 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
     pivs[kn] = p1;
     qs[p1] = kn;
     rps[p1] = rp;
+  };
+  auto publish = [&](const R (&t)[RPL], unsigned used, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
+    R piv;
+    const int p1 = pivot_of(t, used, piv);
+    store_step(t, p1, piv, kn, cb, pbp, mo);
     return p1;
   };
 
@@ -273,15 +282,41 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
         *abortp = 1;
       }
     };
-    // multipliers and pivot row of the step this warp published last: the
-    // owner of a panel runs its steps from these registers
-    R mk[RPL];
+    // multipliers, pivot row and this warp's part of the pivot row of the
+    // step this warp published last: the owner of a panel runs its steps
+    // from these registers. The publisher takes its part of the pivot row
+    // by shuffles as soon as the argmax has named the row, while the
+    // reciprocal is in flight and before the other warps wake.
+    R mk[RPL], pn[CPW];
     int pk = 0;
+    // Publishing step kn from column values t: the argmax, then this warp's
+    // part of the new pivot row pk into pn (through the warp's hand-over slot
+    // of step kn's parity), then the multipliers and the signal.
+    auto fetch_row = [&](int kn) {
+      R* ph = prs + ((kn & 1) * NW + warp) * CPWP;
+      const int ps = pk >> 5, po = pk & 31;
+#pragma unroll
+      for (int r = 0; r < RPL; ++r)
+        if (r == ps && lane == po) {
+#pragma unroll
+          for (int c2 = 0; c2 < CPWP; c2 += 2)
+            reinterpret_cast<R2*>(ph)[c2 / 2] = R2{a[r][c2], c2 + 1 < CPW ? a[r][c2 + 1] : R(0)};
+        }
+      __syncwarp();
+#pragma unroll
+      for (int c2 = 0; c2 < CPW; c2 += 2) {
+        const R2 v = reinterpret_cast<const R2*>(ph)[c2 / 2];
+        pn[c2] = v.x;
+        if (c2 + 1 < CPW) pn[c2 + 1] = v.y;
+      }
+    };
     if (warp == 0) {
-      R t[RPL];
+      R t[RPL], piv;
 #pragma unroll
       for (int r = 0; r < RPL; ++r) t[r] = a[r][0];
-      pk = publish(t, 0u, 0, colr, pring, mk);
+      pk = pivot_of(t, 0u, piv);
+      fetch_row(0);
+      store_step(t, pk, piv, 0, colr, pring, mk);
       mbar_arrive(fbar);
     }
 #pragma unroll 1
@@ -291,9 +326,12 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
       for (int c = 0; c < CPW; ++c) {
         const int k = w0 * CPW + c;
         if (k < n && !dead) {
+          R t[RPL];          // column k+1 after this step, when this warp publishes step k+1
+          bool pub = false;  // (warp-uniform)
+          int sn = 0;        // and its ring slot
           if (warp == w0) {
-            // ---- owner of column k: the step from registers, this warp's
-            //      part of the pivot row by shuffles from the owner lane
+            // ---- owner of column k: the step from registers (pn: its part
+            //      of the pivot row, taken when the step was published)
             const int p = pk, ps = p >> 5, po = p & 31;
             R m[RPL];
 #pragma unroll
@@ -301,31 +339,14 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
               m[r] = mk[r];
               if (r == ps && lane == po) used |= 1u << r;
             }
-            R prow[CPW];
+            pub = c + 1 < CPW && k + 1 < n;   // column k+1 is this warp's too
+            sn = (w0 & 1) * CPW + (c + 1) % CPW;
 #pragma unroll
-            for (int c2 = 0; c2 < CPW; ++c2) {
-              R v = a[0][c2];
+            for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], pn[(c + 1) % CPW], a[r][(c + 1) % CPW]);
 #pragma unroll
-              for (int r = 1; r < RPL; ++r) v = (ps == r) ? a[r][c2] : v;
-              prow[c2] = __shfl_sync(FULL, v, po);
-            }
-            if (c + 1 < CPW && k + 1 < n) {   // column k+1 is this warp's too: publish step k+1
-              R t[RPL];
+            for (int r = 0; r < RPL; ++r)
 #pragma unroll
-              for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[c + 1], a[r][c + 1]);
-#pragma unroll
-              for (int r = 0; r < RPL; ++r)
-#pragma unroll
-                for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
-              const int sn = (w0 & 1) * CPW + c + 1;
-              pk = publish(t, used, k + 1, colr + sn * NPR, pring + sn, mk);
-              mbar_arrive(fbar + sn);
-            } else {
-#pragma unroll
-              for (int r = 0; r < RPL; ++r)
-#pragma unroll
-                for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
-            }
+              for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], pn[c2], a[r][c2]);
 #pragma unroll
             for (int r = 0; r < RPL; ++r) a[r][c] = (lane + 32 * r == p) ? R(1) : -m[r];
           } else {
@@ -358,29 +379,29 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
                 prow[c2] = v.x;
                 prow[c2 + 1] = v.y;
               }
-              if (c + 1 == CPW && k + 1 < n && warp == w0 + 1) {
-                // column k+1 opens this warp's panel: publish step k+1, into
-                // the slots of the panel two before, once every warp has applied it
-                R t[RPL];
+              // column k+1 opens this warp's panel: it publishes step k+1
+              pub = c + 1 == CPW && k + 1 < n && warp == w0 + 1;
 #pragma unroll
-                for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[0], a[r][0]);
+              for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[0], a[r][0]);
 #pragma unroll
-                for (int r = 0; r < RPL; ++r)
+              for (int r = 0; r < RPL; ++r)
 #pragma unroll
-                  for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
-                const int pn = w0 + 1, sn = (pn & 1) * CPW;
-                if (pn >= 2) fail(mbar_wait_or_abort(ebar + (pn & 1), (uint32_t)(((pn - 2) >> 1) & 1), plim, abortp));
-                if (!dead) {
-                  pk = publish(t, used, k + 1, colr + sn * NPR, pring + sn, mk);
-                  mbar_arrive(fbar + sn);
-                }
-              } else {
-#pragma unroll
-                for (int r = 0; r < RPL; ++r)
-#pragma unroll
-                  for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+                for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+              if (pub) {
+                // into the slots of the panel two before, once every warp has applied it
+                const int pnl = w0 + 1;
+                sn = (pnl & 1) * CPW;
+                if (pnl >= 2)
+                  fail(mbar_wait_or_abort(ebar + (pnl & 1), (uint32_t)(((pnl - 2) >> 1) & 1), plim, abortp));
               }
             }
+          }
+          if (pub && !dead) {
+            R piv;
+            pk = pivot_of(t, used, piv);
+            fetch_row(k + 1);
+            store_step(t, pk, piv, k + 1, colr + sn * NPR, pring + sn, mk);
+            mbar_arrive(fbar + sn);
           }
           if (!dead && (c + 1 == CPW || k + 1 == n)) mbar_arrive(ebar + (w0 & 1));   // panel w0 applied
         }
