@@ -520,12 +520,16 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
         pipe_init();
       }
     } else {
+    // the warp that published a step applies it from its registers (the
+    // owner of column k published step k: no shared-memory round trip on
+    // the lookahead warp's path in five of six steps)
     R mo[RPL];
+    int pk = 0;
     if (warp == 0) {
       R t[RPL];
 #pragma unroll
       for (int r = 0; r < RPL; ++r) t[r] = a[r][0];
-      publish(t, 0u, 0, colb, pb, mo);
+      pk = publish(t, 0u, 0, colb, pb, mo);
     }
     __syncthreads();
     // ================================================================ elimination
@@ -536,11 +540,18 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
       for (int c = 0; c < CPW; ++c) {
         const int k = w0 * CPW + c;
         if (k < n) {
-          const int p = pb[k & 1];
-          const int ps = p >> 5, po = p & 31;
+          int p;
           R m[RPL];
+          if (warp == w0) {
+            p = pk;
 #pragma unroll
-          for (int r = 0; r < RPL; ++r) m[r] = colb[(k & 1) * NPR + lane + 32 * r];
+            for (int r = 0; r < RPL; ++r) m[r] = mo[r];
+          } else {
+            p = pb[k & 1];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) m[r] = colb[(k & 1) * NPR + lane + 32 * r];
+          }
+          const int ps = p >> 5, po = p & 31;
 #pragma unroll
           for (int r = 0; r < RPL; ++r)
             if (r == ps && lane == po) used |= 1u << r;
@@ -568,7 +579,7 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
             R t[RPL];
 #pragma unroll
             for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[cl], a[r][cl]);
-            publish(t, used, k + 1, colb + ((k + 1) & 1) * NPR, pb + ((k + 1) & 1), mo);
+            pk = publish(t, used, k + 1, colb + ((k + 1) & 1) * NPR, pb + ((k + 1) & 1), mo);
 #pragma unroll
             for (int r = 0; r < RPL; ++r)
 #pragma unroll
