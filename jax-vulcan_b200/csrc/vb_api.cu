@@ -162,20 +162,61 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   if (coefs.empty()) coefs.push_back(0.0);
   // destinations in decreasing term count (ties: increasing index); threads
   // take them in rank bands (thread t: ranks t, t + LAYER_THREADS, ...) so the
-  // lanes of a warp sum lists of similar length. Descriptor of rank q: first
-  // term, then count | row << 16 | col << 24 (one load per destination).
-  std::vector<uint32_t> order(2 * (size_t)ni * ni);
+  // lanes of a warp sum lists of similar length. The term words of each group
+  // of 32 consecutive ranks are interleaved: term i of rank q at
+  // base(q / 32) + 32 i + q % 32, the group padded to its longest list (the
+  // first rank's), so a warp holding a group loads one line per term.
+  // Descriptor of rank q: its first word, then count | row << 16 | col << 24
+  // (one load per destination).
+  std::vector<uint32_t> order(2 * (size_t)ni * ni), jwi;
   {
-    std::vector<int32_t> perm((size_t)ni * ni);
-    for (size_t d = 0; d < perm.size(); ++d) perm[d] = (int32_t)d;
+    const size_t nd = (size_t)ni * ni;
+    std::vector<int32_t> perm(nd);
+    for (size_t d = 0; d < nd; ++d) perm[d] = (int32_t)d;
     std::stable_sort(perm.begin(), perm.end(),
                      [&](int32_t x, int32_t y) { return jp[x + 1] - jp[x] > jp[y + 1] - jp[y]; });
-    for (size_t q = 0; q < perm.size(); ++q) {
+    std::vector<size_t> gbase((nd + 31) / 32 + 1, 0);
+    for (size_t g = 0; g + 1 < gbase.size(); ++g) {
+      const int32_t d = perm[32 * g];
+      gbase[g + 1] = gbase[g] + 32 * (size_t)(jp[d + 1] - jp[d]);
+    }
+    if (gbase.back() > 0xffffffffu) return fail(VB_ERR_ARG, "Jacobian gather table too large");
+    jwi.assign(std::max<size_t>(gbase.back(), 1), 0u);
+    for (size_t q = 0; q < nd; ++q) {
       const uint32_t d = (uint32_t)perm[q];
       const uint32_t cnt = (uint32_t)(jp[d + 1] - jp[d]);
       if (cnt > 0xffffu) return fail(VB_ERR_ARG, "a Jacobian entry has more than 65535 terms");
-      order[2 * q] = (uint32_t)jp[d];
+      const size_t first = gbase[q / 32] + q % 32;
+      for (uint32_t i = 0; i < cnt; ++i) jwi[first + 32 * (size_t)i] = jw[jp[d] + i];
+      order[2 * q] = (uint32_t)first;
       order[2 * q + 1] = cnt | ((d / (uint32_t)ni) << 16) | ((d % (uint32_t)ni) << 24);
+    }
+  }
+  // species lists t = 2 i (loss), 2 i + 1 (production), words interleaved by
+  // groups of 32 consecutive lists (term k of list t at base(t / 32) + 32 k +
+  // t % 32, each group padded to its longest list); descriptor {first, count}
+  std::vector<uint32_t> sdesc(4 * (size_t)ni), swi;
+  {
+    const size_t nl = 2 * (size_t)ni;
+    auto len = [&](size_t t) -> size_t {
+      const std::vector<int32_t>& ptr = (t & 1) ? pp : lp;
+      return (size_t)(ptr[t / 2 + 1] - ptr[t / 2]);
+    };
+    std::vector<size_t> gbase((nl + 31) / 32 + 1, 0);
+    for (size_t g = 0; g + 1 < gbase.size(); ++g) {
+      size_t mx = 0;
+      for (size_t t = 32 * g; t < std::min(nl, 32 * g + 32); ++t) mx = std::max(mx, len(t));
+      gbase[g + 1] = gbase[g] + 32 * mx;
+    }
+    if (gbase.back() > 0xffffffffu) return fail(VB_ERR_ARG, "species gather table too large");
+    swi.assign(std::max<size_t>(gbase.back(), 1), 0u);
+    for (size_t t = 0; t < nl; ++t) {
+      const std::vector<int32_t>& ptr = (t & 1) ? pp : lp;
+      const std::vector<uint32_t>& w = (t & 1) ? pw : lw;
+      const size_t first = gbase[t / 32] + t % 32, n = len(t);
+      for (size_t k = 0; k < n; ++k) swi[first + 32 * k] = w[ptr[t / 2] + k];
+      sdesc[2 * t] = (uint32_t)first;
+      sdesc[2 * t + 1] = (uint32_t)n;
     }
   }
   std::vector<int32_t> ri(R * T), pi(R * T);
@@ -186,10 +227,9 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   std::vector<Part> parts = {
       {ri.data(), ri.size() * 4, 0}, {pi.data(), pi.size() * 4, 0},
       {r_st, (size_t)R * T * 8, 0},  {p_st, (size_t)R * T * 8, 0},
-      {three, (size_t)R, 0},         {lp.data(), lp.size() * 4, 0},
-      {lw.data(), lw.size() * 4, 0}, {pp.data(), pp.size() * 4, 0},
-      {pw.data(), pw.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
-      {jw.data(), jw.size() * 4, 0}, {coefs.data(), coefs.size() * 8, 0},
+      {three, (size_t)R, 0},         {sdesc.data(), sdesc.size() * 4, 0},
+      {swi.data(), swi.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
+      {jwi.data(), jwi.size() * 4, 0}, {coefs.data(), coefs.size() * 8, 0},
       {order.data(), order.size() * 4, 0}};
   size_t total = 0;
   for (auto& p : parts) { p.off = total; total += (p.bytes + 255) & ~(size_t)255; }
@@ -210,15 +250,13 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   d.r_st = (const double*)(b + parts[2].off);
   d.p_st = (const double*)(b + parts[3].off);
   d.three = (const uint8_t*)(b + parts[4].off);
-  d.loss_ptr = (const int32_t*)(b + parts[5].off);
-  d.loss_w = (const uint32_t*)(b + parts[6].off);
-  d.prod_ptr = (const int32_t*)(b + parts[7].off);
-  d.prod_w = (const uint32_t*)(b + parts[8].off);
-  d.jac_ptr = (const int32_t*)(b + parts[9].off);
-  d.jac_w = (const uint32_t*)(b + parts[10].off);
-  d.coef_tab = (const double*)(b + parts[11].off);
+  d.sum_desc = (const uint2*)(b + parts[5].off);
+  d.sum_w = (const uint32_t*)(b + parts[6].off);
+  d.jac_ptr = (const int32_t*)(b + parts[7].off);
+  d.jac_w = (const uint32_t*)(b + parts[8].off);
+  d.coef_tab = (const double*)(b + parts[9].off);
   d.n_coef = (int)coefs.size();
-  d.jac_desc = (const uint2*)(b + parts[12].off);
+  d.jac_desc = (const uint2*)(b + parts[10].off);
   net->base = base;
   net->bytes = total;
   *out = net;

@@ -136,14 +136,12 @@ __device__ inline void layer_rates(const NetDev& net, const double* yrow, const 
 // The caller synchronises before reading dy_i/dt = part[2i+1] - part[2i].
 __device__ inline void species_sums(const NetDev& net, const double* coef, const double* rate, double* part) {
   for (int t = threadIdx.x; t < 2 * net.ni; t += blockDim.x) {
-    const int i = t >> 1;
-    const int32_t* ptr = (t & 1) ? net.prod_ptr : net.loss_ptr;
-    const uint32_t* w = (t & 1) ? net.prod_w : net.loss_w;
+    const uint2 d = net.sum_desc[t];
     double acc = 0.0;
-    const int e1 = ptr[i + 1];
+    const int e1 = (int)d.x + 32 * (int)d.y;
 #pragma unroll 4
-    for (int e = ptr[i]; e < e1; ++e) {
-      const uint32_t x = w[e];
+    for (int e = (int)d.x; e < e1; e += 32) {
+      const uint32_t x = net.sum_w[e];
       acc = acc + coef[x >> 16] * rate[x & 0xffffu];
     }
     part[t] = acc;
@@ -158,23 +156,28 @@ __device__ inline void load_coefs(const NetDev& net, double* coef) {
 // Dense Jacobian of one layer (chem.py:183-208), each entry summed in the
 // reference's scatter order. Threads take the destinations in rank bands of
 // decreasing term count (jac_desc), so the lanes of a warp run loops of
-// similar length.
+// similar length; the terms of 32 consecutive ranks are interleaved in
+// jac_w (term i of a rank at its first word + 32 i), so a warp whose lanes
+// hold one such group reads one 128-byte line per term.
 // busy: the first threads are also summing species lists in the same phase;
-// the rank bands are rotated so those threads take the lightest ranks of each band.
+// the rank bands are rotated (by whole warps, keeping the groups aligned) so
+// those threads take the lightest ranks of each band.
+__device__ inline int warp_rotation(int busy) { return (busy + 31) & ~31; }
+
 template <typename Store>
 __device__ inline void layer_jacobian_each(const NetDev& net, const double* coef, const double* drate, Store store,
                                            int busy = 0) {
   const int nd = net.ni * net.ni;
   const int stride = blockDim.x;
-  int q = ((int)threadIdx.x - busy + stride) % stride;
+  int q = ((int)threadIdx.x - warp_rotation(busy) % stride + stride) % stride;
   uint2 dn = q < nd ? net.jac_desc[q] : make_uint2(0u, 0u);
   for (; q < nd; q += stride) {
     const uint2 dc = dn;
     if (q + stride < nd) dn = net.jac_desc[q + stride];   // the next destination's descriptor, one ahead
-    const int e0 = (int)dc.x, e1 = e0 + (int)(dc.y & 0xffffu);
+    const int e0 = (int)dc.x, e1 = e0 + 32 * (int)(dc.y & 0xffffu);
     double J = 0.0;
 #pragma unroll 4
-    for (int e = e0; e < e1; ++e) {
+    for (int e = e0; e < e1; e += 32) {
       const uint32_t x = net.jac_w[e];
       J = J + coef[x >> 16] * drate[x & 0xffffu];
     }
@@ -426,14 +429,12 @@ __device__ inline void rates_pair(const NetDev& net, const double* y0, const dou
 __device__ inline void species_sums_pair(const NetDev& net, const double* coef, const double* rate, double* part) {
   const int R = net.nr + 1;
   for (int t = threadIdx.x; t < 2 * net.ni; t += blockDim.x) {
-    const int i = t >> 1;
-    const int32_t* ptr = (t & 1) ? net.prod_ptr : net.loss_ptr;
-    const uint32_t* w = (t & 1) ? net.prod_w : net.loss_w;
+    const uint2 d = net.sum_desc[t];
     double a0 = 0.0, a1 = 0.0;
-    const int e1 = ptr[i + 1];
+    const int e1 = (int)d.x + 32 * (int)d.y;
 #pragma unroll 4
-    for (int e = ptr[i]; e < e1; ++e) {
-      const uint32_t x = w[e];
+    for (int e = (int)d.x; e < e1; e += 32) {
+      const uint32_t x = net.sum_w[e];
       const double c = coef[x >> 16];
       const int s = x & 0xffffu;
       a0 = a0 + c * rate[s];
@@ -451,15 +452,15 @@ __device__ inline void jacobian_pair(const NetDev& net, const double* coef, cons
   const int nd = net.ni * net.ni;
   const int64_t D = (int64_t)(net.nr + 1) * net.T;
   const int stride = blockDim.x;
-  int q = ((int)threadIdx.x - busy + stride) % stride;
+  int q = ((int)threadIdx.x - warp_rotation(busy) % stride + stride) % stride;
   uint2 dn = q < nd ? net.jac_desc[q] : make_uint2(0u, 0u);
   for (; q < nd; q += stride) {
     const uint2 dc = dn;
     if (q + stride < nd) dn = net.jac_desc[q + stride];
-    const int e0 = (int)dc.x, e1 = e0 + (int)(dc.y & 0xffffu);
+    const int e0 = (int)dc.x, e1 = e0 + 32 * (int)(dc.y & 0xffffu);
     double J0 = 0.0, J1 = 0.0;
 #pragma unroll 4
-    for (int e = e0; e < e1; ++e) {
+    for (int e = e0; e < e1; e += 32) {
       const uint32_t x = net.jac_w[e];
       const double c = coef[x >> 16];
       const int s = x & 0xffffu;

@@ -18,16 +18,19 @@ struct NetDev {
   // Gather tables, one 32-bit word per term: the low 16 bits index a rate
   // (loss / prod: reaction r) or a drate slot (Jacobian: r*T+s), the high 16
   // bits a coefficient in coef_tab (the distinct stoichiometries, <= 256).
-  // RHS: for species i, the (r*T+s) slots whose reactant (loss) or product
-  // (prod) index is i, in increasing flat order (segment_sum order); the
-  // coefficient is r_st[r*T+s] or p_st[r*T+s].
-  const int32_t* loss_ptr;       // [ni+1]
-  const uint32_t* loss_w;
-  const int32_t* prod_ptr;       // [ni+1]
-  const uint32_t* prod_w;
+  // RHS: list t = 2 i (loss) or 2 i + 1 (production) of species i, the
+  // (r*T+s) slots whose reactant (loss) or product index is i, in increasing
+  // flat order (segment_sum order); the coefficient is r_st[r*T+s] or
+  // p_st[r*T+s]. The words of each group of 32 consecutive lists are
+  // interleaved (term k of list t at its first word + 32 k), so the lanes of
+  // a warp summing lists t = 32 g .. 32 g + 31 load one line per term.
+  const uint2* sum_desc;         // [2 ni]: {first word in sum_w, term count}
+  const uint32_t* sum_w;
   // Jacobian: for destination d = row*ni+col, the contributions (r, o, s) in
   // increasing flat order (r*2T + o)*T + s (chem.py:193-207 scatter order);
-  // the coefficient is -r_st[r][o] (o < T) or p_st[r][o-T].
+  // the coefficient is -r_st[r][o] (o < T) or p_st[r][o-T]. jac_ptr is the
+  // CSR of that order; jac_w holds the words interleaved by groups of 32
+  // consecutive ranks of jac_desc (term i of a rank at its first word + 32 i).
   const int32_t* jac_ptr;        // [ni*ni+1]
   const uint32_t* jac_w;
   const double* coef_tab;        // [n_coef]
@@ -70,7 +73,7 @@ struct Batch {
   int ld;             // row stride of stored inverse blocks (ni rounded up to even)
   const int64_t* zoff;  // [count+1] prefix sums of layers, or nullptr (uniform)
   // launch shapes chosen by the network's tuning (VbTuning; 0 = automatic)
-  int factor_kernel = 0;   // 1 blocked tensor-core, 2 scalar Gauss-Jordan
+  int factor_kernel = 0;   // 1 blocked tensor-core, 2 scalar Gauss-Jordan, 3 pipelined
   int factor_ctas = 0;     // CTAs per SM of the factor (1 or 2, where both fit)
   int sweep_stages = 0;    // bulk-copy ring depth of the sweeps (1..3)
   int stage1_layers = 0;   // layers per stage-1 CTA (1 or 2)
