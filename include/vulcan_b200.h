@@ -210,7 +210,9 @@ int vb_bt_solve_T(int batch, int nz, int ni, const void* factors, const double* 
 
 /* Mixed-precision block solve (the solver of reference solver.py:33-112 with
  * the demotion inside, same FP64 interface): the diagonal blocks are factored
- * and inverted in FP32, the solution is refined in FP64 on the full
+ * and inverted in FP32 (up to 96 species with every row of each Schur-updated
+ * block first scaled by a power of two to magnitude [1, 2), the inverse
+ * applied as X diag(r)), the solution is refined in FP64 on the full
  * block-tridiagonal system (r = rhs - M x from the FP64 blocks, x += M~^{-1} r
  * with the FP32 inverses) until max|correction| <= tol * max|x|, at most
  * max_refine passes after the first solve. Atmospheres whose refinement

@@ -602,7 +602,10 @@ MixedLayout mixed_layout(int batch, int nz, int ni) {
   MixedLayout m;
   m.w64 = 0;
   m.inv32 = al(L * vb::ws_per_layer(ni, vb::round_even(ni)) * sizeof(double));
-  m.inv64 = m.inv32 + al(L * blk * sizeof(float));
+  // FP32 inverses: the row-equilibrated mixed region (X, row scales) for ni <= 96,
+  // plain inverses of stride ld above
+  const size_t f32 = std::max(L * blk * sizeof(float), (size_t)(L * vb::mx_bytes_per_layer(ni)));
+  m.inv64 = m.inv32 + al(f32);
   m.state = m.inv64 + al(L * blk * sizeof(double));
   m.fallback = m.state + al((size_t)batch * 4);
   m.passes = m.fallback + al((size_t)batch * 4);
@@ -626,8 +629,14 @@ int vb_bt_factor_mixed(int batch, int nz, int ni, const double* diag, const doub
   char* base = (char*)factors;
   VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
   VB_CHECK(vb::launch_pack_blocks(B, diag, sup_d, sub_d, (double*)(base + m.w64), st), "pack");
-  VB_CHECK(vb::launch_factor_into<float>(B, (double*)(base + m.w64), (float*)(base + m.inv32), nullptr, status, st),
-           "fp32 factor");
+  // up to 96 species: rows equilibrated by powers of two before the FP32
+  // inversion (X = (R A')^{-1}, A'^{-1} = X diag(r)); above, plain FP32 inverses
+  if (ni <= 96)
+    VB_CHECK(vb::launch_factor32(B, (double*)(base + m.w64), base + m.inv32, status, st), "fp32 factor");
+  else
+    VB_CHECK(vb::launch_factor_into<float>(B, (double*)(base + m.w64), (float*)(base + m.inv32), nullptr, status,
+                                           st),
+             "fp32 factor");
   return VB_OK;
 }
 
@@ -649,15 +658,16 @@ int vb_bt_solve_mixed(int batch, int nz, int ni, void* factors, const double* rh
   VB_CHECK(cudaMemsetAsync(state, 0, sizeof(int32_t) * batch, st), "state reset");
   VB_CHECK(cudaMemsetAsync(np, 0, sizeof(int32_t) * batch, st), "passes reset");
   const float* inv32 = (const float*)(base + m.inv32);
-  VB_CHECK(vb::launch_refine<float>(B, ws, inv32, rhs, x, state, np, tol, 1, nullptr, st), "fp32 solve");
+  const void* mxr = ni <= 96 ? (const void*)(base + m.inv32) : nullptr;   // equilibrated factors
+  VB_CHECK(vb::launch_refine<float>(B, ws, inv32, mxr, rhs, x, state, np, tol, 1, nullptr, st), "fp32 solve");
   for (int it = 0; it < max_refine; ++it)
-    VB_CHECK(vb::launch_refine<float>(B, ws, inv32, rhs, x, state, np, tol, 0, nullptr, st), "refinement");
+    VB_CHECK(vb::launch_refine<float>(B, ws, inv32, mxr, rhs, x, state, np, tol, 0, nullptr, st), "refinement");
   VB_CHECK(vb::launch_refine_finalize(batch, state, fb, status, st), "finalize");
   // FP64 fallback for the atmospheres whose refinement stalled (the others skip)
   double* inv64 = (double*)(base + m.inv64);
   VB_CHECK(vb::launch_factor_into<double>(B, ws, inv64, fb, status, st), "fp64 factor");
-  VB_CHECK(vb::launch_refine<double>(B, ws, inv64, rhs, x, state, np, tol, 1, fb, st), "fp64 solve");
-  VB_CHECK(vb::launch_refine<double>(B, ws, inv64, rhs, x, state, np, tol, 0, fb, st), "fp64 refinement");
+  VB_CHECK(vb::launch_refine<double>(B, ws, inv64, nullptr, rhs, x, state, np, tol, 1, fb, st), "fp64 solve");
+  VB_CHECK(vb::launch_refine<double>(B, ws, inv64, nullptr, rhs, x, state, np, tol, 0, fb, st), "fp64 refinement");
   if (passes)
     VB_CHECK(cudaMemcpyAsync(passes, np, sizeof(int32_t) * batch, cudaMemcpyDeviceToDevice, st), "passes");
   return VB_OK;

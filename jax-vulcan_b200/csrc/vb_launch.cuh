@@ -81,8 +81,9 @@ cudaError_t launch_conden_relax(int batch, int nz, int ni, const VbRelaxParams& 
                                 cudaStream_t st);
 cudaError_t launch_fp64_probe(double* out, int blocks, int threads, int iters, cudaStream_t);
 template <typename R>
-cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,
-                          int32_t* passes, double tol, int first, const int32_t* only, cudaStream_t st);
+cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const void* mxr, const double* rhs, double* x,
+                          int32_t* state, int32_t* passes, double tol, int first, const int32_t* only,
+                          cudaStream_t st);
 // Mixed-precision Ros2 step (vb_mixed.cu): one solve pass (first: x = M~^{-1} b;
 // else one FP64-residual refinement pass) over rmod -> k1 (xsel 0) / aux (1).
 cudaError_t launch_mx_pass(const Batch& B, double* ws, void* mxr, int xsel, bool first, int32_t* mode,

@@ -19,14 +19,16 @@ namespace vb {
 constexpr int REFINE_THREADS = 256;
 constexpr int REFINE_WARPS = REFINE_THREADS / 32;
 
-// y[i] = sum_m A[i][m] v[m] for an n x n block of row stride ld (one warp per
-// row, lanes over columns); v and y in shared memory.
+// y[i] = sum_m A[i][m] (sc[m] v[m]) for an n x n block of row stride ld (one
+// warp per row, lanes over columns; sc = nullptr: no column scales); v and y
+// in shared memory.
 template <typename T>
-__device__ inline void block_mv(const T* __restrict__ A, int n, int ld, const double* v, double* y) {
+__device__ inline void block_mv(const T* __restrict__ A, int n, int ld, const double* v, double* y,
+                                const double* __restrict__ sc = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = warp; i < n; i += REFINE_WARPS) {
     double s = 0.0;
-    for (int m = lane; m < n; m += 32) s = fma((double)A[(int64_t)i * ld + m], v[m], s);
+    for (int m = lane; m < n; m += 32) s = fma((double)A[(int64_t)i * ld + m], sc ? sc[m] * v[m] : v[m], s);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     if (lane == 0) y[i] = s;
@@ -36,11 +38,13 @@ __device__ inline void block_mv(const T* __restrict__ A, int n, int ld, const do
 // One pass of refinement for every atmosphere (CTA per atmosphere). first:
 // x is taken as 0 (the pass is the plain solve). state[b]: 1 once converged
 // (later passes skip it). only != nullptr: atmospheres with only[b] == 0 skip.
+// The inverses: inv (stride ld), or with mxr != nullptr (R = float) the
+// row-equilibrated factors of the mixed region, A'_j^{-1} = X_j diag(r_j).
 template <typename R>
 __global__ void __launch_bounds__(REFINE_THREADS)
-refine_kernel(Batch B, double* __restrict__ ws, const R* __restrict__ inv, const double* __restrict__ rhs,
-              double* __restrict__ x, int32_t* __restrict__ state, int32_t* __restrict__ passes, double tol,
-              int first, const int32_t* __restrict__ only) {
+refine_kernel(Batch B, double* __restrict__ ws, const R* __restrict__ inv, const void* __restrict__ mxr,
+              const double* __restrict__ rhs, double* __restrict__ x, int32_t* __restrict__ state,
+              int32_t* __restrict__ passes, double tol, int first, const int32_t* __restrict__ only) {
   __shared__ double sx[VB_MAX_NI], sv[VB_MAX_NI], sr[VB_MAX_NI], su[VB_MAX_NI];
   __shared__ double red[REFINE_WARPS][2];
   const int b = blockIdx.x;
@@ -50,6 +54,14 @@ refine_kernel(Batch B, double* __restrict__ ws, const R* __restrict__ inv, const
   const int n = B.ni, nz = g.nz, ld = B.ld;
   WsView w = ws_view(ws, g, n, ld);
   const R* Ib = inv + g.z0 * n * ld;
+  int li = ld;                    // row stride of the inverses
+  const double* rsc = nullptr;    // their column scales [nz][ni], if equilibrated
+  if (mxr) {
+    const MxView m = mx_view(const_cast<void*>(mxr), g.z0, nz, n);
+    Ib = reinterpret_cast<const R*>(m.X);
+    rsc = m.rs;
+    li = round4(n);
+  }
   const double* bb = rhs + g.z0 * n;
   double* xb = x + g.z0 * n;
   double* rp = w.rmod;   // forward-eliminated residual, [nz][ni]
@@ -59,7 +71,8 @@ refine_kernel(Batch B, double* __restrict__ ws, const R* __restrict__ inv, const
       for (int i = threadIdx.x; i < n; i += blockDim.x) sx[i] = xb[(int64_t)j * n + i];
     __syncthreads();
     if (!first) block_mv(w.inv + (int64_t)j * n * ld, n, ld, sx, su);   // A_j x_j (FP64 blocks)
-    if (j > 0) block_mv(Ib + (int64_t)(j - 1) * n * ld, n, ld, sr, sv);  // Inv_{j-1} r'_{j-1}
+    if (j > 0)                                                           // Inv_{j-1} r'_{j-1}
+      block_mv(Ib + (int64_t)(j - 1) * n * li, n, li, sr, sv, rsc ? rsc + (int64_t)(j - 1) * n : nullptr);
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       double r = bb[(int64_t)j * n + i];
@@ -84,7 +97,7 @@ refine_kernel(Batch B, double* __restrict__ ws, const R* __restrict__ inv, const
       sv[i] = v;
     }
     __syncthreads();
-    block_mv(Ib + (int64_t)j * n * ld, n, ld, sv, sr);   // c_j
+    block_mv(Ib + (int64_t)j * n * li, n, li, sv, sr, rsc ? rsc + (int64_t)j * n : nullptr);   // c_j
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const double c = sr[i];
@@ -132,15 +145,16 @@ __global__ void refine_finalize_kernel(int batch, const int32_t* __restrict__ st
 }
 
 template <typename R>
-cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const double* rhs, double* x, int32_t* state,
-                          int32_t* passes, double tol, int first, const int32_t* only, cudaStream_t st) {
-  refine_kernel<R><<<B.count, REFINE_THREADS, 0, st>>>(B, ws, inv, rhs, x, state, passes, tol, first, only);
+cudaError_t launch_refine(const Batch& B, double* ws, const R* inv, const void* mxr, const double* rhs, double* x,
+                          int32_t* state, int32_t* passes, double tol, int first, const int32_t* only,
+                          cudaStream_t st) {
+  refine_kernel<R><<<B.count, REFINE_THREADS, 0, st>>>(B, ws, inv, mxr, rhs, x, state, passes, tol, first, only);
   return cudaGetLastError();
 }
-template cudaError_t launch_refine<float>(const Batch&, double*, const float*, const double*, double*, int32_t*,
-                                          int32_t*, double, int, const int32_t*, cudaStream_t);
-template cudaError_t launch_refine<double>(const Batch&, double*, const double*, const double*, double*, int32_t*,
-                                           int32_t*, double, int, const int32_t*, cudaStream_t);
+template cudaError_t launch_refine<float>(const Batch&, double*, const float*, const void*, const double*, double*,
+                                          int32_t*, int32_t*, double, int, const int32_t*, cudaStream_t);
+template cudaError_t launch_refine<double>(const Batch&, double*, const double*, const void*, const double*, double*,
+                                           int32_t*, int32_t*, double, int, const int32_t*, cudaStream_t);
 
 cudaError_t launch_refine_finalize(int batch, const int32_t* state, int32_t* fallback, int32_t* status,
                                    cudaStream_t st) {
