@@ -757,7 +757,8 @@ def main():
 
     # the two FP64 factor kernels on the same batch (per-launch event split)
     variants = {}
-    for vid, vname in ((2, "scalar_gauss_jordan"), (3, "pipelined_gauss_jordan"), (1, "blocked_dmma")):
+    for vid, vname in ((2, "scalar_gauss_jordan"), (3, "pipelined_gauss_jordan"), (4, "paired_gauss_jordan"),
+                       (1, "blocked_dmma")):
         at.set_tuning(dn, dict(tuned, streams=1, factor_kernel=vid))
         for _ in range(args.warmup):
             one()

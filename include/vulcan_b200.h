@@ -81,7 +81,9 @@ int vb_net_destroy(VbNet* net);
  * device per network and batch; 0 in a field = the automatic choice.
  *   factor_kernel: 1 blocked Gauss-Jordan on the tensor cores, 2 scalar
  *                  Gauss-Jordan, 3 scalar Gauss-Jordan pipelined per column
- *                  panel (0: the process default, vb_set_factor_kernel)
+ *                  panel, 4 scalar Gauss-Jordan with two atmospheres per CTA
+ *                  (uniform batches of 65-72 species; else as 2) (0: the
+ *                  process default, vb_set_factor_kernel)
  *   factor_ctas:   CTAs per SM of the factor, 1 or 2 (honoured for 65-72
  *                  species, the shape with both variants compiled)
  *   sweep_stages:  depth of the sweeps' bulk-copy ring, 1..3 (lowered when
@@ -117,9 +119,10 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff,
 /* Mixed-precision Ros2 step: the same inputs, outputs and FP64 interface as
  * vb_ros2_step, with the demotion inside. The LHS blocks are assembled in
  * FP64 (kept for the residual); each Schur-updated block is row-equilibrated
- * (exact powers of two) and inverted in FP32 by the blocked Gauss-Jordan
- * factor with its rank-8 trailing updates on the TF32 tensor cores (each
- * operand split into a TF32 head and tail, three products); each stage solve
+ * (exact powers of two) and inverted in FP32 by the process's factor kernel
+ * (vb_set_factor_kernel: scalar Gauss-Jordan by default; the blocked kernel
+ * runs its rank-8 trailing updates on the TF32 tensor cores, each operand
+ * split into a TF32 head and tail, three products); each stage solve
  * LHS k = rhs (jax_step.py:300-311) starts from the FP32 factors and is
  * refined in FP64 on the full block-tridiagonal system (r = rhs - LHS k from
  * the FP64 blocks, k += M~^{-1} r) until max|correction| <= tol * max|k|, at
@@ -172,7 +175,10 @@ int vb_set_pipeline_wait_limit(long long polls);
  * elimination pipelined: the warp owning a column panel runs its pivot steps
  * back to back and publishes each (pivot row, multipliers) through a
  * shared-memory ring signalled by mbarriers, the other warps apply the steps
- * as they arrive (bounded waits; no block barrier per step). All replace the
+ * as they arrive (bounded waits; no block barrier per step); 3 = the scalar
+ * elimination with two atmospheres per CTA, their pivot chains interleaved
+ * in the same warps under one barrier per step (FP64 factor of uniform
+ * batches of 65-72 species; the scalar kernel elsewhere). All replace the
  * reference's lu_factor + lu_solve(LU, I) pair (solver.py:46-48). */
 int vb_set_factor_kernel(int variant);
 

@@ -47,8 +47,11 @@ def candidates(ni: int, split: bool = False):
     """Candidate tunings of a network with ni species; ``split``: also the
     two-stream step (uniform batches only)."""
     ctas = (1, 2) if 64 < ni <= 72 else (0,)
+    kernels = (1, 2, 3, 4) if 64 < ni <= 72 else (1, 2, 3)   # 4: the paired kernel (65-72 species)
     streams = (1, 2) if split else (1,)
-    for fk, fc, ss, sn, s1 in itertools.product((1, 2, 3), ctas, (2, 3), streams, (1, 2)):
+    for fk, fc, ss, sn, s1 in itertools.product(kernels, ctas, (2, 3), streams, (1, 2)):
+        if fk == 4 and fc == 2:
+            continue   # one paired CTA per SM holds two atmospheres: no CTA-count choice
         yield {"factor_kernel": fk, "factor_ctas": fc, "sweep_stages": ss, "streams": sn, "stage1_layers": s1}
 
 

@@ -275,10 +275,10 @@ size_t vb_net_device_bytes(const VbNet* net) { return net ? net->bytes : 0; }
 
 int vb_net_set_tuning(VbNet* net, const VbTuning* t) {
   if (!net || !t) return fail(VB_ERR_ARG, "null argument");
-  if (t->factor_kernel < 0 || t->factor_kernel > 3 || t->factor_ctas < 0 || t->factor_ctas > 2 ||
+  if (t->factor_kernel < 0 || t->factor_kernel > 4 || t->factor_ctas < 0 || t->factor_ctas > 2 ||
       t->sweep_stages < 0 || t->sweep_stages > 3 || t->streams < 0 || t->streams > 2 || t->stage1_layers < 0 ||
       t->stage1_layers > 2)
-    return fail(VB_ERR_ARG, "tuning out of range (factor_kernel 0..3, factor_ctas 0..2, sweep_stages 0..3, "
+    return fail(VB_ERR_ARG, "tuning out of range (factor_kernel 0..4, factor_ctas 0..2, sweep_stages 0..3, "
                             "streams 0..2, stage1_layers 0..2)");
   net->tune = *t;
   return VB_OK;
@@ -514,7 +514,7 @@ int vb_set_pipeline_wait_limit(long long polls) {
 }
 
 int vb_set_factor_kernel(int variant) {
-  if (variant < 0 || variant > 2) return fail(VB_ERR_ARG, "factor kernel variant must be 0, 1 or 2");
+  if (variant < 0 || variant > 3) return fail(VB_ERR_ARG, "factor kernel variant must be 0, 1, 2 or 3");
   vb::set_factor_variant(variant);
   return VB_OK;
 }

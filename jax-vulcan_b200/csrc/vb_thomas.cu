@@ -656,6 +656,462 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   if (st_local) atomicOr(status, st_local);
 }
 
+// ---------------------------------------------------------------- paired Gauss-Jordan factor
+// Two atmospheres of one uniform batch per CTA, their pivot chains
+// interleaved in the same warps: every warp holds both atmospheres' tiles
+// (the single kernel's layout), each step's loads, hand-overs and updates are
+// issued for both, and the warp owning the next column takes both argmaxes
+// and reciprocals back to back, so the two chains' latencies overlap and one
+// block barrier serves both. The arithmetic of each atmosphere is the single
+// kernel's, in the same order (FP64, transposed orientation when tr).
+
+// Row-slot value of a per-lane row array (s warp-uniform).
+template <int RPL>
+__device__ __forceinline__ double pick_slot(const double (&v)[RPL], int s) {
+  double x = v[0];
+#pragma unroll
+  for (int r = 1; r < RPL; ++r) x = (s == r) ? v[r] : x;
+  return x;
+}
+
+// Argmax of a column over its unpivoted rows with the full 64-bit |v| key,
+// ties to the lowest row (the single kernel's slow path).
+template <int RPL>
+__device__ __forceinline__ int pivot_full(const double (&t)[RPL], unsigned used, int n, double& piv) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  unsigned long long bk = 0ull;
+  unsigned brow = 0xffffffffu;
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n && !((used >> r) & 1u)) {
+      const unsigned long long kk = pivot_key(t[r]);
+      if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
+    }
+  }
+  const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
+  const unsigned n1 = __reduce_max_sync(FULL, hi);
+  const unsigned n2 = __reduce_max_sync(FULL, hi == n1 ? lo : 0u);
+  const int p1 = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
+  piv = __shfl_sync(FULL, pick_slot(t, p1 >> 5), p1 & 31);
+  return p1;
+}
+
+// Argmaxes of two columns (one per atmosphere), interleaved: the high-word
+// keys of both are reduced together; when both maxima are unique the pivots
+// come from one round of shuffles, else each column takes the full-key path.
+// The chosen rows equal the single kernel's.
+template <int RPL>
+__device__ __forceinline__ void pivot_pair(const double (&t)[2][RPL], const unsigned (&used)[2], int n,
+                                           int (&p1)[2], double (&piv)[2]) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  unsigned hm[2];
+  int cnt[2], mys[2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    unsigned h[RPL];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int i = lane + 32 * r;
+      const bool ok = i < n && !((used[e] >> r) & 1u) && !isnan(t[e][r]);
+      h[r] = ok ? hi_key(t[e][r]) + 1u : 0u;
+    }
+    unsigned m = h[0];
+#pragma unroll
+    for (int r = 1; r < RPL; ++r) m = max(m, h[r]);
+    hm[e] = m;
+    cnt[e] = 0;
+    mys[e] = 0;
+  }
+  const unsigned m1a = __reduce_max_sync(FULL, hm[0]);
+  const unsigned m1b = __reduce_max_sync(FULL, hm[1]);
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const unsigned m1 = e ? m1b : m1a;
+#pragma unroll
+    for (int r = RPL - 1; r >= 0; --r) {
+      const int i = lane + 32 * r;
+      const bool ok = i < n && !((used[e] >> r) & 1u) && !isnan(t[e][r]);
+      const unsigned h = ok ? hi_key(t[e][r]) + 1u : 0u;
+      if (h == m1) {
+        ++cnt[e];
+        mys[e] = r;
+      }
+    }
+  }
+  const unsigned b1a = __ballot_sync(FULL, cnt[0] > 0), b2a = __ballot_sync(FULL, cnt[0] > 1);
+  const unsigned b1b = __ballot_sync(FULL, cnt[1] > 0), b2b = __ballot_sync(FULL, cnt[1] > 1);
+  if (__popc(b1a) == 1 && b2a == 0u && __popc(b1b) == 1 && b2b == 0u) {
+    const int wa = __ffs(b1a) - 1, wb = __ffs(b1b) - 1;
+    p1[0] = __shfl_sync(FULL, lane + 32 * mys[0], wa);
+    p1[1] = __shfl_sync(FULL, lane + 32 * mys[1], wb);
+    piv[0] = __shfl_sync(FULL, pick_slot(t[0], mys[0]), wa);
+    piv[1] = __shfl_sync(FULL, pick_slot(t[1], mys[1]), wb);
+  } else {
+    p1[0] = pivot_full(t[0], used[0], n, piv[0]);
+    p1[1] = pivot_full(t[1], used[1], n, piv[1]);
+  }
+}
+
+// Shared-memory plan of the paired factor: per atmosphere (carved in this
+// order, each piece on a 16-byte boundary) the inverse of the layer, the
+// prefetched next block, multipliers (2 parities), 1/pivot per row, the next
+// layer's rhs and sub_d rows (2 parities), the per-warp pivot-row hand-over,
+// the rhs ping-pong, pivot row per step, step per pivot row, the next
+// step's pivot row (2 parities) and the prefetch mbarrier.
+template <int RPL, int CPW, int NW>
+struct GJP {
+  static constexpr int NPR = 32 * RPL, NPC = CPW * NW, CPWP = (CPW + 1) & ~1;
+  __host__ __device__ static size_t al(size_t x) { return (x + 15) & ~(size_t)15; }
+  static size_t one_bytes(int n, int ld) {
+    const size_t blk = (size_t)n * ld * sizeof(double);
+    return 2 * al(blk) + al(2 * NPR * 8) + al(NPR * 8) + al(4 * NPR * 8) + al(NW * CPWP * 8) + al(2 * NPR * 8) +
+           al(NPC * 4) + al(NPR * 4) + al(2 * 4) + 16;
+  }
+  static size_t smem_bytes(int n, int ld) { return 2 * one_bytes(n, ld); }
+};
+
+struct PairPtrs {
+  const double* Din[2];  // D_j of each atmosphere (row stride ld), layer-major
+  double* out[2];        // inverses (may equal Din: in place)
+  const double* supn[2];
+  const double* subn[2];
+  double* rhs[2];        // rhs rows for the ride-along forward sweep, or nullptr
+  int32_t* status[2];
+};
+
+// Publishes step KN of both atmospheres from their column values T (the
+// single kernel's store of the multipliers, pivot rows and reciprocals, into
+// parity PAR); written as a macro so the register arrays it updates never
+// leave registers.
+#define VB_PAIR_PUBLISH(T, KN, PAR)                                            \
+  do {                                                                         \
+    int p1_[2];                                                                \
+    double piv_[2], rp_[2];                                                    \
+    pivot_pair<RPL>(T, used, n, p1_, piv_);                                    \
+    _Pragma("unroll") for (int e_ = 0; e_ < 2; ++e_) {                         \
+      if (piv_[e_] == 0.0) st_local[e_] |= VB_STATUS_ZERO_PIVOT;               \
+      rp_[e_] = rcp_rn(piv_[e_]);                                              \
+    }                                                                          \
+    _Pragma("unroll") for (int e_ = 0; e_ < 2; ++e_) {                         \
+      _Pragma("unroll") for (int r_ = 0; r_ < RPL; ++r_) {                     \
+        const int i_ = lane + 32 * r_;                                         \
+        mo[e_][r_] = (i_ < n && i_ != p1_[e_]) ? T[e_][r_] * rp_[e_] : 0.0;    \
+        colb[e_][(PAR) * NPR + i_] = mo[e_][r_];                               \
+      }                                                                        \
+      pb[e_][PAR] = p1_[e_];                                                   \
+      pivs[e_][KN] = p1_[e_];                                                  \
+      qs[e_][p1_[e_]] = (KN);                                                  \
+      rps[e_][p1_[e_]] = rp_[e_];                                              \
+      pk[e_] = p1_[e_];                                                        \
+    }                                                                          \
+  } while (0)
+
+template <int RPL, int CPW, int NW>
+__device__ __forceinline__ void gj_factor_pair(int nz, int n, int ld, const PairPtrs& P, bool tr, char* smem_raw,
+                                               long long wlim) {
+  using G = GJP<RPL, CPW, NW>;
+  constexpr int NPR = G::NPR, CPWP = G::CPWP;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned FULL = 0xffffffffu;
+  const int blk = n * ld;
+  const bool with_rhs = P.rhs[0] != nullptr;
+  double *Ib[2], *Db[2], *colb[2], *rps[2], *rsb[2], *prs[2], *vecs[2];
+  int *pivs[2], *qs[2], *pb[2];
+  uint64_t* bar[2];
+  {
+    char* sp = smem_raw;
+    auto take = [&](size_t bytes) {
+      char* q = sp;
+      sp += G::al(bytes);
+      return q;
+    };
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      Ib[e] = reinterpret_cast<double*>(take((size_t)blk * 8));
+      Db[e] = reinterpret_cast<double*>(take((size_t)blk * 8));
+      colb[e] = reinterpret_cast<double*>(take(2 * NPR * 8));
+      rps[e] = reinterpret_cast<double*>(take(NPR * 8));
+      rsb[e] = reinterpret_cast<double*>(take(4 * NPR * 8));
+      prs[e] = reinterpret_cast<double*>(take(NW * CPWP * 8));
+      vecs[e] = reinterpret_cast<double*>(take(2 * NPR * 8));
+      pivs[e] = reinterpret_cast<int*>(take(G::NPC * 4));
+      qs[e] = reinterpret_cast<int*>(take(NPR * 4));
+      pb[e] = reinterpret_cast<int*>(take(2 * 4));
+      bar[e] = reinterpret_cast<uint64_t*>(take(16));
+    }
+  }
+  const uint32_t dbytes = (uint32_t)(blk * sizeof(double));
+  int st_local[2] = {0, 0};
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    for (int q = threadIdx.x; q < blk; q += blockDim.x) Ib[e][q] = 0.0;   // the padding columns stay 0
+    if (with_rhs)
+      for (int i = threadIdx.x; i < n; i += blockDim.x) vecs[e][i] = P.rhs[e][i];
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(bar[0], 1);
+    mbar_init(bar[1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      mbar_expect_tx(bar[e], dbytes);
+      bulk_g2s(Db[e], P.Din[e], dbytes, bar[e]);
+    }
+  }
+  double a[2][RPL][CPW];
+  for (int j = 0; j < nz; ++j) {
+    {
+      const bool ok0 = mbar_wait(bar[0], (uint32_t)(j & 1), wlim);
+      const bool ok1 = mbar_wait(bar[1], (uint32_t)(j & 1), wlim);
+      if (__syncthreads_or(!(ok0 && ok1))) {
+        // give up: wait (bounded) for the copies still in flight, report, return
+        if (threadIdx.x == 0) {
+          mbar_wait(bar[0], (uint32_t)(j & 1), WAIT_LIMIT);
+          mbar_wait(bar[1], (uint32_t)(j & 1), WAIT_LIMIT);
+          atomicOr(P.status[0], VB_STATUS_WATCHDOG);
+          atomicOr(P.status[1], VB_STATUS_WATCHDOG);
+        }
+        return;
+      }
+    }
+    // the next layer's rhs and sub_d rows, for the forward sweeps at the end of the layer
+    double rn[2] = {0.0, 0.0}, sn[2] = {0.0, 0.0};
+    const bool ride = with_rhs && j + 1 < nz && (int)threadIdx.x < n;
+    if (ride) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        rn[e] = P.rhs[e][(int64_t)(j + 1) * n + threadIdx.x];
+        sn[e] = P.subn[e][(int64_t)j * n + threadIdx.x];
+      }
+    }
+    // ---- D_j and the Hadamard Schur update from Inv_{j-1} (solver.py:47)
+    {
+      const int si = tr ? 1 : ld, sm = tr ? ld : 1;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        double sr[RPL], sc[CPW];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) {
+          const int i = lane + 32 * r;
+          sr[r] = (j > 0 && i < n) ? (tr ? P.supn[e] : P.subn[e])[(int64_t)(j - 1) * n + i] : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) {
+          const int m = warp * CPW + c;
+          sc[c] = (j > 0 && m < n) ? (tr ? P.subn[e] : P.supn[e])[(int64_t)(j - 1) * n + m] : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) {
+          const int i = lane + 32 * r;
+#pragma unroll
+          for (int c = 0; c < CPW; ++c) {
+            const int m = warp * CPW + c;
+            double x = 0.0;
+            if (i < n && m < n) {
+              x = Db[e][i * si + m * sm];
+              if (j > 0) {
+                const double cb = tr ? sc[c] * sr[r] : sr[r] * sc[c];
+                double inv = Ib[e][i * si + m * sm];
+                x = x - cb * inv;
+              }
+            }
+            a[e][r][c] = x;
+          }
+        }
+        double* rsj = rsb[e] + (j & 1) * 2 * NPR;   // read by this layer's forward sweep
+        if (ride) {
+          rsj[threadIdx.x] = rn[e];
+          rsj[NPR + threadIdx.x] = sn[e];
+        }
+      }
+    }
+    __syncthreads();   // Db and Ib consumed
+    if (threadIdx.x == 0 && j + 1 < nz) {
+      fence_proxy_async();
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        mbar_expect_tx(bar[e], dbytes);
+        bulk_g2s(Db[e], P.Din[e] + (int64_t)(j + 1) * blk, dbytes, bar[e]);
+      }
+    }
+    // ================================================================ elimination (both chains)
+    unsigned used[2] = {0u, 0u};   // rows lane + 32 r already pivoted
+    double mo[2][RPL];             // multipliers of the step this warp published
+    int pk[2] = {0, 0};            // and its pivot rows
+    if (warp == 0) {
+      double t[2][RPL];
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) t[e][r] = a[e][r][0];
+      VB_PAIR_PUBLISH(t, 0, 0);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int w0 = 0; w0 < NW; ++w0) {
+      if (w0 * CPW >= n) break;
+#pragma unroll
+      for (int c = 0; c < CPW; ++c) {
+        const int k = w0 * CPW + c;
+        if (k < n) {
+          int p[2];
+          double m[2][RPL];
+          if (warp == w0) {   // this warp published step k: from its registers
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              p[e] = pk[e];
+#pragma unroll
+              for (int r = 0; r < RPL; ++r) m[e][r] = mo[e][r];
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              p[e] = pb[e][k & 1];
+#pragma unroll
+              for (int r = 0; r < RPL; ++r) m[e][r] = colb[e][(k & 1) * NPR + lane + 32 * r];
+            }
+          }
+          // this warp's parts of both pivot rows, from their owner lanes
+          double prow[2][CPWP];
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int ps = p[e] >> 5, po = p[e] & 31;
+            double* ph = prs[e] + warp * CPWP;
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+              if (r == ps && lane == po) {
+                used[e] |= 1u << r;
+#pragma unroll
+                for (int c2 = 0; c2 < CPWP; c2 += 2)
+                  reinterpret_cast<double2*>(ph)[c2 / 2] =
+                      make_double2(a[e][r][c2], c2 + 1 < CPW ? a[e][r][c2 + 1] : 0.0);
+              }
+          }
+          __syncwarp();
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+#pragma unroll
+            for (int c2 = 0; c2 < CPWP; c2 += 2) {
+              const double2 v = reinterpret_cast<const double2*>(prs[e] + warp * CPWP)[c2 / 2];
+              prow[e][c2] = v.x;
+              prow[e][c2 + 1] = v.y;
+            }
+          const int cl = (c + 1) % CPW;   // column k+1: slot and owner warp
+          const int wl = (c + 1 < CPW) ? w0 : w0 + 1;
+          if (k + 1 < n && warp == wl) {
+            double t[2][RPL];
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+#pragma unroll
+              for (int r = 0; r < RPL; ++r) t[e][r] = fma(-m[e][r], prow[e][cl], a[e][r][cl]);
+            VB_PAIR_PUBLISH(t, k + 1, (k + 1) & 1);
+          }
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+#pragma unroll
+              for (int c2 = 0; c2 < CPW; ++c2) a[e][r][c2] = fma(-m[e][r], prow[e][c2], a[e][r][c2]);
+          if (warp == w0) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+#pragma unroll
+              for (int r = 0; r < RPL; ++r) a[e][r][c] = (lane + 32 * r == p[e]) ? 1.0 : -m[e][r];
+          }
+          __syncthreads();
+        }
+      }
+    }
+    // ---- scale rows by 1/piv, scatter B^{-1}[q(i)][p_m] = T[i][m] into Ib
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < n) {
+          const double s = rps[e][i];
+          const int qi = qs[e][i];
+#pragma unroll
+          for (int c = 0; c < CPW; ++c) {
+            const int m = warp * CPW + c;
+            if (m < n) {
+              const double v = a[e][r][c] * s;
+              if (!isfinite(v)) st_local[e] |= VB_STATUS_NONFINITE;
+              Ib[e][tr ? pivs[e][m] * ld + qi : qi * ld + pivs[e][m]] = v;
+            }
+          }
+        }
+      }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      // ---- Inv_j to global memory (natural order, padding columns 0)
+      double2* O = reinterpret_cast<double2*>(P.out[e] + (int64_t)j * blk);
+      const double2* S2 = reinterpret_cast<const double2*>(Ib[e]);
+      for (int q = threadIdx.x; q < blk / 2; q += blockDim.x) O[q] = S2[q];
+      // ---- forward sweep of the right-hand side: rhs[j+1] -= sub_d[j] o (Inv_j rhs[j])
+      if (with_rhs && j + 1 < nz) {
+        const double* vc = vecs[e] + (j & 1) * NPR;
+        double* vn = vecs[e] + ((j + 1) & 1) * NPR;
+        const double* rsj = rsb[e] + (j & 1) * 2 * NPR;
+        const int sub = lane & 3;   // four lanes per row, eight rows per warp per pass
+        for (int i0 = warp * 8; i0 < n; i0 += NW * 8) {
+          const int i = i0 + (lane >> 2);
+          double s0 = 0.0, s1 = 0.0;
+          if (i < n) {
+            int m = sub;
+            for (; m + 4 < n; m += 8) {
+              s0 = fma(Ib[e][i * ld + m], vc[m], s0);
+              s1 = fma(Ib[e][i * ld + m + 4], vc[m + 4], s1);
+            }
+            if (m < n) s0 = fma(Ib[e][i * ld + m], vc[m], s0);
+          }
+          double s = s0 + s1;
+          s += __shfl_xor_sync(FULL, s, 1);
+          s += __shfl_xor_sync(FULL, s, 2);
+          if (sub == 0 && i < n) {
+            const double v = rsj[i] - rsj[NPR + i] * s;
+            P.rhs[e][(int64_t)(j + 1) * n + i] = v;
+            vn[i] = v;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+    if (st_local[e]) atomicOr(P.status[e], st_local[e]);
+}
+#undef VB_PAIR_PUBLISH
+
+// Two atmospheres per CTA (2 blockIdx.x, 2 blockIdx.x + 1) of a uniform
+// batch; the inverses replace the blocks in the workspace.
+template <int RPL, int CPW, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
+gj_pair_kernel(Batch B, double* __restrict__ ws, int32_t* __restrict__ status, int with_rhs, int tr,
+               long long wlim) {
+  extern __shared__ __align__(16) char smem_raw[];
+  PairPtrs P;
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int b = 2 * blockIdx.x + e;
+    const Geo g = geo_of(B, b);
+    const WsView w = ws_view(ws, g, B.ni, B.ld);
+    P.Din[e] = w.inv;
+    P.out[e] = w.inv;
+    P.supn[e] = w.supn;
+    P.subn[e] = w.subn;
+    P.rhs[e] = with_rhs ? w.rmod : nullptr;
+    P.status[e] = status + b;
+  }
+  gj_factor_pair<RPL, CPW, NW>(B.nz, B.ni, B.ld, P, tr != 0, smem_raw, wlim);
+}
+
 // out == nullptr: the inverses replace the blocks in the workspace (FP64
 // path); otherwise they go to out (layer-major, ni x ld per layer) and the
 // FP64 blocks stay. only != nullptr: atmospheres with only[b] == 0 are skipped.
@@ -1447,8 +1903,10 @@ static cudaError_t launch_gj_t(const Batch& B, double* ws, int32_t* status, int 
 // Factor kernel of the process: 0 = blocked Gauss-Jordan with the trailing
 // updates on the FP64 tensor cores, 1 = scalar Gauss-Jordan with one block
 // barrier per pivot step, 2 = scalar Gauss-Jordan pipelined per column panel
-// (no block barrier per step). A network's tuning (factor_kernel 1..3 =
-// variant 0..2) overrides it.
+// (no block barrier per step), 3 = scalar Gauss-Jordan with two atmospheres'
+// chains interleaved per CTA (FP64 factor of uniform batches of 65-72
+// species; the scalar kernel elsewhere). A network's tuning (factor_kernel
+// 1..4 = variant 0..3) overrides it.
 static int g_factor_variant = 1;
 void set_factor_variant(int v) { g_factor_variant = v; }
 static int factor_choice(const Batch& B) { return B.factor_kernel ? B.factor_kernel - 1 : g_factor_variant; }
@@ -1513,7 +1971,7 @@ static cudaError_t launch_gj32(const Batch& B, double* ws, void* mxr, int32_t* s
 
 cudaError_t launch_factor32(const Batch& B, double* ws, void* mxr, int32_t* status32, cudaStream_t st) {
   const int v = factor_choice(B);
-  if (v == 1) return launch_gj32<false>(B, ws, mxr, status32, st);
+  if (v == 1 || v == 3) return launch_gj32<false>(B, ws, mxr, status32, st);
   if (v == 2) return launch_gj32<true>(B, ws, mxr, status32, st);
   if (B.ni <= 32) return launch_bgj32_t<4, 4, 4, true>(B, ws, mxr, status32, st);
   if (B.ni <= 64) return launch_bgj32_t<8, 8, 2, true>(B, ws, mxr, status32, st);
@@ -1559,6 +2017,25 @@ static cudaError_t launch_gj(const Batch& B, double* ws, int32_t* status, int wi
   return launch_gj_p<R, false>(B, ws, status, with_rhs, tr, st, out, only);
 }
 
+// Paired factor: the pairs of atmospheres (2b, 2b+1), then an odd last
+// atmosphere by the single kernel.
+static cudaError_t launch_gj_pair(const Batch& B, double* ws, int32_t* status, int with_rhs, int tr,
+                                  cudaStream_t st) {
+  const size_t sm = GJP<3, 6, 12>::smem_bytes(B.ni, B.ld);
+  cudaError_t e = cudaFuncSetAttribute(gj_pair_kernel<3, 6, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const int pairs = B.count / 2;
+  if (pairs > 0) gj_pair_kernel<3, 6, 12><<<pairs, 12 * 32, sm, st>>>(B, ws, status, with_rhs, tr, g_wait_limit);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || (B.count & 1) == 0) return e;
+  Batch B1 = B;
+  B1.count = 1;
+  const int64_t off = (int64_t)(B.count - 1) * B.nz * ws_per_layer(B.ni, B.ld);
+  return launch_gj_t<3, 6, 12, 1, true, double, false>(B1, ws + off, status + (B.count - 1), with_rhs, tr, st,
+                                                       nullptr, nullptr);
+}
+static bool pair_applies(const Batch& B) { return !B.zoff && B.ni > 64 && B.ni <= 72 && B.count >= 2; }
+
 cudaError_t launch_factor_only(const Batch& B, double* ws, const int32_t* only, int32_t* status, cudaStream_t st) {
   const int v = factor_choice(B);
   if (v == 0) return launch_bgj(B, ws, status, 0, 1, st, nullptr, only);
@@ -1570,6 +2047,7 @@ cudaError_t launch_factor(const Batch& B, double* ws, int32_t* status, int with_
   const int tr = for_transposed_solves ? 0 : 1;
   const int v = factor_choice(B);
   if (v == 0) return launch_bgj(B, ws, status, with_rhs, tr, st, nullptr, nullptr);
+  if (v == 3 && pair_applies(B)) return launch_gj_pair(B, ws, status, with_rhs, tr, st);
   return launch_gj<double>(B, ws, status, with_rhs, tr, st, nullptr, nullptr, v == 2);
 }
 

@@ -10,9 +10,10 @@ at = load_pkg("autotune")
 
 def test_candidates_cover_the_compiled_variants():
     c69 = list(at.candidates(69))
-    assert len(c69) == 24 and len(list(at.candidates(69, split=True))) == 48
+    assert len(c69) == 28 and len(list(at.candidates(69, split=True))) == 56
     assert {c["factor_ctas"] for c in c69} == {1, 2}
-    assert {c["factor_kernel"] for c in c69} == {1, 2, 3}
+    assert {c["factor_kernel"] for c in c69} == {1, 2, 3, 4}
+    assert all(c["factor_ctas"] == 1 for c in c69 if c["factor_kernel"] == 4)
     assert {c["sweep_stages"] for c in c69} == {2, 3}
     c30 = list(at.candidates(30))
     assert len(c30) == 12 and all(c["factor_ctas"] == 0 for c in c30)

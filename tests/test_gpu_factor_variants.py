@@ -28,7 +28,7 @@ solver = load_pkg("solver")
 syn = load_pkg("synthetic")
 
 
-@pytest.fixture(params=[0, 1, 2], ids=["blocked_dmma", "scalar_gj", "pipelined_gj"])
+@pytest.fixture(params=[0, 1, 2, 3], ids=["blocked_dmma", "scalar_gj", "pipelined_gj", "paired_gj"])
 def variant(request):
     _lib.check(_lib.lib().vb_set_factor_kernel(request.param), "vb_set_factor_kernel")
     yield request.param
@@ -124,3 +124,34 @@ def test_pipelined_equals_scalar_bit_for_bit(ni, n_fwd):
         _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
     assert int(out[2][2].abs().sum()) == 0
     assert torch.equal(out[1][0], out[2][0]) and torch.equal(out[1][1], out[2][1])
+
+
+@pytest.mark.parametrize("batch", [4, 5])
+def test_paired_equals_scalar_bit_for_bit(batch):
+    """Two atmospheres per CTA with their pivot chains interleaved perform
+    each atmosphere's operations in the scalar kernel's order, so the step
+    equals the scalar kernel's bit for bit (an odd batch: the last
+    atmosphere by the single kernel)."""
+    net = syn.make_network(169, 69, 700)
+    dn = chem.to_device(net.tables)
+    cases = [syn.make_case(seed=(700 + b,), net=net, nz=24, mild=True, k_range=(-40.0, 4.0), moldiff=True)
+             for b in range(batch)]
+    Y = torch.as_tensor(np.stack([c.y for c in cases]), device="cuda")
+    K = torch.as_tensor(np.stack([c.k for c in cases]), device="cuda")
+    A = {kk: (np.stack([c.atm[kk] for c in cases]) if not isinstance(cases[0].atm[kk], bool) else cases[0].atm[kk])
+         for kk in cases[0].atm}
+    dt = torch.as_tensor(np.array([1e-6, 1e-4, 1e-8, 1e-5, 1e-3][:batch]), device="cuda")
+    step = jstep.Ros2Step(dn, jstep.atm_from_dict(A), batch=batch)
+    out = {}
+    try:
+        for v in (1, 3):
+            _lib.check(_lib.lib().vb_set_factor_kernel(v), "vb_set_factor_kernel")
+            sol, delta, status = step(Y, K, dt)
+            torch.cuda.synchronize()
+            out[v] = (sol.clone(), delta.clone(), status.clone())
+    finally:
+        _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
+    assert int(out[3][2].abs().sum()) == 0
+    assert torch.equal(out[1][0], out[3][0]) and torch.equal(out[1][1], out[3][1])
+    sref, dref = orc.ros2_step(cases[0].y, cases[0].k, 1e-6, cases[0].atm, net.tables)
+    assert rel(out[3][0][0].cpu().numpy(), sref) <= 1e-10
