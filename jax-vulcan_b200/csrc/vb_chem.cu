@@ -191,6 +191,7 @@ __device__ inline void layer_jacobian(const NetDev& net, const double* coef, con
 }
 
 // Loads state rows j-1..j+1 (stage 2: yk2 = y + k1/r) and their gas sums.
+template <bool STAGE_GAS = false>
 __device__ inline void load_rows(const double* y, const double* k1, const double* gas, int nz, int ni,
                                  int j, double rinv_r, bool stage2, LayerSmem& L) {
   for (int t = threadIdx.x; t < 3 * (ni + 1); t += blockDim.x) {
@@ -207,12 +208,16 @@ __device__ inline void load_rows(const double* y, const double* k1, const double
     }
     L.y3[t] = v;
   }
+  // STAGE_GAS: the gas mask staged in diagd (free until the diffusion writes
+  // it), so the three sums below read shared memory
+  if (STAGE_GAS)
+    for (int i = threadIdx.x; i < ni; i += blockDim.x) L.diagd[i] = gas[i];
   __syncthreads();
   if (threadIdx.x < 3) {
     int w = threadIdx.x;
     int jj = j - 1 + w;
     double s = 0.0;
-    if (jj >= 0 && jj < nz) s = pairwise_sum_masked(L.y3 + w * (ni + 1), gas, ni);
+    if (jj >= 0 && jj < nz) s = pairwise_sum_masked(L.y3 + w * (ni + 1), STAGE_GAS ? L.diagd : gas, ni);
     L.scal[w] = s;
   }
   __syncthreads();
@@ -220,13 +225,29 @@ __device__ inline void load_rows(const double* y, const double* k1, const double
 
 // diff[i] (with BC fluxes) and the diagonal diffusion term diag_d[i] of row j;
 // also the sup/sub coefficients of row j when requested.
+// STAGED: the row's atmosphere fields are loaded in one round before the
+// arithmetic (RowAcc; faster where registers allow it: the stage-2 kernels).
+// again: a second call in the same kernel (waits until the first has read
+// eddy and lay).
+template <bool STAGED = false>
 __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, int flags, LayerSmem& L,
-                                       double* sup_out, double* sub_out, bool want_diag) {
+                                       double* sup_out, double* sub_out, bool want_diag, bool again = false) {
   double ysm = L.scal[0], ys0 = L.scal[1], ysp = L.scal[2];
-  __shared__ double eddy[3];
+  // the row's per-layer fields staged in one round of loads (the eddy and
+  // molecular terms then read them between their divisions from shared
+  // memory; each species' own fields are loaded together below)
+  __shared__ double eddy[3], lay[21];
+  if (again) __syncthreads();   // the previous call has finished reading eddy and lay
+  if (STAGED) {
+    stage_row_layers(a, nz, j, lay);
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     double A, B, C;
-    eddy_row(a, nz, j, ysm, ys0, ysp, A, B, C);
+    if (STAGED)
+      eddy_row_t<double>(RowAcc{lay, j - 1}, nz, j, ysm, ys0, ysp, A, B, C);
+    else
+      eddy_row(a, nz, j, ysm, ys0, ysp, A, B, C);
     eddy[0] = A; eddy[1] = B; eddy[2] = C;
   }
   __syncthreads();
@@ -237,7 +258,10 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
   const double* yp = L.y3 + 2 * (ni + 1);
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double Am, Bm, Cm;
-    mol_row(a, nz, ni, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
+    if (STAGED)
+      mol_row_t<double>(row_acc(a, lay, ni, j, i), nz, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
+    else
+      mol_row(a, nz, ni, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
     double At = eddy[0] + Am;
     double Bt = eddy[1] + Bm;
     double Ct = eddy[2] + Cm;
@@ -552,7 +576,7 @@ stage2_pair_kernel(NetDev net, Batch B, const double* __restrict__ y, const doub
     L.scal = scal + l;
     L.diff = diff + l * ni;
     L.diagd = nullptr;
-    layer_diffusion(a, nz, ni, j0 + l, flags, L, nullptr, nullptr, false);
+    layer_diffusion<true>(a, nz, ni, j0 + l, flags, L, nullptr, nullptr, false, l > 0);
   }
   {
     const double* kcol = k + g.z0 * R + j0;
@@ -622,7 +646,7 @@ stage1_pair_kernel(NetDev net, Batch B, const double* __restrict__ y, const doub
     L.scal = P.scal + l;
     L.diff = P.diff + l * ni;
     L.diagd = P.diagd + l * ni;
-    layer_diffusion(a, nz, ni, j0 + l, flags, L, P.supb + l * ni, P.subb + l * ni, true);
+    layer_diffusion(a, nz, ni, j0 + l, flags, L, P.supb + l * ni, P.subb + l * ni, true, l > 0);
   }
   rates_pair(net, P.y4 + (ni + 1), P.y4 + 2 * (ni + 1), k + g.z0 * (B.nr + 1) + j0, nz, two, a.M[j0],
              two ? a.M[j0 + 1] : 0.0, P.rate, P.drate);
@@ -698,8 +722,8 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
 
   __shared__ double coefs[MAX_COEF];
   load_coefs(net, coefs);   // visible after the barriers in load_rows
-  load_rows(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
-  layer_diffusion(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
+  load_rows<true>(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
+  layer_diffusion<true>(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
   __syncthreads();
   species_sums(net, coefs, L.rate, L.part);
@@ -755,7 +779,7 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
   LayerSmem L = carve(smem, ni, 0, 1, false);
   AtmRef a = atm_ref(atm + (int64_t)b * VB_ATM_DOUBLES(nz, ni), nz, ni);
   const double* yb = y + (int64_t)b * nz * ni;
-  load_rows(yb, nullptr, a.gas, nz, ni, j, 1.0, false, L);
+  load_rows<true>(yb, nullptr, a.gas, nz, ni, j, 1.0, false, L);
   __syncthreads();
   double* supo = sup_d ? sup_d + ((int64_t)b * (nz - 1) + j) * ni : nullptr;
   double* subo = sub_d ? sub_d + ((int64_t)b * (nz - 1) + (j - 1)) * ni : nullptr;

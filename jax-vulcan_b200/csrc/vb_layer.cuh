@@ -125,6 +125,58 @@ struct AtmPtrAcc {
   __device__ double alpha(int i) const { return a.alpha[i]; }
 };
 
+// The atmosphere fields stencil row j reads, staged before any arithmetic:
+// the per-layer fields of layers j-1, j, j+1 in shared memory (lay[f][s],
+// f = Kzz dzi vz Hpi Ti Tco g, s = layer - (j-1); stage_row_layers) and one
+// species' fields of layers j-1, j in registers. eddy_row_t and mol_row_t
+// read only those indices for row j (boundary rows included), so this
+// accessor returns the values AtmPtrAcc would, without their global-load
+// latency between the divisions.
+struct RowAcc {
+  const double* lay;
+  int j0;                                   // j - 1
+  double Dm, Dj, vmm, vmj, vsm, vsj, ms_, alpha_;
+  __device__ double Kzz(int m) const { return lay[0 * 3 + m - j0]; }
+  __device__ double dzi(int m) const { return lay[1 * 3 + m - j0]; }
+  __device__ double vz(int m) const { return lay[2 * 3 + m - j0]; }
+  __device__ double Hpi(int m) const { return lay[3 * 3 + m - j0]; }
+  __device__ double Ti(int m) const { return lay[4 * 3 + m - j0]; }
+  __device__ double Tco(int m) const { return lay[5 * 3 + m - j0]; }
+  __device__ double g(int m) const { return lay[6 * 3 + m - j0]; }
+  __device__ double Dzz(int m, int) const { return m == j0 ? Dm : Dj; }
+  __device__ double vm(int m, int) const { return m == j0 ? vmm : vmj; }
+  __device__ double vs(int m, int) const { return m == j0 ? vsm : vsj; }
+  __device__ double ms(int) const { return ms_; }
+  __device__ double alpha(int) const { return alpha_; }
+};
+
+// Fills lay[7][3] for row j (threads 0..20; layers outside [0, nz) read 0).
+__device__ inline void stage_row_layers(const AtmRef& a, int nz, int j, double* lay) {
+  if (threadIdx.x < 21) {
+    const int f = threadIdx.x / 3, m = j - 1 + (int)threadIdx.x % 3;
+    const double* src = f == 0 ? a.Kzz : f == 1 ? a.dzi : f == 2 ? a.vz : f == 3 ? a.Hpi : f == 4 ? a.Ti
+                      : f == 5 ? a.Tco : a.g;
+    lay[threadIdx.x] = (m >= 0 && m < nz) ? src[m] : 0.0;
+  }
+}
+
+// A species' fields of layers j-1 and j, loaded together.
+__device__ inline RowAcc row_acc(const AtmRef& a, const double* lay, int ni, int j, int i) {
+  RowAcc R;
+  R.lay = lay;
+  R.j0 = j - 1;
+  const int64_t cj = (int64_t)j * ni + i, cm = cj - ni;
+  R.Dj = a.Dzz[cj];
+  R.vmj = a.vm[cj];
+  R.vsj = a.vs[cj];
+  R.Dm = j > 0 ? a.Dzz[cm] : 0.0;
+  R.vmm = j > 0 ? a.vm[cm] : 0.0;
+  R.vsm = j > 0 ? a.vs[cm] : 0.0;
+  R.ms_ = a.ms[i];
+  R.alpha_ = a.alpha[i];
+  return R;
+}
+
 // Eddy coefficients of stencil row j (reference jax_step.py:167-193).
 template <typename T, typename Acc>
 __device__ inline void eddy_row_t(const Acc& a, int nz, int j, double ysm, double ys0, double ysp, T& A, T& Bc,
