@@ -225,11 +225,12 @@ __device__ inline void load_rows(const double* y, const double* k1, const double
 
 // diff[i] (with BC fluxes) and the diagonal diffusion term diag_d[i] of row j;
 // also the sup/sub coefficients of row j when requested.
-// STAGED: the row's atmosphere fields are loaded in one round before the
-// arithmetic (RowAcc; faster where registers allow it: the stage-2 kernels).
-// again: a second call in the same kernel (waits until the first has read
-// eddy and lay).
-template <bool STAGED = false>
+// STAGED 2: the row's atmosphere fields are loaded in one round before the
+// arithmetic (RowAcc: per-layer fields in shared memory, the species' own in
+// registers; faster in the stage-2 kernels, slower in stage 1, where the
+// extra live registers spill); 0: read where used. again: a second call in
+// the same kernel (waits until the first has read eddy and lay).
+template <int STAGED = 0>
 __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, int flags, LayerSmem& L,
                                        double* sup_out, double* sub_out, bool want_diag, bool again = false) {
   double ysm = L.scal[0], ys0 = L.scal[1], ysp = L.scal[2];
@@ -576,7 +577,7 @@ stage2_pair_kernel(NetDev net, Batch B, const double* __restrict__ y, const doub
     L.scal = scal + l;
     L.diff = diff + l * ni;
     L.diagd = nullptr;
-    layer_diffusion<true>(a, nz, ni, j0 + l, flags, L, nullptr, nullptr, false, l > 0);
+    layer_diffusion<2>(a, nz, ni, j0 + l, flags, L, nullptr, nullptr, false, l > 0);
   }
   {
     const double* kcol = k + g.z0 * R + j0;
@@ -723,7 +724,7 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   __shared__ double coefs[MAX_COEF];
   load_coefs(net, coefs);   // visible after the barriers in load_rows
   load_rows<true>(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
-  layer_diffusion<true>(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
+  layer_diffusion<2>(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
   __syncthreads();
   species_sums(net, coefs, L.rate, L.part);
