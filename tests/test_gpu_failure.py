@@ -98,3 +98,33 @@ def test_pipeline_wait_limit_gives_watchdog_status_and_recovers():
         _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
     assert (st2 == 0).all(), st2
     assert np.array_equal(sol, sol0) and np.array_equal(delta, delta0)
+
+
+def test_paired_factor_wait_limit_gives_watchdog_status_and_recovers():
+    """The two-atmospheres-per-CTA factor (69 species, an odd batch: one pair
+    and the last atmosphere by the single kernel) reports VB_STATUS_WATCHDOG
+    for every atmosphere when its bulk-copy waits give up at once, and the
+    next step equals the first bit for bit."""
+    net = syn.make_network(169, 69, 700)
+    cases = [syn.make_case(seed=800 + b, net=net, nz=12, mild=True, k_range=(-40.0, 4.0)) for b in range(3)]
+    Y = np.stack([c.y for c in cases])
+    K = np.stack([c.k for c in cases])
+    A = {kk: (np.stack([c.atm[kk] for c in cases]) if not isinstance(cases[0].atm[kk], bool)
+              else cases[0].atm[kk]) for kk in cases[0].atm}
+    step = jstep.Ros2Step(chem.to_device(net.tables), jstep.atm_from_dict(A))
+    DT = np.full(3, 1e-6)
+    try:
+        _lib.check(_lib.lib().vb_set_factor_kernel(3), "vb_set_factor_kernel")
+        sol0, delta0, st0 = _step(step, Y, K, DT)
+        assert (st0 == 0).all()
+        try:
+            jstep.set_wait_limit(0)
+            _, _, st = _step(step, Y, K, DT)
+        finally:
+            jstep.set_wait_limit(None)
+        assert (st & WATCHDOG).all(), st
+        sol, delta, st2 = _step(step, Y, K, DT)
+    finally:
+        _lib.check(_lib.lib().vb_set_factor_kernel(1), "vb_set_factor_kernel")
+    assert (st2 == 0).all(), st2
+    assert np.array_equal(sol, sol0) and np.array_equal(delta, delta0)
