@@ -963,7 +963,7 @@ def main():
             "status_ok": check["status_ok"],
             "max_rel_err_vs_oracle": check["max_rel_err_vs_oracle"],
             "correctness": dict(check, note="the specified stiff draw makes a single step ill-conditioned "
-                                            "(Schur block condition numbers far beyond 1/eps), so sol is judged "
+                                            "(Schur block condition numbers far beyond 1/eps), so sol is checked "
                                             "by the backward errors of its two block solves; elementwise errors "
                                             "are reported, not bounded"),
             "mixed_precision": {"well_conditioned": mixed_wc, "stiff": mixed_stiff,

@@ -5,7 +5,7 @@ a B200) from ``bench.make_batch``: ni=69, 700+700 reactions, nz=120,
 dt=1e-6 and the specified stiff draw (k log-uniform in [1e-40, 1e-8], mixing
 ratios down to 1e-20). On that draw a single step is ill-conditioned (Schur
 block condition numbers up to ~1e30 and beyond), so elementwise agreement with
-the oracle is not defined; the step is judged by its two block solves:
+the oracle is not defined; the step is checked through its two block solves:
 
 * every atmosphere: status word 0, sol and delta finite;
 * sampled atmospheres: the normwise backward error
