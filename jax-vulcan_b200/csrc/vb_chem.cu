@@ -225,6 +225,28 @@ __device__ inline void load_rows(const double* y, const double* k1, const double
 
 // diff[i] (with BC fluxes) and the diagonal diffusion term diag_d[i] of row j;
 // also the sup/sub coefficients of row j when requested.
+// Diffusion term of species i on row j from its combined coefficients and
+// state values y(j), y(j-1), y(j+1): the stencil and the boundary fluxes
+// (jax_step.py:223-246, _apply_diffusion_jax).
+__device__ inline double diffusion_term(const AtmRef& a, int nz, int j, int i, int flags, double At, double Bt,
+                                        double Ct, double y0, double ym, double yp) {
+  double d;
+  if (j == 0) {
+    d = At * y0 + Bt * yp;
+  } else if (j == nz - 1) {
+    d = At * y0 + Ct * ym;
+  } else {
+    d = At * y0 + Bt * yp + Ct * ym;
+  }
+  if (j == nz - 1) {
+    d = d + ((flags & VB_USE_TOPFLUX) ? a.top[i] / a.dzi[nz - 2] : 0.0);
+  }
+  if (j == 0) {
+    d = d + ((flags & VB_USE_BOTFLUX) ? (a.bot[i] - y0 * a.vdep[i]) / a.dzi[0] : 0.0);
+  }
+  return d;
+}
+
 // STAGED 2: the row's atmosphere fields are loaded in one round before the
 // arithmetic (RowAcc: per-layer fields in shared memory, the species' own in
 // registers; faster in the stage-2 kernels, slower in stage 1, where the
@@ -246,7 +268,7 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
   if (threadIdx.x == 0) {
     double A, B, C;
     if (STAGED)
-      eddy_row_t<double>(RowAcc{lay, j - 1}, nz, j, ysm, ys0, ysp, A, B, C);
+      eddy_row_t<double>(layer_acc(lay, j), nz, j, ysm, ys0, ysp, A, B, C);
     else
       eddy_row(a, nz, j, ysm, ys0, ysp, A, B, C);
     eddy[0] = A; eddy[1] = B; eddy[2] = C;
@@ -260,27 +282,14 @@ __device__ inline void layer_diffusion(const AtmRef& a, int nz, int ni, int j, i
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
     double Am, Bm, Cm;
     if (STAGED)
-      mol_row_t<double>(row_acc(a, lay, ni, j, i), nz, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
+      mol_row_t<double>(row_acc(a, lay, ni, j, i, j - 1, 3), nz, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm,
+                        Cm);
     else
       mol_row(a, nz, ni, j, i, ysm, ys0, ysp, use_vm, use_set, Am, Bm, Cm);
     double At = eddy[0] + Am;
     double Bt = eddy[1] + Bm;
     double Ct = eddy[2] + Cm;
-    double d;
-    if (j == 0) {
-      d = At * y0[i] + Bt * yp[i];
-    } else if (j == nz - 1) {
-      d = At * y0[i] + Ct * ym[i];
-    } else {
-      d = At * y0[i] + Bt * yp[i] + Ct * ym[i];
-    }
-    if (j == nz - 1) {
-      d = d + ((flags & VB_USE_TOPFLUX) ? a.top[i] / a.dzi[nz - 2] : 0.0);
-    }
-    if (j == 0) {
-      d = d + ((flags & VB_USE_BOTFLUX) ? (a.bot[i] - y0[i] * a.vdep[i]) / a.dzi[0] : 0.0);
-    }
-    L.diff[i] = d;
+    L.diff[i] = diffusion_term(a, nz, j, i, flags, At, Bt, Ct, y0[i], ym[i], yp[i]);
     if (want_diag) L.diagd[i] = At;
     if (sup_out && j < nz - 1) sup_out[i] = Bt;
     if (sub_out && j > 0) sub_out[i] = Ct;
@@ -311,11 +320,14 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   const double c0 = adj ? 0.0 : 1.0 / (r * dt[b]);
 
   __shared__ double coefs[MAX_COEF];
-  load_coefs(net, coefs);   // visible after the barriers in load_rows
-  load_rows(yb, nullptr, a.gas, nz, ni, j, r, false, L);
-  __shared__ double supb[VB_MAX_NI], subb[VB_MAX_NI];
-  layer_diffusion(a, nz, ni, j, flags, L, supb, subb, true);   // needs only the state rows
-  layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
+  load_coefs(net, coefs);
+  // state row j (the rates; padding slot 1.0) and diag_d of row j, written
+  // with the row's diffusion terms by diffusion_rows_kernel ahead of this kernel
+  double* yj = L.y3 + (ni + 1);
+  for (int t = threadIdx.x; t <= ni; t += blockDim.x) yj[t] = t < ni ? yb[(int64_t)j * ni + t] : 1.0;
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) L.diagd[i] = w.aux[(int64_t)j * ni + i];
+  __syncthreads();
+  layer_rates(net, yj, k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, L.drate, true);
   __syncthreads();
   // One phase for the species sums and the Jacobian gather: the first 2*ni
   // threads sum a species list, then join the gather on the light end of
@@ -335,11 +347,8 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
       }
       blk[(int64_t)row * ld + col] = v;
     });
-    for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    for (int i = threadIdx.x; i < ni; i += blockDim.x)
       w.rmod[(int64_t)j * ni + i] = adj_v[g.z0 * ni + (int64_t)j * ni + i];
-      if (j < nz - 1) w.supn[(int64_t)j * ni + i] = supb[i];
-      if (j > 0) w.subn[(int64_t)(j - 1) * ni + i] = subb[i];
-    }
     return;
   }
   layer_jacobian_each(net, coefs, L.drate, [&](int row, int col, double J) {
@@ -355,20 +364,10 @@ stage1_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   }, min(2 * ni, (int)blockDim.x));
   __syncthreads();   // the species sums
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
-    double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
-    bool fixed = fm && fm[i];
-    if (fixed) v = 0.0;
+    // rmod[j] holds the row's diffusion term (diffusion_rows_kernel)
+    double v = (L.part[2 * i + 1] - L.part[2 * i]) + w.rmod[(int64_t)j * ni + i];
+    if (fm && fm[i]) v = 0.0;
     w.rmod[(int64_t)j * ni + i] = v;
-    if (j < nz - 1) {
-      double s2 = -supb[i];
-      if (fixed) s2 = 0.0;
-      w.supn[(int64_t)j * ni + i] = s2;
-    }
-    if (j > 0) {
-      double s2 = -subb[i];
-      if (fixed) s2 = 0.0;
-      w.subn[(int64_t)(j - 1) * ni + i] = s2;
-    }
   }
 }
 
@@ -723,6 +722,9 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
 
   __shared__ double coefs[MAX_COEF];
   load_coefs(net, coefs);   // visible after the barriers in load_rows
+  // the diffusion stays in this kernel (staged loads): as a separate kernel
+  // ahead of it, stage 2 measured slower (1.43 against 1.27 ms at 296
+  // atmospheres), unlike stage 1
   load_rows<true>(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
   layer_diffusion<2>(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
   layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
@@ -796,6 +798,106 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
   }
 }
 
+// ---------------------------------------------------------------- diffusion rows ahead of the stages
+// The eddy + molecular diffusion of every layer (the same functions on the
+// same inputs as layer_diffusion, so the same bits), computed ahead of the
+// stage-1 kernel, whose heavy per-layer CTAs then load one state row and no
+// atmosphere fields. One CTA per block of DIFF_LAYERS consecutive layers of
+// one atmosphere: the block's state rows, their gas sums, per-layer fields
+// and eddy coefficients are formed once, then every (layer, species) item of
+// the block runs in parallel.
+//   mode 0 (stage 1):  rmod[j] = diff, aux[j] = diag_d, supn[j] = -sup_d,
+//                      subn[j-1] = -sub_d (0 on fixed species);
+//   mode 1 (stage 1 of the adjoint): aux[j] = diag_d, supn[j] = sup_d,
+//                      subn[j-1] = sub_d (steady_state_grad.py:153-175).
+// (Stage 2 keeps its diffusion inside: there a separate kernel was slower.)
+constexpr int DIFF_THREADS = 256;
+constexpr int DIFF_LAYERS = 8;
+__host__ __device__ inline size_t diff_block_smem_bytes(int ni) {
+  constexpr int NR = DIFF_LAYERS + 2;
+  return ((size_t)NR * (ni + 1) + ni + NR + 7 * NR + 3 * DIFF_LAYERS) * sizeof(double);
+}
+
+__global__ void __launch_bounds__(DIFF_THREADS)
+diffusion_rows_kernel(Batch B, const double* __restrict__ y, const double* __restrict__ atm, int flags,
+                      const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, int mode) {
+  extern __shared__ double smem[];
+  constexpr int LB = DIFF_LAYERS, NR = LB + 2;
+  const int b = blockIdx.y, jb = blockIdx.x * LB;
+  Geo g = geo_of(B, b);
+  if (jb >= g.nz) return;
+  const int ni = B.ni, nz = g.nz, rs = ni + 1;
+  double* ys = smem;               // [NR][ni+1]: rows jb-1 .. jb+LB (0 outside [0, nz); padding 1.0)
+  double* gas = ys + NR * rs;      // [ni]
+  double* scal = gas + ni;         // [NR]: gas sums of those rows
+  double* lay = scal + NR;         // [7][NR]: Kzz dzi vz Hpi Ti Tco g of those layers
+  double* edd = lay + 7 * NR;      // [LB][3]: eddy A, B, C of the block's layers
+  const AtmRef a = atm_ref(atm + g.atm, nz, ni);
+  const WsView w = ws_view(ws, g, ni, B.ld);
+  const double* yb = y + g.z0 * ni;
+  for (int t = threadIdx.x; t < NR * rs; t += blockDim.x) {
+    const int rr = t / rs, i = t % rs, jj = jb - 1 + rr;
+    double v = 1.0;
+    if (i < ni) v = (jj >= 0 && jj < nz) ? yb[(int64_t)jj * ni + i] : 0.0;
+    ys[t] = v;
+  }
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) gas[i] = a.gas[i];
+  for (int t = threadIdx.x; t < 7 * NR; t += blockDim.x) {
+    const int f = t / NR, m = jb - 1 + t % NR;
+    const double* src = f == 0 ? a.Kzz : f == 1 ? a.dzi : f == 2 ? a.vz : f == 3 ? a.Hpi : f == 4 ? a.Ti
+                      : f == 5 ? a.Tco : a.g;
+    lay[t] = (m >= 0 && m < nz) ? src[m] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < NR) {
+    const int jj = jb - 1 + (int)threadIdx.x;
+    scal[threadIdx.x] = (jj >= 0 && jj < nz) ? pairwise_sum_masked(ys + threadIdx.x * rs, gas, ni) : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < LB) {
+    const int l = threadIdx.x, j = jb + l;
+    if (j < nz) {
+      RowAcc E{};
+      E.lay = lay;
+      E.j0 = j - 1;
+      E.base = jb - 1;
+      E.S = NR;
+      double A, Bc, C;
+      eddy_row_t<double>(E, nz, j, scal[l], scal[l + 1], scal[l + 2], A, Bc, C);
+      edd[3 * l] = A;
+      edd[3 * l + 1] = Bc;
+      edd[3 * l + 2] = C;
+    }
+  }
+  __syncthreads();
+  const double use_vm = (flags & VB_USE_VM_MOL) ? 1.0 : 0.0;
+  const double use_set = (flags & VB_USE_SETTLING) ? 1.0 : 0.0;
+  for (int q = threadIdx.x; q < LB * ni; q += blockDim.x) {
+    const int l = q / ni, i = q % ni, j = jb + l;
+    if (j >= nz) continue;
+    double Am, Bm, Cm;
+    mol_row_t<double>(row_acc(a, lay, ni, j, i, jb - 1, NR), nz, j, i, scal[l], scal[l + 1], scal[l + 2], use_vm,
+                      use_set, Am, Bm, Cm);
+    const double At = edd[3 * l] + Am;
+    const double Bt = edd[3 * l + 1] + Bm;
+    const double Ct = edd[3 * l + 2] + Cm;
+    const double d = diffusion_term(a, nz, j, i, flags, At, Bt, Ct, ys[(l + 1) * rs + i], ys[l * rs + i],
+                                    ys[(l + 2) * rs + i]);
+    if (mode == 0) w.rmod[(int64_t)j * ni + i] = d;
+    w.aux[(int64_t)j * ni + i] = At;
+    const bool fixed = mode == 0 && fix_mask && fix_mask[g.z0 * ni + (int64_t)j * ni + i];
+    if (j < nz - 1) w.supn[(int64_t)j * ni + i] = mode == 1 ? Bt : (fixed ? 0.0 : -Bt);
+    if (j > 0) w.subn[(int64_t)(j - 1) * ni + i] = mode == 1 ? Ct : (fixed ? 0.0 : -Ct);
+  }
+}
+
+static cudaError_t launch_diffusion_rows(const Batch& B, const double* y, const double* atm, int flags,
+                                         const uint8_t* fm, double* ws, int mode, cudaStream_t st) {
+  dim3 grid((B.nz + DIFF_LAYERS - 1) / DIFF_LAYERS, B.count);
+  diffusion_rows_kernel<<<grid, DIFF_THREADS, diff_block_smem_bytes(B.ni), st>>>(B, y, atm, flags, fm, ws, mode);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- launchers
 // Stage-1 / stage-2 kernels of the Ros2 step (VbTuning.stage1_layers): one
 // layer per CTA by default (measured on B200 at 296 config-0 atmospheres, the
@@ -815,6 +917,8 @@ cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, co
     stage1_pair_kernel<<<grid, PAIR_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
     return cudaGetLastError();
   }
+  cudaError_t e = launch_diffusion_rows(B, y, atm, flags, fm, ws, adj_v ? 1 : 0, st);
+  if (e != cudaSuccess) return e;
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, true);
   cudaFuncSetAttribute(stage1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(B.nz, B.count);

@@ -136,13 +136,15 @@ struct RowAcc {
   const double* lay;
   int j0;                                   // j - 1
   double Dm, Dj, vmm, vmj, vsm, vsj, ms_, alpha_;
-  __device__ double Kzz(int m) const { return lay[0 * 3 + m - j0]; }
-  __device__ double dzi(int m) const { return lay[1 * 3 + m - j0]; }
-  __device__ double vz(int m) const { return lay[2 * 3 + m - j0]; }
-  __device__ double Hpi(int m) const { return lay[3 * 3 + m - j0]; }
-  __device__ double Ti(int m) const { return lay[4 * 3 + m - j0]; }
-  __device__ double Tco(int m) const { return lay[5 * 3 + m - j0]; }
-  __device__ double g(int m) const { return lay[6 * 3 + m - j0]; }
+  int base, S;                              // lay[f * S + m - base]: the staged layers base.. of field f
+  __device__ int at(int f, int m) const { return f * S + m - base; }
+  __device__ double Kzz(int m) const { return lay[at(0, m)]; }
+  __device__ double dzi(int m) const { return lay[at(1, m)]; }
+  __device__ double vz(int m) const { return lay[at(2, m)]; }
+  __device__ double Hpi(int m) const { return lay[at(3, m)]; }
+  __device__ double Ti(int m) const { return lay[at(4, m)]; }
+  __device__ double Tco(int m) const { return lay[at(5, m)]; }
+  __device__ double g(int m) const { return lay[at(6, m)]; }
   __device__ double Dzz(int m, int) const { return m == j0 ? Dm : Dj; }
   __device__ double vm(int m, int) const { return m == j0 ? vmm : vmj; }
   __device__ double vs(int m, int) const { return m == j0 ? vsm : vsj; }
@@ -160,11 +162,24 @@ __device__ inline void stage_row_layers(const AtmRef& a, int nz, int j, double* 
   }
 }
 
-// A species' fields of layers j-1 and j, loaded together.
-__device__ inline RowAcc row_acc(const AtmRef& a, const double* lay, int ni, int j, int i) {
+// The staged per-layer fields only (lay[f][3] of row j; the eddy terms).
+__device__ inline RowAcc layer_acc(const double* lay, int j) {
+  RowAcc R{};
+  R.lay = lay;
+  R.j0 = j - 1;
+  R.base = j - 1;
+  R.S = 3;
+  return R;
+}
+
+// A species' fields of layers j-1 and j, loaded together (lay: per-layer
+// fields staged with f-stride S from layer base; a row's own stage: j-1, 3).
+__device__ inline RowAcc row_acc(const AtmRef& a, const double* lay, int ni, int j, int i, int base, int S) {
   RowAcc R;
   R.lay = lay;
   R.j0 = j - 1;
+  R.base = base;
+  R.S = S;
   const int64_t cj = (int64_t)j * ni + i, cm = cj - ni;
   R.Dj = a.Dzz[cj];
   R.vmj = a.vm[cj];
