@@ -721,18 +721,26 @@ stage2_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* _
   const double dtb = res ? 1.0 : dt[b];
 
   __shared__ double coefs[MAX_COEF];
-  load_coefs(net, coefs);   // visible after the barriers in load_rows
-  // the diffusion stays in this kernel (staged loads): as a separate kernel
-  // ahead of it, stage 2 measured slower (1.43 against 1.27 ms at 296
-  // atmospheres), unlike stage 1
-  load_rows<true>(yb, res ? nullptr : w.k1, a.gas, nz, ni, j, r, !res, L);
-  layer_diffusion<2>(a, nz, ni, j, flags, L, nullptr, nullptr, false);   // needs only the state rows
-  layer_rates(net, L.y3 + (ni + 1), k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
+  load_coefs(net, coefs);
+  // state row j (yk2 = y + k1/r, load_rows' expression; padding slot 1.0)
+  double* yj = L.y3 + (ni + 1);
+  for (int t = threadIdx.x; t <= ni; t += blockDim.x) {
+    double v = 1.0;
+    if (t < ni) {
+      v = yb[(int64_t)j * ni + t];
+      if (!res) v = v + w.k1[(int64_t)j * ni + t] / r;
+    }
+    yj[t] = v;
+  }
+  __syncthreads();
+  layer_rates(net, yj, k + g.z0 * (B.nr + 1) + j, nz, a.M[j], L.rate, nullptr, false);
   __syncthreads();
   species_sums(net, coefs, L.rate, L.part);
   __syncthreads();
+  // rmod[j] (resid[j]) holds the row's diffusion term (diffusion_rows_kernel)
+  const double* dif = res ? resid + g.z0 * ni : w.rmod;
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
-    double v = (L.part[2 * i + 1] - L.part[2 * i]) + L.diff[i];
+    double v = (L.part[2 * i + 1] - L.part[2 * i]) + dif[(int64_t)j * ni + i];
     if (res) {
       resid[g.z0 * ni + (int64_t)j * ni + i] = v;
       continue;
@@ -801,7 +809,7 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
 // ---------------------------------------------------------------- diffusion rows ahead of the stages
 // The eddy + molecular diffusion of every layer (the same functions on the
 // same inputs as layer_diffusion, so the same bits), computed ahead of the
-// stage-1 kernel, whose heavy per-layer CTAs then load one state row and no
+// stage kernels, whose heavy per-layer CTAs then load one state row and no
 // atmosphere fields. One CTA per block of DIFF_LAYERS consecutive layers of
 // one atmosphere: the block's state rows, their gas sums, per-layer fields
 // and eddy coefficients are formed once, then every (layer, species) item of
@@ -809,8 +817,9 @@ diffusion_kernel(int nz, int ni, const double* __restrict__ y, const double* __r
 //   mode 0 (stage 1):  rmod[j] = diff, aux[j] = diag_d, supn[j] = -sup_d,
 //                      subn[j-1] = -sub_d (0 on fixed species);
 //   mode 1 (stage 1 of the adjoint): aux[j] = diag_d, supn[j] = sup_d,
-//                      subn[j-1] = sub_d (steady_state_grad.py:153-175).
-// (Stage 2 keeps its diffusion inside: there a separate kernel was slower.)
+//                      subn[j-1] = sub_d (steady_state_grad.py:153-175);
+//   mode 2 (stage 2):  rmod[j] = diff at yk2 = y + k1/r (with resid: resid[j]
+//                      = diff at y, the residual; ws unused).
 constexpr int DIFF_THREADS = 256;
 constexpr int DIFF_LAYERS = 8;
 __host__ __device__ inline size_t diff_block_smem_bytes(int ni) {
@@ -820,7 +829,8 @@ __host__ __device__ inline size_t diff_block_smem_bytes(int ni) {
 
 __global__ void __launch_bounds__(DIFF_THREADS)
 diffusion_rows_kernel(Batch B, const double* __restrict__ y, const double* __restrict__ atm, int flags,
-                      const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, int mode) {
+                      const uint8_t* __restrict__ fix_mask, double* __restrict__ ws, double* __restrict__ resid,
+                      int mode) {
   extern __shared__ double smem[];
   constexpr int LB = DIFF_LAYERS, NR = LB + 2;
   const int b = blockIdx.y, jb = blockIdx.x * LB;
@@ -835,10 +845,19 @@ diffusion_rows_kernel(Batch B, const double* __restrict__ y, const double* __res
   const AtmRef a = atm_ref(atm + g.atm, nz, ni);
   const WsView w = ws_view(ws, g, ni, B.ld);
   const double* yb = y + g.z0 * ni;
+  const bool yk2 = mode == 2 && !resid;   // stage 2: rows of yk2 = y + k1/r (load_rows' expression)
+  const double r = ros2_r();
   for (int t = threadIdx.x; t < NR * rs; t += blockDim.x) {
     const int rr = t / rs, i = t % rs, jj = jb - 1 + rr;
     double v = 1.0;
-    if (i < ni) v = (jj >= 0 && jj < nz) ? yb[(int64_t)jj * ni + i] : 0.0;
+    if (i < ni) {
+      if (jj >= 0 && jj < nz) {
+        v = yb[(int64_t)jj * ni + i];
+        if (yk2) v = v + w.k1[(int64_t)jj * ni + i] / r;
+      } else {
+        v = 0.0;
+      }
+    }
     ys[t] = v;
   }
   for (int i = threadIdx.x; i < ni; i += blockDim.x) gas[i] = a.gas[i];
@@ -883,6 +902,10 @@ diffusion_rows_kernel(Batch B, const double* __restrict__ y, const double* __res
     const double Ct = edd[3 * l + 2] + Cm;
     const double d = diffusion_term(a, nz, j, i, flags, At, Bt, Ct, ys[(l + 1) * rs + i], ys[l * rs + i],
                                     ys[(l + 2) * rs + i]);
+    if (mode == 2) {
+      (resid ? resid + g.z0 * ni : w.rmod)[(int64_t)j * ni + i] = d;
+      continue;
+    }
     if (mode == 0) w.rmod[(int64_t)j * ni + i] = d;
     w.aux[(int64_t)j * ni + i] = At;
     const bool fixed = mode == 0 && fix_mask && fix_mask[g.z0 * ni + (int64_t)j * ni + i];
@@ -892,9 +915,10 @@ diffusion_rows_kernel(Batch B, const double* __restrict__ y, const double* __res
 }
 
 static cudaError_t launch_diffusion_rows(const Batch& B, const double* y, const double* atm, int flags,
-                                         const uint8_t* fm, double* ws, int mode, cudaStream_t st) {
+                                         const uint8_t* fm, double* ws, double* resid, int mode, cudaStream_t st) {
   dim3 grid((B.nz + DIFF_LAYERS - 1) / DIFF_LAYERS, B.count);
-  diffusion_rows_kernel<<<grid, DIFF_THREADS, diff_block_smem_bytes(B.ni), st>>>(B, y, atm, flags, fm, ws, mode);
+  diffusion_rows_kernel<<<grid, DIFF_THREADS, diff_block_smem_bytes(B.ni), st>>>(B, y, atm, flags, fm, ws, resid,
+                                                                                 mode);
   return cudaGetLastError();
 }
 
@@ -917,7 +941,7 @@ cudaError_t launch_stage1(const NetDev& net, const Batch& B, const double* y, co
     stage1_pair_kernel<<<grid, PAIR_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
     return cudaGetLastError();
   }
-  cudaError_t e = launch_diffusion_rows(B, y, atm, flags, fm, ws, adj_v ? 1 : 0, st);
+  cudaError_t e = launch_diffusion_rows(B, y, atm, flags, fm, ws, nullptr, adj_v ? 1 : 0, st);
   if (e != cudaSuccess) return e;
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, true);
   cudaFuncSetAttribute(stage1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -938,6 +962,8 @@ cudaError_t launch_stage2(const NetDev& net, const Batch& B, const double* y, co
     stage2_pair_kernel<<<grid, PAIR_THREADS, sm, st>>>(net, B, y, k, dt, atm, flags, fm, ws);
     return cudaGetLastError();
   }
+  cudaError_t e = launch_diffusion_rows(B, y, atm, flags, fm, ws, resid, 2, st);
+  if (e != cudaSuccess) return e;
   size_t sm = layer_smem_bytes(B.ni, B.nr, net.T, false);
   cudaFuncSetAttribute(stage2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 grid(B.nz, B.count);
