@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -52,17 +53,21 @@ def build(verbose=False, force=False, ptxas_v=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
     headers.append(os.path.join(INCLUDE, "vulcan_b200.h"))
-    objs = []
+    objs, cmds = [], []
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [src] + headers + [__file__]):
-            cmd = [nvcc()] + ARCH + COMMON + extra + (["-Xptxas", "-v"] if ptxas_v else []) + \
-                ["-c", src, "-o", obj]
+            cmds.append([nvcc()] + ARCH + COMMON + extra + (["-Xptxas", "-v"] if ptxas_v else []) +
+                        ["-c", src, "-o", obj])
+    # the units compile independently: one nvcc process per unit, in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for cmd in cmds:
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
         if verbose:
