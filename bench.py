@@ -310,7 +310,7 @@ def run_config2(args, torch):
                                    f"ni in {{30, 69, 89}} (370/1400/2000 reactions), one CUDA-graph replay",
                        "groups": len(batch.groups), "l2": "inputs larger than L2, no flush"},
             "sequential_single_instance": {"value": n / (seq_ms * 1e-3), "unit": UNIT, "ms_per_pass": seq_ms},
-            "speedup_vs_sequential": seq_ms / ms, "gpu_launches": 8 * len(batch.groups) * args.steps,
+            "speedup_vs_sequential": seq_ms / ms, "gpu_launches": 9 * len(batch.groups) * args.steps,
             "tuning": {k: {"tuning": v["tuning"], "ms": v["ms"], "candidates_ms": v["candidates"]}
                        for k, v in batch.tuned.items()},
             "clocks": clk}
@@ -939,7 +939,9 @@ def main():
                             "on two copy streams with double-buffered device arrays (step i's inputs go up and "
                             "step i-1's results come down while the steps compute); rates and atmosphere stay "
                             "resident (as in the reference runner's device carry)"},
-            "gpu_launches": (16 if tuned.get("streams") == 2 else 8) * args.steps,
+            # per step: diffusion rows, stage 1, factor, back sweep, diffusion rows,
+            # stage-2 rates, stage-2 sums, forward sweep, back sweep (twice with two streams)
+            "gpu_launches": (18 if tuned.get("streams") == 2 else 9) * args.steps,
             "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan inverse with partial pivoting of "
                                                     "each layer block, serial in z, one CTA per atmosphere)",
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
@@ -969,11 +971,11 @@ def main():
             "mixed_precision": {"well_conditioned": mixed_wc, "stiff": mixed_stiff,
                                 "vs_single_instance_fp64_well_conditioned":
                                     mixed_wc["value"] * single_ms * 1e-3,
-                                "note": "vb_ros2_step_mixed: FP64 assembly, row-equilibrated FP32 blocked "
-                                        "Gauss-Jordan factor with TF32 tensor-core trailing updates (head/tail "
-                                        "split, three products), FP64-residual refinement of both stages "
-                                        "(<= 3 passes, tol 1e-12), FP64 refactor fallback; errors against the "
-                                        "oracle on atmospheres 0 and B-1"},
+                                "note": "vb_ros2_step_mixed: FP64 assembly, row-equilibrated FP32 "
+                                        "Gauss-Jordan factor (the tuned factor kernel's FP32 instance: "
+                                        f"factor_kernel {tuned.get('factor_kernel')}), FP64-residual "
+                                        "refinement of both stages (<= 3 passes, tol 1e-12), FP64 refactor "
+                                        "fallback; errors against the oracle on atmospheres 0 and B-1"},
             "well_conditioned": {"value": job_value(world, B, wc_ms), "unit": UNIT, "ms_per_step": wc_ms,
                                  "data": "same shapes, order-scaled rate constants (pseudo-first-order rates "
                                          "log-uniform in [1e-40, 1e4] s^-1)",

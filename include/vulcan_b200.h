@@ -110,6 +110,15 @@ size_t vb_net_device_bytes(const VbNet* net);
  * status[B]. zoff: NULL for a uniform batch of `nz` layers, else device int64
  * [B+1] prefix sums (then nz is the maximum layer count). */
 size_t vb_ros2_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host);
+/* Optional extra workspace of vb_ros2_step (no reference counterpart): with
+ * workspace_bytes >= the 256-byte-aligned vb_ros2_workspace_bytes(batch, nz,
+ * ni, NULL) + vb_ros2_assembly_bytes(net, batch, nz) (nz: the maximum layer
+ * count of a ragged batch), the step assembles the stage-2 right-hand side
+ * with one thread per layer (the rate of every reaction and layer staged in
+ * that region, then every species sum formed from coalesced rows of layers)
+ * instead of one CTA per layer; the results are identical. nr+1 doubles per
+ * layer. */
+size_t vb_ros2_assembly_bytes(const VbNet* net, int batch, int nz);
 int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff,
                  const double* y, const double* k, const double* dt,
                  const double* atm, int32_t atm_flags, const uint8_t* fix_mask,

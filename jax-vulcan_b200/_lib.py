@@ -35,6 +35,7 @@ SIGNATURES = {
     "vb_net_set_tuning": (_i, [_p, _p]),
     "vb_net_get_tuning": (_i, [_p, _p]),
     "vb_ros2_workspace_bytes": (_sz, [_i, _i, _i, _p]),
+    "vb_ros2_assembly_bytes": (_sz, [_p, _i, _i]),
     "vb_ros2_step": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _i32, _p, _p, _p, _p, _p, _sz, _p]),
     "vb_ros2_stages": (_i, [_p, _i, _i, _p, _p, _p, _p, _p]),
     "vb_ros2_mixed_workspace_bytes": (_sz, [_i, _i, _i, _p]),

@@ -219,6 +219,16 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
       sdesc[2 * t + 1] = (uint32_t)n;
     }
   }
+  // species lists in natural order (t = 2 i loss, 2 i + 1 production)
+  std::vector<int32_t> snp(2 * (size_t)ni + 1, 0);
+  std::vector<uint32_t> snw;
+  for (int t = 0; t < 2 * ni; ++t) {
+    const std::vector<int32_t>& ptr = (t & 1) ? pp : lp;
+    const std::vector<uint32_t>& w = (t & 1) ? pw : lw;
+    for (int32_t e = ptr[t / 2]; e < ptr[t / 2 + 1]; ++e) snw.push_back(w[e]);
+    snp[t + 1] = (int32_t)snw.size();
+  }
+  if (snw.empty()) snw.push_back(0u);
   std::vector<int32_t> ri(R * T), pi(R * T);
   for (int e = 0; e < R * T; ++e) { ri[e] = (int32_t)r_idx[e]; pi[e] = (int32_t)p_idx[e]; }
 
@@ -230,7 +240,7 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
       {three, (size_t)R, 0},         {sdesc.data(), sdesc.size() * 4, 0},
       {swi.data(), swi.size() * 4, 0}, {jp.data(), jp.size() * 4, 0},
       {jwi.data(), jwi.size() * 4, 0}, {coefs.data(), coefs.size() * 8, 0},
-      {order.data(), order.size() * 4, 0}};
+      {order.data(), order.size() * 4, 0}, {snp.data(), snp.size() * 4, 0}, {snw.data(), snw.size() * 4, 0}};
   size_t total = 0;
   for (auto& p : parts) { p.off = total; total += (p.bytes + 255) & ~(size_t)255; }
   void* base = nullptr;
@@ -257,6 +267,8 @@ int vb_net_create(int ni, int nr, int T, const int64_t* r_idx, const int64_t* p_
   d.coef_tab = (const double*)(b + parts[9].off);
   d.n_coef = (int)coefs.size();
   d.jac_desc = (const uint2*)(b + parts[10].off);
+  d.sum_nptr = (const int32_t*)(b + parts[11].off);
+  d.sum_nw = (const uint32_t*)(b + parts[12].off);
   net->base = base;
   net->bytes = total;
   *out = net;
@@ -311,6 +323,21 @@ static vb::Batch make_batch(const VbNet* net, int batch, int nz, const int64_t* 
 }
 
 // The launch sequence of one Ros2 step (jax_step.py:249-315) on one stream.
+size_t vb_ros2_assembly_bytes(const VbNet* net, int batch, int nz) {
+  if (!net || batch < 1 || nz < 1) return 0;
+  return (size_t)batch * nz * vb::rates_region_doubles(net->dev.nr) * sizeof(double);
+}
+
+// The rate region of the layer-vectorized stage 2 in a vb_ros2_step
+// workspace (after the step's own bytes, on a 256-byte boundary), or nullptr
+// when the workspace does not hold it (the per-layer stage-2 kernel runs then).
+static double* assembly_region(const VbNet* net, int batch, int nz, void* ws, size_t ws_bytes) {
+  const size_t off = (vb_ros2_workspace_bytes(batch, nz, net->dev.ni, nullptr) + 255) & ~(size_t)255;
+  const size_t need = vb_ros2_assembly_bytes(net, batch, nz);
+  if (ws_bytes < off || ws_bytes - off < need) return nullptr;
+  return reinterpret_cast<double*>(static_cast<char*>(ws) + off);
+}
+
 static int ros2_sequence(const VbNet* net, const vb::Batch& B, const double* y, const double* k, const double* dt,
                          const double* atm, int32_t flags, const uint8_t* fix_mask, double* sol, double* delta,
                          int32_t* status, double* ws, cudaStream_t st) {
@@ -385,10 +412,13 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const
     return fail(VB_ERR_ARG, "workspace too small");
   cudaStream_t st = (cudaStream_t)stream;
   double* ws = (double*)workspace;
+  double* rates = assembly_region(net, batch, nz, workspace, ws_bytes);
   VB_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t) * batch, st), "status reset");
-  if (net->tune.streams != 2 || zoff || batch < 2)
-    return ros2_sequence(net, make_batch(net, batch, nz, zoff), y, k, dt, atm, flags, fix_mask, sol, delta, status,
-                         ws, st);
+  if (net->tune.streams != 2 || zoff || batch < 2) {
+    vb::Batch B = make_batch(net, batch, nz, zoff);
+    B.rates = rates;
+    return ros2_sequence(net, B, y, k, dt, atm, flags, fix_mask, sol, delta, status, ws, st);
+  }
   // two halves of a uniform batch, one per stream: the assembly of one half
   // overlaps the factor of the other (they bind different units of the SM)
   SideStream* side = nullptr;
@@ -397,10 +427,13 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff, const
   const int64_t e = (int64_t)h * nz * ni;
   VB_CHECK(cudaEventRecord(side->fork, st), "fork");
   VB_CHECK(cudaStreamWaitEvent(side->s, side->fork, 0), "fork wait");
-  if (int rc = ros2_sequence(net, make_batch(net, h, nz, nullptr), y, k, dt, atm, flags, fix_mask, sol, delta, status,
-                             ws, st))
-    return rc;
-  if (int rc = ros2_sequence(net, make_batch(net, batch - h, nz, nullptr), y + e, k + (int64_t)h * (nr + 1) * nz,
+  vb::Batch B1 = make_batch(net, h, nz, nullptr), B2 = make_batch(net, batch - h, nz, nullptr);
+  if (rates) {
+    B1.rates = rates;
+    B2.rates = rates + (int64_t)h * nz * vb::rates_region_doubles(nr);
+  }
+  if (int rc = ros2_sequence(net, B1, y, k, dt, atm, flags, fix_mask, sol, delta, status, ws, st)) return rc;
+  if (int rc = ros2_sequence(net, B2, y + e, k + (int64_t)h * (nr + 1) * nz,
                              dt + h, atm + (int64_t)h * VB_ATM_DOUBLES(nz, ni), flags, fix_mask ? fix_mask + e : nullptr,
                              sol + e, delta + e, status + h,
                              ws + (int64_t)h * nz * vb::ws_per_layer(ni, vb::round_even(ni)), side->s))

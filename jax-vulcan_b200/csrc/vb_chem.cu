@@ -9,6 +9,8 @@
 // bit-identical to the reference's.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "vb_common.cuh"
 #include "vb_launch.cuh"
 #include "vb_layer.cuh"
@@ -46,26 +48,21 @@ __device__ inline LayerSmem carve(double* s, int ni, int nr, int T, bool jac, bo
   return L;
 }
 
-// Rate (and drate) of reaction slot r with TT terms, in the reference's
-// expression order (chem.py:92-99, 156-182).
+// Rate of one reaction from its reactant values yr[] and stoichiometries
+// st[] (padding slots st = 0), and with jac its derivative by each reactant
+// slot into d[], in the reference's expression order (chem.py:92-99,
+// 156-182). Shared by the per-layer and the layer-vectorized assembly.
 template <int TT>
-__device__ inline void rate_slot(const NetDev& net, int r, const double* yrow, double kr, double M, double* rate,
-                                 double* drate, bool jac) {
-  double f[TT], yr[TT], st[TT];
+__device__ __forceinline__ double rate_terms(const double (&yr)[TT], const double (&st)[TT], double kr, double M,
+                                             bool three, bool jac, double (&d)[TT]) {
+  double f[TT];
 #pragma unroll
-  for (int s = 0; s < TT; ++s) {
-    const int idx = net.r_idx[r * TT + s];
-    st[s] = net.r_st[r * TT + s];
-    yr[s] = yrow[idx];
-    f[s] = st[s] > 0.0 ? pow_st(yr[s], st[s]) : 1.0;
-  }
+  for (int s = 0; s < TT; ++s) f[s] = st[s] > 0.0 ? pow_st(yr[s], st[s]) : 1.0;
   double prod = f[0];
 #pragma unroll
   for (int s = 1; s < TT; ++s) prod = prod * f[s];
   double rt = kr * prod;
-  const bool three = net.three[r] != 0;
   if (three) rt = rt * M;
-  rate[r] = rt;
   if (jac) {
 #pragma unroll
     for (int s = 0; s < TT; ++s) {
@@ -73,12 +70,30 @@ __device__ inline void rate_slot(const NetDev& net, int r, const double* yrow, d
 #pragma unroll
       for (int t = 1; t < TT; ++t) lo = lo * ((t == s) ? 1.0 : f[t]);
       double pm1 = st[s] > 0.0 ? pow_st(yr[s], st[s] - 1.0) : 0.0;
-      double d = st[s] * pm1;
-      d = d * lo;
-      d = d * kr;
-      if (three) d = d * M;
-      drate[r * TT + s] = d;
+      double dd = st[s] * pm1;
+      dd = dd * lo;
+      dd = dd * kr;
+      if (three) dd = dd * M;
+      d[s] = dd;
     }
+  }
+  return rt;
+}
+
+// Rate (and drate) of reaction slot r with TT terms of one layer.
+template <int TT>
+__device__ inline void rate_slot(const NetDev& net, int r, const double* yrow, double kr, double M, double* rate,
+                                 double* drate, bool jac) {
+  double yr[TT], st[TT], d[TT];
+#pragma unroll
+  for (int s = 0; s < TT; ++s) {
+    st[s] = net.r_st[r * TT + s];
+    yr[s] = yrow[net.r_idx[r * TT + s]];
+  }
+  rate[r] = rate_terms<TT>(yr, st, kr, M, net.three[r] != 0, jac, d);
+  if (jac) {
+#pragma unroll
+    for (int s = 0; s < TT; ++s) drate[r * TT + s] = d[s];
   }
 }
 
@@ -922,6 +937,159 @@ static cudaError_t launch_diffusion_rows(const Batch& B, const double* y, const 
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- layer-vectorized stage 2
+// The stage-2 right-hand side with one thread per layer instead of one CTA per
+// layer: every term of a species list is then one coalesced load of a row of
+// layers that the whole warp shares, in place of a dependent chain of table,
+// shared-memory and L2 loads per lane. Two passes:
+//  * lv_rates_kernel: the rate of every reaction slot at every layer of an
+//    atmosphere at yk2 = y + k1/r (the state rows staged transposed in shared
+//    memory; the rate constants k[r][z] read with the layers contiguous, the
+//    reference's layout), into the rate region (rows [nr+1][nz_b]);
+//  * lv_sums_kernel (a CTA per species and atmosphere, a thread per layer):
+//    the species' loss and production sums, rmod = rhs(yk2) - 2/(r dt) k1.
+// Each sum runs over the same terms, in the same order, with the same
+// operations as in stage2_kernel, so the results are identical. (The same
+// scheme for stage 1, with the rate derivatives staged too and the Jacobian
+// rows summed per layer, measured slower than stage1_kernel on B200: 3.0 ms
+// against 2.5 at 296 config-0 atmospheres; its scattered block-row stores
+// and staging buffers cost more than the per-layer gathers.)
+constexpr int LV_LAYERS = 128;         // layers of one thread group (a z-tile)
+constexpr int LV_RATE_THREADS = 512;   // four groups; reactions dealt round the groups
+
+__host__ __device__ inline size_t lv_rates_smem_bytes(int ni) {
+  return (size_t)(ni + 1) * (LV_LAYERS + 1) * sizeof(double);
+}
+
+template <int TT>
+__global__ void __launch_bounds__(LV_RATE_THREADS)
+lv_rates_kernel(NetDev net, Batch B, const double* __restrict__ y, const double* __restrict__ k,
+                const double* __restrict__ atm, double* __restrict__ ws) {
+  extern __shared__ double smem[];
+  constexpr int RU = 4;   // rate constants loaded ahead
+  const int b = blockIdx.y;
+  const Geo g = geo_of(B, b);
+  const int ni = B.ni, nzb = g.nz, R = B.nr + 1, S = LV_LAYERS + 1;
+  const int r_lo = (int)((int64_t)R * blockIdx.x / gridDim.x);
+  const int r_hi = (int)((int64_t)R * (blockIdx.x + 1) / gridDim.x);
+  const double* yb = y + g.z0 * ni;
+  const WsView w = ws_view(ws, g, ni, B.ld);
+  const AtmRef a = atm_ref(atm + g.atm, nzb, ni);
+  const double* kb = k + g.z0 * R;
+  double* rate = B.rates + g.z0 * rates_region_doubles(B.nr);
+  const double r = ros2_r();
+  const int grp = threadIdx.x / LV_LAYERS, zl = threadIdx.x % LV_LAYERS, ngrp = blockDim.x / LV_LAYERS;
+  double* yT = smem;   // [ni+1][S]: yk2 of species i at layer zl (row ni: the padding slot, 1.0)
+  for (int zt = 0; zt < nzb; zt += LV_LAYERS) {
+    const int nzt = min(LV_LAYERS, nzb - zt);
+    __syncthreads();   // the previous tile's reads
+    for (int e = threadIdx.x; e < nzt * ni; e += blockDim.x) {
+      const int zz = e / ni, i = e - zz * ni;
+      const int64_t q = (int64_t)(zt + zz) * ni + i;
+      yT[i * S + zz] = yb[q] + w.k1[q] / r;   // stage2_kernel's expression
+    }
+    for (int zz = threadIdx.x; zz < LV_LAYERS; zz += blockDim.x) yT[ni * S + zz] = 1.0;
+    __syncthreads();
+    const int z = zt + zl;
+    const bool on = zl < nzt;
+    const double M = on ? a.M[z] : 0.0;
+    for (int r0 = r_lo + grp; r0 < r_hi; r0 += RU * ngrp) {
+      double kv[RU];
+#pragma unroll
+      for (int u = 0; u < RU; ++u) {
+        const int rr = r0 + u * ngrp;
+        kv[u] = (on && rr < r_hi) ? __ldcg(kb + (int64_t)rr * nzb + z) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < RU; ++u) {
+        const int rr = r0 + u * ngrp;
+        if (rr < r_hi) {
+          double yr[TT], st[TT], d[TT];
+#pragma unroll
+          for (int s = 0; s < TT; ++s) {
+            st[s] = net.r_st[rr * TT + s];
+            yr[s] = yT[net.r_idx[rr * TT + s] * S + zl];
+          }
+          const double rt = rate_terms<TT>(yr, st, kv[u], M, net.three[rr] != 0, false, d);
+          if (on) rate[(int64_t)rr * nzb + z] = rt;
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(LV_LAYERS)
+lv_sums_kernel(NetDev net, Batch B, const double* __restrict__ dt, const uint8_t* __restrict__ fix_mask,
+               double* __restrict__ ws) {
+  __shared__ double coefs[MAX_COEF];
+  load_coefs(net, coefs);
+  __syncthreads();
+  const int i = blockIdx.x, b = blockIdx.y;
+  const Geo g = geo_of(B, b);
+  const int ni = B.ni, nzb = g.nz;
+  const WsView w = ws_view(ws, g, ni, B.ld);
+  const double* rate = B.rates + g.z0 * rates_region_doubles(B.nr);
+  const double r = ros2_r();
+  for (int zt = 0; zt < nzb; zt += LV_LAYERS) {
+    const int z = zt + (int)threadIdx.x;
+    if (z >= nzb) break;
+    double part[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int e0 = net.sum_nptr[2 * i + t], e1 = net.sum_nptr[2 * i + t + 1];
+      double acc = 0.0;
+#pragma unroll 8
+      for (int e = e0; e < e1; ++e) {
+        const uint32_t x = net.sum_nw[e];
+        acc = acc + coefs[x >> 16] * rate[(int64_t)(x & 0xffffu) * nzb + z];
+      }
+      part[t] = acc;
+    }
+    // rmod holds the row's diffusion term (diffusion_rows_kernel)
+    const int64_t q = (int64_t)z * ni + i;
+    double v = (part[1] - part[0]) + w.rmod[q];
+    if (fix_mask && fix_mask[g.z0 * ni + q]) v = 0.0;
+    w.rmod[q] = v - (2.0 / (r * dt[b])) * w.k1[q];
+  }
+}
+
+// Reaction chunks per atmosphere of lv_rates_kernel: about two waves of
+// three 512-thread CTAs per SM, at least 8 reaction slots per chunk.
+static int lv_rate_chunks(const Batch& B) {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 148;
+  const int want = (6 * sms + B.count - 1) / B.count;
+  return std::max(1, std::min(want, (B.nr + 1) / 8));
+}
+
+static cudaError_t launch_lv_stage2(const NetDev& net, const Batch& B, const double* y, const double* k,
+                                    const double* dt, const double* atm, const uint8_t* fm, double* ws,
+                                    cudaStream_t st) {
+  const size_t sm = lv_rates_smem_bytes(B.ni);
+  dim3 grid(lv_rate_chunks(B), B.count);
+  cudaError_t e = cudaSuccess;
+  auto go = [&](auto kern) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) kern<<<grid, LV_RATE_THREADS, sm, st>>>(net, B, y, k, atm, ws);
+  };
+  switch (net.T) {
+    case 1: go(lv_rates_kernel<1>); break;
+    case 2: go(lv_rates_kernel<2>); break;
+    case 3: go(lv_rates_kernel<3>); break;
+    case 4: go(lv_rates_kernel<4>); break;
+    case 5: go(lv_rates_kernel<5>); break;
+    case 6: go(lv_rates_kernel<6>); break;
+    case 7: go(lv_rates_kernel<7>); break;
+    default: go(lv_rates_kernel<8>); break;
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  lv_sums_kernel<<<dim3(B.ni, B.count), LV_LAYERS, 0, st>>>(net, B, dt, fm, ws);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- launchers
 // Stage-1 / stage-2 kernels of the Ros2 step (VbTuning.stage1_layers): one
 // layer per CTA by default (measured on B200 at 296 config-0 atmospheres, the
@@ -954,6 +1122,11 @@ cudaError_t launch_stage2(const NetDev& net, const Batch& B, const double* y, co
                           const double* dt, const double* atm, int flags, const uint8_t* fm, double* ws,
                           cudaStream_t st, double* resid) {
   const int layers = B.stage1_layers ? B.stage1_layers : kStage1DefaultLayers;
+  if (B.rates && !resid && layers != 2) {
+    cudaError_t e = launch_diffusion_rows(B, y, atm, flags, fm, ws, nullptr, 2, st);
+    if (e == cudaSuccess) e = launch_lv_stage2(net, B, y, k, dt, atm, fm, ws, st);
+    return e;
+  }
   if (!resid && layers == 2) {
     size_t sm = pair2_smem_bytes(B.ni, B.nr);
     cudaError_t e = cudaFuncSetAttribute(stage2_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

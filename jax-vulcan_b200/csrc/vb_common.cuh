@@ -38,6 +38,11 @@ struct NetDev {
   // Destinations in decreasing term count: {first term in jac_w,
   // count | row << 16 | col << 24}.
   const uint2* jac_desc;         // [ni*ni]
+  // The species lists in natural order, for the layer-vectorized stage 2
+  // (one thread per layer, every term of a list read by the whole warp):
+  // list t (2 i loss, 2 i + 1 production) at sum_nw[sum_nptr[t] .. sum_nptr[t+1]).
+  const int32_t* sum_nptr;       // [2 ni + 1]
+  const uint32_t* sum_nw;
 };
 
 constexpr int LAYER_THREADS = 256;
@@ -77,7 +82,14 @@ struct Batch {
   int factor_ctas = 0;     // CTAs per SM of the factor (1 or 2, where both fit)
   int sweep_stages = 0;    // bulk-copy ring depth of the sweeps (1..3)
   int stage1_layers = 0;   // layers per stage-1 CTA (1 or 2)
+  // rate region of the layer-vectorized stage 2 (rates_region_doubles per
+  // layer), or nullptr: the per-layer stage-2 kernel
+  double* rates = nullptr;
 };
+
+// Doubles per layer of the rate region: the rate of every reaction slot, rows
+// [nr+1][nz_b] per atmosphere (layers contiguous).
+__host__ __device__ inline int64_t rates_region_doubles(int nr) { return (int64_t)nr + 1; }
 
 struct Geo {
   int nz;

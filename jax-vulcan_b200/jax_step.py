@@ -99,11 +99,16 @@ class Ros2Step:
     """
 
     def __init__(self, net: NetworkArrays, atm: AtmStatic, batch: int | None = None, mixed: bool = False,
-                 max_refine: int = 3, tol: float = 1e-12):
+                 max_refine: int = 3, tol: float = 1e-12, assembly: bool = True):
         """``mixed=True``: the mixed-precision step (``vb_ros2_step_mixed``:
         FP32 row-equilibrated factor on the TF32 tensor cores, FP64 refinement
         of both stages, at most ``max_refine`` passes to ``tol``, FP64
-        fallback); ``self.passes`` then holds the passes run per atmosphere."""
+        fallback); ``self.passes`` then holds the passes run per atmosphere.
+        ``assembly`` (FP64 step): allocate the rate region of the
+        layer-vectorized stage 2 (``vb_ros2_assembly_bytes``: nr+1 doubles
+        per layer), so the stage-2 right-hand side is formed with a thread per
+        layer; False: the per-layer stage-2 kernel (same results, less
+        memory)."""
         self.net = net
         self.mixed = bool(mixed)
         self.max_refine = int(max_refine)
@@ -120,6 +125,9 @@ class Ros2Step:
         L = _lib.lib()
         size = L.vb_ros2_mixed_workspace_bytes if self.mixed else L.vb_ros2_workspace_bytes
         self.ws_bytes = int(size(self.batch, self.nz, ni, None))
+        if assembly and not self.mixed:
+            self.ws_bytes = ((self.ws_bytes + 255) & ~255) + int(
+                L.vb_ros2_assembly_bytes(net.handle, self.batch, self.nz))
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
         self.status = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
         self.passes = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
@@ -190,7 +198,10 @@ class RaggedRos2Step:
     ``pack`` / ``unpack`` convert from and to per-atmosphere arrays.
     """
 
-    def __init__(self, net: NetworkArrays, atms):
+    def __init__(self, net: NetworkArrays, atms, assembly: bool = True):
+        """``assembly``: allocate the rate region of the layer-vectorized
+        stage 2 (as ``Ros2Step``; sized for ``batch`` atmospheres of the
+        largest layer count)."""
         self.net = net
         atms = list(atms)
         self.batch = len(atms)
@@ -210,6 +221,9 @@ class RaggedRos2Step:
         self.blob = torch.cat(blobs).contiguous()
         L = _lib.lib()
         self.ws_bytes = int(L.vb_ros2_workspace_bytes(self.batch, self.nz_max, ni, self.zoff_host.ctypes.data))
+        if assembly:
+            self.ws_bytes = ((int(L.vb_ros2_workspace_bytes(self.batch, self.nz_max, ni, None)) + 255) & ~255) + \
+                int(L.vb_ros2_assembly_bytes(net.handle, self.batch, self.nz_max))
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")
         self.status = torch.zeros(self.batch, dtype=torch.int32, device="cuda")
 
