@@ -4,8 +4,9 @@
 // factor: for each layer j (serial in z)
 //     A'_j  = D_j - (sub_d[j-1] sup_d[j-1]^T) o A'_{j-1}^{-1}     (solver.py:47)
 //     Inv_j = A'_j^{-1}                                            (solver.py:46,48)
-// Each A'_j is inverted in place by Gauss-Jordan elimination with partial
-// pivoting on a register-resident tile (implicit pivoting: no row exchanges),
+// Each A'_j is inverted in place by Gauss-Jordan elimination with threshold
+// partial pivoting (pivot_key32) on a register-resident tile (implicit
+// pivoting: no row exchanges),
 // one serial chain of ni pivot steps per layer with one block barrier each.
 // The forward sweep of the first right-hand side rides along
 // (solver.py:73-88). The stored inverses turn every later solve into
@@ -17,19 +18,26 @@
 
 namespace vb {
 
-// Pivot key of a candidate: |v| as an order-preserving 64-bit pattern (NaN -> 0).
-__device__ __forceinline__ unsigned long long pivot_key(double v) {
-  double a = fabs(v);
-  return (a >= 0.0) ? (unsigned long long)__double_as_longlong(a) : 0ull;
-}
-__device__ __forceinline__ unsigned long long pivot_key(float v) {
-  float a = fabsf(v);
-  return (a >= 0.0f) ? ((unsigned long long)__float_as_uint(a) << 32) : 0ull;
-}
-
 // High word of |v| (sign cleared): orders |v| up to ties of the low word.
 __device__ __forceinline__ unsigned hi_key(double v) { return (unsigned)__double2hiint(v) & 0x7fffffffu; }
 __device__ __forceinline__ unsigned hi_key(float v) { return __float_as_uint(v) & 0x7fffffffu; }
+
+// Pivot choice of every factor kernel. The key of a candidate row is the top
+// 24 bits of |v| (the sign-cleared high word shifted right by 7: the exponent
+// and the leading 13 mantissa bits in FP64, 16 in FP32) above 255 - row, so
+// one 32-bit max reduction over the warp names the pivot row: the largest
+// magnitude to within a relative 2^-13 (FP64) or 2^-16 (FP32), the lowest row
+// among those (threshold partial pivoting with threshold 1 - 2^-13; strict
+// partial pivoting takes the exact maximum, at the price of a second
+// reduction, ballots and shuffles on the pivot chain). A NaN counts as
+// magnitude 0. Rows that may not pivot (pivoted, padding) take key 0, below
+// every candidate (row <= 127, so a candidate's low byte is >= 128).
+template <typename R>
+__device__ __forceinline__ unsigned pivot_key32(R v, int row) {
+  const unsigned mag = isnan(v) ? 0u : (hi_key(v) >> 7);
+  return (mag << 8) | (unsigned)(255 - row);
+}
+__device__ __forceinline__ int pivot_row(unsigned kmax) { return 255 - (int)(kmax & 255u); }
 
 // Correctly rounded reciprocal (the value of 1 / x).
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
@@ -108,8 +116,8 @@ struct GJK {
 //    (q(i): the step whose pivot row is i), applied (transposed back when
 //    tr) by the scatter into Ib.
 //  * One block barrier per step. During step k the owner warp of column
-//    k+1 updates that column first, takes its argmax (three redux.sync on the
-//    64-bit |v| key, ties to the lowest row, as LAPACK's idamax), inverts the
+//    k+1 updates that column first, takes its argmax (one redux.sync on
+//    the packed pivot_key32: threshold partial pivoting), inverts the
 //    pivot and publishes p_{k+1} with the scaled multipliers; the other warps
 //    update meanwhile. A warp takes its part of the pivot row from the owner
 //    lane through a per-warp shared slot (no block barrier).
@@ -191,52 +199,17 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   }
 
   // argmax of column kn (values t, already updated) over the unpivoted rows,
-  // run by the warp that owns the column; publishes the pivot and multipliers.
-  // Fast path: a unique maximum of the high word of |t| (valid rows keyed +1,
-  // NaN as 0) decides. Otherwise the full 64-bit key, ties to the lowest row.
+  // run by the warp that owns the column (pivot_key32: one max reduction
+  // names the row); the pivot value comes from its owner lane.
   auto pivot_of = [&](const R (&t)[RPL], unsigned used, R& piv) {
-    unsigned h[RPL];
+    unsigned km = 0u;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
-      const bool ok = i < n && !((used >> r) & 1u) && !isnan(t[r]);
-      h[r] = ok ? hi_key(t[r]) + 1u : 0u;
+      if (i < n && !((used >> r) & 1u)) km = max(km, pivot_key32(t[r], i));
     }
-    unsigned hm = h[0];
-#pragma unroll
-    for (int r = 1; r < RPL; ++r) hm = max(hm, h[r]);
-    const unsigned m1 = __reduce_max_sync(FULL, hm);
-    int cnt = 0, mys = 0;
-#pragma unroll
-    for (int r = RPL - 1; r >= 0; --r)
-      if (h[r] == m1) {
-        ++cnt;
-        mys = r;
-      }
-    const unsigned b1 = __ballot_sync(FULL, cnt > 0);
-    const unsigned b2 = __ballot_sync(FULL, cnt > 1);
-    int p1;
-    if (__popc(b1) == 1 && b2 == 0u) {
-      const int wl = __ffs(b1) - 1;
-      p1 = __shfl_sync(FULL, lane + 32 * mys, wl);
-      piv = __shfl_sync(FULL, pick(t, mys), wl);
-    } else {
-      unsigned long long bk = 0ull;
-      unsigned brow = 0xffffffffu;
-#pragma unroll
-      for (int r = 0; r < RPL; ++r) {
-        const int i = lane + 32 * r;
-        if (i < n && !((used >> r) & 1u)) {
-          const unsigned long long kk = pivot_key(t[r]);
-          if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
-        }
-      }
-      const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-      const unsigned n1 = __reduce_max_sync(FULL, hi);
-      const unsigned n2 = __reduce_max_sync(FULL, hi == n1 ? lo : 0u);
-      p1 = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
-      piv = __shfl_sync(FULL, pick(t, p1 >> 5), p1 & 31);
-    }
+    const int p1 = pivot_row(__reduce_max_sync(FULL, km));
+    piv = __shfl_sync(FULL, pick(t, p1 >> 5), p1 & 31);
     return p1;
   };
   // multipliers t / piv of step kn into cb (0 on the pivot row), its pivot
@@ -674,85 +647,28 @@ __device__ __forceinline__ double pick_slot(const double (&v)[RPL], int s) {
   return x;
 }
 
-// Argmax of a column over its unpivoted rows with the full 64-bit |v| key,
-// ties to the lowest row (the single kernel's slow path).
-template <int RPL>
-__device__ __forceinline__ int pivot_full(const double (&t)[RPL], unsigned used, int n, double& piv) {
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  unsigned long long bk = 0ull;
-  unsigned brow = 0xffffffffu;
-#pragma unroll
-  for (int r = 0; r < RPL; ++r) {
-    const int i = lane + 32 * r;
-    if (i < n && !((used >> r) & 1u)) {
-      const unsigned long long kk = pivot_key(t[r]);
-      if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)i; }
-    }
-  }
-  const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-  const unsigned n1 = __reduce_max_sync(FULL, hi);
-  const unsigned n2 = __reduce_max_sync(FULL, hi == n1 ? lo : 0u);
-  const int p1 = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
-  piv = __shfl_sync(FULL, pick_slot(t, p1 >> 5), p1 & 31);
-  return p1;
-}
-
-// Argmaxes of two columns (one per atmosphere), interleaved: the high-word
-// keys of both are reduced together; when both maxima are unique the pivots
-// come from one round of shuffles, else each column takes the full-key path.
-// The chosen rows equal the single kernel's.
+// Argmaxes of two columns (one per atmosphere), interleaved: both keys
+// (pivot_key32) reduced back to back, then both pivot values shuffled from
+// their owner lanes. The chosen rows equal the single kernel's.
 template <int RPL>
 __device__ __forceinline__ void pivot_pair(const double (&t)[2][RPL], const unsigned (&used)[2], int n,
                                            int (&p1)[2], double (&piv)[2]) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  unsigned hm[2];
-  int cnt[2], mys[2];
+  unsigned km[2] = {0u, 0u};
 #pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    unsigned h[RPL];
+  for (int e = 0; e < 2; ++e)
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
-      const bool ok = i < n && !((used[e] >> r) & 1u) && !isnan(t[e][r]);
-      h[r] = ok ? hi_key(t[e][r]) + 1u : 0u;
+      if (i < n && !((used[e] >> r) & 1u)) km[e] = max(km[e], pivot_key32(t[e][r], i));
     }
-    unsigned m = h[0];
-#pragma unroll
-    for (int r = 1; r < RPL; ++r) m = max(m, h[r]);
-    hm[e] = m;
-    cnt[e] = 0;
-    mys[e] = 0;
-  }
-  const unsigned m1a = __reduce_max_sync(FULL, hm[0]);
-  const unsigned m1b = __reduce_max_sync(FULL, hm[1]);
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    const unsigned m1 = e ? m1b : m1a;
-#pragma unroll
-    for (int r = RPL - 1; r >= 0; --r) {
-      const int i = lane + 32 * r;
-      const bool ok = i < n && !((used[e] >> r) & 1u) && !isnan(t[e][r]);
-      const unsigned h = ok ? hi_key(t[e][r]) + 1u : 0u;
-      if (h == m1) {
-        ++cnt[e];
-        mys[e] = r;
-      }
-    }
-  }
-  const unsigned b1a = __ballot_sync(FULL, cnt[0] > 0), b2a = __ballot_sync(FULL, cnt[0] > 1);
-  const unsigned b1b = __ballot_sync(FULL, cnt[1] > 0), b2b = __ballot_sync(FULL, cnt[1] > 1);
-  if (__popc(b1a) == 1 && b2a == 0u && __popc(b1b) == 1 && b2b == 0u) {
-    const int wa = __ffs(b1a) - 1, wb = __ffs(b1b) - 1;
-    p1[0] = __shfl_sync(FULL, lane + 32 * mys[0], wa);
-    p1[1] = __shfl_sync(FULL, lane + 32 * mys[1], wb);
-    piv[0] = __shfl_sync(FULL, pick_slot(t[0], mys[0]), wa);
-    piv[1] = __shfl_sync(FULL, pick_slot(t[1], mys[1]), wb);
-  } else {
-    p1[0] = pivot_full(t[0], used[0], n, piv[0]);
-    p1[1] = pivot_full(t[1], used[1], n, piv[1]);
-  }
+  const unsigned m1a = __reduce_max_sync(FULL, km[0]);
+  const unsigned m1b = __reduce_max_sync(FULL, km[1]);
+  p1[0] = pivot_row(m1a);
+  p1[1] = pivot_row(m1b);
+  piv[0] = __shfl_sync(FULL, pick_slot(t[0], p1[0] >> 5), p1[0] & 31);
+  piv[1] = __shfl_sync(FULL, pick_slot(t[1], p1[1] >> 5), p1[1] & 31);
 }
 
 // Shared-memory plan of the paired factor: per atmosphere (carved in this
@@ -1369,51 +1285,15 @@ __device__ __forceinline__ void bgj_factor_atmosphere(int nz, int n, int ld, int
       if (s < cnt) {
         const int te = s >> 1, ee = s & 1;
         const bool own = t == te;
-        // ---- argmax of column s over the unpivoted rows (ties to the lowest row)
-        unsigned h[MR];
+        // ---- argmax of column s over the unpivoted rows (pivot_key32)
+        unsigned km = 0u;
 #pragma unroll
         for (int a = 0; a < MR; ++a) {
-          const R v = acc[a][ee];
-          const bool ok = own && 8 * a + g < n && !((used >> a) & 1u) && !isnan(v);
-          h[a] = ok ? hi_key(v) + 1u : 0u;
+          const int r = 8 * a + g;
+          if (own && r < n && !((used >> a) & 1u)) km = max(km, pivot_key32(acc[a][ee], r));
         }
-        unsigned hm = h[0];
-#pragma unroll
-        for (int a = 1; a < MR; ++a) hm = max(hm, h[a]);
-        const unsigned m1 = __reduce_max_sync(FULL, hm);
-        int c1 = 0, mys = 0;
-#pragma unroll
-        for (int a = MR - 1; a >= 0; --a)
-          if (h[a] == m1) {
-            ++c1;
-            mys = a;
-          }
-        if (!own) c1 = 0;
-        const unsigned b1 = __ballot_sync(FULL, c1 > 0);
-        const unsigned b2 = __ballot_sync(FULL, c1 > 1);
-        int p;
-        R piv;
-        if (m1 > 0u && __popc(b1) == 1 && b2 == 0u) {
-          const int wl = __ffs(b1) - 1;
-          p = __shfl_sync(FULL, 8 * mys + g, wl);
-          piv = __shfl_sync(FULL, pick(mys, ee), wl);
-        } else {
-          unsigned long long bk = 0ull;
-          unsigned brow = 0xffffffffu;
-#pragma unroll
-          for (int a = 0; a < MR; ++a) {
-            const int r = 8 * a + g;
-            if (own && r < n && !((used >> a) & 1u)) {
-              const unsigned long long kk = pivot_key(acc[a][ee]);
-              if (brow == 0xffffffffu || kk > bk) { bk = kk; brow = (unsigned)r; }
-            }
-          }
-          const unsigned hi = (unsigned)(bk >> 32), lo = (unsigned)bk;
-          const unsigned n1 = __reduce_max_sync(FULL, hi);
-          const unsigned n2 = __reduce_max_sync(FULL, hi == n1 ? lo : 0u);
-          p = (int)__reduce_min_sync(FULL, (hi == n1 && lo == n2) ? brow : 0xffffffffu);
-          piv = __shfl_sync(FULL, pick(p >> 3, ee), ((p & 7) << 2) | te);
-        }
+        const int p = pivot_row(__reduce_max_sync(FULL, km));
+        const R piv = __shfl_sync(FULL, pick(p >> 3, ee), ((p & 7) << 2) | te);
         if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
         const int ap = p >> 3, gp = p & 7;
         // column s to every lane of the quad, and this lane's part of row p

@@ -1,6 +1,8 @@
 """The algebra of the block factor's in-place Gauss-Jordan inversion, restated
-on the CPU (`csrc/vb_thomas.cu`, gj_factor_atmosphere): implicit partial
-pivoting (no row exchanges, ties to the lowest row), pivot rows left
+on the CPU (`csrc/vb_thomas.cu`, gj_factor_atmosphere): implicit threshold
+partial pivoting (no row exchanges; the pivot row is the lowest row whose
+magnitude matches the column maximum in the top 24 bits of its FP64 pattern,
+pivot_key32), pivot rows left
 unnormalised during the elimination and scaled by 1/pivot at the end, the
 result stored permuted (B^{-1}[q(i)][p_m] = T[i][m]), and the two
 orientations: elimination on A^T (the Ros2 step and forward solves, which
@@ -9,6 +11,17 @@ or on A (the adjoint's transposed solves, which need |X A - I|). The GPU
 kernel itself is compared with the oracle in the -m gpu tests."""
 import numpy as np
 import pytest
+
+
+def pivot_row(col, cand):
+    """The kernel's pivot choice among the candidate rows `cand` of a column:
+    key = (top 24 bits of |v|, i.e. the sign-cleared high word >> 7) << 8 |
+    (255 - row), NaN as magnitude 0; the row of the largest key."""
+    v = np.abs(col[cand]).astype(np.float64)
+    hi = (v.view(np.uint64) >> np.uint64(32)) & np.uint64(0x7fffffff)
+    mag = np.where(np.isnan(v), np.uint64(0), hi >> np.uint64(7)).astype(np.int64)
+    key = (mag << 8) | (255 - cand)
+    return int(cand[np.argmax(key)])
 
 
 def gauss_jordan_inverse(A, transposed):
@@ -21,7 +34,7 @@ def gauss_jordan_inverse(A, transposed):
     rps = np.zeros(n)          # 1 / pivot of row i
     for k in range(n):
         cand = np.flatnonzero(~used)
-        p = cand[np.argmax(np.abs(Bm[cand, k]))]        # first maximum: lowest row
+        p = pivot_row(Bm[:, k], cand)
         rp = 1.0 / Bm[p, k]
         m = np.where(np.arange(n) != p, Bm[:, k] * rp, 0.0)
         Bm -= np.outer(m, Bm[p])                         # pivot row unchanged (m_p = 0)
@@ -51,8 +64,26 @@ def test_ties_go_to_the_lowest_row():
     assert np.abs(X @ A - np.eye(3)).max() < 1e-15
     # the permutation bookkeeping holds for any tie order; the choice itself is
     # the lowest row, as LAPACK's idamax
-    cand = np.array([1, 2])
-    assert cand[np.argmax(np.abs(A[cand, 0]))] == 1
+    assert pivot_row(A[:, 0], np.array([1, 2])) == 1
+
+
+def test_threshold_pivot_choice():
+    """Magnitudes equal in their top 24 bits count as ties (the lowest row
+    wins); a larger exponent or a leading-mantissa difference wins outright;
+    pivoted rows and NaN never beat a candidate with a finite magnitude."""
+    rows = np.array([3, 5, 7])
+    near = 1.0 + 2.0 ** -20                         # same top 24 bits as 1.0
+    assert pivot_row(np.array([0, 0, 0, 1.0, 0, -near, 0, 0.5]), rows) == 3
+    assert pivot_row(np.array([0, 0, 0, 1.0, 0, -(1.0 + 2.0 ** -12), 0, 0.5]), rows) == 5
+    assert pivot_row(np.array([0, 0, 0, 1e-30, 0, 1e-29, 0, np.nan]), rows) == 5
+    assert pivot_row(np.array([0, 0, 0, np.nan, 0, 0.0, 0, np.nan]), rows) == 3
+    # within the threshold the choice is a pivot at least (1 - 2^-13) of the maximum
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        col = rng.standard_normal(40) * 10.0 ** rng.integers(-3, 3, 40)
+        cand = np.sort(rng.choice(40, 25, replace=False))
+        p = pivot_row(col, cand)
+        assert abs(col[p]) >= (1 - 2.0 ** -13) * np.abs(col[cand]).max()
 
 
 def test_orientation_on_the_stiff_config0_chain():
