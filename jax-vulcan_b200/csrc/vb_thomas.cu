@@ -214,9 +214,8 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
   };
   // multipliers t / piv of step kn into cb (0 on the pivot row), its pivot
   // row into *pbp, pivs[kn], qs[p1] and 1 / piv into rps[p1]
-  auto store_step = [&](const R (&t)[RPL], int p1, R piv, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
+  auto store_step_rp = [&](const R (&t)[RPL], int p1, R piv, R rp, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
     if (piv == R(0)) st_local |= VB_STATUS_ZERO_PIVOT;
-    const R rp = rcp_rn(piv);
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
@@ -227,6 +226,9 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
     pivs[kn] = p1;
     qs[p1] = kn;
     rps[p1] = rp;
+  };
+  auto store_step = [&](const R (&t)[RPL], int p1, R piv, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
+    store_step_rp(t, p1, piv, rcp_rn(piv), kn, cb, pbp, mo);
   };
   auto publish = [&](const R (&t)[RPL], unsigned used, int kn, R* cb, int* pbp, R (&mo)[RPL]) {
     R piv;
@@ -549,14 +551,17 @@ __device__ __forceinline__ void gj_factor_atmosphere(int nz, int n, int ld, cons
           const int cl = (c + 1) % CPW;                     // column k+1: slot and owner warp
           const int wl = (c + 1 < CPW) ? w0 : w0 + 1;
           if (k + 1 < n && warp == wl) {
-            R t[RPL];
+            R t[RPL], piv;
 #pragma unroll
             for (int r = 0; r < RPL; ++r) t[r] = fma(-m[r], prow[cl], a[r][cl]);
-            pk = publish(t, used, k + 1, colb + ((k + 1) & 1) * NPR, pb + ((k + 1) & 1), mo);
+            const int p1 = pivot_of(t, used, piv);
+            const R rp = rcp_rn(piv);   // in flight while the rest of step k is applied
 #pragma unroll
             for (int r = 0; r < RPL; ++r)
 #pragma unroll
               for (int c2 = 0; c2 < CPW; ++c2) a[r][c2] = fma(-m[r], prow[c2], a[r][c2]);
+            store_step_rp(t, p1, piv, rp, k + 1, colb + ((k + 1) & 1) * NPR, pb + ((k + 1) & 1), mo);
+            pk = p1;
           } else {
 #pragma unroll
             for (int r = 0; r < RPL; ++r)
