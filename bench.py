@@ -942,7 +942,7 @@ def main():
             # per step: diffusion rows, stage 1, factor, back sweep, diffusion rows,
             # stage-2 rates, stage-2 sums, forward sweep, back sweep (twice with two streams)
             "gpu_launches": (18 if tuned.get("streams") == 2 else 9) * args.steps,
-            "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan inverse with partial pivoting of "
+            "roofline": {"bound": "fp64", "kernel": "factor (Gauss-Jordan inverse with threshold partial pivoting of "
                                                     "each layer block, serial in z, one CTA per atmosphere)",
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 else None, "traffic": fac_traffic,
