@@ -142,7 +142,10 @@ int vb_ros2_step(const VbNet* net, int batch, int nz, const int64_t* zoff,
  * refinement passes run per atmosphere over both stages. ni <= 96. The
  * workspace holds the FP64 step workspace, the FP32 inverses and row scales,
  * and per-atmosphere state (vb_ros2_mixed_workspace_bytes; a ragged batch
- * sizes it with zoff_host = NULL and nz = its maximum layer count). */
+ * sizes it with zoff_host = NULL and nz = its maximum layer count). As with
+ * vb_ros2_step, a workspace of at least the 256-byte-aligned
+ * vb_ros2_mixed_workspace_bytes + vb_ros2_assembly_bytes(net, batch, nz)
+ * bytes selects the thread-per-layer stage 2 (identical results). */
 size_t vb_ros2_mixed_workspace_bytes(int batch, int nz, int ni, const int64_t* zoff_host);
 int vb_ros2_step_mixed(const VbNet* net, int batch, int nz, const int64_t* zoff,
                        const double* y, const double* k, const double* dt,

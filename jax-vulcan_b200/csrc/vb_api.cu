@@ -487,6 +487,13 @@ int vb_ros2_step_mixed(const VbNet* net, int batch, int nz, const int64_t* zoff,
   cudaStream_t st = (cudaStream_t)stream;
   vb::Batch B = make_batch(net, batch, nz, zoff);
   char* base = (char*)workspace;
+  // the optional rate region of the thread-per-layer stage 2, after the
+  // mixed step's own bytes on a 256-byte boundary
+  {
+    const size_t off = (L.total + 255) & ~(size_t)255;
+    if (ws_bytes >= off && ws_bytes - off >= vb_ros2_assembly_bytes(net, batch, nz))
+      B.rates = reinterpret_cast<double*>(base + off);
+  }
   double* ws = (double*)base;
   void* mxr = base + L.mx;
   int32_t* mode = (int32_t*)(base + L.mode);

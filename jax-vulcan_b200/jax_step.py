@@ -104,11 +104,10 @@ class Ros2Step:
         FP32 row-equilibrated factor on the TF32 tensor cores, FP64 refinement
         of both stages, at most ``max_refine`` passes to ``tol``, FP64
         fallback); ``self.passes`` then holds the passes run per atmosphere.
-        ``assembly`` (FP64 step): allocate the rate region of the
-        layer-vectorized stage 2 (``vb_ros2_assembly_bytes``: nr+1 doubles
-        per layer), so the stage-2 right-hand side is formed with a thread per
-        layer; False: the per-layer stage-2 kernel (same results, less
-        memory)."""
+        ``assembly``: allocate the rate region of the layer-vectorized
+        stage 2 (``vb_ros2_assembly_bytes``: nr+1 doubles per layer), so the
+        stage-2 right-hand side is formed with a thread per layer; False: the
+        per-layer stage-2 kernel (same results, less memory)."""
         self.net = net
         self.mixed = bool(mixed)
         self.max_refine = int(max_refine)
@@ -125,7 +124,7 @@ class Ros2Step:
         L = _lib.lib()
         size = L.vb_ros2_mixed_workspace_bytes if self.mixed else L.vb_ros2_workspace_bytes
         self.ws_bytes = int(size(self.batch, self.nz, ni, None))
-        if assembly and not self.mixed:
+        if assembly:
             self.ws_bytes = ((self.ws_bytes + 255) & ~255) + int(
                 L.vb_ros2_assembly_bytes(net.handle, self.batch, self.nz))
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device="cuda")

@@ -128,3 +128,20 @@ def test_ragged_batch_identical():
     for x, y in zip(*res):
         assert torch.equal(x, y)
     assert int(res[0][2].abs().sum()) == 0
+
+
+def test_mixed_step_identical():
+    """The mixed-precision step (FP32 factor, FP64 refinement) with and
+    without the rate region: the same stage-2 sums, so the same refinement
+    passes and the same bits."""
+    net = syn.make_network(0, 69, 700)
+    dn = chem.to_device(net.tables)
+    cases = [syn.make_case(seed=(720 + b,), net=net, nz=60, mild=True, k_range=(-40.0, 4.0)) for b in range(3)]
+    Y, K, DT, A = batch_of(cases)
+    res = []
+    for assembly in (True, False):
+        step = jstep.Ros2Step(dn, jstep.atm_from_dict(A), mixed=True, assembly=assembly)
+        sol, delta, status = step(Y, K, DT)
+        res.append((sol.clone(), delta.clone(), status.clone(), step.passes.clone()))
+    for x, y in zip(*res):
+        assert torch.equal(x, y)
